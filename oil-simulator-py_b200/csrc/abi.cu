@@ -1,0 +1,427 @@
+// extern "C" entry points declared in include/impes_b200.h.
+#include "amg.cuh"
+#include "model.cuh"
+#include <algorithm>
+#include <cmath>
+#include <map>
+
+namespace impes {
+const char* last_error_cstr();
+}
+
+struct impes_amg {
+  impes::AMG a;
+};
+struct impes_model {
+  impes::Model m;
+};
+
+using namespace impes;
+
+namespace {
+
+template <typename F>
+int guarded(F&& f) {
+  try {
+    f();
+    return IMPES_OK;
+  } catch (const Error& e) {
+    set_last_error(e.what());
+    return e.code;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return IMPES_ERR_ARG;
+  } catch (...) {
+    set_last_error("unknown error");
+    return IMPES_ERR_ARG;
+  }
+}
+
+inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+}  // namespace
+
+extern "C" {
+
+const char* impes_last_error(void) { return last_error_cstr(); }
+int impes_abi_version(void) { return 1; }
+
+// ------------------------------------------------------------------ AMG
+int impes_amg_create(impes_amg** out, const impes_amg_params* p) {
+  return guarded([&] {
+    IMPES_REQUIRE(out && p, IMPES_ERR_ARG, "null argument");
+    IMPES_REQUIRE(p->max_levels >= 1 && p->coarsest_size >= 1, IMPES_ERR_ARG, "bad level limits");
+    IMPES_REQUIRE(p->nullspace_dim >= 0 && p->nullspace_dim <= 3, IMPES_ERR_ARG,
+                  "nullspace_dim must be 0..3");
+    auto* h = new impes_amg();
+    h->a.prm = *p;
+    h->a.prm.nullspace_blend = std::max(0.0, std::min(1.0, p->nullspace_blend));
+    h->a.prm.nullspace_reg = std::max(1e-10, p->nullspace_reg);
+    *out = h;
+  });
+}
+
+int impes_amg_destroy(impes_amg* h) {
+  return guarded([&] { delete h; });
+}
+
+int impes_amg_setup(impes_amg* h, int n, int nnz, const int* rowptr, const int* col,
+                    const double* val, void* stream) {
+  return guarded([&] {
+    IMPES_REQUIRE(h && rowptr && col && val, IMPES_ERR_ARG, "null argument");
+    amg_setup(h->a, n, nnz, rowptr, col, val, S(stream));
+  });
+}
+
+int impes_amg_update(impes_amg* h, const double* val, void* stream) {
+  return guarded([&] {
+    IMPES_REQUIRE(h && val, IMPES_ERR_ARG, "null argument");
+    amg_update(h->a, val, S(stream));
+  });
+}
+
+int impes_amg_solve_vcycles(impes_amg* h, const double* b, double* x, double tol, int max_cycles,
+                            int* cycles, double* rel_res, void* stream) {
+  return guarded([&] {
+    IMPES_REQUIRE(h && b && x, IMPES_ERR_ARG, "null argument");
+    IMPES_REQUIRE(h->a.built, IMPES_ERR_STATE, "solve before setup");
+    IMPES_REQUIRE(max_cycles >= 1, IMPES_ERR_ARG, "max_cycles must be >= 1");
+    amg_solve_vcycles(h->a, b, x, tol, max_cycles, cycles, rel_res, S(stream));
+  });
+}
+
+int impes_amg_apply(impes_amg* h, const double* b, double* x, int cycles, double apply_tol,
+                    int apply_max_cycles, void* stream) {
+  return guarded([&] {
+    IMPES_REQUIRE(h && b && x, IMPES_ERR_ARG, "null argument");
+    IMPES_REQUIRE(h->a.built, IMPES_ERR_STATE, "apply before setup");
+    amg_apply(h->a, b, x, cycles, apply_tol, apply_max_cycles, S(stream));
+  });
+}
+
+int impes_amg_vcycle_scaled(impes_amg* h, const double* b_scaled, double* x_scaled, int precision,
+                            void* stream) {
+  return guarded([&] {
+    IMPES_REQUIRE(h && b_scaled && x_scaled, IMPES_ERR_ARG, "null argument");
+    IMPES_REQUIRE(h->a.built, IMPES_ERR_STATE, "V-cycle before setup");
+    amg_vcycle_scaled(h->a, b_scaled, x_scaled, precision, S(stream));
+  });
+}
+
+int impes_amg_fgmres(impes_amg* h, const double* b, double* x, const impes_krylov_params* kp,
+                     impes_krylov_stats* stats, void* stream) {
+  return guarded([&] {
+    IMPES_REQUIRE(h && b && x && kp, IMPES_ERR_ARG, "null argument");
+    IMPES_REQUIRE(h->a.built, IMPES_ERR_STATE, "solve before setup");
+    IMPES_REQUIRE(kp->restart >= 1 && kp->max_iters >= 0, IMPES_ERR_ARG, "bad Krylov limits");
+    impes_krylov_stats st{};
+    amg_fgmres(h->a, b, x, *kp, st, S(stream));
+    if (stats) *stats = st;
+  });
+}
+
+int impes_amg_num_levels(impes_amg* h, int* nlev) {
+  return guarded([&] {
+    IMPES_REQUIRE(h && nlev, IMPES_ERR_ARG, "null argument");
+    *nlev = (int)h->a.levels.size();
+  });
+}
+
+int impes_amg_level_info(impes_amg* h, int lvl, impes_amg_level_desc* info) {
+  return guarded([&] {
+    IMPES_REQUIRE(h && info, IMPES_ERR_ARG, "null argument");
+    IMPES_REQUIRE(lvl >= 0 && lvl < (int)h->a.levels.size(), IMPES_ERR_ARG, "level out of range");
+    const Level& L = *h->a.levels[lvl];
+    info->n = L.n;
+    info->nnz = L.nnz;
+    info->p_cols = L.coarsest ? 0 : L.nc;
+    info->p_nnz = L.coarsest ? 0 : L.pnnz;
+    info->is_coarsest = L.coarsest ? 1 : 0;
+  });
+}
+
+int impes_amg_level_export(impes_amg* h, int lvl, int* A_rowptr, int* A_col, double* A_val,
+                           double* inv_relax, int* P_rowptr, int* P_col, double* P_val,
+                           void* stream) {
+  return guarded([&] {
+    IMPES_REQUIRE(h, IMPES_ERR_ARG, "null argument");
+    IMPES_REQUIRE(lvl >= 0 && lvl < (int)h->a.levels.size(), IMPES_ERR_ARG, "level out of range");
+    const Level& L = *h->a.levels[lvl];
+    cudaStream_t s = S(stream);
+    auto cp = [&](void* dst, const void* src, size_t bytes) {
+      if (dst && bytes) IMPES_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, s));
+    };
+    cp(A_rowptr, L.rowptr.p, sizeof(int) * (L.n + 1));
+    cp(A_col, L.col.p, sizeof(int) * L.nnz);
+    cp(A_val, L.val.p, sizeof(double) * L.nnz);
+    cp(inv_relax, L.inv_relax.p, sizeof(double) * L.n);
+    if (!L.coarsest) {
+      cp(P_rowptr, L.prow.p, sizeof(int) * (L.n + 1));
+      cp(P_col, L.pcol.p, sizeof(int) * L.pnnz);
+      cp(P_val, L.pval.p, sizeof(double) * L.pnnz);
+    }
+  });
+}
+
+int impes_amg_equilibration(impes_amg* h, double* dhalf_inv, int* enabled, void* stream) {
+  return guarded([&] {
+    IMPES_REQUIRE(h && enabled, IMPES_ERR_ARG, "null argument");
+    IMPES_REQUIRE(h->a.built, IMPES_ERR_STATE, "query before setup");
+    IMPES_CUDA(cudaMemcpyAsync(h->a.hint.p, h->a.iflag.p + 1, sizeof(int), cudaMemcpyDeviceToHost, S(stream)));
+    IMPES_CUDA(cudaStreamSynchronize(S(stream)));
+    h->a.equilibrated = h->a.hint.p[0] != 0;
+    *enabled = h->a.equilibrated ? 1 : 0;
+    if (dhalf_inv && h->a.equilibrated)
+      IMPES_CUDA(cudaMemcpyAsync(dhalf_inv, h->a.dhalf_inv.p, sizeof(double) * h->a.levels[0]->n,
+                                 cudaMemcpyDeviceToDevice, S(stream)));
+  });
+}
+
+// ---------------------------------------------------------------- model
+int impes_model_create(impes_model** out, const impes_model_desc* d, const impes_well_desc* wells,
+                       int nwells, const double* pvt, const double* kx, const double* ky,
+                       const double* kz, const double* poro, void* stream) {
+  return guarded([&] {
+    IMPES_REQUIRE(out && d && kx && ky && kz && poro, IMPES_ERR_ARG, "null argument");
+    IMPES_REQUIRE(d->nx >= 1 && d->ny >= 1 && d->nz >= 1, IMPES_ERR_ARG, "grid dims must be >= 1");
+    long long N = (long long)d->nx * d->ny * d->nz;
+    IMPES_REQUIRE(N * 7 < (1LL << 31), IMPES_ERR_ARG, "grid too large for int32 CSR");
+    IMPES_REQUIRE(nwells >= 0 && nwells <= kMaxWells, IMPES_ERR_ARG, "too many wells");
+    IMPES_REQUIRE(nwells == 0 || wells, IMPES_ERR_ARG, "null wells");
+    IMPES_REQUIRE(d->pvt_rows == 0 || (pvt && d->pvt_rows >= 2 && d->pvt_rows <= kMaxPvtRows),
+                  IMPES_ERR_ARG, "PVT table must have 2..128 rows");
+    IMPES_REQUIRE(d->max_substeps >= 1, IMPES_ERR_ARG, "max_substeps must be >= 1");
+    cudaStream_t s = S(stream);
+    auto* h = new impes_model();
+    Model& m = h->m;
+    try {
+      ModelParams& P = m.P;
+      P.nx = d->nx; P.ny = d->ny; P.nz = d->nz; P.N = (int)N;
+      P.dx = d->dx; P.dy = d->dy; P.dz = d->dz;
+      P.mu_o = d->mu_o; P.mu_w = d->mu_w; P.mu_g = d->mu_g;
+      P.rho_o_ref = d->rho_o_ref; P.rho_w_ref = d->rho_w_ref; P.rho_g_ref = d->rho_g_ref;
+      P.c_o = d->c_o; P.c_w = d->c_w; P.c_g = d->c_g; P.c_r = d->c_r; P.cf = d->cf;
+      P.relperm_model = d->relperm_model;
+      P.nw = d->nw; P.no = d->no; P.ng = d->ng; P.now = d->now; P.nog = d->nog;
+      P.ko_end_w = d->ko_end_w; P.ko_end_g = d->ko_end_g;
+      P.sw_cr = d->sw_cr; P.so_r = d->so_r; P.sg_cr = d->sg_cr;
+      P.pc_scale = d->pc_scale; P.pc_exponent = d->pc_exponent;
+      P.pc_og_scale = d->pc_og_scale; P.pc_og_exponent = d->pc_og_exponent;
+      P.gravity = d->gravity; P.rate_scale = d->global_rate_scale; P.max_dS = d->max_saturation_change;
+      P.max_substeps = d->max_substeps; P.pvt_rows = d->pvt_rows;
+      P.nwells = nwells;
+      // wells: flat cell (simulation.py:1629), -1 when outside the grid
+      std::map<int, std::vector<int>> by_cell;
+      m.wells_host.resize(nwells);
+      for (int w = 0; w < nwells; ++w) {
+        const impes_well_desc& W = wells[w];
+        WellDev& D = m.wells_host[w];
+        bool inside = W.i >= 0 && W.j >= 0 && W.k >= 0 && W.i < d->nx && W.j < d->ny && W.k < d->nz;
+        IMPES_REQUIRE(inside, IMPES_ERR_ARG, "well outside the grid");
+        D.cell = (W.i * d->ny + W.j) * d->nz + W.k;
+        D.is_injector = W.is_injector; D.control_bhp = W.control_bhp;
+        D.value = W.value; D.well_index = W.well_index;
+        D.injected_phase = W.injected_phase; D.surface_rate = W.surface_rate;
+        D.surface_phase = W.surface_phase; D.limit_mask = W.limit_mask;
+        for (int q = 0; q < 4; ++q) D.limits[q] = W.limits[q];
+        D.has_bhp_min = W.has_bhp_min; D.bhp_min = W.bhp_min;
+        by_cell[D.cell].push_back(w);
+      }
+      std::vector<int> wc_ptr(1, 0), wc_wells;
+      for (auto& kv : by_cell) {
+        m.wc_cells_host.push_back(kv.first);
+        for (int w : kv.second) wc_wells.push_back(w);
+        wc_ptr.push_back((int)wc_wells.size());
+      }
+      P.nwc = (int)m.wc_cells_host.size();
+      m.wells.alloc(std::max(nwells, 1));
+      m.wc_cells.alloc(std::max(P.nwc, 1));
+      m.wc_ptr.alloc(P.nwc + 1);
+      m.wc_wells.alloc(std::max(nwells, 1));
+      if (nwells) {
+        IMPES_CUDA(cudaMemcpyAsync(m.wells.p, m.wells_host.data(), sizeof(WellDev) * nwells, cudaMemcpyHostToDevice, s));
+        IMPES_CUDA(cudaMemcpyAsync(m.wc_cells.p, m.wc_cells_host.data(), sizeof(int) * P.nwc, cudaMemcpyHostToDevice, s));
+        IMPES_CUDA(cudaMemcpyAsync(m.wc_wells.p, wc_wells.data(), sizeof(int) * nwells, cudaMemcpyHostToDevice, s));
+      }
+      IMPES_CUDA(cudaMemcpyAsync(m.wc_ptr.p, wc_ptr.data(), sizeof(int) * (P.nwc + 1), cudaMemcpyHostToDevice, s));
+      m.pvt.alloc(std::max(1, d->pvt_rows * 9));
+      if (d->pvt_rows)
+        IMPES_CUDA(cudaMemcpyAsync(m.pvt.p, pvt, sizeof(double) * d->pvt_rows * 9, cudaMemcpyHostToDevice, s));
+      m.balances.alloc(12);
+      IMPES_CUDA(cudaMemsetAsync(m.balances.p, 0, sizeof(double) * 12, s));
+      m.well_mode.alloc(std::max(nwells, 1));
+      m.well_q.alloc(std::max(nwells, 1));
+      m.well_rates.alloc(std::max(4 * nwells, 1));
+      std::vector<int> modes(std::max(nwells, 1), -1);
+      std::vector<double> nan(std::max(4 * nwells, 1), std::nan(""));
+      IMPES_CUDA(cudaMemcpyAsync(m.well_mode.p, modes.data(), sizeof(int) * modes.size(), cudaMemcpyHostToDevice, s));
+      IMPES_CUDA(cudaMemcpyAsync(m.well_q.p, nan.data(), sizeof(double) * std::max(nwells, 1), cudaMemcpyHostToDevice, s));
+      IMPES_CUDA(cudaMemcpyAsync(m.well_rates.p, nan.data(), sizeof(double) * nan.size(), cudaMemcpyHostToDevice, s));
+      model_build_static(m, kx, ky, kz, poro, s);
+      m.csr_val.alloc(m.nnz);
+      m.rhs.alloc(P.N);
+      IMPES_CUDA(cudaStreamSynchronize(s));
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    *out = h;
+  });
+}
+
+int impes_model_destroy(impes_model* m) {
+  return guarded([&] { delete m; });
+}
+
+int impes_model_nnz(impes_model* h, int* n, int* nnz) {
+  return guarded([&] {
+    IMPES_REQUIRE(h && n && nnz, IMPES_ERR_ARG, "null argument");
+    *n = h->m.P.N;
+    *nnz = h->m.nnz;
+  });
+}
+
+int impes_csr_pattern(impes_model* h, int* rowptr, int* col, void* stream) {
+  return guarded([&] {
+    IMPES_REQUIRE(h && rowptr && col, IMPES_ERR_ARG, "null argument");
+    model_pattern(h->m, rowptr, col, S(stream));
+  });
+}
+
+int impes_well_cells(impes_model* h, int* cells_host) {
+  return guarded([&] {
+    IMPES_REQUIRE(h && (cells_host || h->m.P.nwells == 0), IMPES_ERR_ARG, "null argument");
+    for (int w = 0; w < h->m.P.nwells; ++w) cells_host[w] = h->m.wells_host[w].cell;
+  });
+}
+
+int impes_model_export_static(impes_model* h, double* tx, double* ty, double* tz, double* pv,
+                              void* stream) {
+  return guarded([&] {
+    IMPES_REQUIRE(h, IMPES_ERR_ARG, "null argument");
+    const Model& m = h->m;
+    cudaStream_t s = S(stream);
+    const ModelParams& P = m.P;
+    auto cp = [&](void* dst, const void* src, size_t bytes) {
+      if (dst && bytes) IMPES_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, s));
+    };
+    cp(tx, m.tx.p, sizeof(double) * (size_t)(P.nx - 1) * P.ny * P.nz);
+    cp(ty, m.ty.p, sizeof(double) * (size_t)P.nx * (P.ny - 1) * P.nz);
+    cp(tz, m.tz.p, sizeof(double) * (size_t)P.nx * P.ny * (P.nz - 1));
+    cp(pv, m.pv.p, sizeof(double) * P.N);
+  });
+}
+
+int impes_assemble(impes_model* h, const double* p, const double* sw, const double* sg, double dt,
+                   double* csr_val, double* rhs, void* stream) {
+  return guarded([&] {
+    IMPES_REQUIRE(h && p && sw && sg && csr_val && rhs, IMPES_ERR_ARG, "null argument");
+    IMPES_REQUIRE(dt > 0, IMPES_ERR_ARG, "dt must be positive");
+    model_assemble(h->m, p, sw, sg, dt, csr_val, rhs, S(stream));
+  });
+}
+
+int impes_saturation(impes_model* h, const double* p_new, double* sw, double* sg, double* so,
+                     double dt, impes_sat_stats* stats, void* stream) {
+  return guarded([&] {
+    IMPES_REQUIRE(h && p_new && sw && sg && so, IMPES_ERR_ARG, "null argument");
+    IMPES_REQUIRE(dt > 0, IMPES_ERR_ARG, "dt must be positive");
+    model_saturation(h->m, p_new, sw, sg, so, dt, S(stream));
+    if (stats) {
+      impes_sat_stats st{};
+      double hb[12];
+      cudaStream_t s = S(stream);
+      IMPES_CUDA(cudaMemcpyAsync(hb, h->m.balances.p, sizeof(hb), cudaMemcpyDeviceToHost, s));
+      IMPES_CUDA(cudaMemcpyAsync(&st.substeps, h->m.nsub.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+      IMPES_CUDA(cudaStreamSynchronize(s));
+      for (int q = 0; q < 6; ++q) { st.mass_balance[q] = hb[q]; st.component[q] = hb[6 + q]; }
+      *stats = st;
+    }
+  });
+}
+
+int impes_step(impes_model* h, impes_amg* amg, double* p, double* sw, double* sg, double* so,
+               double dt, int solver, const impes_krylov_params* kp, int max_cycles,
+               impes_krylov_stats* kstats, impes_sat_stats* sstats, void* stream) {
+  return guarded([&] {
+    IMPES_REQUIRE(h && amg && p && sw && sg && so && kp, IMPES_ERR_ARG, "null argument");
+    IMPES_REQUIRE(dt > 0, IMPES_ERR_ARG, "dt must be positive");
+    Model& m = h->m;
+    cudaStream_t s = S(stream);
+    model_assemble(m, p, sw, sg, dt, m.csr_val.p, m.rhs.p, s);
+    AMG& a = amg->a;
+    if (!a.built || a.levels[0]->n != m.P.N)
+      amg_setup(a, m.P.N, m.nnz, m.rowptr.p, m.col.p, m.csr_val.p, s);
+    else
+      amg_update(a, m.csr_val.p, s);
+    impes_krylov_stats st{};
+    if (solver == 0) {
+      int cyc = 0;
+      double rel = 0.0;
+      amg_solve_vcycles(a, m.rhs.p, p, kp->tol, std::max(1, max_cycles), &cyc, &rel, s);
+      st.iterations = cyc;
+      st.rel_res = rel;
+      st.true_rel_res = rel;
+      st.converged = rel < kp->tol;
+    } else {
+      impes_krylov_params k = *kp;
+      amg_fgmres(a, m.rhs.p, p, k, st, s);
+    }
+    if (kstats) *kstats = st;
+    model_saturation(m, p, sw, sg, so, dt, s);
+    if (sstats) {
+      double hb[12];
+      impes_sat_stats ss{};
+      IMPES_CUDA(cudaMemcpyAsync(hb, m.balances.p, sizeof(hb), cudaMemcpyDeviceToHost, s));
+      IMPES_CUDA(cudaMemcpyAsync(&ss.substeps, m.nsub.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+      IMPES_CUDA(cudaStreamSynchronize(s));
+      for (int q = 0; q < 6; ++q) { ss.mass_balance[q] = hb[q]; ss.component[q] = hb[6 + q]; }
+      *sstats = ss;
+    }
+  });
+}
+
+int impes_model_balances(impes_model* h, impes_sat_stats* stats, void* stream) {
+  return guarded([&] {
+    IMPES_REQUIRE(h && stats, IMPES_ERR_ARG, "null argument");
+    double hb[12];
+    impes_sat_stats st{};
+    cudaStream_t s = S(stream);
+    IMPES_CUDA(cudaMemcpyAsync(hb, h->m.balances.p, sizeof(hb), cudaMemcpyDeviceToHost, s));
+    IMPES_CUDA(cudaMemcpyAsync(&st.substeps, h->m.nsub.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    IMPES_CUDA(cudaStreamSynchronize(s));
+    for (int q = 0; q < 6; ++q) { st.mass_balance[q] = hb[q]; st.component[q] = hb[6 + q]; }
+    *stats = st;
+  });
+}
+
+int impes_model_reset_balances(impes_model* h, void* stream) {
+  return guarded([&] {
+    IMPES_REQUIRE(h, IMPES_ERR_ARG, "null argument");
+    IMPES_CUDA(cudaMemsetAsync(h->m.balances.p, 0, sizeof(double) * 12, S(stream)));
+  });
+}
+
+int impes_well_states(impes_model* h, impes_well_state* out, void* stream) {
+  return guarded([&] {
+    IMPES_REQUIRE(h && (out || h->m.P.nwells == 0), IMPES_ERR_ARG, "null argument");
+    const int nw = h->m.P.nwells;
+    if (!nw) return;
+    std::vector<int> modes(nw);
+    std::vector<double> q(nw), rates(4 * nw);
+    cudaStream_t s = S(stream);
+    IMPES_CUDA(cudaMemcpyAsync(modes.data(), h->m.well_mode.p, sizeof(int) * nw, cudaMemcpyDeviceToHost, s));
+    IMPES_CUDA(cudaMemcpyAsync(q.data(), h->m.well_q.p, sizeof(double) * nw, cudaMemcpyDeviceToHost, s));
+    IMPES_CUDA(cudaMemcpyAsync(rates.data(), h->m.well_rates.p, sizeof(double) * 4 * nw, cudaMemcpyDeviceToHost, s));
+    IMPES_CUDA(cudaStreamSynchronize(s));
+    for (int w = 0; w < nw; ++w) {
+      out[w].last_mode = modes[w];
+      out[w].has_q_total = !std::isnan(q[w]);
+      out[w].last_q_total = q[w];
+      out[w].has_surface_rates = !std::isnan(rates[4 * w]);
+      for (int k = 0; k < 4; ++k) out[w].surface_rates[k] = rates[4 * w + k];
+    }
+  });
+}
+
+}  // extern "C"

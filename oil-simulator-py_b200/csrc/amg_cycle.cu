@@ -1,0 +1,612 @@
+// AMG cycling: CSR kernels, l1-Jacobi smoothing, V-cycle, coarsest solve,
+// stand-alone V-cycle solve, apply, and flexible GMRES.
+//
+// Reference: researchim-ai/oil-simulator-py src/solver/classical_amg.py
+//   _spmv_csr :976-1009, _smooth :1016-1035, _v_cycle :1037-1106,
+//   solve :1108-1155, apply :1157-1180.  FGMRES has no reference counterpart.
+//
+// Kernels are templated on the value type (double for the FP64 path, float for
+// the FP32 V-cycle of the mixed path) and on the number of lanes that share a
+// row (1 for the 7-point level, up to 32 for wide coarse rows).
+#include "amg.cuh"
+#include <algorithm>
+#include <cmath>
+
+namespace impes {
+namespace {
+
+constexpr int TB = 256;
+constexpr double kOmega = 0.7;  // classical_amg.py:1022
+
+enum CsrMode { Y_AX = 0, Y_B_MINUS_AX = 1, Y_SMOOTH = 2, Y_ADD_AX = 3, Y_SMOOTH0 = 4, Y_W_AX = 5 };
+
+// One group of LPR lanes per row.  MODE selects the fused epilogue:
+//  Y_AX: y = A x;  Y_B_MINUS_AX: y = b - A x;  Y_SMOOTH: y = x + w*inv*(b - A x);
+//  Y_ADD_AX: y += A x (prolongation);  Y_SMOOTH0: y = w*inv*b (x = 0);
+//  Y_W_AX: y = wt .* (A x) (weighted operator of FGMRES, wt passed as inv).
+template <typename T, int LPR, int MODE>
+__global__ void __launch_bounds__(TB) k_csr(int n, const int* __restrict__ rowptr,
+                                            const int* __restrict__ col, const T* __restrict__ val,
+                                            const T* __restrict__ x, const T* __restrict__ b,
+                                            const T* __restrict__ inv, T* __restrict__ y) {
+  const int g = threadIdx.x / LPR, lane = threadIdx.x % LPR;
+  const int rows_per_block = TB / LPR;
+  for (long long row = (long long)blockIdx.x * rows_per_block + g; row < n;
+       row += (long long)gridDim.x * rows_per_block) {
+    T acc = T(0);
+    if (MODE != Y_SMOOTH0) {
+      const int a = rowptr[row], e = rowptr[row + 1];
+      for (int k = a + lane; k < e; k += LPR) acc += val[k] * x[col[k]];
+#pragma unroll
+      for (int o = LPR / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, LPR);
+    }
+    if (lane == 0) {
+      if (MODE == Y_AX) y[row] = acc;
+      else if (MODE == Y_B_MINUS_AX) y[row] = b[row] - acc;
+      else if (MODE == Y_SMOOTH) y[row] = x[row] + T(kOmega) * inv[row] * (b[row] - acc);
+      else if (MODE == Y_ADD_AX) y[row] = y[row] + acc;
+      else if (MODE == Y_SMOOTH0) y[row] = T(kOmega) * inv[row] * b[row];
+      else if (MODE == Y_W_AX) y[row] = inv[row] * acc;
+    }
+  }
+}
+
+template <typename T, int MODE>
+void launch_csr(int n, int avg, const int* rowptr, const int* col, const T* val, const T* x,
+                const T* b, const T* inv, T* y, cudaStream_t s) {
+  if (n <= 0) return;
+  int lpr = avg <= 8 ? 1 : avg <= 16 ? 4 : avg <= 48 ? 8 : avg <= 96 ? 16 : 32;
+  if (MODE == Y_SMOOTH0) lpr = 1;
+  auto grid = [&](int l) { return grid_for(((size_t)n * l + TB - 1) / TB * TB, TB, 16); };
+  switch (lpr) {
+    case 1: k_csr<T, 1, MODE><<<grid(1), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y); break;
+    case 4: k_csr<T, 4, MODE><<<grid(4), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y); break;
+    case 8: k_csr<T, 8, MODE><<<grid(8), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y); break;
+    case 16: k_csr<T, 16, MODE><<<grid(16), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y); break;
+    default: k_csr<T, 32, MODE><<<grid(32), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y); break;
+  }
+  IMPES_CHECK_LAUNCH();
+}
+
+#define GRID_LOOP(i, n) \
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (n); i += (long long)gridDim.x * blockDim.x)
+
+template <typename A, typename B>
+__global__ void k_convert(long long n, const A* in, B* out) { GRID_LOOP(i, n) out[i] = (B)in[i]; }
+template <typename A, typename B>
+__global__ void k_div_convert(long long n, const A* in, const double* w, B* out) {
+  GRID_LOOP(i, n) out[i] = (B)(in[i] / w[i]);
+}
+__global__ void k_mul(long long n, const double* a, const double* b, double* out) {
+  GRID_LOOP(i, n) out[i] = a[i] * b[i];
+}
+__global__ void k_mul_inplace(long long n, double* a, const double* b) { GRID_LOOP(i, n) a[i] *= b[i]; }
+__global__ void k_zero(long long n, double* a) { GRID_LOOP(i, n) a[i] = 0.0; }
+
+// ---------------------------------------------------- deterministic dots
+constexpr int kDotBlocks = 296;   // 2 x 148 SMs, fixed so partials have a fixed order
+constexpr int kMD = 8;            // vectors per multi-dot launch
+
+// partial[q * kDotBlocks + block] = sum over the block of V[q] . w   (q < k)
+__global__ void __launch_bounds__(TB) k_multidot(long long n, const double* __restrict__ Vbase,
+                                                 long long ldv, int k, const double* __restrict__ w,
+                                                 double* __restrict__ partial) {
+  __shared__ double s[kMD][TB / 32];
+  double acc[kMD];
+#pragma unroll
+  for (int q = 0; q < kMD; ++q) acc[q] = 0.0;
+  GRID_LOOP(i, n) {
+    const double wi = w[i];
+#pragma unroll
+    for (int q = 0; q < kMD; ++q)
+      if (q < k) acc[q] += Vbase[q * ldv + i] * wi;
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < kMD; ++q) {
+    double v = warp_sum(acc[q]);
+    if (lane == 0) s[q][wid] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < kMD && threadIdx.x < k) {
+    double t = 0.0;
+    for (int u = 0; u < TB / 32; ++u) t += s[threadIdx.x][u];
+    partial[threadIdx.x * kDotBlocks + blockIdx.x] = t;
+  }
+}
+// out[q] (+)= sum of partials, fixed order
+__global__ void k_dot_finalize(int k, const double* partial, double* out, int accumulate) {
+  const int q = blockIdx.x;
+  __shared__ double s[32];
+  double t = 0.0;
+  for (int b = threadIdx.x; b < kDotBlocks; b += 32) t += partial[q * kDotBlocks + b];
+  t = warp_sum(t);
+  if (threadIdx.x == 0) out[q] = accumulate ? out[q] + t : t;
+  (void)s;
+  (void)k;
+}
+// w -= sum_q h[q] V[q]; optionally partial norms of the result
+__global__ void __launch_bounds__(TB) k_update(long long n, const double* __restrict__ Vbase,
+                                               long long ldv, int k, const double* __restrict__ h,
+                                               double* __restrict__ w, double* __restrict__ partial) {
+  __shared__ double sh[128];
+  __shared__ double s[TB / 32];
+  for (int q = threadIdx.x; q < k; q += blockDim.x) sh[q] = h[q];
+  __syncthreads();
+  double acc = 0.0;
+  GRID_LOOP(i, n) {
+    double v = w[i];
+    for (int q = 0; q < k; ++q) v -= sh[q] * Vbase[q * ldv + i];
+    w[i] = v;
+    acc += v * v;
+  }
+  if (partial) {
+    double t = warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double u = 0.0;
+      for (int q = 0; q < TB / 32; ++q) u += s[q];
+      partial[blockIdx.x] = u;
+    }
+  }
+}
+__global__ void k_scale_by_inv_sqrt(long long n, const double* in, double* out, const double* nrm2) {
+  const double inv = 1.0 / sqrt(*nrm2);
+  GRID_LOOP(i, n) out[i] = in[i] * inv;
+}
+
+// --------------------------------------------------- coarsest dense solve
+// Dense copy of the coarsest matrix with DOF 0 pinned (classical_amg.py:1045-1055).
+__global__ void k_dense_pinned(int n, const int* rowptr, const int* col, const double* val, double* M) {
+  GRID_LOOP(t, (long long)n * n) M[t] = 0.0;
+}
+__global__ void k_dense_fill(int n, const int* rowptr, const int* col, const double* val, double* M) {
+  GRID_LOOP(i, n) {
+    for (int e = rowptr[i]; e < rowptr[i + 1]; ++e) {
+      int j = col[e];
+      if (i == 0 || j == 0) continue;
+      M[(long long)i * n + j] = val[e];
+    }
+    if (i == 0) M[0] = 1.0;
+  }
+}
+// In-place Gauss-Jordan inversion with partial pivoting, one block.
+constexpr int kGJ = 1024;
+__global__ void __launch_bounds__(kGJ) k_gauss_jordan(int n, double* M, int* perm, int* singular) {
+  __shared__ double s_val[kGJ / 32];
+  __shared__ int s_idx[kGJ / 32];
+  __shared__ int s_p;
+  __shared__ double s_inv;
+  extern __shared__ double s_row[];  // n (pivot row) + n (pivot column)
+  double* s_col = s_row + n;
+  for (int k = 0; k < n; ++k) {
+    // pivot: first index of max |M[i][k]|, i >= k
+    double best = -1.0;
+    int bi = k;
+    for (int i = k + threadIdx.x; i < n; i += blockDim.x) {
+      double v = fabs(M[(long long)i * n + k]);
+      if (v > best) { best = v; bi = i; }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      double ov = __shfl_down_sync(0xffffffffu, best, o);
+      int oi = __shfl_down_sync(0xffffffffu, bi, o);
+      if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+    }
+    if ((threadIdx.x & 31) == 0) { s_val[threadIdx.x >> 5] = best; s_idx[threadIdx.x >> 5] = bi; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double bv = -1.0; int b = k;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
+        if (s_val[w] > bv || (s_val[w] == bv && s_idx[w] < b)) { bv = s_val[w]; b = s_idx[w]; }
+      s_p = b;
+      perm[k] = b;
+      if (!(bv > 0.0)) *singular = 1;
+    }
+    __syncthreads();
+    const int p = s_p;
+    if (p != k)
+      for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        double a = M[(long long)k * n + j];
+        M[(long long)k * n + j] = M[(long long)p * n + j];
+        M[(long long)p * n + j] = a;
+      }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double piv = M[(long long)k * n + k];
+      s_inv = piv != 0.0 ? 1.0 / piv : 0.0;
+    }
+    __syncthreads();
+    const double inv = s_inv;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+      double v = (j == k) ? inv : M[(long long)k * n + j] * inv;
+      M[(long long)k * n + j] = v;
+      s_row[j] = v;
+    }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      s_col[i] = M[(long long)i * n + k];
+    }
+    __syncthreads();
+    for (long long t = threadIdx.x; t < (long long)n * n; t += blockDim.x) {
+      int i = (int)(t / n), j = (int)(t % n);
+      if (i == k) continue;
+      double f = s_col[i];
+      if (j == k) M[t] = -f * s_row[k];
+      else M[t] -= f * s_row[j];
+    }
+    __syncthreads();
+  }
+  // undo the row interchanges as column interchanges, last first
+  for (int k = n - 1; k >= 0; --k) {
+    int p = perm[k];
+    if (p != k)
+      for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        double a = M[(long long)i * n + k];
+        M[(long long)i * n + k] = M[(long long)i * n + p];
+        M[(long long)i * n + p] = a;
+      }
+    __syncthreads();
+  }
+}
+// x = Ainv * b with b[0] pinned to 0; one warp per row group
+template <typename T>
+__global__ void k_coarse_apply(int n, const double* __restrict__ Ainv, const T* __restrict__ b,
+                               T* __restrict__ x) {
+  extern __shared__ double s_b[];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s_b[i] = (i == 0) ? 0.0 : (double)b[i];
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int i = blockIdx.x * nw + warp; i < n; i += gridDim.x * nw) {
+    double acc = 0.0;
+    for (int j = lane; j < n; j += 32) acc += Ainv[(long long)i * n + j] * s_b[j];
+    acc = warp_sum(acc);
+    if (lane == 0) x[i] = (T)acc;
+  }
+}
+template <typename T>
+__global__ void k_pin_copy(int n, const T* b, T* out) { GRID_LOOP(i, n) out[i] = (i == 0) ? T(0) : b[i]; }
+
+}  // namespace
+
+// =================================================================== host
+void coarse_factor(AMG& h, Level& L, cudaStream_t s) {
+  if (L.n > 500 || L.n == 0) return;
+  const int n = L.n;
+  L.lu.ensure((size_t)n * n);
+  L.piv.ensure(n);
+  k_dense_pinned<<<grid_for((size_t)n * n, TB), TB, 0, s>>>(n, L.rowptr.p, L.col.p, L.val.p, L.lu.p);
+  k_dense_fill<<<grid_for(n, TB), TB, 0, s>>>(n, L.rowptr.p, L.col.p, L.val.p, L.lu.p);
+  IMPES_CUDA(cudaMemsetAsync(h.iflag.p + 2, 0, sizeof(int), s));
+  k_gauss_jordan<<<1, kGJ, 2 * n * sizeof(double), s>>>(n, L.lu.p, L.piv.p, h.iflag.p + 2);
+  IMPES_CHECK_LAUNCH();
+}
+
+void spmv(const Level& L, const double* x, double* y, cudaStream_t s) {
+  launch_csr<double, Y_AX>(L.n, L.avg_row, L.rowptr.p, L.col.p, L.val.p, x, nullptr, nullptr, y, s);
+}
+
+double dot_host(AMG& h, const double* a, const double* b, int n, cudaStream_t s) {
+  h.red.ensure((size_t)kMD * kDotBlocks);
+  k_multidot<<<kDotBlocks, TB, 0, s>>>(n, a, 0, 1, b, h.red.p);
+  k_dot_finalize<<<1, 32, 0, s>>>(1, h.red.p, h.scal.p, 0);
+  IMPES_CHECK_LAUNCH();
+  IMPES_CUDA(cudaMemcpyAsync(h.hbuf.p, h.scal.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+  IMPES_CUDA(cudaStreamSynchronize(s));
+  return h.hbuf.p[0];
+}
+
+namespace {
+
+template <typename T> struct LV;
+template <> struct LV<double> {
+  static const double* val(const Level& L) { return L.val.p; }
+  static const double* inv(const Level& L) { return L.inv_relax.p; }
+  static const double* pval(const Level& L) { return L.pval.p; }
+  static const double* rval(const Level& L) { return L.rval.p; }
+  static double* x(Level& L) { return L.x.p; }
+  static double* b(Level& L) { return L.b.p; }
+  static double* r(Level& L) { return L.r.p; }
+  static double* t(Level& L) { return L.t.p; }
+};
+template <> struct LV<float> {
+  static const float* val(const Level& L) { return L.valf.p; }
+  static const float* inv(const Level& L) { return L.inv_relaxf.p; }
+  static const float* pval(const Level& L) { return L.pvalf.p; }
+  static const float* rval(const Level& L) { return L.rvalf.p; }
+  static float* x(Level& L) { return L.xf.p; }
+  static float* b(Level& L) { return L.bf.p; }
+  static float* r(Level& L) { return L.rf.p; }
+  static float* t(Level& L) { return L.tf.p; }
+};
+
+// nu l1-Jacobi sweeps (classical_amg.py:1016-1035); returns the buffer holding x
+template <typename T>
+T* smooth(Level& L, T* x, T* spare, const T* b, int nu, bool zero_x, cudaStream_t s) {
+  for (int it = 0; it < nu; ++it) {
+    if (zero_x && it == 0) {
+      launch_csr<T, Y_SMOOTH0>(L.n, L.avg_row, L.rowptr.p, L.col.p, LV<T>::val(L), nullptr, b,
+                               LV<T>::inv(L), x, s);
+      continue;
+    }
+    launch_csr<T, Y_SMOOTH>(L.n, L.avg_row, L.rowptr.p, L.col.p, LV<T>::val(L), x, b,
+                            LV<T>::inv(L), spare, s);
+    std::swap(x, spare);
+  }
+  return x;
+}
+
+// _v_cycle (classical_amg.py:1037-1106) on level l: input b in LV<T>::b(L),
+// initial x in LV<T>::x(L) (ignored when zero_x); returns the buffer with x.
+template <typename T>
+T* vcycle(AMG& h, int l, bool zero_x, cudaStream_t s) {
+  Level& L = *h.levels[l];
+  if (L.coarsest) {
+    if (L.n <= 500) {
+      const int n = L.n;
+      k_coarse_apply<T><<<std::max(1, (n + 7) / 8), 256, n * sizeof(double), s>>>(n, L.lu.p,
+                                                                                 LV<T>::b(L), LV<T>::x(L));
+      IMPES_CHECK_LAUNCH();
+      return LV<T>::x(L);
+    }
+    // n > 500: 50 l1-Jacobi sweeps from zero on the pinned right-hand side
+    T* bp = LV<T>::r(L);
+    k_pin_copy<T><<<grid_for(L.n, TB), TB, 0, s>>>(L.n, LV<T>::b(L), bp);
+    return smooth<T>(L, LV<T>::x(L), LV<T>::t(L), bp, 50, true, s);
+  }
+  T* x = smooth<T>(L, LV<T>::x(L), LV<T>::t(L), LV<T>::b(L), 3, zero_x, s);
+  T* spare = (x == LV<T>::x(L)) ? LV<T>::t(L) : LV<T>::x(L);
+  Level& Nc = *h.levels[l + 1];
+  launch_csr<T, Y_B_MINUS_AX>(L.n, L.avg_row, L.rowptr.p, L.col.p, LV<T>::val(L), x, LV<T>::b(L),
+                              nullptr, LV<T>::r(L), s);
+  launch_csr<T, Y_AX>(L.nc, L.r_avg, L.rrow.p, L.rcol.p, LV<T>::rval(L), LV<T>::r(L), nullptr,
+                      nullptr, LV<T>::b(Nc), s);
+  T* ec = vcycle<T>(h, l + 1, true, s);
+  launch_csr<T, Y_ADD_AX>(L.n, L.p_avg, L.prow.p, L.pcol.p, LV<T>::pval(L), ec, nullptr, nullptr, x, s);
+  return smooth<T>(L, x, spare, LV<T>::b(L), 2, false, s);
+}
+
+}  // namespace
+
+// V-cycle on the equilibrated system: xs = V(0, bs)  (FP64 or FP32 inside)
+void amg_vcycle_scaled(AMG& h, const double* bs, double* xs, int precision, cudaStream_t s) {
+  Level& L0 = *h.levels[0];
+  const int n = L0.n;
+  if (precision == 1) {
+    IMPES_REQUIRE(h.prm.mixed_precision, IMPES_ERR_STATE, "fp32 V-cycle needs mixed_precision=1");
+    k_convert<double, float><<<grid_for(n, TB), TB, 0, s>>>(n, bs, L0.bf.p);
+    float* x = vcycle<float>(h, 0, true, s);
+    k_convert<float, double><<<grid_for(n, TB), TB, 0, s>>>(n, x, xs);
+  } else {
+    IMPES_CUDA(cudaMemcpyAsync(L0.b.p, bs, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    double* x = vcycle<double>(h, 0, true, s);
+    IMPES_CUDA(cudaMemcpyAsync(xs, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  }
+  IMPES_CHECK_LAUNCH();
+}
+
+// ClassicalAMG.solve (classical_amg.py:1108-1155)
+void amg_solve_vcycles(AMG& h, const double* b, double* x, double tol, int max_cycles, int* cycles,
+                       double* rel, cudaStream_t s) {
+  Level& L0 = *h.levels[0];
+  const int n = L0.n;
+  DBuf<double> bs(n), r(n);
+  k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, h.dhalf_inv.p, b, bs.p);
+  IMPES_CHECK_LAUNCH();
+  const double bn = std::sqrt(dot_host(h, bs.p, bs.p, n, s));
+  IMPES_CUDA(cudaMemcpyAsync(L0.b.p, bs.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  double rr = INFINITY;
+  int c = 0;
+  double* xs = nullptr;
+  for (c = 1; c <= max_cycles; ++c) {
+    xs = vcycle<double>(h, 0, c == 1, s);
+    if (xs != L0.x.p)
+      IMPES_CUDA(cudaMemcpyAsync(L0.x.p, xs, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    xs = L0.x.p;
+    launch_csr<double, Y_B_MINUS_AX>(n, L0.avg_row, L0.rowptr.p, L0.col.p, L0.val.p, xs, bs.p,
+                                     nullptr, r.p, s);
+    rr = std::sqrt(dot_host(h, r.p, r.p, n, s)) / (bn + 1e-30);
+    if (!(rr == rr)) throw Error(IMPES_ERR_NAN, "NaN residual in V-cycle solve");
+    if (rr < tol) break;
+  }
+  if (c > max_cycles) c = max_cycles;
+  k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, h.dhalf_inv.p, L0.x.p, x);
+  IMPES_CHECK_LAUNCH();
+  if (cycles) *cycles = c;
+  if (rel) *rel = rr;
+}
+
+// ClassicalAMG.apply (classical_amg.py:1157-1180)
+void amg_apply(AMG& h, const double* b, double* x, int cycles, double apply_tol,
+               int apply_max_cycles, cudaStream_t s) {
+  Level& L0 = *h.levels[0];
+  const int n = L0.n;
+  DBuf<double> bs(n), r(n);
+  k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, h.dhalf_inv.p, b, bs.p);
+  IMPES_CUDA(cudaMemcpyAsync(L0.b.p, bs.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  const double bn = std::sqrt(dot_host(h, bs.p, bs.p, n, s));
+  int c = 0;
+  while (c < apply_max_cycles) {
+    double* xs = vcycle<double>(h, 0, c == 0, s);
+    if (xs != L0.x.p)
+      IMPES_CUDA(cudaMemcpyAsync(L0.x.p, xs, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    ++c;
+    launch_csr<double, Y_B_MINUS_AX>(n, L0.avg_row, L0.rowptr.p, L0.col.p, L0.val.p, L0.x.p, bs.p,
+                                     nullptr, r.p, s);
+    double rel = std::sqrt(dot_host(h, r.p, r.p, n, s)) / (bn + 1e-30);
+    if (c >= cycles && rel < apply_tol) break;
+  }
+  k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, h.dhalf_inv.p, L0.x.p, x);
+  IMPES_CHECK_LAUNCH();
+}
+
+// ------------------------------------------------------------------ FGMRES
+namespace {
+
+__global__ void k_givens(int j, int ldh, double* H, double* cs, double* sn, double* g, double* est) {
+  double* hj = H + (long long)j * ldh;  // column j, rows 0..j+1
+  for (int i = 0; i < j; ++i) {
+    double t = cs[i] * hj[i] + sn[i] * hj[i + 1];
+    hj[i + 1] = -sn[i] * hj[i] + cs[i] * hj[i + 1];
+    hj[i] = t;
+  }
+  double a = hj[j], b = hj[j + 1];
+  double d = hypot(a, b);
+  double c = d > 0 ? a / d : 1.0, s = d > 0 ? b / d : 0.0;
+  cs[j] = c; sn[j] = s;
+  hj[j] = d; hj[j + 1] = 0.0;
+  g[j + 1] = -s * g[j];
+  g[j] = c * g[j];
+  *est = fabs(g[j + 1]);
+}
+__global__ void k_set_hcol(int j, int ldh, double* H, const double* nrm2) {
+  H[(long long)j * ldh + j + 1] = sqrt(*nrm2);
+}
+// y = R^{-1} g (upper triangular k x k, column-major with leading dim ldh)
+__global__ void k_backsolve(int k, int ldh, const double* H, const double* g, double* y) {
+  for (int i = k - 1; i >= 0; --i) {
+    double s = g[i];
+    for (int j = i + 1; j < k; ++j) s -= H[(long long)j * ldh + i] * y[j];
+    y[i] = s / H[(long long)i * ldh + i];
+  }
+}
+__global__ void k_combine(long long n, const double* __restrict__ Z, long long ldz, int k,
+                          const double* __restrict__ y, double* __restrict__ x) {
+  __shared__ double sy[128];
+  for (int q = threadIdx.x; q < k; q += blockDim.x) sy[q] = y[q];
+  __syncthreads();
+  GRID_LOOP(i, n) {
+    double v = x[i];
+    for (int q = 0; q < k; ++q) v += sy[q] * Z[q * ldz + i];
+    x[i] = v;
+  }
+}
+__global__ void k_hadd(int k, double* h, const double* y) {
+  for (int i = threadIdx.x; i < k; i += blockDim.x) h[i] += y[i];
+}
+__global__ void k_fill(long long n, double* a, double v) { GRID_LOOP(i, n) a[i] = v; }
+__global__ void k_init_g(double* g, int m1, const double* nrm2) {
+  for (int i = 0; i < m1; ++i) g[i] = 0.0;
+  g[0] = sqrt(*nrm2);
+}
+
+}  // namespace
+
+// Right-preconditioned flexible GMRES on the equilibrated system, with a row
+// weighting wt that selects the minimised norm: wt = 1 gives the reference's
+// equilibrated norm, wt = D^-1/2 (or 1/|a_ii| without equilibration) the Jacobi
+// norm ||D^-1 r||.  Operator K = diag(wt) A_s, preconditioner M(v) = V(v ./ wt).
+// Orthogonalisation is classical Gram-Schmidt with one re-orthogonalisation
+// pass; all reductions use a fixed block count (deterministic).
+void amg_fgmres(AMG& h, const double* b, double* x, const impes_krylov_params& kp,
+                impes_krylov_stats& st, cudaStream_t s) {
+  Level& L0 = *h.levels[0];
+  const int n = L0.n;
+  const int m = std::max(1, std::min(kp.restart, 120));
+  if (h.krylov_m != m || h.V.n < (size_t)(m + 1) * n) {
+    h.V.alloc((size_t)(m + 1) * n);
+    h.Z.alloc((size_t)m * n);
+    h.H.alloc((size_t)(m + 2) * (m + 1));
+    h.cs.alloc(m + 1); h.sn.alloc(m + 1); h.g.alloc(m + 2); h.y.alloc(m + 1);
+    h.kw.alloc(n); h.kb.alloc(n); h.kx.alloc(n);
+    h.krylov_m = m;
+  }
+  h.red.ensure((size_t)kMD * kDotBlocks + kDotBlocks);
+  const int ldh = m + 2;
+  const bool jac = kp.norm == IMPES_NORM_JACOBI;
+  double* wt = jac ? h.jac_w.p : h.kw.p;
+  if (!jac) k_fill<<<grid_for(n, TB), TB, 0, s>>>(n, h.kw.p, 1.0);
+  double* bs = h.kb.p;   // b_s = dhalf .* b
+  double* xs = h.kx.p;   // x_s
+  k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, h.dhalf_inv.p, b, bs);
+  if (kp.use_x0)
+    k_div_convert<double, double><<<grid_for(n, TB), TB, 0, s>>>(n, x, h.dhalf_inv.p, xs);
+  else
+    k_zero<<<grid_for(n, TB), TB, 0, s>>>(n, xs);
+  IMPES_CHECK_LAUNCH();
+  double* r0 = h.V.p;
+  k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, wt, bs, r0);
+  const double bnorm = std::sqrt(dot_host(h, r0, r0, n, s));
+  st = impes_krylov_stats{0, 0, 0, 0.0, 0.0};
+  if (!(bnorm > 0.0)) {
+    if (!(bnorm == bnorm)) throw Error(IMPES_ERR_NAN, "non-finite right-hand side");
+    k_zero<<<grid_for(n, TB), TB, 0, s>>>(n, x);
+    st.converged = 1;
+    return;
+  }
+  double* dscal = h.scal.p;  // [0] squared norm, [1] residual estimate
+  int total = 0;
+  double est_rel = INFINITY;
+  const int prec = kp.precision;
+  if (prec == 1)
+    IMPES_REQUIRE(h.prm.mixed_precision, IMPES_ERR_STATE, "fp32 V-cycle needs mixed_precision=1");
+  while (true) {
+    // V[0] = wt .* (b_s - A_s x_s), beta = ||V[0]||
+    launch_csr<double, Y_B_MINUS_AX>(n, L0.avg_row, L0.rowptr.p, L0.col.p, L0.val.p, xs, bs,
+                                     nullptr, h.V.p, s);
+    k_mul_inplace<<<grid_for(n, TB), TB, 0, s>>>(n, h.V.p, wt);
+    k_multidot<<<kDotBlocks, TB, 0, s>>>(n, h.V.p, 0, 1, h.V.p, h.red.p);
+    k_dot_finalize<<<1, 32, 0, s>>>(1, h.red.p, dscal, 0);
+    IMPES_CUDA(cudaMemcpyAsync(h.hbuf.p, dscal, sizeof(double), cudaMemcpyDeviceToHost, s));
+    IMPES_CUDA(cudaStreamSynchronize(s));
+    const double beta = std::sqrt(h.hbuf.p[0]);
+    if (!(beta == beta)) throw Error(IMPES_ERR_NAN, "NaN residual in FGMRES");
+    est_rel = beta / bnorm;
+    st.rel_res = est_rel;
+    if (est_rel < kp.tol || total >= kp.max_iters) break;
+    k_init_g<<<1, 1, 0, s>>>(h.g.p, m + 1, dscal);
+    k_scale_by_inv_sqrt<<<grid_for(n, TB), TB, 0, s>>>(n, h.V.p, h.V.p, dscal);
+    int j = 0;
+    for (; j < m && total < kp.max_iters; ++j) {
+      double* vj = h.V.p + (size_t)j * n;
+      double* zj = h.Z.p + (size_t)j * n;
+      double* w = h.V.p + (size_t)(j + 1) * n;
+      // z_j = V(v_j ./ wt)
+      if (prec == 1) {
+        k_div_convert<double, float><<<grid_for(n, TB), TB, 0, s>>>(n, vj, wt, L0.bf.p);
+        float* zf = vcycle<float>(h, 0, true, s);
+        k_convert<float, double><<<grid_for(n, TB), TB, 0, s>>>(n, zf, zj);
+      } else {
+        k_div_convert<double, double><<<grid_for(n, TB), TB, 0, s>>>(n, vj, wt, L0.b.p);
+        double* zd = vcycle<double>(h, 0, true, s);
+        IMPES_CUDA(cudaMemcpyAsync(zj, zd, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+      }
+      // w = wt .* (A_s z_j)
+      launch_csr<double, Y_W_AX>(n, L0.avg_row, L0.rowptr.p, L0.col.p, L0.val.p, zj, nullptr, wt, w, s);
+      double* hcol = h.H.p + (size_t)j * ldh;
+      for (int pass = 0; pass < 2; ++pass) {
+        double* coef = pass == 0 ? hcol : h.y.p;
+        for (int q0 = 0; q0 <= j; q0 += kMD) {
+          int k = std::min(kMD, j + 1 - q0);
+          k_multidot<<<kDotBlocks, TB, 0, s>>>(n, h.V.p + (size_t)q0 * n, n, k, w, h.red.p);
+          k_dot_finalize<<<k, 32, 0, s>>>(k, h.red.p, coef + q0, 0);
+        }
+        k_update<<<kDotBlocks, TB, 0, s>>>(n, h.V.p, n, j + 1, coef, w,
+                                           pass == 1 ? h.red.p : nullptr);
+      }
+      k_hadd<<<1, 128, 0, s>>>(j + 1, hcol, h.y.p);
+      k_dot_finalize<<<1, 32, 0, s>>>(1, h.red.p, dscal, 0);   // ||w||^2 from k_update
+      k_set_hcol<<<1, 1, 0, s>>>(j, ldh, h.H.p, dscal);
+      k_scale_by_inv_sqrt<<<grid_for(n, TB), TB, 0, s>>>(n, w, w, dscal);
+      k_givens<<<1, 1, 0, s>>>(j, ldh, h.H.p, h.cs.p, h.sn.p, h.g.p, dscal + 1);
+      IMPES_CHECK_LAUNCH();
+      ++total;
+      IMPES_CUDA(cudaMemcpyAsync(h.hbuf.p, dscal + 1, sizeof(double), cudaMemcpyDeviceToHost, s));
+      IMPES_CUDA(cudaStreamSynchronize(s));
+      est_rel = h.hbuf.p[0] / bnorm;
+      if (!(est_rel == est_rel)) throw Error(IMPES_ERR_NAN, "NaN in FGMRES");
+      if (est_rel < kp.tol) { ++j; break; }
+    }
+    // x_s += Z y with y = R^-1 g; the loop head re-checks the true residual
+    k_backsolve<<<1, 1, 0, s>>>(j, ldh, h.H.p, h.g.p, h.y.p);
+    k_combine<<<grid_for(n, TB), TB, 0, s>>>(n, h.Z.p, n, j, h.y.p, xs);
+    IMPES_CHECK_LAUNCH();
+    st.restarts++;
+  }
+  st.iterations = total;
+  st.converged = est_rel < kp.tol;
+  st.true_rel_res = est_rel;
+  k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, h.dhalf_inv.p, xs, x);
+  IMPES_CHECK_LAUNCH();
+}
+
+}  // namespace impes

@@ -1,0 +1,1020 @@
+// Ruge-Stueben AMG setup and matrix update on the device.
+//
+// Reference: researchim-ai/oil-simulator-py src/solver/classical_amg.py
+//   find_strong_connections :34-82, classical_coarsening :85-146,
+//   build_prolongation_rs_full :149-427, solve_energy_weights :1469-1501,
+//   generate_nullspace / orthonormalize_columns :1395-1466, _csr_spmm/rap_torch
+//   :519-657, ClassicalAMG.__init__ :699-938, update_matrix :1308-1392.
+//
+// Setup runs once per hierarchy (host-orchestrated, it syncs for sizes);
+// amg_update() is the per-step path: equilibration + Galerkin numeric products
+// for every level on a frozen pattern, all on the stream without host syncs.
+//
+// Galerkin products use a two-level "union" SpGEMM: the symbolic phase forms
+// each output row as the union of inner rows selected by an outer row, through a
+// per-warp open-addressing hash table in shared memory; the numeric phase keeps
+// each output row in shared memory and accumulates inner rows one outer entry at
+// a time (lanes own distinct output columns, so the sums are deterministic).
+#include "amg.cuh"
+#include <algorithm>
+#include <cmath>
+
+namespace impes {
+namespace {
+
+constexpr int TB = 256;
+
+__device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
+  uint64_t z = x + 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+// Deterministic [0,1) tie-break replacing torch.rand (classical_amg.py:125).
+__device__ __forceinline__ double tiebreak(uint32_t seed, int level, int i) {
+  uint64_t key = ((uint64_t)(seed & 0xFFFFFFu) << 40) | ((uint64_t)(level & 0xFF) << 32) |
+                 (uint64_t)(uint32_t)i;
+  return (double)(splitmix64(key) >> 11) * (1.0 / 9007199254740992.0);
+}
+
+#define GRID_LOOP(i, n) \
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (n); i += (long long)gridDim.x * blockDim.x)
+
+// ------------------------------------------------------------ validation
+__global__ void k_validate_csr(int n, int nnz, const int* rowptr, const int* col, int* flag) {
+  GRID_LOOP(i, n) {
+    int a = rowptr[i], b = rowptr[i + 1];
+    if (a > b || a < 0 || b > nnz) atomicOr(flag, 1);
+    for (int e = a; e < b && e < nnz && e >= 0; ++e) {
+      int c = col[e];
+      if (c < 0 || c >= n) atomicOr(flag, 2);
+      if (e > a && col[e - 1] >= c) atomicOr(flag, 4);
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (rowptr[0] != 0 || rowptr[n] != nnz) atomicOr(flag, 1);
+  }
+}
+
+__global__ void k_nonfinite(const double* v, long long n, int* flag) {
+  GRID_LOOP(i, n) if (!isfinite(v[i])) atomicOr(flag, 8);
+}
+
+// ------------------------------------------------------- diag / scaling
+// _extract_diag (classical_amg.py:940-955): value of the diagonal entry, 0 if none.
+__global__ void k_diag(int n, const int* rowptr, const int* col, const double* val, double* d) {
+  GRID_LOOP(i, n) {
+    double v = 0.0;
+    for (int e = rowptr[i]; e < rowptr[i + 1]; ++e)
+      if (col[e] == i) v = val[e];
+    d[i] = v;
+  }
+}
+// count of |d| (clamped at 1e-30) below the threshold -> lower-median test
+__global__ void k_count_below(int n, const double* d, double thr, int* cnt) {
+  int local = 0;
+  GRID_LOOP(i, n) local += (fmax(fabs(d[i]), 1e-30) < thr);
+  local = warp_sum_int(local);
+  if ((threadIdx.x & 31) == 0 && local) atomicAdd(cnt, local);
+}
+// dhalf = D^-1/2 when the lower median of |diag| is below the threshold, else 1;
+// Jacobi weights of the FGMRES norm in the scaled space.
+__global__ void k_equil_prepare(int n, const double* d, const int* below, double* dh, double* jw,
+                                int* flag_out) {
+  const bool on = below[0] >= (n - 1) / 2 + 1;
+  GRID_LOOP(i, n) {
+    const double a = fmax(fabs(d[i]), 1e-30);
+    const double hv = on ? 1.0 / sqrt(a) : 1.0;
+    dh[i] = hv;
+    jw[i] = on ? hv : 1.0 / a;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *flag_out = on ? 1 : 0;
+}
+// A_s = D^-1/2 A D^-1/2 as vals * dh[row] * dh[col] (classical_amg.py:776-780)
+__global__ void k_equilibrate(int n, const int* rowptr, const int* col, const double* vin,
+                              const double* dh, double* vout) {
+  GRID_LOOP(i, n) {
+    double di = dh[i];
+    for (int e = rowptr[i]; e < rowptr[i + 1]; ++e) vout[e] = vin[e] * di * dh[col[e]];
+  }
+}
+
+// l1-Jacobi weights (classical_amg.py:885-889, 1298-1306)
+__global__ void k_inv_relax(int n, const int* rowptr, const int* col, const double* val,
+                            double* inv) {
+  GRID_LOOP(i, n) {
+    double d = 0.0, ra = 0.0;
+    for (int e = rowptr[i]; e < rowptr[i + 1]; ++e) {
+      double v = val[e];
+      if (col[e] == i) d = v;
+      ra += fabs(v);
+    }
+    double denom = fmax(fabs(d), 0.3 * ra);
+    denom = denom < 1e-30 ? 1e-30 : denom;
+    double r = 1.0 / denom;
+    inv[i] = r > 1e2 ? 1e2 : r;
+  }
+}
+
+// --------------------------------------------------------------- strength
+// find_strong_connections (classical_amg.py:34-82)
+__global__ void k_strength(int n, const int* rowptr, const int* col, const double* val,
+                           double theta, unsigned char* strong) {
+  GRID_LOOP(i, n) {
+    const int a = rowptr[i], b = rowptr[i + 1];
+    double diag = 0.0;
+    for (int e = a; e < b; ++e)
+      if (col[e] == i) diag = fabs(val[e]);
+    const double den = fabs(diag) + 1e-30;
+    double mx = 0.0;
+    for (int e = a; e < b; ++e) {
+      double s = val[e] / den;
+      bool cand = (col[e] != i) && (s < 0);
+      double na = cand ? -s : 0.0;
+      mx = fmax(mx, na);
+    }
+    const double thr = theta * mx;
+    for (int e = a; e < b; ++e) {
+      double s = val[e] / den;
+      bool cand = (col[e] != i) && (s < 0);
+      strong[e] = (cand && (-s >= thr)) ? 1 : 0;
+    }
+  }
+}
+
+// ------------------------------------------------- symmetric strong graph
+__global__ void k_sym_count(int n, const int* rowptr, const int* col, const unsigned char* strong,
+                            int* cnt) {
+  GRID_LOOP(i, n) {
+    for (int e = rowptr[i]; e < rowptr[i + 1]; ++e)
+      if (strong[e]) { atomicAdd(&cnt[i], 1); atomicAdd(&cnt[col[e]], 1); }
+  }
+}
+__global__ void k_sym_fill(int n, const int* rowptr, const int* col, const unsigned char* strong,
+                           int* fill, int* gcol) {
+  GRID_LOOP(i, n) {
+    for (int e = rowptr[i]; e < rowptr[i + 1]; ++e)
+      if (strong[e]) {
+        int j = col[e];
+        gcol[atomicAdd(&fill[i], 1)] = j;
+        gcol[atomicAdd(&fill[j], 1)] = (int)i;
+      }
+  }
+}
+// sort + unique each row of the symmetric graph (the {min,max} coalesce at :113-116)
+__global__ void k_sym_unique(int n, const int* gptr, int* gcol, int* ucnt) {
+  GRID_LOOP(i, n) {
+    int a = gptr[i], b = gptr[i + 1];
+    for (int x = a + 1; x < b; ++x) {
+      int v = gcol[x], y = x - 1;
+      while (y >= a && gcol[y] > v) { gcol[y + 1] = gcol[y]; --y; }
+      gcol[y + 1] = v;
+    }
+    int u = 0;
+    for (int x = a; x < b; ++x)
+      if (u == 0 || gcol[a + u - 1] != gcol[x]) gcol[a + u++] = gcol[x];
+    ucnt[i] = u;
+  }
+}
+// score = deg + 1e-3 * w (classical_amg.py:124-126)
+__global__ void k_score(int n, const int* ucnt, uint32_t seed, int level, double* score) {
+  GRID_LOOP(i, n) score[i] = (double)ucnt[i] + 1e-3 * tiebreak(seed, level, (int)i);
+}
+// C = score > neighbour max.  The reference's two scatter_reduce_(amax,
+// include_self=False) passes (:129-132) leave, for every node with a
+// lower-index neighbour, the max over lower-index neighbours only; else the max
+// over higher-index neighbours; else 0.
+__global__ void k_cselect(int n, const int* gptr, const int* gcol, const int* ucnt,
+                          const double* score, unsigned char* C) {
+  GRID_LOOP(i, n) {
+    double lo = -INFINITY, up = -INFINITY;
+    bool hlo = false, hup = false;
+    for (int x = gptr[i]; x < gptr[i] + ucnt[i]; ++x) {
+      int j = gcol[x];
+      double s = score[j];
+      if (j < i) { hlo = true; lo = fmax(lo, s); }
+      else { hup = true; up = fmax(up, s); }
+    }
+    double nm = hlo ? lo : (hup ? up : 0.0);
+    C[i] = score[i] > nm;
+  }
+}
+// coverage lift (:136-141); has_C is int8 in the reference, so the count wraps mod 256
+__global__ void k_lift(int n, const int* gptr, const int* gcol, const int* ucnt,
+                       const unsigned char* C, signed char* cf, int* nc) {
+  int local = 0;
+  GRID_LOOP(i, n) {
+    int h = 0;
+    for (int x = gptr[i]; x < gptr[i] + ucnt[i]; ++x) h += C[gcol[x]];
+    signed char f = C[i] ? 0 : (((h & 0xFF) == 0) ? 0 : 1);
+    cf[i] = f;
+    local += (f == 0);
+  }
+  local = warp_sum_int(local);
+  if ((threadIdx.x & 31) == 0 && local) atomicAdd(nc, local);
+}
+// orphan promotion (:178-189): F rows without a strong C neighbour become C
+__global__ void k_orphans(int n, const int* rowptr, const int* col, const unsigned char* strong,
+                          const signed char* cf_in, signed char* cf_out, int* cflag) {
+  GRID_LOOP(i, n) {
+    signed char f = cf_in[i];
+    if (f == 1) {
+      bool has = false;
+      for (int e = rowptr[i]; e < rowptr[i + 1]; ++e)
+        if (strong[e] && col[e] != i && cf_in[col[e]] == 0) { has = true; break; }
+      if (!has) f = 0;
+    }
+    cf_out[i] = f;
+    cflag[i] = (f == 0);
+  }
+}
+
+// ----------------------------------------------------------- interpolation
+// Per-row sums of build_prolongation_rs_full (:193-236).
+__global__ void k_p_stats(int n, const int* rowptr, const int* col, const double* val,
+                          const unsigned char* strong, const signed char* cf, double* pdiag,
+                          double* ssum, double* wcsum, double* wfsum, int* scnt) {
+  GRID_LOOP(i, n) {
+    double d = 0.0, s = 0.0, wc = 0.0, wf = 0.0;
+    int c = 0;
+    const bool F = cf[i] == 1;
+    for (int e = rowptr[i]; e < rowptr[i + 1]; ++e) {
+      int j = col[e];
+      double v = val[e];
+      if (j == i) { d += v; continue; }
+      if (!F) continue;
+      bool jC = cf[j] == 0;
+      if (strong[e] && jC) { s += -v; ++c; }
+      else if (!strong[e] && jC) wc += -v;
+      else if (!strong[e] && !jC) wf += -v;
+    }
+    pdiag[i] = fabs(d) > 1e-14 ? d : 1.0;
+    ssum[i] = s; wcsum[i] = wc; wfsum[i] = wf; scnt[i] = c;
+  }
+}
+__device__ __forceinline__ bool ff_valid(int j, const int* scnt, const double* ssum) {
+  return scnt[j] > 0 && ssum[j] > 1e-14;
+}
+__global__ void k_p_count(int n, const int* rowptr, const int* col, const unsigned char* strong,
+                          const signed char* cf, const int* scnt, const double* ssum, int* cnt) {
+  GRID_LOOP(i, n) {
+    if (cf[i] == 0) { cnt[i] = 1; continue; }
+    int c = scnt[i];
+    for (int e = rowptr[i]; e < rowptr[i + 1]; ++e) {
+      int j = col[e];
+      if (j != i && strong[e] && cf[j] == 1 && ff_valid(j, scnt, ssum)) c += scnt[j];
+    }
+    cnt[i] = c;
+  }
+}
+__device__ __forceinline__ double nan_to_zero(double v) { return isfinite(v) ? v : 0.0; }
+
+__global__ void k_p_fill(int n, const int* rowptr, const int* col, const double* val,
+                         const unsigned char* strong, const signed char* cf, const int* f2c,
+                         const double* pdiag, const double* ssum, const double* wcsum,
+                         const double* wfsum, const int* scnt, const int* cptr, int* ccol,
+                         double* cval) {
+  GRID_LOOP(i, n) {
+    int o = cptr[i];
+    if (cf[i] == 0) { ccol[o] = f2c[i]; cval[o] = 1.0; continue; }
+    const int a = rowptr[i], b = rowptr[i + 1];
+    const double di = pdiag[i];
+    double fws = wfsum[i];
+    for (int e = a; e < b; ++e) {  // invalid F-F entries join the weak sum (:280-284)
+      int j = col[e];
+      if (j != i && strong[e] && cf[j] == 1 && !ff_valid(j, scnt, ssum)) fws += -val[e];
+    }
+    const double tw = wcsum[i] + fws;
+    const double corr = ssum[i] > 1e-14 ? tw / ssum[i] : 0.0;
+    for (int e = a; e < b; ++e) {  // direct RS weights (:240-246, 292-296)
+      int j = col[e];
+      if (j != i && strong[e] && cf[j] == 0) {
+        double v = nan_to_zero(-val[e] / di) * (1.0 + corr);
+        ccol[o] = f2c[j];
+        cval[o] = v < 0.0 ? 0.0 : v;
+        ++o;
+      }
+    }
+    for (int e = a; e < b; ++e) {  // F-F distribution (:248-278)
+      int j = col[e];
+      if (j == i || !strong[e] || cf[j] != 1 || !ff_valid(j, scnt, ssum)) continue;
+      const double fac = nan_to_zero(-val[e] / di);
+      const double sj = ssum[j];
+      for (int f = rowptr[j]; f < rowptr[j + 1]; ++f) {
+        int c = col[f];
+        if (c != j && strong[f] && cf[c] == 0) {
+          double w = sj > 1e-14 ? -val[f] / sj : 0.0;
+          double v = fac * w;
+          ccol[o] = f2c[c];
+          cval[o] = v < 0.0 ? 0.0 : v;
+          ++o;
+        }
+      }
+    }
+  }
+}
+// stable sort by column and sum duplicates (the COO coalesce at :323-331)
+__global__ void k_p_merge(int n, const int* cptr, int* ccol, double* cval, int* mcnt) {
+  GRID_LOOP(i, n) {
+    int a = cptr[i], b = cptr[i + 1];
+    for (int x = a + 1; x < b; ++x) {
+      int c = ccol[x]; double v = cval[x]; int y = x - 1;
+      while (y >= a && ccol[y] > c) { ccol[y + 1] = ccol[y]; cval[y + 1] = cval[y]; --y; }
+      ccol[y + 1] = c; cval[y + 1] = v;
+    }
+    int u = 0;
+    for (int x = a; x < b; ++x) {
+      if (u > 0 && ccol[a + u - 1] == ccol[x]) cval[a + u - 1] += cval[x];
+      else { ccol[a + u] = ccol[x]; cval[a + u] = cval[x]; ++u; }
+    }
+    mcnt[i] = u;
+  }
+}
+__global__ void k_p_compact(int n, const int* cptr, const int* ccol, const double* cval,
+                            const int* prow, int* pcol, double* pval) {
+  GRID_LOOP(i, n) {
+    int a = cptr[i], o = prow[i], m = prow[i + 1] - prow[i];
+    for (int x = 0; x < m; ++x) { pcol[o + x] = ccol[a + x]; pval[o + x] = cval[a + x]; }
+  }
+}
+// row sums of F rows; zero rows need the injection fallback (:347-385)
+__global__ void k_p_rowsum(int n, const int* prow, const double* pval, const signed char* cf,
+                           double* rsum, int* nzero) {
+  int local = 0;
+  GRID_LOOP(i, n) {
+    double s = 0.0;
+    for (int e = prow[i]; e < prow[i + 1]; ++e) s += pval[e];
+    rsum[i] = s;
+    local += (cf[i] == 1 && !(s > 1e-14));
+  }
+  local = warp_sum_int(local);
+  if ((threadIdx.x & 31) == 0 && local) atomicAdd(nzero, local);
+}
+// injection target of a zero F row: first coarse neighbour in A's row
+__global__ void k_p_zero_extra(int n, const int* rowptr, const int* col, const signed char* cf,
+                               const int* f2c, const double* rsum, int* extra, const int* prow,
+                               int* newcnt) {
+  GRID_LOOP(i, n) {
+    int x = -1;
+    if (cf[i] == 1 && !(rsum[i] > 1e-14)) {
+      for (int e = rowptr[i]; e < rowptr[i + 1]; ++e)
+        if (cf[col[e]] == 0) { x = f2c[col[e]]; break; }
+    }
+    extra[i] = x;
+    newcnt[i] = prow[i + 1] - prow[i] + (x >= 0);
+  }
+}
+__global__ void k_p_insert(int n, const int* prow, const int* pcol, const double* pval,
+                           const int* extra, const int* nrow, int* ncol, double* nval) {
+  GRID_LOOP(i, n) {
+    int o = nrow[i];
+    if (extra[i] >= 0) { ncol[o] = extra[i]; nval[o] = 1.0; ++o; }
+    for (int e = prow[i]; e < prow[i + 1]; ++e) { ncol[o] = pcol[e]; nval[o] = pval[e]; ++o; }
+  }
+}
+// scale F rows by 1/row_sum and clamp at 0 (:386-388)
+__global__ void k_p_scale(int n, const int* prow, double* pval, const signed char* cf,
+                          const double* rsum) {
+  GRID_LOOP(i, n) {
+    double sc = (cf[i] == 1 && rsum[i] > 1e-14) ? 1.0 / rsum[i] : 1.0;
+    for (int e = prow[i]; e < prow[i + 1]; ++e) {
+      double v = pval[e] * sc;
+      pval[e] = v < 0.0 ? 0.0 : v;
+    }
+  }
+}
+// Energy-minimising blend (:390-419, solve_energy_weights :1469-1501).
+// (A^T A + reg I)^-1 A^T y = A^T (A A^T + reg I)^-1 y with A = [B_c; 1^T] of
+// size (m+1) x k, so each F row solves an (m+1) x (m+1) SPD system (m <= 3).
+// B_c takes the FINE basis rows at the row's COARSE column indices, as the
+// reference indexes basis_dev[cols_row].
+__global__ void k_p_blend(int n, const int* prow, const int* pcol, double* pval,
+                          const signed char* cf, const double* basis, int m, double blend,
+                          double reg) {
+  GRID_LOOP(i, n) {
+    if (cf[i] != 1) continue;
+    const int a = prow[i], b = prow[i + 1];
+    if (b <= a) continue;
+    const int M = m + 1;
+    double G[4][4];
+    for (int p = 0; p < M; ++p)
+      for (int q = 0; q < M; ++q) G[p][q] = 0.0;
+    for (int e = a; e < b; ++e) {
+      double col_[4];
+      const double* br = basis + (long long)pcol[e] * m;
+      for (int p = 0; p < m; ++p) col_[p] = br[p];
+      col_[m] = 1.0;
+      for (int p = 0; p < M; ++p)
+        for (int q = 0; q < M; ++q) G[p][q] += col_[p] * col_[q];
+    }
+    for (int p = 0; p < M; ++p) G[p][p] += reg;
+    double y[4];
+    for (int p = 0; p < m; ++p) y[p] = basis[(long long)i * m + p];
+    y[m] = 1.0;
+    // Cholesky G = L L^T, then two triangular solves
+    double L[4][4];
+    bool ok = true;
+    for (int p = 0; p < M; ++p) {
+      for (int q = 0; q <= p; ++q) {
+        double s = G[p][q];
+        for (int r = 0; r < q; ++r) s -= L[p][r] * L[q][r];
+        if (p == q) {
+          if (!(s > 0.0)) { ok = false; s = 1.0; }
+          L[p][p] = sqrt(s);
+        } else {
+          L[p][q] = s / L[q][q];
+        }
+      }
+    }
+    if (!ok) continue;
+    double z[4];
+    for (int p = 0; p < M; ++p) {
+      double s = y[p];
+      for (int r = 0; r < p; ++r) s -= L[p][r] * z[r];
+      z[p] = s / L[p][p];
+    }
+    for (int p = M - 1; p >= 0; --p) {
+      double s = z[p];
+      for (int r = p + 1; r < M; ++r) s -= L[r][p] * z[r];
+      z[p] = s / L[p][p];
+    }
+    double wsum = 0.0;
+    for (int e = a; e < b; ++e) {
+      const double* br = basis + (long long)pcol[e] * m;
+      double w = z[m];
+      for (int p = 0; p < m; ++p) w += br[p] * z[p];
+      w = w < 0.0 ? 0.0 : w;
+      wsum += w;
+    }
+    if (wsum <= 1e-12) continue;
+    for (int e = a; e < b; ++e) {
+      const double* br = basis + (long long)pcol[e] * m;
+      double w = z[m];
+      for (int p = 0; p < m; ++p) w += br[p] * z[p];
+      w = w < 0.0 ? 0.0 : w;
+      pval[e] = (1.0 - blend) * pval[e] + blend * (w / wsum);
+    }
+  }
+}
+
+// ---------------------------------------------------------- R = P^T
+__global__ void k_col_count(int n, const int* prow, const int* pcol, int* cnt) {
+  GRID_LOOP(i, n) for (int e = prow[i]; e < prow[i + 1]; ++e) atomicAdd(&cnt[pcol[e]], 1);
+}
+__global__ void k_r_fill(int n, const int* prow, const int* pcol, int* fill, int* rcol, int* rsrc) {
+  GRID_LOOP(i, n) {
+    for (int e = prow[i]; e < prow[i + 1]; ++e) {
+      int s = atomicAdd(&fill[pcol[e]], 1);
+      rcol[s] = (int)i;
+      rsrc[s] = e;
+    }
+  }
+}
+__global__ void k_r_sort(int nc, const int* rrow, int* rcol, int* rsrc) {
+  GRID_LOOP(I, nc) {
+    int a = rrow[I], b = rrow[I + 1];
+    for (int x = a + 1; x < b; ++x) {
+      int c = rcol[x], s = rsrc[x], y = x - 1;
+      while (y >= a && rcol[y] > c) { rcol[y + 1] = rcol[y]; rsrc[y + 1] = rsrc[y]; --y; }
+      rcol[y + 1] = c; rsrc[y + 1] = s;
+    }
+  }
+}
+__global__ void k_gather(long long n, const int* src, const double* in, double* out) {
+  GRID_LOOP(e, n) out[e] = in[src[e]];
+}
+
+// ------------------------------------------------ union SpGEMM (symbolic)
+// candidate upper bound of each output row: sum of inner row lengths
+__global__ void k_union_bound(int rows, const int* optr, const int* ocol, const int* iptr, int* bound) {
+  GRID_LOOP(r, rows) {
+    int s = 0;
+    for (int e = optr[r]; e < optr[r + 1]; ++e) s += iptr[ocol[e] + 1] - iptr[ocol[e]];
+    bound[r] = s;
+  }
+}
+__global__ void k_max_i32(long long n, const int* v, int* out) {
+  int m = 0;
+  GRID_LOOP(i, n) m = max(m, v[i]);
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_down_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+__device__ __forceinline__ unsigned hash_slot(int key, unsigned mask) {
+  return ((unsigned)key * 2654435761u) & mask;
+}
+// One warp per output row.  Pass 1 (cols == nullptr): count distinct columns.
+// Pass 2: write the sorted distinct columns at outptr[row].
+__global__ void k_union_rows(int rows, const int* optr, const int* ocol, const int* iptr,
+                             const int* icol, int hsize, int* ucnt, const int* outptr,
+                             int* outcol) {
+  extern __shared__ int sh[];
+  const int wpb = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int* table = sh + warp * (2 * hsize + 1);
+  int* list = table + hsize;
+  int* lcount = list + hsize;
+  const unsigned mask = (unsigned)hsize - 1;
+  for (long long r = (long long)blockIdx.x * wpb + warp; r < rows; r += (long long)gridDim.x * wpb) {
+    for (int s = lane; s < hsize; s += 32) table[s] = -1;
+    if (lane == 0) *lcount = 0;
+    __syncwarp();
+    for (int e = optr[r]; e < optr[r + 1]; ++e) {
+      const int j = ocol[e];
+      for (int f = iptr[j] + lane; f < iptr[j + 1]; f += 32) {
+        const int key = icol[f];
+        unsigned h = hash_slot(key, mask);
+        while (true) {
+          int prev = atomicCAS(&table[h], -1, key);
+          if (prev == -1) { list[atomicAdd(lcount, 1)] = key; break; }
+          if (prev == key) break;
+          h = (h + 1) & mask;
+        }
+      }
+      __syncwarp();
+    }
+    __syncwarp();
+    const int u = *lcount;
+    if (outcol == nullptr) {
+      if (lane == 0) ucnt[r] = u;
+    } else {
+      const int base = outptr[r];
+      for (int x = lane; x < u; x += 32) {
+        int v = list[x], rank = 0;
+        for (int y = 0; y < u; ++y) rank += (list[y] < v);
+        outcol[base + rank] = v;
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// ------------------------------------------------ union SpGEMM (numeric)
+// out[r, J] = sum_e oval[e] * inner[ocol[e], J]; each output row lives in shared
+// memory; for one outer entry the lanes own distinct columns (deterministic).
+template <int WPB>
+__global__ void k_union_numeric(int rows, const int* __restrict__ optr, const int* __restrict__ ocol,
+                                const double* __restrict__ oval, const int* __restrict__ iptr,
+                                const int* __restrict__ icol, const double* __restrict__ ival,
+                                const int* __restrict__ outptr, const int* __restrict__ outcol,
+                                double* __restrict__ outval, int maxrow) {
+  extern __shared__ unsigned char shraw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int* scol = (int*)shraw + warp * maxrow;
+  double* sacc = (double*)((int*)shraw + WPB * maxrow + ((WPB * maxrow) & 1)) + warp * maxrow;
+  for (long long r = (long long)blockIdx.x * WPB + warp; r < rows; r += (long long)gridDim.x * WPB) {
+    const int ob = outptr[r], L = outptr[r + 1] - ob;
+    for (int x = lane; x < L; x += 32) { scol[x] = outcol[ob + x]; sacc[x] = 0.0; }
+    __syncwarp();
+    for (int e = optr[r]; e < optr[r + 1]; ++e) {
+      const int j = ocol[e];
+      const double a = oval[e];
+      for (int f = iptr[j] + lane; f < iptr[j + 1]; f += 32) {
+        const int key = icol[f];
+        int lo = 0, hi = L - 1;
+        while (lo < hi) {
+          int mid = (lo + hi) >> 1;
+          if (scol[mid] < key) lo = mid + 1; else hi = mid;
+        }
+        sacc[lo] += a * ival[f];
+      }
+      __syncwarp();
+    }
+    for (int x = lane; x < L; x += 32) outval[ob + x] = sacc[x];
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------- basis (nullspace)
+// torch.linspace(0, 1, n) evaluated from both ends about the midpoint.
+__global__ void k_linspace(int n, double* c) {
+  GRID_LOOP(i, n) {
+    double step = n > 1 ? 1.0 / (double)(n - 1) : 0.0;
+    long long half = n / 2;
+    c[i] = (i < half) ? 0.0 + step * (double)i : 1.0 - step * (double)(n - i - 1);
+  }
+}
+__global__ void k_fill_col(int n, int m, int c, double* B, const double* v, double a, double sub) {
+  GRID_LOOP(i, n) B[(long long)i * m + c] = (v ? v[i] : 1.0) * a - sub;
+}
+__global__ void k_col_extract(int n, int m, int c, const double* B, double* v) {
+  GRID_LOOP(i, n) v[i] = B[(long long)i * m + c];
+}
+__global__ void k_axpy(int n, double a, const double* x, double* y) {
+  GRID_LOOP(i, n) y[i] += a * x[i];
+}
+__global__ void k_scale_into(int n, double a, const double* x, double* y) {
+  GRID_LOOP(i, n) y[i] = x[i] * a;
+}
+__global__ void k_square(int n, const double* x, double* y) {
+  GRID_LOOP(i, n) y[i] = x[i] * x[i];
+}
+__global__ void k_add_scalar(int n, double* x, double a) {
+  GRID_LOOP(i, n) x[i] -= a;
+}
+// Bc = R * B (n_c x m)
+__global__ void k_restrict_basis(int nc, int m, const int* rrow, const int* rcol, const double* rval,
+                                 const double* B, double* Bc) {
+  GRID_LOOP(I, nc) {
+    double acc[3] = {0, 0, 0};
+    for (int e = rrow[I]; e < rrow[I + 1]; ++e) {
+      const double* br = B + (long long)rcol[e] * m;
+      for (int p = 0; p < m; ++p) acc[p] += rval[e] * br[p];
+    }
+    for (int p = 0; p < m; ++p) Bc[(long long)I * m + p] = acc[p];
+  }
+}
+
+__global__ void k_to_float(long long n, const double* in, float* out) {
+  GRID_LOOP(i, n) out[i] = (float)in[i];
+}
+
+}  // namespace
+
+// =================================================================== host
+namespace {
+
+struct Ctx {
+  AMG& h;
+  cudaStream_t s;
+};
+
+int to_host_int(AMG& h, const int* d, cudaStream_t s) {
+  IMPES_CUDA(cudaMemcpyAsync(h.hint.p, d, sizeof(int), cudaMemcpyDeviceToHost, s));
+  IMPES_CUDA(cudaStreamSynchronize(s));
+  return h.hint.p[0];
+}
+
+// orthonormalize_columns (classical_amg.py:1395-1407) on an n x m row-major basis.
+// Returns the number of kept columns (compacted to the front).
+int orthonormalize(AMG& h, double* B, int n, int m, cudaStream_t s) {
+  DBuf<double> v(n), q(n), out((size_t)n * m);
+  std::vector<DBuf<double>> kept;
+  for (int c = 0; c < m; ++c) {
+    k_col_extract<<<grid_for(n, TB), TB, 0, s>>>(n, m, c, B, v.p);
+    for (auto& qq : kept) {
+      double d = dot_host(h, v.p, qq.p, n, s);
+      k_axpy<<<grid_for(n, TB), TB, 0, s>>>(n, -d, qq.p, v.p);
+    }
+    double nv = std::sqrt(dot_host(h, v.p, v.p, n, s));
+    if (nv > 1e-10) {
+      DBuf<double> qn(n);
+      k_scale_into<<<grid_for(n, TB), TB, 0, s>>>(n, 1.0 / nv, v.p, qn.p);
+      kept.push_back(std::move(qn));
+    }
+  }
+  int mk = (int)kept.size();
+  if (mk == 0) {
+    DBuf<double> one(n);
+    k_fill_col<<<grid_for(n, TB), TB, 0, s>>>(n, 1, 0, one.p, nullptr, 1.0 / (std::sqrt((double)n) + 1e-30), 0.0);
+    kept.push_back(std::move(one));
+    mk = 1;
+  }
+  for (int c = 0; c < mk; ++c)
+    k_fill_col<<<grid_for(n, TB), TB, 0, s>>>(n, mk, c, B, kept[c].p, 1.0, 0.0);
+  IMPES_CUDA(cudaStreamSynchronize(s));
+  return mk;
+}
+
+// generate_nullspace (classical_amg.py:1426-1466) for dim <= 3.
+int level0_basis(AMG& h, DBuf<double>& B, int n, int dim, cudaStream_t s) {
+  if (dim <= 0) return 0;
+  dim = std::min(dim, 3);
+  B.alloc((size_t)n * 3);
+  DBuf<double> coords(n), tmp(n), c0(n), cur(n);
+  std::vector<DBuf<double>> basis;
+  {
+    DBuf<double> one(n);
+    double inv = 1.0 / (std::sqrt((double)n) + 1e-30);
+    k_fill_col<<<grid_for(n, TB), TB, 0, s>>>(n, 1, 0, one.p, nullptr, inv, 0.0);
+    basis.push_back(std::move(one));
+  }
+  k_linspace<<<grid_for(n, TB), TB, 0, s>>>(n, coords.p);
+  k_fill_col<<<grid_for(n, TB), TB, 0, s>>>(n, 1, 0, c0.p, nullptr, 1.0, 0.0);  // ones
+  double mean = dot_host(h, coords.p, c0.p, n, s) / n;
+  if ((int)basis.size() < dim) {
+    k_scale_into<<<grid_for(n, TB), TB, 0, s>>>(n, 1.0, coords.p, cur.p);
+    k_add_scalar<<<grid_for(n, TB), TB, 0, s>>>(n, cur.p, mean);
+    double nr = std::sqrt(dot_host(h, cur.p, cur.p, n, s));
+    if (nr > 1e-8) {
+      DBuf<double> q(n);
+      k_scale_into<<<grid_for(n, TB), TB, 0, s>>>(n, 1.0 / nr, cur.p, q.p);
+      basis.push_back(std::move(q));
+    }
+  }
+  if ((int)basis.size() < dim) {
+    k_square<<<grid_for(n, TB), TB, 0, s>>>(n, coords.p, cur.p);
+    double m2 = dot_host(h, cur.p, c0.p, n, s) / n;
+    k_add_scalar<<<grid_for(n, TB), TB, 0, s>>>(n, cur.p, m2);
+    double nr = std::sqrt(dot_host(h, cur.p, cur.p, n, s));
+    if (nr > 1e-8) {
+      for (auto& b : basis) {
+        double d = dot_host(h, cur.p, b.p, n, s);
+        k_axpy<<<grid_for(n, TB), TB, 0, s>>>(n, -d, b.p, cur.p);
+      }
+      double nr2 = std::sqrt(dot_host(h, cur.p, cur.p, n, s));
+      if (nr2 > 1e-8) {
+        DBuf<double> q(n);
+        k_scale_into<<<grid_for(n, TB), TB, 0, s>>>(n, 1.0 / nr2, cur.p, q.p);
+        basis.push_back(std::move(q));
+      }
+    }
+  }
+  int m = (int)basis.size();
+  for (int c = 0; c < m; ++c)
+    k_fill_col<<<grid_for(n, TB), TB, 0, s>>>(n, m, c, B.p, basis[c].p, 1.0, 0.0);
+  return orthonormalize(h, B.p, n, m, s);
+}
+
+// symbolic union product: output pattern (ptr, col), returns nnz and max row length
+void union_symbolic(AMG& h, int rows, const int* optr, const int* ocol, const int* iptr,
+                    const int* icol, DBuf<int>& outptr, DBuf<int>& outcol, int& maxrow,
+                    cudaStream_t s) {
+  DBuf<int> bound(rows), ucnt(rows + 1);
+  k_union_bound<<<grid_for(rows, TB), TB, 0, s>>>(rows, optr, ocol, iptr, bound.p);
+  IMPES_CUDA(cudaMemsetAsync(h.iflag.p, 0, sizeof(int), s));
+  k_max_i32<<<grid_for(rows, TB), TB, 0, s>>>(rows, bound.p, h.iflag.p);
+  int maxc = to_host_int(h, h.iflag.p, s);
+  int hsize = 32;
+  while (hsize < 2 * maxc) hsize <<= 1;
+  size_t per_warp = sizeof(int) * (2 * (size_t)hsize + 1);
+  int wpb = (int)std::max<size_t>(1, std::min<size_t>(8, (48u << 10) / per_warp));
+  size_t smem = per_warp * wpb;
+  IMPES_REQUIRE(smem <= (200u << 10), IMPES_ERR_ARG, "Galerkin row too wide for the hash table");
+  IMPES_CUDA(cudaFuncSetAttribute(k_union_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  unsigned grid = (unsigned)std::min<long long>((rows + wpb - 1) / wpb, (long long)num_sms() * 32);
+  k_union_rows<<<std::max(1u, grid), 32 * wpb, smem, s>>>(rows, optr, ocol, iptr, icol, hsize,
+                                                          ucnt.p, nullptr, nullptr);
+  IMPES_CHECK_LAUNCH();
+  outptr.alloc(rows + 1);
+  int nnz = exclusive_scan_i32(ucnt.p, outptr.p, rows, s);
+  outcol.alloc(std::max(nnz, 1));
+  k_union_rows<<<std::max(1u, grid), 32 * wpb, smem, s>>>(rows, optr, ocol, iptr, icol, hsize,
+                                                          nullptr, outptr.p, outcol.p);
+  IMPES_CHECK_LAUNCH();
+  IMPES_CUDA(cudaMemsetAsync(h.iflag.p, 0, sizeof(int), s));
+  k_max_i32<<<grid_for(rows, TB), TB, 0, s>>>(rows, ucnt.p, h.iflag.p);
+  maxrow = to_host_int(h, h.iflag.p, s);
+}
+
+void union_numeric(int rows, const int* optr, const int* ocol, const double* oval, const int* iptr,
+                   const int* icol, const double* ival, const int* outptr, const int* outcol,
+                   double* outval, int maxrow, cudaStream_t s) {
+  if (rows == 0) return;
+  maxrow = std::max(maxrow, 1);
+  size_t per_warp = (size_t)maxrow * (sizeof(int) + sizeof(double));
+  if (per_warp * 8 + 16 <= (96u << 10)) {
+    constexpr int W = 8;
+    size_t smem = per_warp * W + 16;
+    IMPES_CUDA(cudaFuncSetAttribute(k_union_numeric<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    unsigned grid = (unsigned)std::min<long long>((rows + W - 1) / W, (long long)num_sms() * 16);
+    k_union_numeric<W><<<grid, 32 * W, smem, s>>>(rows, optr, ocol, oval, iptr, icol, ival, outptr,
+                                                   outcol, outval, maxrow);
+  } else {
+    constexpr int W = 1;
+    size_t smem = per_warp * W + 16;
+    IMPES_REQUIRE(smem <= (220u << 10), IMPES_ERR_ARG, "Galerkin row too wide for shared memory");
+    IMPES_CUDA(cudaFuncSetAttribute(k_union_numeric<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    unsigned grid = (unsigned)std::min<long long>(rows, (long long)num_sms() * 32);
+    k_union_numeric<W><<<grid, 32 * W, smem, s>>>(rows, optr, ocol, oval, iptr, icol, ival, outptr,
+                                                   outcol, outval, maxrow);
+  }
+  IMPES_CHECK_LAUNCH();
+}
+
+void compute_inv_relax(AMG& h, Level& L, cudaStream_t s) {
+  L.inv_relax.ensure(std::max(L.n, 1));
+  k_inv_relax<<<grid_for(L.n, TB), TB, 0, s>>>(L.n, L.rowptr.p, L.col.p, L.val.p, L.inv_relax.p);
+  IMPES_CHECK_LAUNCH();
+}
+
+void alloc_level_vectors(Level& L) {
+  size_t n = std::max(L.n, 1);
+  L.x.ensure(n); L.b.ensure(n); L.r.ensure(n); L.t.ensure(n);
+  L.xf.ensure(n); L.bf.ensure(n); L.rf.ensure(n); L.tf.ensure(n);
+}
+
+// Equilibration of level-0 values (classical_amg.py:763-788 / 1334-1355).  The
+// ON/OFF decision (lower median of |diag| below the threshold) stays on the
+// device: with it OFF, dhalf = 1 and the scaling kernel copies values exactly.
+void equilibrate_level0(AMG& h, const double* val_in, cudaStream_t s) {
+  Level& L0 = *h.levels[0];
+  const int n = L0.n;
+  h.dhalf_inv.ensure(n);
+  h.jac_w.ensure(n);
+  h.diag_tmp.ensure(n);
+  k_diag<<<grid_for(n, TB), TB, 0, s>>>(n, L0.rowptr.p, L0.col.p, val_in, h.diag_tmp.p);
+  IMPES_CUDA(cudaMemsetAsync(h.iflag.p, 0, sizeof(int), s));
+  k_count_below<<<grid_for(n, TB), TB, 0, s>>>(n, h.diag_tmp.p, h.prm.equilibration_threshold, h.iflag.p);
+  k_equil_prepare<<<grid_for(n, TB), TB, 0, s>>>(n, h.diag_tmp.p, h.iflag.p, h.dhalf_inv.p,
+                                                 h.jac_w.p, h.iflag.p + 1);
+  k_equilibrate<<<grid_for(n, TB), TB, 0, s>>>(n, L0.rowptr.p, L0.col.p, val_in, h.dhalf_inv.p,
+                                               L0.val.p);
+  IMPES_CHECK_LAUNCH();
+}
+
+}  // namespace
+
+void level_precision_copies(AMG& h, Level& L, cudaStream_t s) {
+  if (!h.prm.mixed_precision) return;
+  L.valf.ensure(std::max(L.nnz, 1));
+  L.inv_relaxf.ensure(std::max(L.n, 1));
+  k_to_float<<<grid_for(L.nnz, TB), TB, 0, s>>>(L.nnz, L.val.p, L.valf.p);
+  k_to_float<<<grid_for(L.n, TB), TB, 0, s>>>(L.n, L.inv_relax.p, L.inv_relaxf.p);
+  if (!L.coarsest && L.pnnz) {
+    L.pvalf.ensure(L.pnnz);
+    L.rvalf.ensure(L.pnnz);
+    k_to_float<<<grid_for(L.pnnz, TB), TB, 0, s>>>(L.pnnz, L.pval.p, L.pvalf.p);
+    k_to_float<<<grid_for(L.pnnz, TB), TB, 0, s>>>(L.pnnz, L.rval.p, L.rvalf.p);
+  }
+  IMPES_CHECK_LAUNCH();
+}
+
+void amg_setup(AMG& h, int n, int nnz, const int* rowptr, const int* col, const double* val,
+               cudaStream_t s) {
+  IMPES_REQUIRE(n > 0 && nnz > 0, IMPES_ERR_ARG, "empty matrix");
+  h.levels.clear();
+  h.built = false;
+  h.iflag.ensure(8);
+  h.red.ensure(4096);
+  h.scal.ensure(256);
+  // validate the caller's CSR before reading it
+  IMPES_CUDA(cudaMemsetAsync(h.iflag.p, 0, sizeof(int), s));
+  k_validate_csr<<<grid_for(n, TB), TB, 0, s>>>(n, nnz, rowptr, col, h.iflag.p);
+  k_nonfinite<<<grid_for(nnz, TB), TB, 0, s>>>(val, nnz, h.iflag.p);
+  int bad = to_host_int(h, h.iflag.p, s);
+  IMPES_REQUIRE(!(bad & 7), IMPES_ERR_BAD_CSR, "malformed CSR (row pointers, column range or order)");
+  IMPES_REQUIRE(!(bad & 8), IMPES_ERR_NAN, "non-finite matrix value");
+
+  auto L0p = std::make_unique<Level>();
+  Level& L0 = *L0p;
+  L0.n = n; L0.nnz = nnz;
+  L0.rowptr.alloc(n + 1); L0.col.alloc(nnz); L0.val.alloc(nnz);
+  IMPES_CUDA(cudaMemcpyAsync(L0.rowptr.p, rowptr, sizeof(int) * (n + 1), cudaMemcpyDeviceToDevice, s));
+  IMPES_CUDA(cudaMemcpyAsync(L0.col.p, col, sizeof(int) * nnz, cudaMemcpyDeviceToDevice, s));
+  h.levels.push_back(std::move(L0p));
+  equilibrate_level0(h, val, s);
+
+  DBuf<double> basis;
+  int m = level0_basis(h, basis, n, h.prm.nullspace_dim, s);
+  const double theta = h.prm.theta;
+  for (int lvl = 0; lvl < h.prm.max_levels; ++lvl) {
+    Level& L = *h.levels.back();
+    L.avg_row = std::max(1, L.nnz / std::max(L.n, 1));
+    const int nl = L.n;
+    compute_inv_relax(h, L, s);
+    alloc_level_vectors(L);
+    if (nl <= h.prm.coarsest_size) { L.coarsest = true; break; }
+    // strength + C/F split
+    DBuf<unsigned char> strong(L.nnz);
+    k_strength<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.rowptr.p, L.col.p, L.val.p, theta, strong.p);
+    DBuf<int> gcnt(nl + 1), gptr(nl + 1), fill(nl + 1);
+    IMPES_CUDA(cudaMemsetAsync(gcnt.p, 0, sizeof(int) * (nl + 1), s));
+    k_sym_count<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.rowptr.p, L.col.p, strong.p, gcnt.p);
+    int gn = exclusive_scan_i32(gcnt.p, gptr.p, nl, s);
+    DBuf<int> gcol(std::max(gn, 1)), ucnt(nl);
+    IMPES_CUDA(cudaMemcpyAsync(fill.p, gptr.p, sizeof(int) * nl, cudaMemcpyDeviceToDevice, s));
+    k_sym_fill<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.rowptr.p, L.col.p, strong.p, fill.p, gcol.p);
+    k_sym_unique<<<grid_for(nl, TB), TB, 0, s>>>(nl, gptr.p, gcol.p, ucnt.p);
+    DBuf<double> score(nl);
+    k_score<<<grid_for(nl, TB), TB, 0, s>>>(nl, ucnt.p, h.prm.tiebreak_seed, lvl, score.p);
+    DBuf<unsigned char> C(nl);
+    k_cselect<<<grid_for(nl, TB), TB, 0, s>>>(nl, gptr.p, gcol.p, ucnt.p, score.p, C.p);
+    DBuf<signed char> cf(nl), cf2(nl);
+    IMPES_CUDA(cudaMemsetAsync(h.iflag.p, 0, sizeof(int), s));
+    k_lift<<<grid_for(nl, TB), TB, 0, s>>>(nl, gptr.p, gcol.p, ucnt.p, C.p, cf.p, h.iflag.p);
+    IMPES_CHECK_LAUNCH();
+    int n_coarse = to_host_int(h, h.iflag.p, s);
+    if ((double)n_coarse >= nl * 0.9) { L.coarsest = true; break; }  // :832
+    // orphans + fine->coarse map
+    DBuf<int> cflag(nl + 1), f2c(nl + 1);
+    k_orphans<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.rowptr.p, L.col.p, strong.p, cf.p, cf2.p, cflag.p);
+    const int nc = exclusive_scan_i32(cflag.p, f2c.p, nl, s);
+    // interpolation
+    DBuf<double> pdiag(nl), ssum(nl), wcsum(nl), wfsum(nl);
+    DBuf<int> scnt(nl), ccnt(nl + 1), cptr(nl + 1);
+    k_p_stats<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.rowptr.p, L.col.p, L.val.p, strong.p, cf2.p,
+                                              pdiag.p, ssum.p, wcsum.p, wfsum.p, scnt.p);
+    k_p_count<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.rowptr.p, L.col.p, strong.p, cf2.p, scnt.p,
+                                              ssum.p, ccnt.p);
+    int ctot = exclusive_scan_i32(ccnt.p, cptr.p, nl, s);
+    DBuf<int> ccol(std::max(ctot, 1));
+    DBuf<double> cval(std::max(ctot, 1));
+    k_p_fill<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.rowptr.p, L.col.p, L.val.p, strong.p, cf2.p,
+                                             f2c.p, pdiag.p, ssum.p, wcsum.p, wfsum.p, scnt.p,
+                                             cptr.p, ccol.p, cval.p);
+    DBuf<int> mcnt(nl + 1);
+    k_p_merge<<<grid_for(nl, TB), TB, 0, s>>>(nl, cptr.p, ccol.p, cval.p, mcnt.p);
+    L.nc = nc;
+    L.prow.alloc(nl + 1);
+    L.pnnz = exclusive_scan_i32(mcnt.p, L.prow.p, nl, s);
+    L.pcol.alloc(std::max(L.pnnz, 1));
+    L.pval.alloc(std::max(L.pnnz, 1));
+    k_p_compact<<<grid_for(nl, TB), TB, 0, s>>>(nl, cptr.p, ccol.p, cval.p, L.prow.p, L.pcol.p, L.pval.p);
+    DBuf<double> rsum(nl);
+    IMPES_CUDA(cudaMemsetAsync(h.iflag.p, 0, sizeof(int), s));
+    k_p_rowsum<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.prow.p, L.pval.p, cf2.p, rsum.p, h.iflag.p);
+    int nzero = to_host_int(h, h.iflag.p, s);
+    if (nzero > 0) {
+      DBuf<int> extra(nl), ncnt(nl + 1), nrow(nl + 1);
+      k_p_zero_extra<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.rowptr.p, L.col.p, cf2.p, f2c.p, rsum.p,
+                                                     extra.p, L.prow.p, ncnt.p);
+      int nn = exclusive_scan_i32(ncnt.p, nrow.p, nl, s);
+      DBuf<int> ncol(nn);
+      DBuf<double> nval(nn);
+      k_p_insert<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.prow.p, L.pcol.p, L.pval.p, extra.p, nrow.p,
+                                                 ncol.p, nval.p);
+      IMPES_CUDA(cudaStreamSynchronize(s));
+      L.prow = std::move(nrow); L.pcol = std::move(ncol); L.pval = std::move(nval);
+      L.pnnz = nn;
+      k_p_rowsum<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.prow.p, L.pval.p, cf2.p, rsum.p, h.iflag.p);
+    }
+    k_p_scale<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.prow.p, L.pval.p, cf2.p, rsum.p);
+    IMPES_CHECK_LAUNCH();
+    if (m > 0 && h.prm.nullspace_blend > 0.0) {
+      m = orthonormalize(h, basis.p, nl, m, s);   // build_prolongation_rs_full :393-396
+      k_p_blend<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.prow.p, L.pcol.p, L.pval.p, cf2.p, basis.p, m,
+                                                h.prm.nullspace_blend, h.prm.nullspace_reg);
+      IMPES_CHECK_LAUNCH();
+    }
+    // R = P^T (sorted rows) and its values
+    DBuf<int> rcnt(nc + 1), rfill(nc + 1);
+    IMPES_CUDA(cudaMemsetAsync(rcnt.p, 0, sizeof(int) * (nc + 1), s));
+    k_col_count<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.prow.p, L.pcol.p, rcnt.p);
+    L.rrow.alloc(nc + 1);
+    exclusive_scan_i32(rcnt.p, L.rrow.p, nc, s);
+    L.rcol.alloc(std::max(L.pnnz, 1)); L.rsrc.alloc(std::max(L.pnnz, 1)); L.rval.alloc(std::max(L.pnnz, 1));
+    IMPES_CUDA(cudaMemcpyAsync(rfill.p, L.rrow.p, sizeof(int) * nc, cudaMemcpyDeviceToDevice, s));
+    k_r_fill<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.prow.p, L.pcol.p, rfill.p, L.rcol.p, L.rsrc.p);
+    k_r_sort<<<grid_for(nc, TB), TB, 0, s>>>(nc, L.rrow.p, L.rcol.p, L.rsrc.p);
+    k_gather<<<grid_for(L.pnnz, TB), TB, 0, s>>>(L.pnnz, L.rsrc.p, L.pval.p, L.rval.p);
+    IMPES_CHECK_LAUNCH();
+    L.p_avg = std::max(1, L.pnnz / std::max(nl, 1));
+    L.r_avg = std::max(1, L.pnnz / std::max(nc, 1));
+    // Galerkin: AP = A P, A_c = R (AP)
+    auto Ncp = std::make_unique<Level>();
+    Level& Nc = *Ncp;
+    Nc.n = nc;
+    union_symbolic(h, nl, L.rowptr.p, L.col.p, L.prow.p, L.pcol.p, L.aprow, L.apcol, L.ap_maxrow, s);
+    int apnnz;
+    IMPES_CUDA(cudaMemcpyAsync(h.hint.p, L.aprow.p + nl, sizeof(int), cudaMemcpyDeviceToHost, s));
+    IMPES_CUDA(cudaStreamSynchronize(s));
+    apnnz = h.hint.p[0];
+    L.apval.alloc(std::max(apnnz, 1));
+    union_symbolic(h, nc, L.rrow.p, L.rcol.p, L.aprow.p, L.apcol.p, Nc.rowptr, Nc.col, L.ac_maxrow, s);
+    IMPES_CUDA(cudaMemcpyAsync(h.hint.p, Nc.rowptr.p + nc, sizeof(int), cudaMemcpyDeviceToHost, s));
+    IMPES_CUDA(cudaStreamSynchronize(s));
+    Nc.nnz = h.hint.p[0];
+    Nc.val.alloc(std::max(Nc.nnz, 1));
+    union_numeric(nl, L.rowptr.p, L.col.p, L.val.p, L.prow.p, L.pcol.p, L.pval.p, L.aprow.p,
+                  L.apcol.p, L.apval.p, L.ap_maxrow, s);
+    union_numeric(nc, L.rrow.p, L.rcol.p, L.rval.p, L.aprow.p, L.apcol.p, L.apval.p, Nc.rowptr.p,
+                  Nc.col.p, Nc.val.p, L.ac_maxrow, s);
+    // coarse basis (classical_amg.py:906-914)
+    if (m > 0) {
+      DBuf<double> Bc((size_t)std::max(nc, 1) * m);
+      k_restrict_basis<<<grid_for(nc, TB), TB, 0, s>>>(nc, m, L.rrow.p, L.rcol.p, L.rval.p, basis.p, Bc.p);
+      IMPES_CHECK_LAUNCH();
+      m = orthonormalize(h, Bc.p, nc, m, s);
+      basis = std::move(Bc);
+    }
+    IMPES_CUDA(cudaStreamSynchronize(s));
+    h.levels.push_back(std::move(Ncp));
+  }
+  Level& Lc = *h.levels.back();
+  if (!Lc.coarsest) {  // max_levels reached (:917-934)
+    Lc.avg_row = std::max(1, Lc.nnz / std::max(Lc.n, 1));
+    compute_inv_relax(h, Lc, s);
+    alloc_level_vectors(Lc);
+    Lc.coarsest = true;
+  }
+  coarse_factor(h, Lc, s);
+  for (auto& L : h.levels) level_precision_copies(h, *L, s);
+  IMPES_CUDA(cudaStreamSynchronize(s));
+  h.built = true;
+}
+
+void amg_update(AMG& h, const double* val, cudaStream_t s) {
+  IMPES_REQUIRE(h.built, IMPES_ERR_STATE, "update before setup");
+  equilibrate_level0(h, val, s);
+  for (size_t l = 0; l < h.levels.size(); ++l) {
+    Level& L = *h.levels[l];
+    compute_inv_relax(h, L, s);
+    if (L.coarsest) break;
+    Level& Nc = *h.levels[l + 1];
+    union_numeric(L.n, L.rowptr.p, L.col.p, L.val.p, L.prow.p, L.pcol.p, L.pval.p, L.aprow.p,
+                  L.apcol.p, L.apval.p, L.ap_maxrow, s);
+    union_numeric(L.nc, L.rrow.p, L.rcol.p, L.rval.p, L.aprow.p, L.apcol.p, L.apval.p,
+                  Nc.rowptr.p, Nc.col.p, Nc.val.p, L.ac_maxrow, s);
+  }
+  coarse_factor(h, *h.levels.back(), s);
+  for (auto& L : h.levels) {
+    if (!h.prm.mixed_precision) break;
+    L->valf.ensure(std::max(L->nnz, 1));
+    L->inv_relaxf.ensure(std::max(L->n, 1));
+    k_to_float<<<grid_for(L->nnz, TB), TB, 0, s>>>(L->nnz, L->val.p, L->valf.p);
+    k_to_float<<<grid_for(L->n, TB), TB, 0, s>>>(L->n, L->inv_relax.p, L->inv_relaxf.p);
+  }
+  IMPES_CHECK_LAUNCH();
+}
+
+}  // namespace impes

@@ -1,0 +1,70 @@
+// Shared host utilities: thread-local error text and a device exclusive scan.
+#include "common.cuh"
+
+namespace impes {
+
+static thread_local std::string g_last_error;
+
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+const char* last_error_cstr() { return g_last_error.c_str(); }
+
+namespace {
+constexpr int kScanBlock = 1024;
+
+// Phase 1: per-block inclusive scan in shared memory; block totals to `sums`.
+__global__ void k_scan_block(const int* __restrict__ in, int* __restrict__ out, int n,
+                             int* __restrict__ sums) {
+  __shared__ int s[kScanBlock];
+  int i = blockIdx.x * kScanBlock + threadIdx.x;
+  int v = (i < n) ? in[i] : 0;
+  s[threadIdx.x] = v;
+  __syncthreads();
+  for (int o = 1; o < kScanBlock; o <<= 1) {
+    int t = (threadIdx.x >= (unsigned)o) ? s[threadIdx.x - o] : 0;
+    __syncthreads();
+    s[threadIdx.x] += t;
+    __syncthreads();
+  }
+  if (i < n) out[i] = s[threadIdx.x] - v;  // exclusive
+  if (threadIdx.x == kScanBlock - 1) sums[blockIdx.x] = s[threadIdx.x];
+}
+
+// Phase 2: add the scanned block offsets; last element gets the total.
+__global__ void k_scan_add(int* __restrict__ out, int n, const int* __restrict__ offs) {
+  int i = blockIdx.x * kScanBlock + threadIdx.x;
+  if (i < n) out[i] += offs[blockIdx.x];
+}
+__global__ void k_scan_total(const int* __restrict__ in, int* __restrict__ out, int n) {
+  out[n] = (n > 0) ? out[n - 1] + in[n - 1] : 0;
+}
+}  // namespace
+
+void exclusive_scan_i32_dev(const int* d_in, int* d_out, int n, cudaStream_t stream) {
+  if (n <= 0) {
+    IMPES_CUDA(cudaMemsetAsync(d_out, 0, sizeof(int), stream));
+    return;
+  }
+  int nb = (n + kScanBlock - 1) / kScanBlock;
+  DBuf<int> sums(nb), offs(nb + 1);
+  k_scan_block<<<nb, kScanBlock, 0, stream>>>(d_in, d_out, n, sums.p);
+  IMPES_CHECK_LAUNCH();
+  if (nb > 1) {
+    exclusive_scan_i32_dev(sums.p, offs.p, nb, stream);
+    k_scan_add<<<nb, kScanBlock, 0, stream>>>(d_out, n, offs.p);
+    IMPES_CHECK_LAUNCH();
+  }
+  k_scan_total<<<1, 1, 0, stream>>>(d_in, d_out, n);
+  IMPES_CHECK_LAUNCH();
+  // temporaries are freed at scope exit: make sure the kernels using them ran
+  IMPES_CUDA(cudaStreamSynchronize(stream));
+}
+
+int exclusive_scan_i32(const int* d_in, int* d_out, int n, cudaStream_t stream) {
+  exclusive_scan_i32_dev(d_in, d_out, n, stream);
+  int total = 0;
+  IMPES_CUDA(cudaMemcpyAsync(&total, d_out + n, sizeof(int), cudaMemcpyDeviceToHost, stream));
+  IMPES_CUDA(cudaStreamSynchronize(stream));
+  return total;
+}
+
+}  // namespace impes

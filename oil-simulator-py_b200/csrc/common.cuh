@@ -1,0 +1,154 @@
+// Shared device/host utilities for the IMPES + AMG library (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string>
+#include <vector>
+#include <stdexcept>
+
+#include "../../include/impes_b200.h"
+
+namespace impes {
+
+// ------------------------------------------------------------------ errors
+struct Error : public std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void set_last_error(const std::string& msg);
+
+#define IMPES_CUDA(call)                                                        \
+  do {                                                                          \
+    cudaError_t e_ = (call);                                                    \
+    if (e_ != cudaSuccess)                                                      \
+      throw ::impes::Error(IMPES_ERR_CUDA, std::string(#call) + ": " +          \
+                                               cudaGetErrorString(e_));         \
+  } while (0)
+
+#define IMPES_CHECK_LAUNCH() IMPES_CUDA(cudaGetLastError())
+
+#define IMPES_REQUIRE(cond, code, msg)                                          \
+  do {                                                                          \
+    if (!(cond)) throw ::impes::Error((code), (msg));                           \
+  } while (0)
+
+// ------------------------------------------------------------ device buffer
+// Owning device allocation (library workspace; callers own their own I/O).
+template <typename T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  explicit DBuf(size_t count) { alloc(count); }
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  DBuf(DBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DBuf& operator=(DBuf&& o) noexcept {
+    if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+    return *this;
+  }
+  ~DBuf() { release(); }
+  void alloc(size_t count) {
+    release();
+    n = count;
+    if (count) {
+      cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+      if (e != cudaSuccess) {
+        p = nullptr; n = 0;
+        throw Error(IMPES_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+      }
+    }
+  }
+  void ensure(size_t count) { if (count > n) alloc(count); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr; n = 0;
+  }
+  T* get() const { return p; }
+  size_t bytes() const { return n * sizeof(T); }
+};
+
+// Small pinned host scratch for device->host scalars.
+template <typename T>
+struct HostPinned {
+  T* p = nullptr;
+  size_t n = 0;
+  explicit HostPinned(size_t count = 1) {
+    n = count;
+    if (cudaMallocHost(&p, count * sizeof(T)) != cudaSuccess) {
+      p = nullptr;
+      throw Error(IMPES_ERR_OOM, "cudaMallocHost failed");
+    }
+  }
+  ~HostPinned() { if (p) cudaFreeHost(p); }
+  HostPinned(const HostPinned&) = delete;
+  HostPinned& operator=(const HostPinned&) = delete;
+};
+
+inline int num_sms() {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (sms <= 0) sms = 148;
+  }
+  return sms;
+}
+
+inline unsigned grid_for(size_t n, int block, int max_per_sm = 8) {
+  size_t g = (n + block - 1) / block;
+  size_t cap = (size_t)num_sms() * max_per_sm * 8;
+  if (g > cap) g = cap;
+  return (unsigned)(g ? g : 1);
+}
+
+// --------------------------------------------------------- device helpers
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ int warp_sum_int(int v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block-wide sum in a fixed tree order (deterministic for a fixed block size).
+template <int BLOCK>
+__device__ __forceinline__ double block_sum(double v, double* smem /*>= BLOCK/32*/) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  v = warp_sum(v);
+  if (lane == 0) smem[wid] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (wid == 0) {
+    r = (lane < BLOCK / 32) ? smem[lane] : 0.0;
+    r = warp_sum(r);
+  }
+  __syncthreads();
+  return r;  // valid in thread 0
+}
+
+// ------------------------------------------------------------- host helpers
+// Exclusive scan of int32 counts into int32 offsets (returns total).  Runs a
+// three-phase block scan on `stream`; `total_host` is filled after a sync.
+int exclusive_scan_i32(const int* d_in, int* d_out, int n, cudaStream_t stream);
+// Same, result left on the device in d_out[n] (no host sync).
+void exclusive_scan_i32_dev(const int* d_in, int* d_out, int n, cudaStream_t stream);
+
+}  // namespace impes

@@ -1,0 +1,217 @@
+"""Generate the golden fixtures by running the reference itself (build container only).
+
+Usage:  python tests/golden/make_golden.py [REFERENCE_ROOT]
+
+REFERENCE_ROOT defaults to /root/reference (researchim-ai/oil-simulator-py).
+The reference is imported unmodified; the harness only
+  * puts a placeholder ``matplotlib`` first on sys.path (plotting is unused here),
+  * sets ``torch.set_default_dtype(torch.float64)`` before building objects,
+  * overwrites ``Reservoir.permeability_{x,y,z}``, ``porosity`` and
+    ``porous_volume`` with the seeded fields before ``Simulator()`` is built,
+  * replaces ``Fluid._eval_pvt``'s float32 cast with float64 (same ``np.interp``),
+  * replaces ``solver.pressure_amg.amg_solve`` by a direct ``spsolve`` of the
+    reference's own assembled (A, b), recording both (the trajectory oracle),
+  * feeds ``torch.rand`` the deterministic C/F tie-break vector while
+    ``ClassicalAMG`` builds its hierarchy.
+Outputs go to ``tests/golden/*.npz``.  The fixtures hold their own inputs
+(config JSON, rock fields) so tests never need the reference.
+"""
+from __future__ import annotations
+
+import contextlib
+import io
+import json
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+sys.path[:0] = [os.path.join(HERE, "_stubs"), os.path.join(REF, "src"),
+                os.path.join(REPO, "oil-simulator-py_b200"), REPO]
+
+import torch  # noqa: E402
+import scipy.sparse as sp  # noqa: E402
+import scipy.sparse.linalg as spla  # noqa: E402
+
+torch.set_default_dtype(torch.float64)
+torch.set_num_threads(4)
+
+from simulator.reservoir import Reservoir  # noqa: E402
+from simulator.fluid import Fluid  # noqa: E402
+from simulator.well import WellManager  # noqa: E402
+from simulator.simulation import Simulator  # noqa: E402
+import solver.pressure_amg as pamg  # noqa: E402
+from solver.classical_amg import ClassicalAMG  # noqa: E402
+
+from impes_b200 import scenarios  # noqa: E402  (input generator only)
+from oracle.amg import tiebreak  # noqa: E402  (the shared tie-break definition)
+
+
+def _eval_pvt64(self, p_tensor, key):
+    p_mpa = (p_tensor.detach().to("cpu").numpy() / 1e6).astype(np.float64)
+    vals = self.pvt.eval(p_mpa)[key]
+    return torch.from_numpy(vals).to(self.device, dtype=torch.float64).reshape(self.dimensions)
+
+
+Fluid._eval_pvt = _eval_pvt64
+
+
+def build_reference(cfg, fields, tmpdir):
+    cfg = json.loads(json.dumps(cfg))
+    fc = cfg["fluid"]
+    if isinstance(fc.get("pvt"), dict) and "table" in fc["pvt"]:
+        path = os.path.join(tmpdir, "pvt.json")
+        with open(path, "w") as f:
+            json.dump(fc["pvt"]["table"], f)
+        fc.pop("pvt")
+        fc["pvt_path"] = path
+    sim_cfg = dict(cfg["simulation"])
+    sim_cfg["pressure_solver"] = "amg"
+    dev = torch.device("cpu")
+    with contextlib.redirect_stdout(io.StringIO()):
+        res = Reservoir(cfg["reservoir"], dev)
+        res.permeability_x = torch.from_numpy(np.ascontiguousarray(fields["kx"]))
+        res.permeability_y = torch.from_numpy(np.ascontiguousarray(fields["ky"]))
+        res.permeability_z = torch.from_numpy(np.ascontiguousarray(fields["kz"]))
+        res.porosity = torch.from_numpy(np.ascontiguousarray(fields["poro"]))
+        res.porous_volume = res.cell_volume * res.porosity
+        wm = WellManager(cfg["wells"], res)
+        fl = Fluid(fc, res, dev)
+        sim = Simulator(res, fl, wm, sim_cfg, dev)
+    return sim, fl, wm
+
+
+def run_trajectory(name, cfg, fields, steps, dt_days):
+    rec = {"A": [], "b": []}
+
+    def direct(A, b, **kw):
+        A = A.coalesce().to_sparse_csr() if A.layout == torch.sparse_coo else A
+        crow, col, val = A.crow_indices().numpy(), A.col_indices().numpy(), A.values().numpy()
+        rec["A"].append((crow.copy(), col.copy(), val.copy()))
+        rec["b"].append(b.numpy().copy())
+        M = sp.csr_matrix((val, col, crow), shape=A.shape)
+        return torch.from_numpy(spla.spsolve(M.tocsc(), b.numpy()))
+
+    pamg.amg_solve = direct
+    out = {}
+    with tempfile.TemporaryDirectory() as td:
+        sim, fl, wm = build_reference(cfg, fields, td)
+        ps, sws, sgs, mbs = [], [], [], []
+        for _ in range(steps):
+            with contextlib.redirect_stdout(io.StringIO()):
+                ok = sim.run_step(dt_days * 86400.0)
+            assert ok
+            ps.append(fl.pressure.numpy().ravel().copy())
+            sws.append(fl.s_w.numpy().ravel().copy())
+            sgs.append(fl.s_g.numpy().ravel().copy())
+            mb = sim.mass_balance
+            cb = sim.component_balance
+            mbs.append([mb[ph][io_] for ph in ("water", "oil", "gas") for io_ in ("in", "out")]
+                       + [cb[c][k] for c in ("oil", "gas") for k in ("in", "out", "accum")])
+        wells = [(w.cell_index_flat, w.last_q_total if w.last_q_total is not None else np.nan)
+                 for w in wm.get_wells()]
+    crow, col, val = rec["A"][0]
+    out.update(
+        cfg=json.dumps(cfg), kx=fields["kx"], ky=fields["ky"], kz=fields["kz"], poro=fields["poro"],
+        dt=dt_days * 86400.0,
+        A0_crow=crow.astype(np.int32), A0_col=col.astype(np.int32), A0_val=val,
+        b0=rec["b"][0], b_all=np.stack(rec["b"]),
+        A_val_all=np.stack([a[2] for a in rec["A"]]),
+        p=np.stack(ps), sw=np.stack(sws), sg=np.stack(sgs), balances=np.array(mbs),
+        well_cells=np.array([w[0] for w in wells], dtype=np.int64),
+        well_last_q=np.array([w[1] for w in wells]),
+    )
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+    print(name, "N", fields["kx"].size, "steps", steps, "p range", ps[-1].min(), ps[-1].max(),
+          "sw max", sws[-1].max(), "sg max", sgs[-1].max())
+    return out
+
+
+def amg_fixture(name, traj, seed=7, coarsest=50):
+    """Reference ClassicalAMG on a recorded pressure matrix, with a fixed tie-break."""
+    crow, col = traj["A0_crow"].astype(np.int64), traj["A0_col"].astype(np.int64)
+    A = torch.sparse_csr_tensor(torch.from_numpy(crow), torch.from_numpy(col),
+                                torch.from_numpy(traj["A0_val"]), size=(len(crow) - 1,) * 2)
+    calls = {"n": 0}
+    real_rand = torch.rand
+
+    def fake_rand(n, *a, **kw):
+        v = torch.from_numpy(tiebreak(seed, calls["n"], int(n)))
+        calls["n"] += 1
+        return v
+
+    torch.rand = fake_rand
+    try:
+        with contextlib.redirect_stdout(io.StringIO()):
+            amg = ClassicalAMG(A, theta=0.25, max_levels=10, coarsest_size=coarsest)
+    finally:
+        torch.rand = real_rand
+    b = torch.from_numpy(traj["b0"])
+    out = {"seed": seed, "coarsest": coarsest, "n_levels": len(amg.levels),
+           "Dhalf_inv": amg.Dhalf_inv.numpy() if amg.Dhalf_inv is not None else np.zeros(0)}
+    for l, lv in enumerate(amg.levels):
+        Al = lv["A"]
+        out[f"L{l}_A_crow"] = Al.crow_indices().numpy().astype(np.int32)
+        out[f"L{l}_A_col"] = Al.col_indices().numpy().astype(np.int32)
+        out[f"L{l}_A_val"] = Al.values().numpy()
+        out[f"L{l}_inv_relax"] = lv["inv_relax"].numpy()
+        if lv["P"] is not None:
+            P = lv["P"]
+            out[f"L{l}_P_crow"] = P.crow_indices().numpy().astype(np.int32)
+            out[f"L{l}_P_col"] = P.col_indices().numpy().astype(np.int32)
+            out[f"L{l}_P_val"] = P.values().numpy()
+            out[f"L{l}_P_shape"] = np.array(P.shape)
+    with contextlib.redirect_stdout(io.StringIO()):
+        bs = amg.Dhalf_inv * b if amg.Dhalf_inv is not None else b
+        out["vcycle1"] = amg._v_cycle(0, torch.zeros_like(bs), bs).numpy()
+        out["solve_x"] = amg.solve(b, tol=1e-30, max_iter=4).numpy()
+        out["apply_x"] = amg.apply(b, cycles=2).numpy()
+        # update with the next step's values (frozen hierarchy, new Galerkin products)
+        A2 = torch.sparse_csr_tensor(torch.from_numpy(crow), torch.from_numpy(col),
+                                     torch.from_numpy(traj["A_val_all"][1]), size=A.shape)
+        amg.update_matrix(A2)
+        for l, lv in enumerate(amg.levels):
+            out[f"U{l}_A_val"] = lv["A"].values().numpy()
+            out[f"U{l}_A_crow"] = lv["A"].crow_indices().numpy().astype(np.int32)
+            out[f"U{l}_A_col"] = lv["A"].col_indices().numpy().astype(np.int32)
+            out[f"U{l}_inv_relax"] = lv["inv_relax"].numpy()
+        b2 = torch.from_numpy(traj["b_all"][1])
+        out["update_solve_x"] = amg.solve(b2, tol=1e-30, max_iter=3).numpy()
+    out["b"] = traj["b0"]
+    out["b2"] = traj["b_all"][1]
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+    print(name, "levels", [lv["n"] for lv in amg.levels])
+
+
+def main():
+    # two-phase 2-D, config-0 physics on a 32x32 grid (small enough for a fixture)
+    cfg, f = scenarios.two_phase_2d(seed=0, nx=32, ny=32, nz=1, steps=4)
+    t0 = run_trajectory("two_phase_32x32", cfg, f, steps=4, dt_days=1.0)
+    amg_fixture("amg_two_phase_32x32", t0)
+    # the 64x64x1 configuration itself, first two steps
+    cfg, f = scenarios.two_phase_2d(seed=0, steps=2)
+    run_trajectory("two_phase_64x64", cfg, f, steps=2, dt_days=1.0)
+    # the adjoint sub-case grid: 16x16x2, sigma 0.7, dt 2 d (gravity active)
+    cfg, f = scenarios.adjoint_case(seed=3, nx=16, ny=16, nz=2, steps=10)
+    run_trajectory("two_phase_16x16x2", cfg, f, steps=10, dt_days=2.0)
+    # black oil 5-spot physics (PVT, Stone II, gravity, capillarity) on 10x10x4
+    cfg, f = scenarios.black_oil_5spot(seed=1, nx=10, ny=10, nz=4, steps=5, inj_rate=20.0)
+    run_trajectory("black_oil_10x10x4", cfg, f, steps=5, dt_days=5.0)
+    # gas-injection physics (surface-rate gas injectors, BHP producers) on 12x12x3
+    # (the 2e5 sm3/d stress rate makes the reference's own saturation update diverge
+    # on small grids, so the trajectory fixture uses a rate its explicit update can carry)
+    cfg, f = scenarios.gas_injection_1m(seed=2, nx=12, ny=12, nz=3, steps=4, gas_rate=1.0e2,
+                                        n_inj_side=1, n_prod_side=2)
+    cfg["fluid"]["capillary_pressure_og"] = {"pc_scale": 2.0e4, "pc_exponent": 1.5}
+    cfg["wells"].append({"name": "PS", "type": "producer", "i": 6, "j": 2, "k": 0, "radius": 0.1,
+                         "control_type": "rate", "control_value": 5.0, "rate_type": "surface",
+                         "surface_phase": "oil", "limits": {"wopr": 3.0}})
+    run_trajectory("gas_injection_12x12x3", cfg, f, steps=4, dt_days=2.0)
+
+
+if __name__ == "__main__":
+    main()
