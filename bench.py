@@ -1,0 +1,368 @@
+#!/usr/bin/env python
+"""IMPES cell-steps/s on the B200 (mixed vs FP64 AMG-FGMRES at a 1e-6 residual).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: the 200x200x25 (1e6-cell) three-phase gas-injection case -- seeded
+correlated log-normal permeability, 20-row black-oil PVT table, Stone II,
+gravity, capillarity, 9 surface-rate gas injectors at 2e5 sm3/d and 16 BHP
+producers at 15 MPa, dt = 2 days.  A step is one full IMPES step (assembly,
+Galerkin update of the frozen AMG hierarchy, FGMRES pressure solve to a 1e-6
+Jacobi-scaled relative residual, explicit saturation update) with the state
+resident in HBM; L2 is flushed (512 MiB write) before every timed step.
+
+``value`` is the mixed-precision path (fp32 V-cycle in fp64 FGMRES); the same
+protocol is applied to the all-fp64 path and reported under ``fp64``.  ``e2e``
+repeats the measurement through the public ``Simulator.run_step`` with the state
+copied from and back to pinned host memory inside the timed region.
+
+Single grids do not shard: with N > 1 every rank runs its own replica (weak
+scaling), timed on the device and reduced with max over ranks.
+
+``--impl reference`` times the CPU restatement of the reference's own step (its
+stand-alone V-cycle AMG with tol 1e-6 and 40 cycles) on the host cores, on a
+bounded spatial sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+for _p in (os.path.join(REPO, "oil-simulator-py_b200"), REPO):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "IMPES cell-steps/s, mixed vs FP64 AMG at 1e-6 residual; adjoint/forward time"
+WORKLOAD = ("gas_injection_1m: 200x200x25 = 1,000,000 cells, ln k ~ N(ln 150 mD, 1.0^2) "
+            "Gaussian-correlated (radius 5), 20-row black-oil PVT, Stone II, gravity, capillarity, "
+            "9 surface-rate gas injectors (2e5 sm3/d), 16 BHP producers (15 MPa), dt 2 d")
+PRESSURE_TOL = 1e-6
+L2_FLUSH_BYTES = 512 << 20
+CPU_SAMPLE = (100, 100, 25)     # spatial sample of the workload for the CPU legs
+
+
+def read_peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+# ------------------------------------------------------------------ CPU legs
+def cpu_sample_workload(seed=2):
+    from impes_b200 import scenarios
+    nx, ny, nz = CPU_SAMPLE
+    return scenarios.gas_injection_1m(seed=seed, nx=nx, ny=ny, nz=nz)
+
+
+def run_cpu_reference(steps: int, warmup: int):
+    """The oracle's restatement of the reference step on the host cores.
+    Returns (cell-steps/s, seconds timed, cells, threads, description)."""
+    from oracle.amg import AMGSolver
+    from oracle.impes import Model
+    cfg, f = cpu_sample_workload()
+    m = Model(cfg, f["kx"], f["ky"], f["kz"], f["poro"], pvt_table=f["pvt"])
+    solver = AMGSolver(tol=1e-6, max_cycles=40, theta=0.25, max_levels=10, coarsest_size=200, seed=0)
+    dt = 2 * 86400.0
+    for _ in range(max(warmup, 1)):       # the first step builds the hierarchy
+        m.step(dt, solve=solver)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        m.step(dt, solve=solver)
+    secs = time.perf_counter() - t0
+    cells = m.N
+    desc = (f"oracle restatement of the reference IMPES step (stand-alone RS-AMG V-cycles, tol 1e-6 "
+            f"equilibrated, max 40 cycles) on a {CPU_SAMPLE[0]}x{CPU_SAMPLE[1]}x{CPU_SAMPLE[2]} sample "
+            f"of the workload, {steps} timed steps after {max(warmup, 1)} warm-up (setup excluded); "
+            f"numpy/scipy, single-threaded sparse kernels")
+    return cells * steps / secs, secs, cells, 1, desc
+
+
+# ------------------------------------------------------------------ GPU legs
+class ClockSampler:
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(REPO, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+
+    def __enter__(self):
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 7:
+                    continue
+                try:
+                    sm.append(float(parts[0]))
+                    mx = float(parts[1])
+                except ValueError:
+                    continue
+                for nm, v in zip(names, parts[3:7]):
+                    if v.lower() == "active":
+                        reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def make_sim(cfg, fields, precision, device):
+    from impes_b200.simulator import build_from_config
+    c = json.loads(json.dumps(cfg))
+    c["simulation"]["pressure_solver"] = "gmres_amg"
+    c["simulation"]["amg"].update({"tol": PRESSURE_TOL, "norm": "jacobi", "precision": precision,
+                                   "restart": 30, "max_iters": 400, "seed": 0})
+    return build_from_config(c, fields, device=device)
+
+
+def time_steps(sim, steps, dt, flush, stream):
+    """Device time of `steps` IMPES steps (L2 flushed before each, outside the events)."""
+    import torch
+    total = 0.0
+    iters = []
+    for _ in range(steps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        ok = sim.run_step(dt)
+        b.record(stream)
+        b.synchronize()
+        if not ok:
+            raise RuntimeError("IMPES step failed to converge")
+        total += a.elapsed_time(b)
+        iters.append(sim.last_krylov["iterations"])
+    return total, iters
+
+
+def time_e2e(sim, fl, steps, dt, flush, stream):
+    """Public API with host state: H2D of (p, Sw, Sg), run_step, D2H of (p, Sw, Sg)."""
+    import torch
+    host = [t.detach().cpu().pin_memory() for t in (fl.pressure, fl.s_w, fl.s_g)]
+    total = 0.0
+    for _ in range(steps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fl.pressure.copy_(host[0], non_blocking=True)
+        fl.s_w.copy_(host[1], non_blocking=True)
+        fl.s_g.copy_(host[2], non_blocking=True)
+        if not sim.run_step(dt):
+            raise RuntimeError("IMPES step failed to converge")
+        host[0].copy_(fl.pressure, non_blocking=True)
+        host[1].copy_(fl.s_w, non_blocking=True)
+        host[2].copy_(fl.s_g, non_blocking=True)
+        b.record(stream)
+        b.synchronize()
+        total += a.elapsed_time(b)
+    nbytes = sum(h.numel() * h.element_size() for h in host)
+    return total, nbytes
+
+
+def read_traffic(kernel: str):
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, if any."""
+    path = os.path.join(REPO, "profiles", f"{kernel}_gas_injection_1m.md")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1].strip())
+    except OSError:
+        pass
+    return None
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    from impes_b200 import _lib, scenarios
+
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=device)
+    cfg, fields = scenarios.gas_injection_1m(seed=2)
+    dt = cfg["simulation"]["time_step_days"] * 86400.0
+    cells = cfg["reservoir"]["dimensions"][0] * cfg["reservoir"]["dimensions"][1] * cfg["reservoir"]["dimensions"][2]
+    stream = torch.cuda.current_stream(device)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=device)
+
+    results = {}
+    for precision in ("fp64", "mixed"):
+        _, fl, _, sim = make_sim(cfg, fields, precision, device)
+        torch.cuda.synchronize()
+        t_setup = time.perf_counter()
+        for _ in range(args.warmup):           # the first warm-up step builds the hierarchy
+            if not sim.run_step(dt):
+                raise RuntimeError("warm-up step failed to converge")
+        torch.cuda.synchronize()
+        setup_s = time.perf_counter() - t_setup
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        launches0 = _lib.kernel_launches()
+        _lib.timing_enable(True)
+        _lib.timing_collect()
+        with ClockSampler(local) as clk:
+            ms, iters = time_steps(sim, args.steps, dt, flush, stream)
+        phases = _lib.timing_collect()
+        _lib.timing_enable(False)
+        launches = _lib.kernel_launches() - launches0
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        tmax = torch.tensor([ms], dtype=torch.float64, device=device)
+        if dist is not None:
+            dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        ms_max = float(tmax.item())
+        e2e_ms, e2e_bytes = time_e2e(sim, fl, args.steps, dt, flush, stream)
+        te = torch.tensor([e2e_ms], dtype=torch.float64, device=device)
+        if dist is not None:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        results[precision] = dict(ms=ms_max, iters=iters, phases=phases, clocks=clk.summary(),
+                                  launches=launches, e2e_ms=float(te.item()), e2e_bytes=e2e_bytes,
+                                  setup_s=setup_s, p=fl.pressure.clone(), sw=fl.s_w.clone())
+        sim.close()
+        del sim, fl
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    hbm_peak, peak_kind = read_peaks()
+    mixed, fp64 = results["mixed"], results["fp64"]
+    steps = args.steps
+    value = world * cells * steps / (mixed["ms"] / 1e3)
+    fp64_value = world * cells * steps / (fp64["ms"] / 1e3)
+    # dominant kernel: the level-0 l1-Jacobi sweep of the mixed path
+    n_s, ms_s, by_s = mixed["phases"]["smooth_l0"]
+    avg_ms = ms_s / max(n_s, 1)
+    bytes_launch = by_s / max(n_s, 1)
+    achieved = bytes_launch / (avg_ms / 1e3) / 1e9
+    traffic = read_traffic("smooth_l0")
+    share = {k: round(v[1] / mixed["ms"], 4) for k, v in mixed["phases"].items() if k != "solve"}
+    drift_sw = float((results["mixed"]["sw"] - results["fp64"]["sw"]).abs().max())
+    drift_p = float(((results["mixed"]["p"] - results["fp64"]["p"]).abs().max()
+                     / results["fp64"]["p"].abs().max()))
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "cell-steps/s",
+        "n_gpus": world,
+        "steps": steps,
+        "warmup": args.warmup,
+        "ms_per_step": mixed["ms"] / steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64 Krylov/assembly/saturation + f32 V-cycle",
+        "data": "synthetic (seeded; no dataset)",
+        "config": {"workload": WORKLOAD, "cells": cells, "precision": "mixed",
+                   "pressure_solver": "FGMRES(30) + RS-AMG V-cycle", "pressure_tol": PRESSURE_TOL,
+                   "residual_norm": "||D^-1 r|| / ||D^-1 b|| (Jacobi-scaled)",
+                   "l2": "flushed before every timed step (512 MiB write)",
+                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "vcycles_per_step": statistics.mean(mixed["iters"]),
+        "fp64": {"value": fp64_value, "ms_per_step": fp64["ms"] / steps,
+                 "vcycles_per_step": statistics.mean(fp64["iters"]),
+                 "mixed_speedup": fp64["ms"] / mixed["ms"]},
+        "mixed_vs_fp64_drift": {"sw_abs_max": drift_sw, "p_rel_max": drift_p},
+        "setup_s": {"mixed": mixed["setup_s"], "fp64": fp64["setup_s"]},
+        "phase_share": share,
+        "e2e": {"value": world * cells * steps / (mixed["e2e_ms"] / 1e3), "unit": "cell-steps/s",
+                "h2d_bytes_per_step": mixed["e2e_bytes"], "d2h_bytes_per_step": mixed["e2e_bytes"]},
+        "roofline": {"kernel": "k_csr<float,1,Y_SMOOTH> (level-0 l1-Jacobi sweep)", "bound": "hbm",
+                     "achieved": achieved, "peak": hbm_peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": achieved / hbm_peak, "traffic": traffic,
+                     "bytes_per_launch": bytes_launch, "avg_launch_us": avg_ms * 1e3,
+                     "launches_timed": n_s},
+        "clocks": mixed["clocks"],
+        "gpu_launches": mixed["launches"],
+    }
+    if not args.no_cpu_baseline and world == 1:
+        v, secs, ccells, cores, desc = run_cpu_reference(steps=1, warmup=1)
+        line["cpu_baseline"] = {"value": v, "unit": "cell-steps/s", "cores": cores, "kind": "port",
+                                "sample": desc, "seconds": secs}
+    print(json.dumps(line), flush=True)
+
+
+def run_reference(args, world, rank, local):
+    if rank != 0:
+        return
+    v, secs, cells, cores, desc = run_cpu_reference(steps=args.steps, warmup=args.warmup)
+    line = {
+        "metric": METRIC, "impl": "reference", "value": v, "unit": "cell-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded; no dataset)",
+        "config": {"workload": WORKLOAD, "cells": cells, "sample": list(CPU_SAMPLE),
+                   "pressure_solver": "stand-alone RS-AMG V-cycles (reference semantics)",
+                   "pressure_tol": PRESSURE_TOL, "residual_norm": "||D^-1/2 r|| / ||D^-1/2 b||"},
+        "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": cores, "kind": "port", "sample": desc},
+        "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    world, rank, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, world, rank, local)
+    else:
+        run_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -246,6 +246,32 @@ int impes_model_balances(impes_model* m, impes_sat_stats* stats, void* stream);
 int impes_model_reset_balances(impes_model* m, void* stream);
 int impes_well_states(impes_model* m, impes_well_state* out_host, void* stream);
 
+/* ======================================================== instrumentation ===
+ * CUDA-event timers around the phases of the step (no reference counterpart:
+ * the reference prints perf_counter timings, classical_amg.py:799-875).  Events
+ * are recorded on the stream of the timed call; collecting synchronises.
+ * Not thread-safe: one timing session per process. */
+enum {
+  IMPES_PH_ASSEMBLE = 0,   /* K1 pressure assembly                        */
+  IMPES_PH_SATURATION = 1, /* K4 saturation update (wells + flux + substeps) */
+  IMPES_PH_GALERKIN = 2,   /* update_matrix: equilibration + P^T A P, all levels */
+  IMPES_PH_VCYCLE = 3,     /* one V-cycle from level 0                    */
+  IMPES_PH_SMOOTH_L0 = 4,  /* one l1-Jacobi sweep on level 0              */
+  IMPES_PH_SPMV_L0 = 5,    /* FGMRES operator product on level 0          */
+  IMPES_PH_ORTHO = 6,      /* FGMRES Gram-Schmidt of one iteration        */
+  IMPES_PH_SOLVE = 7,      /* whole pressure solve                        */
+  IMPES_NUM_PHASES = 8
+};
+typedef struct {
+  long long count[8];   /* timed launches per phase                     */
+  double ms[8];         /* summed device time per phase                 */
+  double bytes[8];      /* summed algorithmic bytes per phase           */
+} impes_timing;
+int impes_timing_enable(int on);
+int impes_timing_collect(impes_timing* out);
+/* Kernel launches issued by the library since load. */
+unsigned long long impes_kernel_launches(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -260,6 +260,7 @@ int impes_model_create(impes_model** out, const impes_model_desc* d, const impes
       model_build_static(m, kx, ky, kz, poro, s);
       m.csr_val.alloc(m.nnz);
       m.rhs.alloc(P.N);
+      m.p_save.alloc(P.N);
       IMPES_CUDA(cudaStreamSynchronize(s));
     } catch (...) {
       delete h;
@@ -355,19 +356,35 @@ int impes_step(impes_model* h, impes_amg* amg, double* p, double* sw, double* sg
     else
       amg_update(a, m.csr_val.p, s);
     impes_krylov_stats st{};
-    if (solver == 0) {
-      int cyc = 0;
-      double rel = 0.0;
-      amg_solve_vcycles(a, m.rhs.p, p, kp->tol, std::max(1, max_cycles), &cyc, &rel, s);
-      st.iterations = cyc;
-      st.rel_res = rel;
-      st.true_rel_res = rel;
-      st.converged = rel < kp->tol;
-    } else {
-      impes_krylov_params k = *kp;
-      amg_fgmres(a, m.rhs.p, p, k, st, s);
+    // a failed pressure solve leaves the state as it was (the caller may retry
+    // with a smaller dt, as _impes_step does at simulation.py:833-862)
+    IMPES_CUDA(cudaMemcpyAsync(m.p_save.p, p, sizeof(double) * m.P.N, cudaMemcpyDeviceToDevice, s));
+    auto restore = [&] {
+      cudaMemcpyAsync(p, m.p_save.p, sizeof(double) * m.P.N, cudaMemcpyDeviceToDevice, s);
+      cudaStreamSynchronize(s);
+    };
+    try {
+      if (solver == 0) {
+        int cyc = 0;
+        double rel = 0.0;
+        amg_solve_vcycles(a, m.rhs.p, p, kp->tol, std::max(1, max_cycles), &cyc, &rel, s);
+        st.iterations = cyc;
+        st.rel_res = rel;
+        st.true_rel_res = rel;
+        st.converged = rel < kp->tol;
+      } else {
+        impes_krylov_params k = *kp;
+        amg_fgmres(a, m.rhs.p, p, k, st, s);
+      }
+    } catch (...) {
+      restore();
+      throw;
     }
     if (kstats) *kstats = st;
+    if (solver != 0 && !st.converged) {
+      restore();
+      throw Error(IMPES_ERR_NOT_CONVERGED, "FGMRES did not reach the pressure tolerance");
+    }
     model_saturation(m, p, sw, sg, so, dt, s);
     if (sstats) {
       double hb[12];
@@ -423,5 +440,33 @@ int impes_well_states(impes_model* h, impes_well_state* out, void* stream) {
     }
   });
 }
+
+int impes_timing_enable(int on) {
+  return guarded([&] { timers().on = on != 0; });
+}
+
+int impes_timing_collect(impes_timing* out) {
+  return guarded([&] {
+    IMPES_REQUIRE(out, IMPES_ERR_ARG, "null argument");
+    impes_timing t{};
+    PhaseTimers& T = timers();
+    for (auto& r : T.recs) {
+      IMPES_CUDA(cudaEventSynchronize(r.b));
+      float ms = 0.f;
+      IMPES_CUDA(cudaEventElapsedTime(&ms, r.a, r.b));
+      if (r.phase >= 0 && r.phase < IMPES_NUM_PHASES) {
+        t.count[r.phase] += 1;
+        t.ms[r.phase] += ms;
+        t.bytes[r.phase] += r.bytes;
+      }
+      T.pool.push_back(r.a);
+      T.pool.push_back(r.b);
+    }
+    T.recs.clear();
+    *out = t;
+  });
+}
+
+unsigned long long impes_kernel_launches(void) { return launches(); }
 
 }  // extern "C"

@@ -31,8 +31,10 @@ struct Level {
   // cycle vectors (fp64 and fp32)
   DBuf<double> x, b, r, t;
   DBuf<float> xf, bf, rf, tf;
-  // coarsest level: dense pinned LU (n <= 500), row-major, with pivots
-  DBuf<double> lu;
+  // coarsest level (n <= 500): inverse of the dense matrix with DOF 0 pinned
+  // (the reference's coarse solve), row-major; when the coarsest level is also
+  // level 0, lu_free holds the unpinned inverse used as FGMRES preconditioner
+  DBuf<double> lu, lu_free;
   DBuf<int> piv;
 };
 
@@ -52,7 +54,7 @@ struct AMG {
   // FGMRES workspace
   int krylov_m = 0;
   DBuf<double> V, Z, H, cs, sn, g, y, kw, kb, kx;
-  int coarse_singular = 0;
+  bool krylov_mode = false;        // V-cycles issued by FGMRES
 };
 
 // amg_setup.cu

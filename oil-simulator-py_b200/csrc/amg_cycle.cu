@@ -59,11 +59,11 @@ void launch_csr(int n, int avg, const int* rowptr, const int* col, const T* val,
   if (MODE == Y_SMOOTH0) lpr = 1;
   auto grid = [&](int l) { return grid_for(((size_t)n * l + TB - 1) / TB * TB, TB, 16); };
   switch (lpr) {
-    case 1: k_csr<T, 1, MODE><<<grid(1), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y); break;
-    case 4: k_csr<T, 4, MODE><<<grid(4), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y); break;
-    case 8: k_csr<T, 8, MODE><<<grid(8), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y); break;
-    case 16: k_csr<T, 16, MODE><<<grid(16), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y); break;
-    default: k_csr<T, 32, MODE><<<grid(32), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y); break;
+    case 1: k_csr<T, 1, MODE><<<grid(1), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y); ::impes::count_launch(); break;
+    case 4: k_csr<T, 4, MODE><<<grid(4), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y); ::impes::count_launch(); break;
+    case 8: k_csr<T, 8, MODE><<<grid(8), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y); ::impes::count_launch(); break;
+    case 16: k_csr<T, 16, MODE><<<grid(16), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y); ::impes::count_launch(); break;
+    default: k_csr<T, 32, MODE><<<grid(32), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y); ::impes::count_launch(); break;
   }
   IMPES_CHECK_LAUNCH();
 }
@@ -161,14 +161,15 @@ __global__ void k_scale_by_inv_sqrt(long long n, const double* in, double* out, 
 __global__ void k_dense_pinned(int n, const int* rowptr, const int* col, const double* val, double* M) {
   GRID_LOOP(t, (long long)n * n) M[t] = 0.0;
 }
-__global__ void k_dense_fill(int n, const int* rowptr, const int* col, const double* val, double* M) {
+__global__ void k_dense_fill(int n, const int* rowptr, const int* col, const double* val, double* M,
+                             int pin) {
   GRID_LOOP(i, n) {
     for (int e = rowptr[i]; e < rowptr[i + 1]; ++e) {
       int j = col[e];
-      if (i == 0 || j == 0) continue;
+      if (pin && (i == 0 || j == 0)) continue;
       M[(long long)i * n + j] = val[e];
     }
-    if (i == 0) M[0] = 1.0;
+    if (pin && i == 0) M[0] = 1.0;
   }
 }
 // In-place Gauss-Jordan inversion with partial pivoting, one block.
@@ -248,12 +249,12 @@ __global__ void __launch_bounds__(kGJ) k_gauss_jordan(int n, double* M, int* per
     __syncthreads();
   }
 }
-// x = Ainv * b with b[0] pinned to 0; one warp per row group
+// x = Ainv * b (b[0] pinned to 0 when pin); one warp per row group
 template <typename T>
 __global__ void k_coarse_apply(int n, const double* __restrict__ Ainv, const T* __restrict__ b,
-                               T* __restrict__ x) {
+                               T* __restrict__ x, int pin) {
   extern __shared__ double s_b[];
-  for (int i = threadIdx.x; i < n; i += blockDim.x) s_b[i] = (i == 0) ? 0.0 : (double)b[i];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s_b[i] = (pin && i == 0) ? 0.0 : (double)b[i];
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   for (int i = blockIdx.x * nw + warp; i < n; i += gridDim.x * nw) {
@@ -274,11 +275,27 @@ void coarse_factor(AMG& h, Level& L, cudaStream_t s) {
   const int n = L.n;
   L.lu.ensure((size_t)n * n);
   L.piv.ensure(n);
-  k_dense_pinned<<<grid_for((size_t)n * n, TB), TB, 0, s>>>(n, L.rowptr.p, L.col.p, L.val.p, L.lu.p);
-  k_dense_fill<<<grid_for(n, TB), TB, 0, s>>>(n, L.rowptr.p, L.col.p, L.val.p, L.lu.p);
-  IMPES_CUDA(cudaMemsetAsync(h.iflag.p + 2, 0, sizeof(int), s));
-  k_gauss_jordan<<<1, kGJ, 2 * n * sizeof(double), s>>>(n, L.lu.p, L.piv.p, h.iflag.p + 2);
+  k_dense_pinned<<<grid_for((size_t)n * n, TB), TB, 0, s>>>(n, L.rowptr.p, L.col.p, L.val.p, L.lu.p); ::impes::count_launch();
   IMPES_CHECK_LAUNCH();
+  k_dense_fill<<<grid_for(n, TB), TB, 0, s>>>(n, L.rowptr.p, L.col.p, L.val.p, L.lu.p, 1); ::impes::count_launch();
+  IMPES_CHECK_LAUNCH();
+  IMPES_CUDA(cudaMemsetAsync(h.iflag.p + 2, 0, sizeof(int), s));
+  k_gauss_jordan<<<1, kGJ, 2 * n * sizeof(double), s>>>(n, L.lu.p, L.piv.p, h.iflag.p + 2); ::impes::count_launch();
+  IMPES_CHECK_LAUNCH();
+  if (&L == h.levels[0].get()) {
+    // single-level hierarchy: the pinned solve would freeze x[0] inside FGMRES
+    L.lu_free.ensure((size_t)n * n);
+    k_dense_pinned<<<grid_for((size_t)n * n, TB), TB, 0, s>>>(n, L.rowptr.p, L.col.p, L.val.p, L.lu_free.p); ::impes::count_launch();
+    IMPES_CHECK_LAUNCH();
+    k_dense_fill<<<grid_for(n, TB), TB, 0, s>>>(n, L.rowptr.p, L.col.p, L.val.p, L.lu_free.p, 0); ::impes::count_launch();
+    IMPES_CHECK_LAUNCH();
+    IMPES_CUDA(cudaMemsetAsync(h.iflag.p + 3, 0, sizeof(int), s));
+    k_gauss_jordan<<<1, kGJ, 2 * n * sizeof(double), s>>>(n, L.lu_free.p, L.piv.p, h.iflag.p + 3); ::impes::count_launch();
+    IMPES_CHECK_LAUNCH();
+    IMPES_CUDA(cudaMemcpyAsync(h.hint.p + 3, h.iflag.p + 3, sizeof(int), cudaMemcpyDeviceToHost, s));
+    IMPES_CUDA(cudaStreamSynchronize(s));
+    if (h.hint.p[3]) L.lu_free.release();  // singular without the pin: keep the pinned solve
+  }
 }
 
 void spmv(const Level& L, const double* x, double* y, cudaStream_t s) {
@@ -287,8 +304,8 @@ void spmv(const Level& L, const double* x, double* y, cudaStream_t s) {
 
 double dot_host(AMG& h, const double* a, const double* b, int n, cudaStream_t s) {
   h.red.ensure((size_t)kMD * kDotBlocks);
-  k_multidot<<<kDotBlocks, TB, 0, s>>>(n, a, 0, 1, b, h.red.p);
-  k_dot_finalize<<<1, 32, 0, s>>>(1, h.red.p, h.scal.p, 0);
+  k_multidot<<<kDotBlocks, TB, 0, s>>>(n, a, 0, 1, b, h.red.p); ::impes::count_launch();
+  k_dot_finalize<<<1, 32, 0, s>>>(1, h.red.p, h.scal.p, 0); ::impes::count_launch();
   IMPES_CHECK_LAUNCH();
   IMPES_CUDA(cudaMemcpyAsync(h.hbuf.p, h.scal.p, sizeof(double), cudaMemcpyDeviceToHost, s));
   IMPES_CUDA(cudaStreamSynchronize(s));
@@ -319,20 +336,47 @@ template <> struct LV<float> {
   static float* t(Level& L) { return L.tf.p; }
 };
 
-// nu l1-Jacobi sweeps (classical_amg.py:1016-1035); returns the buffer holding x
+// Algorithmic bytes of CSR products (value size sv, vector size sx).
+inline double spmv_bytes(double sv, double sx, double nnz, double rows, double cols) {
+  return (sv + 4.0) * nnz + 4.0 * (rows + 1) + sx * cols + sx * rows;
+}
+inline double sweep_bytes(double s, double nnz, double n) { return (s + 4.0) * nnz + 4.0 * n + 4.0 * s * n; }
+
+// nu l1-Jacobi sweeps (classical_amg.py:1016-1035); returns the buffer holding x.
+// Level-0 sweeps with a non-zero iterate are timed as IMPES_PH_SMOOTH_L0.
 template <typename T>
-T* smooth(Level& L, T* x, T* spare, const T* b, int nu, bool zero_x, cudaStream_t s) {
+T* smooth(Level& L, T* x, T* spare, const T* b, int nu, bool zero_x, cudaStream_t s, bool top = false) {
   for (int it = 0; it < nu; ++it) {
     if (zero_x && it == 0) {
       launch_csr<T, Y_SMOOTH0>(L.n, L.avg_row, L.rowptr.p, L.col.p, LV<T>::val(L), nullptr, b,
                                LV<T>::inv(L), x, s);
       continue;
     }
+    const int tid = top ? timers().begin(IMPES_PH_SMOOTH_L0, s) : -1;
     launch_csr<T, Y_SMOOTH>(L.n, L.avg_row, L.rowptr.p, L.col.p, LV<T>::val(L), x, b,
                             LV<T>::inv(L), spare, s);
+    timers().end(tid, s, sweep_bytes(sizeof(T), L.nnz, L.n));
     std::swap(x, spare);
   }
   return x;
+}
+
+// Algorithmic bytes of one V-cycle from level l down (5 sweeps, residual,
+// restriction, prolongation, vector updates; dense coarsest apply).
+template <typename T>
+double vcycle_bytes(const AMG& h, int l) {
+  const double sz = sizeof(T);
+  double tot = 0.0;
+  for (size_t q = l; q < h.levels.size(); ++q) {
+    const Level& L = *h.levels[q];
+    if (L.coarsest) {
+      tot += L.n <= 500 ? 8.0 * L.n * (double)L.n + 2.0 * sz * L.n : 50.0 * sweep_bytes(sz, L.nnz, L.n);
+      break;
+    }
+    tot += 5.0 * sweep_bytes(sz, L.nnz, L.n) + spmv_bytes(sz, sz, L.nnz, L.n, L.n) +
+           spmv_bytes(sz, sz, L.pnnz, L.nc, L.n) + spmv_bytes(sz, sz, L.pnnz, L.n, L.nc) + 2.0 * sz * L.n;
+  }
+  return tot;
 }
 
 // _v_cycle (classical_amg.py:1037-1106) on level l: input b in LV<T>::b(L),
@@ -343,17 +387,19 @@ T* vcycle(AMG& h, int l, bool zero_x, cudaStream_t s) {
   if (L.coarsest) {
     if (L.n <= 500) {
       const int n = L.n;
-      k_coarse_apply<T><<<std::max(1, (n + 7) / 8), 256, n * sizeof(double), s>>>(n, L.lu.p,
-                                                                                 LV<T>::b(L), LV<T>::x(L));
+      const bool free_ = (l == 0) && h.krylov_mode && L.lu_free.p != nullptr;
+      k_coarse_apply<T><<<std::max(1, (n + 7) / 8), 256, n * sizeof(double), s>>>(
+          n, free_ ? L.lu_free.p : L.lu.p, LV<T>::b(L), LV<T>::x(L), free_ ? 0 : 1); ::impes::count_launch();
       IMPES_CHECK_LAUNCH();
       return LV<T>::x(L);
     }
     // n > 500: 50 l1-Jacobi sweeps from zero on the pinned right-hand side
     T* bp = LV<T>::r(L);
-    k_pin_copy<T><<<grid_for(L.n, TB), TB, 0, s>>>(L.n, LV<T>::b(L), bp);
+    k_pin_copy<T><<<grid_for(L.n, TB), TB, 0, s>>>(L.n, LV<T>::b(L), bp); ::impes::count_launch();
     return smooth<T>(L, LV<T>::x(L), LV<T>::t(L), bp, 50, true, s);
   }
-  T* x = smooth<T>(L, LV<T>::x(L), LV<T>::t(L), LV<T>::b(L), 3, zero_x, s);
+  const int tid = (l == 0) ? timers().begin(IMPES_PH_VCYCLE, s) : -1;
+  T* x = smooth<T>(L, LV<T>::x(L), LV<T>::t(L), LV<T>::b(L), 3, zero_x, s, l == 0);
   T* spare = (x == LV<T>::x(L)) ? LV<T>::t(L) : LV<T>::x(L);
   Level& Nc = *h.levels[l + 1];
   launch_csr<T, Y_B_MINUS_AX>(L.n, L.avg_row, L.rowptr.p, L.col.p, LV<T>::val(L), x, LV<T>::b(L),
@@ -362,7 +408,9 @@ T* vcycle(AMG& h, int l, bool zero_x, cudaStream_t s) {
                       nullptr, LV<T>::b(Nc), s);
   T* ec = vcycle<T>(h, l + 1, true, s);
   launch_csr<T, Y_ADD_AX>(L.n, L.p_avg, L.prow.p, L.pcol.p, LV<T>::pval(L), ec, nullptr, nullptr, x, s);
-  return smooth<T>(L, x, spare, LV<T>::b(L), 2, false, s);
+  T* out = smooth<T>(L, x, spare, LV<T>::b(L), 2, false, s, l == 0);
+  timers().end(tid, s, vcycle_bytes<T>(h, l));
+  return out;
 }
 
 }  // namespace
@@ -373,9 +421,9 @@ void amg_vcycle_scaled(AMG& h, const double* bs, double* xs, int precision, cuda
   const int n = L0.n;
   if (precision == 1) {
     IMPES_REQUIRE(h.prm.mixed_precision, IMPES_ERR_STATE, "fp32 V-cycle needs mixed_precision=1");
-    k_convert<double, float><<<grid_for(n, TB), TB, 0, s>>>(n, bs, L0.bf.p);
+    k_convert<double, float><<<grid_for(n, TB), TB, 0, s>>>(n, bs, L0.bf.p); ::impes::count_launch();
     float* x = vcycle<float>(h, 0, true, s);
-    k_convert<float, double><<<grid_for(n, TB), TB, 0, s>>>(n, x, xs);
+    k_convert<float, double><<<grid_for(n, TB), TB, 0, s>>>(n, x, xs); ::impes::count_launch();
   } else {
     IMPES_CUDA(cudaMemcpyAsync(L0.b.p, bs, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     double* x = vcycle<double>(h, 0, true, s);
@@ -390,7 +438,7 @@ void amg_solve_vcycles(AMG& h, const double* b, double* x, double tol, int max_c
   Level& L0 = *h.levels[0];
   const int n = L0.n;
   DBuf<double> bs(n), r(n);
-  k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, h.dhalf_inv.p, b, bs.p);
+  k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, h.dhalf_inv.p, b, bs.p); ::impes::count_launch();
   IMPES_CHECK_LAUNCH();
   const double bn = std::sqrt(dot_host(h, bs.p, bs.p, n, s));
   IMPES_CUDA(cudaMemcpyAsync(L0.b.p, bs.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
@@ -409,7 +457,7 @@ void amg_solve_vcycles(AMG& h, const double* b, double* x, double tol, int max_c
     if (rr < tol) break;
   }
   if (c > max_cycles) c = max_cycles;
-  k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, h.dhalf_inv.p, L0.x.p, x);
+  k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, h.dhalf_inv.p, L0.x.p, x); ::impes::count_launch();
   IMPES_CHECK_LAUNCH();
   if (cycles) *cycles = c;
   if (rel) *rel = rr;
@@ -421,7 +469,7 @@ void amg_apply(AMG& h, const double* b, double* x, int cycles, double apply_tol,
   Level& L0 = *h.levels[0];
   const int n = L0.n;
   DBuf<double> bs(n), r(n);
-  k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, h.dhalf_inv.p, b, bs.p);
+  k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, h.dhalf_inv.p, b, bs.p); ::impes::count_launch();
   IMPES_CUDA(cudaMemcpyAsync(L0.b.p, bs.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
   const double bn = std::sqrt(dot_host(h, bs.p, bs.p, n, s));
   int c = 0;
@@ -435,7 +483,7 @@ void amg_apply(AMG& h, const double* b, double* x, int cycles, double apply_tol,
     double rel = std::sqrt(dot_host(h, r.p, r.p, n, s)) / (bn + 1e-30);
     if (c >= cycles && rel < apply_tol) break;
   }
-  k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, h.dhalf_inv.p, L0.x.p, x);
+  k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, h.dhalf_inv.p, L0.x.p, x); ::impes::count_launch();
   IMPES_CHECK_LAUNCH();
 }
 
@@ -497,8 +545,22 @@ __global__ void k_init_g(double* g, int m1, const double* nrm2) {
 // norm ||D^-1 r||.  Operator K = diag(wt) A_s, preconditioner M(v) = V(v ./ wt).
 // Orthogonalisation is classical Gram-Schmidt with one re-orthogonalisation
 // pass; all reductions use a fixed block count (deterministic).
+namespace {
+struct KrylovModeGuard {
+  AMG& h;
+  explicit KrylovModeGuard(AMG& a) : h(a) { h.krylov_mode = true; }
+  ~KrylovModeGuard() { h.krylov_mode = false; }
+};
+}  // namespace
+
 void amg_fgmres(AMG& h, const double* b, double* x, const impes_krylov_params& kp,
                 impes_krylov_stats& st, cudaStream_t s) {
+  KrylovModeGuard guard(h);
+  struct SolveTimer {
+    cudaStream_t s;
+    int id;
+    ~SolveTimer() { try { timers().end(id, s, 0.0); } catch (...) {} }
+  } solve_timer{s, timers().begin(IMPES_PH_SOLVE, s)};
   Level& L0 = *h.levels[0];
   const int n = L0.n;
   const int m = std::max(1, std::min(kp.restart, 120));
@@ -514,22 +576,22 @@ void amg_fgmres(AMG& h, const double* b, double* x, const impes_krylov_params& k
   const int ldh = m + 2;
   const bool jac = kp.norm == IMPES_NORM_JACOBI;
   double* wt = jac ? h.jac_w.p : h.kw.p;
-  if (!jac) k_fill<<<grid_for(n, TB), TB, 0, s>>>(n, h.kw.p, 1.0);
+  if (!jac) { k_fill<<<grid_for(n, TB), TB, 0, s>>>(n, h.kw.p, 1.0); ::impes::count_launch(); }
   double* bs = h.kb.p;   // b_s = dhalf .* b
   double* xs = h.kx.p;   // x_s
-  k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, h.dhalf_inv.p, b, bs);
+  k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, h.dhalf_inv.p, b, bs); ::impes::count_launch();
   if (kp.use_x0)
-    k_div_convert<double, double><<<grid_for(n, TB), TB, 0, s>>>(n, x, h.dhalf_inv.p, xs);
+    { k_div_convert<double, double><<<grid_for(n, TB), TB, 0, s>>>(n, x, h.dhalf_inv.p, xs); ::impes::count_launch(); }
   else
-    k_zero<<<grid_for(n, TB), TB, 0, s>>>(n, xs);
+    { k_zero<<<grid_for(n, TB), TB, 0, s>>>(n, xs); ::impes::count_launch(); }
   IMPES_CHECK_LAUNCH();
   double* r0 = h.V.p;
-  k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, wt, bs, r0);
+  k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, wt, bs, r0); ::impes::count_launch();
   const double bnorm = std::sqrt(dot_host(h, r0, r0, n, s));
   st = impes_krylov_stats{0, 0, 0, 0.0, 0.0};
   if (!(bnorm > 0.0)) {
     if (!(bnorm == bnorm)) throw Error(IMPES_ERR_NAN, "non-finite right-hand side");
-    k_zero<<<grid_for(n, TB), TB, 0, s>>>(n, x);
+    k_zero<<<grid_for(n, TB), TB, 0, s>>>(n, x); ::impes::count_launch();
     st.converged = 1;
     return;
   }
@@ -543,9 +605,9 @@ void amg_fgmres(AMG& h, const double* b, double* x, const impes_krylov_params& k
     // V[0] = wt .* (b_s - A_s x_s), beta = ||V[0]||
     launch_csr<double, Y_B_MINUS_AX>(n, L0.avg_row, L0.rowptr.p, L0.col.p, L0.val.p, xs, bs,
                                      nullptr, h.V.p, s);
-    k_mul_inplace<<<grid_for(n, TB), TB, 0, s>>>(n, h.V.p, wt);
-    k_multidot<<<kDotBlocks, TB, 0, s>>>(n, h.V.p, 0, 1, h.V.p, h.red.p);
-    k_dot_finalize<<<1, 32, 0, s>>>(1, h.red.p, dscal, 0);
+    k_mul_inplace<<<grid_for(n, TB), TB, 0, s>>>(n, h.V.p, wt); ::impes::count_launch();
+    k_multidot<<<kDotBlocks, TB, 0, s>>>(n, h.V.p, 0, 1, h.V.p, h.red.p); ::impes::count_launch();
+    k_dot_finalize<<<1, 32, 0, s>>>(1, h.red.p, dscal, 0); ::impes::count_launch();
     IMPES_CUDA(cudaMemcpyAsync(h.hbuf.p, dscal, sizeof(double), cudaMemcpyDeviceToHost, s));
     IMPES_CUDA(cudaStreamSynchronize(s));
     const double beta = std::sqrt(h.hbuf.p[0]);
@@ -553,8 +615,8 @@ void amg_fgmres(AMG& h, const double* b, double* x, const impes_krylov_params& k
     est_rel = beta / bnorm;
     st.rel_res = est_rel;
     if (est_rel < kp.tol || total >= kp.max_iters) break;
-    k_init_g<<<1, 1, 0, s>>>(h.g.p, m + 1, dscal);
-    k_scale_by_inv_sqrt<<<grid_for(n, TB), TB, 0, s>>>(n, h.V.p, h.V.p, dscal);
+    k_init_g<<<1, 1, 0, s>>>(h.g.p, m + 1, dscal); ::impes::count_launch();
+    k_scale_by_inv_sqrt<<<grid_for(n, TB), TB, 0, s>>>(n, h.V.p, h.V.p, dscal); ::impes::count_launch();
     int j = 0;
     for (; j < m && total < kp.max_iters; ++j) {
       double* vj = h.V.p + (size_t)j * n;
@@ -562,32 +624,36 @@ void amg_fgmres(AMG& h, const double* b, double* x, const impes_krylov_params& k
       double* w = h.V.p + (size_t)(j + 1) * n;
       // z_j = V(v_j ./ wt)
       if (prec == 1) {
-        k_div_convert<double, float><<<grid_for(n, TB), TB, 0, s>>>(n, vj, wt, L0.bf.p);
+        k_div_convert<double, float><<<grid_for(n, TB), TB, 0, s>>>(n, vj, wt, L0.bf.p); ::impes::count_launch();
         float* zf = vcycle<float>(h, 0, true, s);
-        k_convert<float, double><<<grid_for(n, TB), TB, 0, s>>>(n, zf, zj);
+        k_convert<float, double><<<grid_for(n, TB), TB, 0, s>>>(n, zf, zj); ::impes::count_launch();
       } else {
-        k_div_convert<double, double><<<grid_for(n, TB), TB, 0, s>>>(n, vj, wt, L0.b.p);
+        k_div_convert<double, double><<<grid_for(n, TB), TB, 0, s>>>(n, vj, wt, L0.b.p); ::impes::count_launch();
         double* zd = vcycle<double>(h, 0, true, s);
         IMPES_CUDA(cudaMemcpyAsync(zj, zd, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
       }
       // w = wt .* (A_s z_j)
+      const int tsp = timers().begin(IMPES_PH_SPMV_L0, s);
       launch_csr<double, Y_W_AX>(n, L0.avg_row, L0.rowptr.p, L0.col.p, L0.val.p, zj, nullptr, wt, w, s);
+      timers().end(tsp, s, spmv_bytes(8.0, 8.0, L0.nnz, n, n) + 8.0 * n);
+      const int tor = timers().begin(IMPES_PH_ORTHO, s);
       double* hcol = h.H.p + (size_t)j * ldh;
       for (int pass = 0; pass < 2; ++pass) {
         double* coef = pass == 0 ? hcol : h.y.p;
         for (int q0 = 0; q0 <= j; q0 += kMD) {
           int k = std::min(kMD, j + 1 - q0);
-          k_multidot<<<kDotBlocks, TB, 0, s>>>(n, h.V.p + (size_t)q0 * n, n, k, w, h.red.p);
-          k_dot_finalize<<<k, 32, 0, s>>>(k, h.red.p, coef + q0, 0);
+          k_multidot<<<kDotBlocks, TB, 0, s>>>(n, h.V.p + (size_t)q0 * n, n, k, w, h.red.p); ::impes::count_launch();
+          k_dot_finalize<<<k, 32, 0, s>>>(k, h.red.p, coef + q0, 0); ::impes::count_launch();
         }
         k_update<<<kDotBlocks, TB, 0, s>>>(n, h.V.p, n, j + 1, coef, w,
-                                           pass == 1 ? h.red.p : nullptr);
+                                           pass == 1 ? h.red.p : nullptr); ::impes::count_launch();
       }
-      k_hadd<<<1, 128, 0, s>>>(j + 1, hcol, h.y.p);
-      k_dot_finalize<<<1, 32, 0, s>>>(1, h.red.p, dscal, 0);   // ||w||^2 from k_update
-      k_set_hcol<<<1, 1, 0, s>>>(j, ldh, h.H.p, dscal);
-      k_scale_by_inv_sqrt<<<grid_for(n, TB), TB, 0, s>>>(n, w, w, dscal);
-      k_givens<<<1, 1, 0, s>>>(j, ldh, h.H.p, h.cs.p, h.sn.p, h.g.p, dscal + 1);
+      k_hadd<<<1, 128, 0, s>>>(j + 1, hcol, h.y.p); ::impes::count_launch();
+      k_dot_finalize<<<1, 32, 0, s>>>(1, h.red.p, dscal, 0); ::impes::count_launch();   // ||w||^2 from k_update
+      k_set_hcol<<<1, 1, 0, s>>>(j, ldh, h.H.p, dscal); ::impes::count_launch();
+      k_scale_by_inv_sqrt<<<grid_for(n, TB), TB, 0, s>>>(n, w, w, dscal); ::impes::count_launch();
+      timers().end(tor, s, 8.0 * n * (2.0 * (j + 1) + 3.0));
+      k_givens<<<1, 1, 0, s>>>(j, ldh, h.H.p, h.cs.p, h.sn.p, h.g.p, dscal + 1); ::impes::count_launch();
       IMPES_CHECK_LAUNCH();
       ++total;
       IMPES_CUDA(cudaMemcpyAsync(h.hbuf.p, dscal + 1, sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -597,15 +663,15 @@ void amg_fgmres(AMG& h, const double* b, double* x, const impes_krylov_params& k
       if (est_rel < kp.tol) { ++j; break; }
     }
     // x_s += Z y with y = R^-1 g; the loop head re-checks the true residual
-    k_backsolve<<<1, 1, 0, s>>>(j, ldh, h.H.p, h.g.p, h.y.p);
-    k_combine<<<grid_for(n, TB), TB, 0, s>>>(n, h.Z.p, n, j, h.y.p, xs);
+    k_backsolve<<<1, 1, 0, s>>>(j, ldh, h.H.p, h.g.p, h.y.p); ::impes::count_launch();
+    k_combine<<<grid_for(n, TB), TB, 0, s>>>(n, h.Z.p, n, j, h.y.p, xs); ::impes::count_launch();
     IMPES_CHECK_LAUNCH();
     st.restarts++;
   }
   st.iterations = total;
   st.converged = est_rel < kp.tol;
   st.true_rel_res = est_rel;
-  k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, h.dhalf_inv.p, xs, x);
+  k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, h.dhalf_inv.p, xs, x); ::impes::count_launch();
   IMPES_CHECK_LAUNCH();
 }
 

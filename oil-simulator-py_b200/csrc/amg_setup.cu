@@ -650,27 +650,27 @@ int orthonormalize(AMG& h, double* B, int n, int m, cudaStream_t s) {
   DBuf<double> v(n), q(n), out((size_t)n * m);
   std::vector<DBuf<double>> kept;
   for (int c = 0; c < m; ++c) {
-    k_col_extract<<<grid_for(n, TB), TB, 0, s>>>(n, m, c, B, v.p);
+    k_col_extract<<<grid_for(n, TB), TB, 0, s>>>(n, m, c, B, v.p); ::impes::count_launch();
     for (auto& qq : kept) {
       double d = dot_host(h, v.p, qq.p, n, s);
-      k_axpy<<<grid_for(n, TB), TB, 0, s>>>(n, -d, qq.p, v.p);
+      k_axpy<<<grid_for(n, TB), TB, 0, s>>>(n, -d, qq.p, v.p); ::impes::count_launch();
     }
     double nv = std::sqrt(dot_host(h, v.p, v.p, n, s));
     if (nv > 1e-10) {
       DBuf<double> qn(n);
-      k_scale_into<<<grid_for(n, TB), TB, 0, s>>>(n, 1.0 / nv, v.p, qn.p);
+      k_scale_into<<<grid_for(n, TB), TB, 0, s>>>(n, 1.0 / nv, v.p, qn.p); ::impes::count_launch();
       kept.push_back(std::move(qn));
     }
   }
   int mk = (int)kept.size();
   if (mk == 0) {
     DBuf<double> one(n);
-    k_fill_col<<<grid_for(n, TB), TB, 0, s>>>(n, 1, 0, one.p, nullptr, 1.0 / (std::sqrt((double)n) + 1e-30), 0.0);
+    k_fill_col<<<grid_for(n, TB), TB, 0, s>>>(n, 1, 0, one.p, nullptr, 1.0 / (std::sqrt((double)n) + 1e-30), 0.0); ::impes::count_launch();
     kept.push_back(std::move(one));
     mk = 1;
   }
   for (int c = 0; c < mk; ++c)
-    k_fill_col<<<grid_for(n, TB), TB, 0, s>>>(n, mk, c, B, kept[c].p, 1.0, 0.0);
+    { k_fill_col<<<grid_for(n, TB), TB, 0, s>>>(n, mk, c, B, kept[c].p, 1.0, 0.0); ::impes::count_launch(); }
   IMPES_CUDA(cudaStreamSynchronize(s));
   return mk;
 }
@@ -685,43 +685,43 @@ int level0_basis(AMG& h, DBuf<double>& B, int n, int dim, cudaStream_t s) {
   {
     DBuf<double> one(n);
     double inv = 1.0 / (std::sqrt((double)n) + 1e-30);
-    k_fill_col<<<grid_for(n, TB), TB, 0, s>>>(n, 1, 0, one.p, nullptr, inv, 0.0);
+    k_fill_col<<<grid_for(n, TB), TB, 0, s>>>(n, 1, 0, one.p, nullptr, inv, 0.0); ::impes::count_launch();
     basis.push_back(std::move(one));
   }
-  k_linspace<<<grid_for(n, TB), TB, 0, s>>>(n, coords.p);
-  k_fill_col<<<grid_for(n, TB), TB, 0, s>>>(n, 1, 0, c0.p, nullptr, 1.0, 0.0);  // ones
+  k_linspace<<<grid_for(n, TB), TB, 0, s>>>(n, coords.p); ::impes::count_launch();
+  k_fill_col<<<grid_for(n, TB), TB, 0, s>>>(n, 1, 0, c0.p, nullptr, 1.0, 0.0); ::impes::count_launch();  // ones
   double mean = dot_host(h, coords.p, c0.p, n, s) / n;
   if ((int)basis.size() < dim) {
-    k_scale_into<<<grid_for(n, TB), TB, 0, s>>>(n, 1.0, coords.p, cur.p);
-    k_add_scalar<<<grid_for(n, TB), TB, 0, s>>>(n, cur.p, mean);
+    k_scale_into<<<grid_for(n, TB), TB, 0, s>>>(n, 1.0, coords.p, cur.p); ::impes::count_launch();
+    k_add_scalar<<<grid_for(n, TB), TB, 0, s>>>(n, cur.p, mean); ::impes::count_launch();
     double nr = std::sqrt(dot_host(h, cur.p, cur.p, n, s));
     if (nr > 1e-8) {
       DBuf<double> q(n);
-      k_scale_into<<<grid_for(n, TB), TB, 0, s>>>(n, 1.0 / nr, cur.p, q.p);
+      k_scale_into<<<grid_for(n, TB), TB, 0, s>>>(n, 1.0 / nr, cur.p, q.p); ::impes::count_launch();
       basis.push_back(std::move(q));
     }
   }
   if ((int)basis.size() < dim) {
-    k_square<<<grid_for(n, TB), TB, 0, s>>>(n, coords.p, cur.p);
+    k_square<<<grid_for(n, TB), TB, 0, s>>>(n, coords.p, cur.p); ::impes::count_launch();
     double m2 = dot_host(h, cur.p, c0.p, n, s) / n;
-    k_add_scalar<<<grid_for(n, TB), TB, 0, s>>>(n, cur.p, m2);
+    k_add_scalar<<<grid_for(n, TB), TB, 0, s>>>(n, cur.p, m2); ::impes::count_launch();
     double nr = std::sqrt(dot_host(h, cur.p, cur.p, n, s));
     if (nr > 1e-8) {
       for (auto& b : basis) {
         double d = dot_host(h, cur.p, b.p, n, s);
-        k_axpy<<<grid_for(n, TB), TB, 0, s>>>(n, -d, b.p, cur.p);
+        k_axpy<<<grid_for(n, TB), TB, 0, s>>>(n, -d, b.p, cur.p); ::impes::count_launch();
       }
       double nr2 = std::sqrt(dot_host(h, cur.p, cur.p, n, s));
       if (nr2 > 1e-8) {
         DBuf<double> q(n);
-        k_scale_into<<<grid_for(n, TB), TB, 0, s>>>(n, 1.0 / nr2, cur.p, q.p);
+        k_scale_into<<<grid_for(n, TB), TB, 0, s>>>(n, 1.0 / nr2, cur.p, q.p); ::impes::count_launch();
         basis.push_back(std::move(q));
       }
     }
   }
   int m = (int)basis.size();
   for (int c = 0; c < m; ++c)
-    k_fill_col<<<grid_for(n, TB), TB, 0, s>>>(n, m, c, B.p, basis[c].p, 1.0, 0.0);
+    { k_fill_col<<<grid_for(n, TB), TB, 0, s>>>(n, m, c, B.p, basis[c].p, 1.0, 0.0); ::impes::count_launch(); }
   return orthonormalize(h, B.p, n, m, s);
 }
 
@@ -730,9 +730,9 @@ void union_symbolic(AMG& h, int rows, const int* optr, const int* ocol, const in
                     const int* icol, DBuf<int>& outptr, DBuf<int>& outcol, int& maxrow,
                     cudaStream_t s) {
   DBuf<int> bound(rows), ucnt(rows + 1);
-  k_union_bound<<<grid_for(rows, TB), TB, 0, s>>>(rows, optr, ocol, iptr, bound.p);
+  k_union_bound<<<grid_for(rows, TB), TB, 0, s>>>(rows, optr, ocol, iptr, bound.p); ::impes::count_launch();
   IMPES_CUDA(cudaMemsetAsync(h.iflag.p, 0, sizeof(int), s));
-  k_max_i32<<<grid_for(rows, TB), TB, 0, s>>>(rows, bound.p, h.iflag.p);
+  k_max_i32<<<grid_for(rows, TB), TB, 0, s>>>(rows, bound.p, h.iflag.p); ::impes::count_launch();
   int maxc = to_host_int(h, h.iflag.p, s);
   int hsize = 32;
   while (hsize < 2 * maxc) hsize <<= 1;
@@ -743,16 +743,16 @@ void union_symbolic(AMG& h, int rows, const int* optr, const int* ocol, const in
   IMPES_CUDA(cudaFuncSetAttribute(k_union_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   unsigned grid = (unsigned)std::min<long long>((rows + wpb - 1) / wpb, (long long)num_sms() * 32);
   k_union_rows<<<std::max(1u, grid), 32 * wpb, smem, s>>>(rows, optr, ocol, iptr, icol, hsize,
-                                                          ucnt.p, nullptr, nullptr);
+                                                          ucnt.p, nullptr, nullptr); ::impes::count_launch();
   IMPES_CHECK_LAUNCH();
   outptr.alloc(rows + 1);
   int nnz = exclusive_scan_i32(ucnt.p, outptr.p, rows, s);
   outcol.alloc(std::max(nnz, 1));
   k_union_rows<<<std::max(1u, grid), 32 * wpb, smem, s>>>(rows, optr, ocol, iptr, icol, hsize,
-                                                          nullptr, outptr.p, outcol.p);
+                                                          nullptr, outptr.p, outcol.p); ::impes::count_launch();
   IMPES_CHECK_LAUNCH();
   IMPES_CUDA(cudaMemsetAsync(h.iflag.p, 0, sizeof(int), s));
-  k_max_i32<<<grid_for(rows, TB), TB, 0, s>>>(rows, ucnt.p, h.iflag.p);
+  k_max_i32<<<grid_for(rows, TB), TB, 0, s>>>(rows, ucnt.p, h.iflag.p); ::impes::count_launch();
   maxrow = to_host_int(h, h.iflag.p, s);
 }
 
@@ -768,7 +768,7 @@ void union_numeric(int rows, const int* optr, const int* ocol, const double* ova
     IMPES_CUDA(cudaFuncSetAttribute(k_union_numeric<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     unsigned grid = (unsigned)std::min<long long>((rows + W - 1) / W, (long long)num_sms() * 16);
     k_union_numeric<W><<<grid, 32 * W, smem, s>>>(rows, optr, ocol, oval, iptr, icol, ival, outptr,
-                                                   outcol, outval, maxrow);
+                                                   outcol, outval, maxrow); ::impes::count_launch();
   } else {
     constexpr int W = 1;
     size_t smem = per_warp * W + 16;
@@ -776,14 +776,14 @@ void union_numeric(int rows, const int* optr, const int* ocol, const double* ova
     IMPES_CUDA(cudaFuncSetAttribute(k_union_numeric<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     unsigned grid = (unsigned)std::min<long long>(rows, (long long)num_sms() * 32);
     k_union_numeric<W><<<grid, 32 * W, smem, s>>>(rows, optr, ocol, oval, iptr, icol, ival, outptr,
-                                                   outcol, outval, maxrow);
+                                                   outcol, outval, maxrow); ::impes::count_launch();
   }
   IMPES_CHECK_LAUNCH();
 }
 
 void compute_inv_relax(AMG& h, Level& L, cudaStream_t s) {
   L.inv_relax.ensure(std::max(L.n, 1));
-  k_inv_relax<<<grid_for(L.n, TB), TB, 0, s>>>(L.n, L.rowptr.p, L.col.p, L.val.p, L.inv_relax.p);
+  k_inv_relax<<<grid_for(L.n, TB), TB, 0, s>>>(L.n, L.rowptr.p, L.col.p, L.val.p, L.inv_relax.p); ::impes::count_launch();
   IMPES_CHECK_LAUNCH();
 }
 
@@ -802,13 +802,13 @@ void equilibrate_level0(AMG& h, const double* val_in, cudaStream_t s) {
   h.dhalf_inv.ensure(n);
   h.jac_w.ensure(n);
   h.diag_tmp.ensure(n);
-  k_diag<<<grid_for(n, TB), TB, 0, s>>>(n, L0.rowptr.p, L0.col.p, val_in, h.diag_tmp.p);
+  k_diag<<<grid_for(n, TB), TB, 0, s>>>(n, L0.rowptr.p, L0.col.p, val_in, h.diag_tmp.p); ::impes::count_launch();
   IMPES_CUDA(cudaMemsetAsync(h.iflag.p, 0, sizeof(int), s));
-  k_count_below<<<grid_for(n, TB), TB, 0, s>>>(n, h.diag_tmp.p, h.prm.equilibration_threshold, h.iflag.p);
+  k_count_below<<<grid_for(n, TB), TB, 0, s>>>(n, h.diag_tmp.p, h.prm.equilibration_threshold, h.iflag.p); ::impes::count_launch();
   k_equil_prepare<<<grid_for(n, TB), TB, 0, s>>>(n, h.diag_tmp.p, h.iflag.p, h.dhalf_inv.p,
-                                                 h.jac_w.p, h.iflag.p + 1);
+                                                 h.jac_w.p, h.iflag.p + 1); ::impes::count_launch();
   k_equilibrate<<<grid_for(n, TB), TB, 0, s>>>(n, L0.rowptr.p, L0.col.p, val_in, h.dhalf_inv.p,
-                                               L0.val.p);
+                                               L0.val.p); ::impes::count_launch();
   IMPES_CHECK_LAUNCH();
 }
 
@@ -818,13 +818,13 @@ void level_precision_copies(AMG& h, Level& L, cudaStream_t s) {
   if (!h.prm.mixed_precision) return;
   L.valf.ensure(std::max(L.nnz, 1));
   L.inv_relaxf.ensure(std::max(L.n, 1));
-  k_to_float<<<grid_for(L.nnz, TB), TB, 0, s>>>(L.nnz, L.val.p, L.valf.p);
-  k_to_float<<<grid_for(L.n, TB), TB, 0, s>>>(L.n, L.inv_relax.p, L.inv_relaxf.p);
+  k_to_float<<<grid_for(L.nnz, TB), TB, 0, s>>>(L.nnz, L.val.p, L.valf.p); ::impes::count_launch();
+  k_to_float<<<grid_for(L.n, TB), TB, 0, s>>>(L.n, L.inv_relax.p, L.inv_relaxf.p); ::impes::count_launch();
   if (!L.coarsest && L.pnnz) {
     L.pvalf.ensure(L.pnnz);
     L.rvalf.ensure(L.pnnz);
-    k_to_float<<<grid_for(L.pnnz, TB), TB, 0, s>>>(L.pnnz, L.pval.p, L.pvalf.p);
-    k_to_float<<<grid_for(L.pnnz, TB), TB, 0, s>>>(L.pnnz, L.rval.p, L.rvalf.p);
+    k_to_float<<<grid_for(L.pnnz, TB), TB, 0, s>>>(L.pnnz, L.pval.p, L.pvalf.p); ::impes::count_launch();
+    k_to_float<<<grid_for(L.pnnz, TB), TB, 0, s>>>(L.pnnz, L.rval.p, L.rvalf.p); ::impes::count_launch();
   }
   IMPES_CHECK_LAUNCH();
 }
@@ -839,8 +839,8 @@ void amg_setup(AMG& h, int n, int nnz, const int* rowptr, const int* col, const 
   h.scal.ensure(256);
   // validate the caller's CSR before reading it
   IMPES_CUDA(cudaMemsetAsync(h.iflag.p, 0, sizeof(int), s));
-  k_validate_csr<<<grid_for(n, TB), TB, 0, s>>>(n, nnz, rowptr, col, h.iflag.p);
-  k_nonfinite<<<grid_for(nnz, TB), TB, 0, s>>>(val, nnz, h.iflag.p);
+  k_validate_csr<<<grid_for(n, TB), TB, 0, s>>>(n, nnz, rowptr, col, h.iflag.p); ::impes::count_launch();
+  k_nonfinite<<<grid_for(nnz, TB), TB, 0, s>>>(val, nnz, h.iflag.p); ::impes::count_launch();
   int bad = to_host_int(h, h.iflag.p, s);
   IMPES_REQUIRE(!(bad & 7), IMPES_ERR_BAD_CSR, "malformed CSR (row pointers, column range or order)");
   IMPES_REQUIRE(!(bad & 8), IMPES_ERR_NAN, "non-finite matrix value");
@@ -866,87 +866,87 @@ void amg_setup(AMG& h, int n, int nnz, const int* rowptr, const int* col, const 
     if (nl <= h.prm.coarsest_size) { L.coarsest = true; break; }
     // strength + C/F split
     DBuf<unsigned char> strong(L.nnz);
-    k_strength<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.rowptr.p, L.col.p, L.val.p, theta, strong.p);
+    k_strength<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.rowptr.p, L.col.p, L.val.p, theta, strong.p); ::impes::count_launch();
     DBuf<int> gcnt(nl + 1), gptr(nl + 1), fill(nl + 1);
     IMPES_CUDA(cudaMemsetAsync(gcnt.p, 0, sizeof(int) * (nl + 1), s));
-    k_sym_count<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.rowptr.p, L.col.p, strong.p, gcnt.p);
+    k_sym_count<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.rowptr.p, L.col.p, strong.p, gcnt.p); ::impes::count_launch();
     int gn = exclusive_scan_i32(gcnt.p, gptr.p, nl, s);
     DBuf<int> gcol(std::max(gn, 1)), ucnt(nl);
     IMPES_CUDA(cudaMemcpyAsync(fill.p, gptr.p, sizeof(int) * nl, cudaMemcpyDeviceToDevice, s));
-    k_sym_fill<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.rowptr.p, L.col.p, strong.p, fill.p, gcol.p);
-    k_sym_unique<<<grid_for(nl, TB), TB, 0, s>>>(nl, gptr.p, gcol.p, ucnt.p);
+    k_sym_fill<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.rowptr.p, L.col.p, strong.p, fill.p, gcol.p); ::impes::count_launch();
+    k_sym_unique<<<grid_for(nl, TB), TB, 0, s>>>(nl, gptr.p, gcol.p, ucnt.p); ::impes::count_launch();
     DBuf<double> score(nl);
-    k_score<<<grid_for(nl, TB), TB, 0, s>>>(nl, ucnt.p, h.prm.tiebreak_seed, lvl, score.p);
+    k_score<<<grid_for(nl, TB), TB, 0, s>>>(nl, ucnt.p, h.prm.tiebreak_seed, lvl, score.p); ::impes::count_launch();
     DBuf<unsigned char> C(nl);
-    k_cselect<<<grid_for(nl, TB), TB, 0, s>>>(nl, gptr.p, gcol.p, ucnt.p, score.p, C.p);
+    k_cselect<<<grid_for(nl, TB), TB, 0, s>>>(nl, gptr.p, gcol.p, ucnt.p, score.p, C.p); ::impes::count_launch();
     DBuf<signed char> cf(nl), cf2(nl);
     IMPES_CUDA(cudaMemsetAsync(h.iflag.p, 0, sizeof(int), s));
-    k_lift<<<grid_for(nl, TB), TB, 0, s>>>(nl, gptr.p, gcol.p, ucnt.p, C.p, cf.p, h.iflag.p);
+    k_lift<<<grid_for(nl, TB), TB, 0, s>>>(nl, gptr.p, gcol.p, ucnt.p, C.p, cf.p, h.iflag.p); ::impes::count_launch();
     IMPES_CHECK_LAUNCH();
     int n_coarse = to_host_int(h, h.iflag.p, s);
     if ((double)n_coarse >= nl * 0.9) { L.coarsest = true; break; }  // :832
     // orphans + fine->coarse map
     DBuf<int> cflag(nl + 1), f2c(nl + 1);
-    k_orphans<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.rowptr.p, L.col.p, strong.p, cf.p, cf2.p, cflag.p);
+    k_orphans<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.rowptr.p, L.col.p, strong.p, cf.p, cf2.p, cflag.p); ::impes::count_launch();
     const int nc = exclusive_scan_i32(cflag.p, f2c.p, nl, s);
     // interpolation
     DBuf<double> pdiag(nl), ssum(nl), wcsum(nl), wfsum(nl);
     DBuf<int> scnt(nl), ccnt(nl + 1), cptr(nl + 1);
     k_p_stats<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.rowptr.p, L.col.p, L.val.p, strong.p, cf2.p,
-                                              pdiag.p, ssum.p, wcsum.p, wfsum.p, scnt.p);
+                                              pdiag.p, ssum.p, wcsum.p, wfsum.p, scnt.p); ::impes::count_launch();
     k_p_count<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.rowptr.p, L.col.p, strong.p, cf2.p, scnt.p,
-                                              ssum.p, ccnt.p);
+                                              ssum.p, ccnt.p); ::impes::count_launch();
     int ctot = exclusive_scan_i32(ccnt.p, cptr.p, nl, s);
     DBuf<int> ccol(std::max(ctot, 1));
     DBuf<double> cval(std::max(ctot, 1));
     k_p_fill<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.rowptr.p, L.col.p, L.val.p, strong.p, cf2.p,
                                              f2c.p, pdiag.p, ssum.p, wcsum.p, wfsum.p, scnt.p,
-                                             cptr.p, ccol.p, cval.p);
+                                             cptr.p, ccol.p, cval.p); ::impes::count_launch();
     DBuf<int> mcnt(nl + 1);
-    k_p_merge<<<grid_for(nl, TB), TB, 0, s>>>(nl, cptr.p, ccol.p, cval.p, mcnt.p);
+    k_p_merge<<<grid_for(nl, TB), TB, 0, s>>>(nl, cptr.p, ccol.p, cval.p, mcnt.p); ::impes::count_launch();
     L.nc = nc;
     L.prow.alloc(nl + 1);
     L.pnnz = exclusive_scan_i32(mcnt.p, L.prow.p, nl, s);
     L.pcol.alloc(std::max(L.pnnz, 1));
     L.pval.alloc(std::max(L.pnnz, 1));
-    k_p_compact<<<grid_for(nl, TB), TB, 0, s>>>(nl, cptr.p, ccol.p, cval.p, L.prow.p, L.pcol.p, L.pval.p);
+    k_p_compact<<<grid_for(nl, TB), TB, 0, s>>>(nl, cptr.p, ccol.p, cval.p, L.prow.p, L.pcol.p, L.pval.p); ::impes::count_launch();
     DBuf<double> rsum(nl);
     IMPES_CUDA(cudaMemsetAsync(h.iflag.p, 0, sizeof(int), s));
-    k_p_rowsum<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.prow.p, L.pval.p, cf2.p, rsum.p, h.iflag.p);
+    k_p_rowsum<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.prow.p, L.pval.p, cf2.p, rsum.p, h.iflag.p); ::impes::count_launch();
     int nzero = to_host_int(h, h.iflag.p, s);
     if (nzero > 0) {
       DBuf<int> extra(nl), ncnt(nl + 1), nrow(nl + 1);
       k_p_zero_extra<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.rowptr.p, L.col.p, cf2.p, f2c.p, rsum.p,
-                                                     extra.p, L.prow.p, ncnt.p);
+                                                     extra.p, L.prow.p, ncnt.p); ::impes::count_launch();
       int nn = exclusive_scan_i32(ncnt.p, nrow.p, nl, s);
       DBuf<int> ncol(nn);
       DBuf<double> nval(nn);
       k_p_insert<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.prow.p, L.pcol.p, L.pval.p, extra.p, nrow.p,
-                                                 ncol.p, nval.p);
+                                                 ncol.p, nval.p); ::impes::count_launch();
       IMPES_CUDA(cudaStreamSynchronize(s));
       L.prow = std::move(nrow); L.pcol = std::move(ncol); L.pval = std::move(nval);
       L.pnnz = nn;
-      k_p_rowsum<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.prow.p, L.pval.p, cf2.p, rsum.p, h.iflag.p);
+      k_p_rowsum<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.prow.p, L.pval.p, cf2.p, rsum.p, h.iflag.p); ::impes::count_launch();
     }
-    k_p_scale<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.prow.p, L.pval.p, cf2.p, rsum.p);
+    k_p_scale<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.prow.p, L.pval.p, cf2.p, rsum.p); ::impes::count_launch();
     IMPES_CHECK_LAUNCH();
     if (m > 0 && h.prm.nullspace_blend > 0.0) {
       m = orthonormalize(h, basis.p, nl, m, s);   // build_prolongation_rs_full :393-396
       k_p_blend<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.prow.p, L.pcol.p, L.pval.p, cf2.p, basis.p, m,
-                                                h.prm.nullspace_blend, h.prm.nullspace_reg);
+                                                h.prm.nullspace_blend, h.prm.nullspace_reg); ::impes::count_launch();
       IMPES_CHECK_LAUNCH();
     }
     // R = P^T (sorted rows) and its values
     DBuf<int> rcnt(nc + 1), rfill(nc + 1);
     IMPES_CUDA(cudaMemsetAsync(rcnt.p, 0, sizeof(int) * (nc + 1), s));
-    k_col_count<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.prow.p, L.pcol.p, rcnt.p);
+    k_col_count<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.prow.p, L.pcol.p, rcnt.p); ::impes::count_launch();
     L.rrow.alloc(nc + 1);
     exclusive_scan_i32(rcnt.p, L.rrow.p, nc, s);
     L.rcol.alloc(std::max(L.pnnz, 1)); L.rsrc.alloc(std::max(L.pnnz, 1)); L.rval.alloc(std::max(L.pnnz, 1));
     IMPES_CUDA(cudaMemcpyAsync(rfill.p, L.rrow.p, sizeof(int) * nc, cudaMemcpyDeviceToDevice, s));
-    k_r_fill<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.prow.p, L.pcol.p, rfill.p, L.rcol.p, L.rsrc.p);
-    k_r_sort<<<grid_for(nc, TB), TB, 0, s>>>(nc, L.rrow.p, L.rcol.p, L.rsrc.p);
-    k_gather<<<grid_for(L.pnnz, TB), TB, 0, s>>>(L.pnnz, L.rsrc.p, L.pval.p, L.rval.p);
+    k_r_fill<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.prow.p, L.pcol.p, rfill.p, L.rcol.p, L.rsrc.p); ::impes::count_launch();
+    k_r_sort<<<grid_for(nc, TB), TB, 0, s>>>(nc, L.rrow.p, L.rcol.p, L.rsrc.p); ::impes::count_launch();
+    k_gather<<<grid_for(L.pnnz, TB), TB, 0, s>>>(L.pnnz, L.rsrc.p, L.pval.p, L.rval.p); ::impes::count_launch();
     IMPES_CHECK_LAUNCH();
     L.p_avg = std::max(1, L.pnnz / std::max(nl, 1));
     L.r_avg = std::max(1, L.pnnz / std::max(nc, 1));
@@ -972,7 +972,7 @@ void amg_setup(AMG& h, int n, int nnz, const int* rowptr, const int* col, const 
     // coarse basis (classical_amg.py:906-914)
     if (m > 0) {
       DBuf<double> Bc((size_t)std::max(nc, 1) * m);
-      k_restrict_basis<<<grid_for(nc, TB), TB, 0, s>>>(nc, m, L.rrow.p, L.rcol.p, L.rval.p, basis.p, Bc.p);
+      k_restrict_basis<<<grid_for(nc, TB), TB, 0, s>>>(nc, m, L.rrow.p, L.rcol.p, L.rval.p, basis.p, Bc.p); ::impes::count_launch();
       IMPES_CHECK_LAUNCH();
       m = orthonormalize(h, Bc.p, nc, m, s);
       basis = std::move(Bc);
@@ -995,6 +995,12 @@ void amg_setup(AMG& h, int n, int nnz, const int* rowptr, const int* col, const 
 
 void amg_update(AMG& h, const double* val, cudaStream_t s) {
   IMPES_REQUIRE(h.built, IMPES_ERR_STATE, "update before setup");
+  const int tid = timers().begin(IMPES_PH_GALERKIN, s);
+  double bytes = 0.0;
+  for (size_t l = 0; l + 1 < h.levels.size(); ++l) {
+    const Level& L = *h.levels[l];
+    bytes += 12.0 * L.nnz + 24.0 * L.pnnz + 8.0 * h.levels[l + 1]->nnz;
+  }
   equilibrate_level0(h, val, s);
   for (size_t l = 0; l < h.levels.size(); ++l) {
     Level& L = *h.levels[l];
@@ -1011,10 +1017,11 @@ void amg_update(AMG& h, const double* val, cudaStream_t s) {
     if (!h.prm.mixed_precision) break;
     L->valf.ensure(std::max(L->nnz, 1));
     L->inv_relaxf.ensure(std::max(L->n, 1));
-    k_to_float<<<grid_for(L->nnz, TB), TB, 0, s>>>(L->nnz, L->val.p, L->valf.p);
-    k_to_float<<<grid_for(L->n, TB), TB, 0, s>>>(L->n, L->inv_relax.p, L->inv_relaxf.p);
+    k_to_float<<<grid_for(L->nnz, TB), TB, 0, s>>>(L->nnz, L->val.p, L->valf.p); ::impes::count_launch();
+    k_to_float<<<grid_for(L->n, TB), TB, 0, s>>>(L->n, L->inv_relax.p, L->inv_relaxf.p); ::impes::count_launch();
   }
   IMPES_CHECK_LAUNCH();
+  timers().end(tid, s, bytes);
 }
 
 }  // namespace impes

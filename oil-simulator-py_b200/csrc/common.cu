@@ -1,12 +1,22 @@
 // Shared host utilities: thread-local error text and a device exclusive scan.
 #include "common.cuh"
+#include <atomic>
 
 namespace impes {
 
 static thread_local std::string g_last_error;
 
 void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+static std::atomic<unsigned long long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+unsigned long long launches() { return g_launches.load(std::memory_order_relaxed); }
 const char* last_error_cstr() { return g_last_error.c_str(); }
+
+PhaseTimers& timers() {
+  static PhaseTimers t;
+  return t;
+}
 
 namespace {
 constexpr int kScanBlock = 1024;
@@ -46,14 +56,14 @@ void exclusive_scan_i32_dev(const int* d_in, int* d_out, int n, cudaStream_t str
   }
   int nb = (n + kScanBlock - 1) / kScanBlock;
   DBuf<int> sums(nb), offs(nb + 1);
-  k_scan_block<<<nb, kScanBlock, 0, stream>>>(d_in, d_out, n, sums.p);
+  k_scan_block<<<nb, kScanBlock, 0, stream>>>(d_in, d_out, n, sums.p); ::impes::count_launch();
   IMPES_CHECK_LAUNCH();
   if (nb > 1) {
     exclusive_scan_i32_dev(sums.p, offs.p, nb, stream);
-    k_scan_add<<<nb, kScanBlock, 0, stream>>>(d_out, n, offs.p);
+    k_scan_add<<<nb, kScanBlock, 0, stream>>>(d_out, n, offs.p); ::impes::count_launch();
     IMPES_CHECK_LAUNCH();
   }
-  k_scan_total<<<1, 1, 0, stream>>>(d_in, d_out, n);
+  k_scan_total<<<1, 1, 0, stream>>>(d_in, d_out, n); ::impes::count_launch();
   IMPES_CHECK_LAUNCH();
   // temporaries are freed at scope exit: make sure the kernels using them ran
   IMPES_CUDA(cudaStreamSynchronize(stream));

@@ -20,6 +20,10 @@ struct Error : public std::runtime_error {
 
 void set_last_error(const std::string& msg);
 
+// Number of kernel launches issued by this library (every launch site calls it).
+void count_launch();
+unsigned long long launches();
+
 #define IMPES_CUDA(call)                                                        \
   do {                                                                          \
     cudaError_t e_ = (call);                                                    \
@@ -143,6 +147,38 @@ __device__ __forceinline__ double block_sum(double v, double* smem /*>= BLOCK/32
   __syncthreads();
   return r;  // valid in thread 0
 }
+
+// ------------------------------------------------------------ phase timers
+// CUDA-event pairs around phases of the step; global, enabled on demand.
+struct PhaseTimers {
+  struct Rec { int phase; cudaEvent_t a, b; double bytes; };
+  bool on = false;
+  std::vector<Rec> recs;
+  std::vector<cudaEvent_t> pool;
+  cudaEvent_t take() {
+    if (pool.empty()) {
+      cudaEvent_t e;
+      IMPES_CUDA(cudaEventCreate(&e));
+      return e;
+    }
+    cudaEvent_t e = pool.back();
+    pool.pop_back();
+    return e;
+  }
+  int begin(int phase, cudaStream_t s) {
+    if (!on) return -1;
+    Rec r{phase, take(), take(), 0.0};
+    IMPES_CUDA(cudaEventRecord(r.a, s));
+    recs.push_back(r);
+    return (int)recs.size() - 1;
+  }
+  void end(int idx, cudaStream_t s, double bytes) {
+    if (idx < 0) return;
+    recs[idx].bytes = bytes;
+    IMPES_CUDA(cudaEventRecord(recs[idx].b, s));
+  }
+};
+PhaseTimers& timers();
 
 // ------------------------------------------------------------- host helpers
 // Exclusive scan of int32 counts into int32 offsets (returns total).  Runs a

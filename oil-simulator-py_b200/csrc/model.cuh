@@ -56,6 +56,7 @@ struct Model {
   DBuf<double> well_q;                 // per well last_q_total (NaN unset)
   DBuf<double> well_rates;             // per well 4 surface rates (NaN unset)
   DBuf<double> csr_val, rhs;           // assembled system (owned for impes_step)
+  DBuf<double> p_save;                 // pressure before the solve (restored on failure)
   DBuf<int> rowptr, col;               // static pattern
   int red_blocks = 0;
 };

@@ -194,18 +194,32 @@ struct Brick {
   int nbi, nbj, nbk;   // bricks per dimension
 };
 
+// Interior extents <= 8 (z), <= 8 or 16 (y), and at most 256 cells per brick;
+// each dimension is split evenly so no brick is mostly empty.
 Brick make_brick(const ModelParams& P) {
   Brick b;
-  b.TK = std::min(P.nz, 8);
-  b.TJ = std::min(P.ny, P.nz == 1 ? 16 : 8);
-  b.TI = std::max(1, std::min(P.nx, 256 / (b.TK * b.TJ)));
+  b.nbk = (P.nz + 7) / 8;
+  b.TK = (P.nz + b.nbk - 1) / b.nbk;
+  int tj = std::min(P.ny, P.nz == 1 ? 16 : 8);
+  b.nbj = (P.ny + tj - 1) / tj;
+  b.TJ = (P.ny + b.nbj - 1) / b.nbj;
+  int ti = std::max(1, std::min(P.nx, 256 / (b.TK * b.TJ)));
+  b.nbi = (P.nx + ti - 1) / ti;
+  b.TI = (P.nx + b.nbi - 1) / b.nbi;
   b.hi = P.nx > 1; b.hj = P.ny > 1; b.hk = P.nz > 1;
   b.HI = b.TI + 2 * b.hi; b.HJ = b.TJ + 2 * b.hj; b.HK = b.TK + 2 * b.hk;
-  b.nbi = (P.nx + b.TI - 1) / b.TI;
-  b.nbj = (P.ny + b.TJ - 1) / b.TJ;
-  b.nbk = (P.nz + b.TK - 1) / b.TK;
   return b;
 }
+
+// Raise a kernel's dynamic shared-memory limit when a launch needs more.
+template <typename K>
+void ensure_smem(K kernel, size_t bytes, size_t& current) {
+  if (bytes > current) {
+    IMPES_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    current = bytes;
+  }
+}
+size_t g_smem_k1 = 48 << 10, g_smem_k4 = 48 << 10;
 
 __device__ __forceinline__ void brick_origin(const Brick& b, int& i0, int& j0, int& k0) {
   int bid = blockIdx.x;
@@ -921,12 +935,12 @@ void model_build_static(Model& m, const double* kx, const double* ky, const doub
   m.tz.alloc(std::max<long long>(1, (long long)P.nx * P.ny * (P.nz - 1)));
   m.pv.alloc(P.N);
   k_transmissibility<<<grid_for(P.N, 256), 256, 0, s>>>(P, kx, ky, kz, poro, m.tx.p, m.ty.p,
-                                                        m.tz.p, m.pv.p);
+                                                        m.tz.p, m.pv.p); ::impes::count_launch();
   IMPES_CHECK_LAUNCH();
   m.nnz = (int)pattern_rowptr(P.N, P.nx, P.ny, P.nz);
   m.rowptr.alloc(P.N + 1);
   m.col.alloc(m.nnz);
-  k_pattern<<<grid_for(P.N + 1, 256), 256, 0, s>>>(P, m.rowptr.p, m.col.p);
+  k_pattern<<<grid_for(P.N + 1, 256), 256, 0, s>>>(P, m.rowptr.p, m.col.p); ::impes::count_launch();
   IMPES_CHECK_LAUNCH();
   Brick b = make_brick(P);
   int blocks = b.nbi * b.nbj * b.nbk;
@@ -938,9 +952,6 @@ void model_build_static(Model& m, const double* kx, const double* ky, const doub
   m.dsw.alloc(P.N);
   m.dsg.alloc(P.N);
   m.wq.alloc(std::max(1, 3 * P.nwc));
-  size_t sm1 = brick_smem(b, kK1Fields), sm4 = brick_smem(b, kK4Fields);
-  IMPES_CUDA(cudaFuncSetAttribute(k_assemble, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
-  IMPES_CUDA(cudaFuncSetAttribute(k_saturation_flux, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm4));
 }
 
 void model_pattern(Model& m, int* rowptr, int* col, cudaStream_t s) {
@@ -952,36 +963,43 @@ void model_assemble(Model& m, const double* p, const double* sw, const double* s
                     double* csr_val, double* rhs, cudaStream_t s) {
   Brick b = make_brick(m.P);
   int blocks = b.nbi * b.nbj * b.nbk;
+  ensure_smem(k_assemble, brick_smem(b, kK1Fields), g_smem_k1);
+  const double F = 0.5 * (double)(m.nnz - m.P.N);
+  const int tid = timers().begin(IMPES_PH_ASSEMBLE, s);
   k_assemble<<<blocks, 256, brick_smem(b, kK1Fields), s>>>(
       m.P, b, m.pvt.p, p, sw, sg, m.tx.p, m.ty.p, m.tz.p, m.pv.p, m.wells.p, m.wc_cells.p,
-      m.wc_ptr.p, m.wc_wells.p, m.well_mode.p, dt, csr_val, rhs);
+      m.wc_ptr.p, m.wc_wells.p, m.well_mode.p, dt, csr_val, rhs); ::impes::count_launch();
   IMPES_CHECK_LAUNCH();
+  timers().end(tid, s, 8.0 * (6.0 * m.P.N + 3.0 * F));   // reads p, Sw, Sg, PV, T; writes A, b
 }
 
 void model_saturation(Model& m, const double* p_new, double* sw, double* sg, double* so, double dt,
                       cudaStream_t s) {
   const ModelParams& P = m.P;
+  const int tid = timers().begin(IMPES_PH_SATURATION, s);
   if (P.nwells > 0) {
     k_well_sources<<<1, 128, 0, s>>>(P, m.pvt.p, m.wells.p, m.wc_cells.p, p_new, sw, sg, m.pv.p,
-                                     dt, m.wq.p, m.balances.p, m.well_q.p, m.well_rates.p);
+                                     dt, m.wq.p, m.balances.p, m.well_q.p, m.well_rates.p); ::impes::count_launch();
     IMPES_CHECK_LAUNCH();
   }
   Brick b = make_brick(P);
   int blocks = b.nbi * b.nbj * b.nbk;
+  ensure_smem(k_saturation_flux, brick_smem(b, kK4Fields), g_smem_k4);
   k_saturation_flux<<<blocks, 256, brick_smem(b, kK4Fields), s>>>(
       P, b, m.pvt.p, p_new, sw, sg, m.tx.p, m.ty.p, m.tz.p, m.pv.p, m.wc_cells.p, m.wq.p, dt,
-      m.dsw.p, m.dsg.p, m.red.p, m.counter.p, m.nsub.p);
+      m.dsw.p, m.dsg.p, m.red.p, m.counter.p, m.nsub.p); ::impes::count_launch();
   IMPES_CHECK_LAUNCH();
   if (P.pvt_rows > 0 && P.nwells > 0) {
     k_well_substeps<<<1, 128, 0, s>>>(P, m.pvt.p, m.wells.p, p_new, sw, sg, m.dsw.p, m.dsg.p,
-                                      m.nsub.p, dt, m.balances.p);
+                                      m.nsub.p, dt, m.balances.p); ::impes::count_launch();
     IMPES_CHECK_LAUNCH();
   }
   unsigned g = grid_for(P.N, kSatBlock);
   k_saturation_substeps<<<g, kSatBlock, 0, s>>>(P, m.pvt.p, p_new, sw, sg, so, m.dsw.p, m.dsg.p,
                                                 m.pv.p, m.nsub.p, m.red.p, m.counter.p + 1,
-                                                m.balances.p);
+                                                m.balances.p); ::impes::count_launch();
   IMPES_CHECK_LAUNCH();
+  timers().end(tid, s, 8.0 * (6.0 * P.N + 0.5 * (double)(m.nnz - P.N)));
 }
 
 }  // namespace impes

@@ -87,6 +87,12 @@ class SatStats(C.Structure):
                 ("component", C.c_double * 6)]
 
 
+class Timing(C.Structure):
+    _fields_ = [("count", C.c_longlong * 8), ("ms", C.c_double * 8), ("bytes", C.c_double * 8)]
+
+
+PHASES = ("assemble", "saturation", "galerkin", "vcycle", "smooth_l0", "spmv_l0", "ortho", "solve")
+
 _P = C.c_void_p
 _I = C.c_int
 _D = C.c_double
@@ -121,6 +127,9 @@ _SIGNATURES = {
     "impes_model_balances": ([_P, C.POINTER(SatStats), _P], _I),
     "impes_model_reset_balances": ([_P, _P], _I),
     "impes_well_states": ([_P, C.POINTER(WellState), _P], _I),
+    "impes_timing_enable": ([_I], _I),
+    "impes_timing_collect": ([C.POINTER(Timing)], _I),
+    "impes_kernel_launches": ([], C.c_ulonglong),
 }
 
 EXPORTED = tuple(_SIGNATURES)
@@ -154,6 +163,21 @@ def ptr(t) -> int | None:
     if not t.is_contiguous():
         raise ValueError("tensor must be contiguous")
     return t.data_ptr()
+
+
+def timing_enable(on: bool = True):
+    check(lib.impes_timing_enable(1 if on else 0), "impes_timing_enable")
+
+
+def timing_collect() -> dict:
+    """{phase: (launches, total ms, algorithmic bytes)} since the last collect."""
+    t = Timing()
+    check(lib.impes_timing_collect(C.byref(t)), "impes_timing_collect")
+    return {name: (int(t.count[k]), float(t.ms[k]), float(t.bytes[k])) for k, name in enumerate(PHASES)}
+
+
+def kernel_launches() -> int:
+    return int(lib.impes_kernel_launches())
 
 
 def stream_of(device=None) -> int:

@@ -477,8 +477,16 @@ class Simulator:
         """One time step (simulation.py:126-135)."""
         return self._impes_step(dt)
 
+    def _set_well_cells(self):
+        # simulation.py:1629-1630 replaces the x-fastest index with (i*ny + j)*nz + k
+        r = self.reservoir
+        for w in self.well_manager.get_wells():
+            w.cell_index_flat = (w.i * r.ny + w.j) * r.nz + w.k
+
     def _impes_step(self, dt):
-        """``_impes_step`` (simulation.py:822-865): one attempt on the device."""
+        """``_impes_step`` (simulation.py:822-865).  A pressure solve that misses its
+        tolerance leaves the state untouched and is retried with dt divided by
+        ``dt_reduction_factor``, up to ``max_time_step_attempts`` attempts."""
         self._ensure_amg()
         fl = self.fluid
         for name in ("pressure", "s_w", "s_g"):
@@ -488,22 +496,32 @@ class Simulator:
         if fl.s_o.dtype != torch.float64 or fl.s_o.device != self.device or not fl.s_o.is_contiguous():
             fl.s_o = torch.empty_like(fl.s_w)
         kp = self.krylov_params()
-        ks, ss = _lib.KrylovStats(), _lib.SatStats()
+        ks = _lib.KrylovStats()
         solver = 0 if self.pressure_solver == "amg" else 1
         if self.pressure_solver not in ("amg", "gmres_amg", "cg", "cg_amg"):
             raise ValueError(f"unknown pressure_solver {self.pressure_solver!r}")
-        with torch.cuda.device(self.device):
-            check(lib.impes_step(self._h, self._amg_h, ptr(fl.pressure), ptr(fl.s_w), ptr(fl.s_g),
-                                 ptr(fl.s_o), float(dt), solver, C.byref(kp), self.amg_max_cycles,
-                                 C.byref(ks), None, _lib.stream_of(self.device)), "impes_step")
-        self.last_krylov = {"iterations": ks.iterations, "restarts": ks.restarts,
-                            "converged": bool(ks.converged), "rel_res": ks.rel_res,
-                            "true_rel_res": ks.true_rel_res}
-        fl.prev_pressure = fl.pressure.clone()
-        fl.prev_sw = fl.s_w.clone()
-        self._wells_stale = True
-        self.step_count += 1
-        return True
+        max_attempts = int(self.sim_params.get("max_time_step_attempts", 5))
+        factor = float(self.sim_params.get("dt_reduction_factor", 2.0))
+        current_dt = float(dt)
+        self._set_well_cells()
+        for _ in range(max(1, max_attempts)):
+            with torch.cuda.device(self.device):
+                st = lib.impes_step(self._h, self._amg_h, ptr(fl.pressure), ptr(fl.s_w), ptr(fl.s_g),
+                                    ptr(fl.s_o), current_dt, solver, C.byref(kp), self.amg_max_cycles,
+                                    C.byref(ks), None, _lib.stream_of(self.device))
+            self.last_krylov = {"iterations": ks.iterations, "restarts": ks.restarts,
+                                "converged": bool(ks.converged), "rel_res": ks.rel_res,
+                                "true_rel_res": ks.true_rel_res, "dt": current_dt}
+            if st == _lib.ERR_NOT_CONVERGED:
+                current_dt /= factor
+                continue
+            check(st, "impes_step")
+            fl.prev_pressure = fl.pressure.clone()
+            fl.prev_sw = fl.s_w.clone()
+            self._wells_stale = True
+            self.step_count += 1
+            return True
+        return False
 
     # ------------------------------------------------------- diagnostics
     def _balances(self):
@@ -571,6 +589,7 @@ class Simulator:
         rhs = torch.empty(p.numel(), dtype=torch.float64, device=self.device)
         check(lib.impes_assemble(self._h, ptr(p), ptr(s_w), ptr(s_g), float(dt), ptr(val), ptr(rhs),
                                  _lib.stream_of(self.device)), "impes_assemble")
+        self._set_well_cells()
         self._wells_stale = True
         return rowptr, col, val, rhs
 

@@ -1,0 +1,39 @@
+"""Helpers shared by the GPU parity tests."""
+import json
+
+import numpy as np
+import scipy.sparse as sp
+
+from oracle.impes import Model
+
+
+def cfg_fields(g):
+    cfg = json.loads(str(g["cfg"]))
+    fields = {k: g[k] for k in ("kx", "ky", "kz", "poro")}
+    return cfg, fields
+
+
+def oracle_model(g):
+    cfg, f = cfg_fields(g)
+    return Model(cfg, f["kx"], f["ky"], f["kz"], f["poro"])
+
+
+def gpu_sim(cfg, fields, **amg):
+    from impes_b200.simulator import build_from_config
+    cfg = json.loads(json.dumps(cfg))
+    cfg.setdefault("simulation", {}).setdefault("amg", {}).update(amg)
+    return build_from_config(cfg, fields, device="cuda")
+
+
+def to_np(t):
+    return t.detach().reshape(-1).cpu().numpy()
+
+
+def rel_max(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def csr_from(rowptr, col, val, n, m=None):
+    return sp.csr_matrix((to_np(val) if hasattr(val, "cpu") else val,
+                          to_np(col) if hasattr(col, "cpu") else col,
+                          to_np(rowptr) if hasattr(rowptr, "cpu") else rowptr), shape=(n, m or n))

@@ -9,7 +9,8 @@ from conftest import REPO
 def declared_functions():
     src = open(os.path.join(REPO, "include", "impes_b200.h")).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return sorted(set(re.findall(r"^\s*(?:const\s+)?\w+\s*\*?\s*(impes_\w+)\s*\(", src, flags=re.M)))
+    return sorted(set(re.findall(r"^\s*(?:const\s+|unsigned\s+|long\s+)*\w+\s*\*?\s*(impes_\w+)\s*\(",
+                                 src, flags=re.M)))
 
 
 def test_library_exports_every_declared_symbol():

@@ -1,0 +1,164 @@
+"""Full IMPES steps on the GPU against the reference trajectories (direct-solve
+pressure oracle) and the drop-in API."""
+import json
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from gpu_util import cfg_fields, gpu_sim, oracle_model, to_np
+
+pytestmark = pytest.mark.gpu
+
+CASES = ["two_phase_32x32", "two_phase_64x64", "two_phase_16x16x2", "black_oil_10x10x4",
+         "gas_injection_12x12x3"]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("name", CASES)
+def test_trajectory_matches_reference(golden, name, precision):
+    """p to 1e-8 relative and Sw/Sg to 1e-8 absolute at every step against the
+    reference's trajectory with an exact pressure solve."""
+    g = golden(name)
+    cfg, f = cfg_fields(g)
+    _, fl, _, sim = gpu_sim(cfg, f, tol=1e-13, norm="jacobi", precision=precision, max_iters=400,
+                            restart=40)
+    dt = float(g["dt"])
+    for s in range(g["p"].shape[0]):
+        sim.run_step(dt)
+        p = to_np(fl.pressure)
+        assert np.abs(p - g["p"][s]).max() <= 1e-8 * np.abs(g["p"][s]).max(), (s, sim.last_krylov)
+        assert np.abs(to_np(fl.s_w) - g["sw"][s]).max() <= 1e-8
+        assert np.abs(to_np(fl.s_g) - g["sg"][s]).max() <= 1e-8
+    mb = sim.mass_balance
+    got = np.array([mb[ph][io] for ph in ("water", "oil", "gas") for io in ("in", "out")])
+    ref = g["balances"][-1][:6]
+    assert np.all(np.abs(got - ref) <= 1e-6 * np.maximum(np.abs(ref), 1e-9))
+
+
+def test_reference_vcycle_mode_matches_oracle(golden):
+    """pressure_solver='amg': stand-alone V-cycles with the reference's stopping
+    rule, compared with the oracle's restatement of amg_solve (same tie-break)."""
+    from oracle.amg import AMGSolver
+    g = golden("two_phase_32x32")
+    cfg, f = cfg_fields(g)
+    cfg["simulation"]["pressure_solver"] = "amg"
+    _, fl, _, sim = gpu_sim(cfg, f, tol=1e-30, max_cycles=6, coarsest_size=50, seed=4)
+    m = oracle_model(g)
+    solver = AMGSolver(tol=1e-30, max_cycles=6, coarsest_size=50, seed=4)
+    dt = float(g["dt"])
+    for _ in range(2):
+        sim.run_step(dt)
+        m.step(dt, solve=solver)
+        p = to_np(fl.pressure)
+        assert np.abs(p - m.p).max() <= 1e-7 * np.abs(m.p).max()
+        assert np.abs(to_np(fl.s_w) - m.sw).max() <= 1e-7
+
+
+def test_mixed_precision_drift_small(golden):
+    """fp32 V-cycle inside fp64 FGMRES: saturation drift vs the fp64 path < 1e-6."""
+    g = golden("black_oil_10x10x4")
+    cfg, f = cfg_fields(g)
+    _, f64, _, s64 = gpu_sim(cfg, f, tol=1e-10, precision="fp64")
+    _, f32, _, s32 = gpu_sim(cfg, f, tol=1e-10, precision="mixed")
+    for _ in range(5):
+        s64.run_step(float(g["dt"]))
+        s32.run_step(float(g["dt"]))
+    assert np.abs(to_np(f64.s_w) - to_np(f32.s_w)).max() < 1e-6
+    assert np.abs(to_np(f64.pressure) - to_np(f32.pressure)).max() < 1e-6 * to_np(f64.pressure).max()
+
+
+def test_step_is_deterministic(golden):
+    g = golden("two_phase_16x16x2")
+    cfg, f = cfg_fields(g)
+    outs = []
+    for _ in range(2):
+        _, fl, _, sim = gpu_sim(cfg, f, tol=1e-10)
+        for _ in range(3):
+            sim.run_step(float(g["dt"]))
+        outs.append((fl.pressure.clone(), fl.s_w.clone()))
+    assert torch.equal(outs[0][0], outs[1][0]) and torch.equal(outs[0][1], outs[1][1])
+
+
+def test_dropin_modules_and_json_schema(tmp_path):
+    """The reference's import paths and both well schemas; PVT from a JSON file."""
+    from impes_b200 import scenarios
+    from simulator.fluid import Fluid
+    from simulator.reservoir import Reservoir
+    from simulator.simulation import Simulator
+    from simulator.well import WellManager
+    from solver.pressure_amg import amg_solve
+    from solver.classical_amg import ClassicalAMG  # noqa: F401
+    pvt_path = tmp_path / "pvt.json"
+    pvt_path.write_text(json.dumps(scenarios.pvt_table_black_oil()))
+    cfg = {
+        "reservoir": {"dimensions": [8, 6, 3], "grid_size": [10.0, 10.0, 4.0], "porosity": 0.22,
+                      "permeability": 120.0, "k_vertical_fraction": 0.2},
+        "fluid": {"pressure": 22.0, "s_w": 0.25, "s_g": 0.02, "pvt_path": str(pvt_path),
+                  "relative_permeability": {"model": "stone2", "nw": 2, "ng": 2.5}},
+        "wells": [
+            {"name": "I", "type": "injector", "coordinates": [0, 0, 1], "radius": 0.1,
+             "control": {"type": "rate", "value": 20.0}, "injected_phase": "water"},
+            {"name": "P", "type": "producer", "i": 7, "j": 5, "k": 1, "radius": 0.1,
+             "control_type": "bhp", "control_value": 18.0},
+        ],
+        "simulation": {"solver_type": "impes", "pressure_solver": "gmres_amg",
+                       "amg": {"tol": 1e-12, "max_iters": 300}},
+    }
+    dev = torch.device("cuda")
+    res = Reservoir(cfg["reservoir"], dev)
+    wm = WellManager(cfg["wells"], res)
+    fl = Fluid(cfg["fluid"], res, dev)
+    sim = Simulator(res, fl, wm, cfg["simulation"], dev)
+    assert sim.run_step(86400.0)
+    from oracle.impes import Model
+    m = Model(cfg)
+    m.step(86400.0)
+    assert np.abs(to_np(fl.pressure) - m.p).max() <= 1e-8 * np.abs(m.p).max()
+    assert np.abs(to_np(fl.s_w) - m.sw).max() <= 1e-8
+    assert np.abs(to_np(fl.s_g) - m.sg).max() <= 1e-8
+    assert wm.get_wells()[1].cell_index_flat == (7 * 6 + 5) * 3 + 1
+    # amg_solve keeps the reference's signature and returns b's dtype
+    rowptr, col, val, rhs = sim.assemble(86400.0)
+    A = torch.sparse_csr_tensor(rowptr.long(), col.long(), val, size=(rhs.numel(),) * 2)
+    x = amg_solve(A, rhs.float(), tol=1e-6, max_cycles=5)
+    assert x.dtype == torch.float32 and x.shape == rhs.shape
+
+
+def test_bhp_min_autoswitch_and_limits():
+    """bhp_min never reduces the outflow (the reference's assertion,
+    tests/test_phase_limits_and_autoswitch.py:70-71).  With the reference's sign
+    convention the producer's required BHP is p_block + |q|/(WI lambda), never
+    below bhp_min, so the switch at simulation.py:1636-1650 does not fire; a
+    surface oil limit throttles the rate."""
+    from impes_b200 import scenarios
+    from impes_b200.simulator import build_from_config
+    base = {
+        "reservoir": {"dimensions": [5, 5, 1], "grid_size": [10, 10, 10], "porosity": 0.2,
+                      "permeability": 100.0, "k_vertical_fraction": 1.0},
+        "fluid": {"pressure": 10.0, "s_w": 0.2, "s_g": 0.0, "pvt": {"table": scenarios.pvt_table_black_oil()}},
+        "simulation": {"solver_type": "impes", "amg": {"tol": 1e-12, "coarsest_size": 10}},
+    }
+    cfg1 = json.loads(json.dumps(base))
+    cfg1["wells"] = [{"name": "P1", "type": "producer", "i": 2, "j": 2, "k": 0, "radius": 0.1,
+                      "control_type": "rate", "control_value": 20000.0}]
+    cfg2 = json.loads(json.dumps(base))
+    cfg2["wells"] = [{"name": "P2", "type": "producer", "i": 2, "j": 2, "k": 0, "radius": 0.1,
+                      "control_type": "rate", "control_value": 20000.0, "bhp_min": 9.5}]
+    _, _, wm1, s1 = build_from_config(cfg1, device="cuda")
+    _, _, wm2, s2 = build_from_config(cfg2, device="cuda")
+    s1.run_step(86400.0)
+    s2.run_step(86400.0)
+    q1 = abs(wm1.get_wells()[0].last_q_total or 0.0)
+    q2 = abs(wm2.get_wells()[0].last_q_total or 0.0)
+    assert q2 <= q1 + 1e-9
+    assert wm1.get_wells()[0].last_mode == "rate" and wm2.get_wells()[0].last_mode == "rate"
+    cfg3 = json.loads(json.dumps(base))
+    cfg3["fluid"].update({"pressure": 20.0, "s_w": 0.3, "s_g": 0.02})
+    cfg3["wells"] = [{"name": "PS", "type": "producer", "i": 2, "j": 2, "k": 0, "radius": 0.1,
+                      "control_type": "rate", "control_value": 50000.0, "rate_type": "surface",
+                      "surface_phase": "oil", "limits": {"wopr": 100.0}}]
+    _, _, wm3, s3 = build_from_config(cfg3, device="cuda")
+    s3.run_step(86400.0)
+    assert wm3.get_wells()[0].last_surface_rates["oil"] <= 100.0 * 1.10
