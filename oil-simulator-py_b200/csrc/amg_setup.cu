@@ -500,22 +500,44 @@ __global__ void k_max_i32(long long n, const int* v, int* out) {
   if ((threadIdx.x & 31) == 0) atomicMax(out, m);
 }
 
+// max of the bounds that stay in shared memory
+__global__ void k_max_narrow(long long n, const int* v, int limit, int* out) {
+  int m = 0;
+  GRID_LOOP(i, n) if (v[i] <= limit) m = max(m, v[i]);
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_down_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
 __device__ __forceinline__ unsigned hash_slot(int key, unsigned mask) {
   return ((unsigned)key * 2654435761u) & mask;
 }
-// One warp per output row.  Pass 1 (cols == nullptr): count distinct columns.
+// Hash capacity of a row with `bound` candidates: power of two >= 2*bound.
+__host__ __device__ __forceinline__ int hash_cap(int bound) {
+  int h = 32;
+  while (h < 2 * bound) h <<= 1;
+  return h;
+}
+// Rows with more than kWideBound candidates keep their hash table in global
+// scratch (offset goff[r], table + list of cap ints each); others use shared memory.
+constexpr int kWideBound = 2048;
+__global__ void k_wide_size(int rows, const int* bound, long long* gsize) {
+  GRID_LOOP(r, rows) gsize[r] = bound[r] > kWideBound ? 2LL * hash_cap(bound[r]) : 0LL;
+}
+
+// One warp per output row.  Pass 1 (outcol == nullptr): count distinct columns.
 // Pass 2: write the sorted distinct columns at outptr[row].
 __global__ void k_union_rows(int rows, const int* optr, const int* ocol, const int* iptr,
-                             const int* icol, int hsize, int* ucnt, const int* outptr,
-                             int* outcol) {
+                             const int* icol, int hsize, const int* bound, const long long* goff,
+                             int* gscratch, int* ucnt, const int* outptr, int* outcol) {
   extern __shared__ int sh[];
   const int wpb = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int* table = sh + warp * (2 * hsize + 1);
-  int* list = table + hsize;
-  int* lcount = list + hsize;
-  const unsigned mask = (unsigned)hsize - 1;
+  int* lcount = sh + warp * (2 * hsize + 1);
   for (long long r = (long long)blockIdx.x * wpb + warp; r < rows; r += (long long)gridDim.x * wpb) {
-    for (int s = lane; s < hsize; s += 32) table[s] = -1;
+    const bool wide = bound[r] > kWideBound;
+    const int cap = wide ? hash_cap(bound[r]) : hsize;
+    int* table = wide ? gscratch + goff[r] : lcount + 1;
+    int* list = table + cap;
+    const unsigned mask = (unsigned)cap - 1;
+    for (int q = lane; q < cap; q += 32) table[q] = -1;
     if (lane == 0) *lcount = 0;
     __syncwarp();
     for (int e = optr[r]; e < optr[r + 1]; ++e) {
@@ -532,6 +554,7 @@ __global__ void k_union_rows(int rows, const int* optr, const int* ocol, const i
       }
       __syncwarp();
     }
+    __threadfence_block();
     __syncwarp();
     const int u = *lcount;
     if (outcol == nullptr) {
@@ -731,28 +754,41 @@ void union_symbolic(AMG& h, int rows, const int* optr, const int* ocol, const in
                     cudaStream_t s) {
   DBuf<int> bound(rows), ucnt(rows + 1);
   k_union_bound<<<grid_for(rows, TB), TB, 0, s>>>(rows, optr, ocol, iptr, bound.p); ::impes::count_launch();
+  IMPES_CHECK_LAUNCH();
+  // global scratch for the wide rows
+  DBuf<long long> gsize(rows + 1), goff(rows + 1);
+  k_wide_size<<<grid_for(rows, TB), TB, 0, s>>>(rows, bound.p, gsize.p); ::impes::count_launch();
+  IMPES_CHECK_LAUNCH();
+  std::vector<long long> hs(rows);
+  IMPES_CUDA(cudaMemcpyAsync(hs.data(), gsize.p, sizeof(long long) * rows, cudaMemcpyDeviceToHost, s));
+  IMPES_CUDA(cudaStreamSynchronize(s));
+  std::vector<long long> ho(rows + 1, 0);
+  for (int r = 0; r < rows; ++r) ho[r + 1] = ho[r] + hs[r];
+  IMPES_CUDA(cudaMemcpyAsync(goff.p, ho.data(), sizeof(long long) * (rows + 1), cudaMemcpyHostToDevice, s));
+  DBuf<int> gscratch(std::max<long long>(ho[rows], 1));
+  // shared-memory table size for the narrow rows
   IMPES_CUDA(cudaMemsetAsync(h.iflag.p, 0, sizeof(int), s));
-  k_max_i32<<<grid_for(rows, TB), TB, 0, s>>>(rows, bound.p, h.iflag.p); ::impes::count_launch();
-  int maxc = to_host_int(h, h.iflag.p, s);
-  int hsize = 32;
-  while (hsize < 2 * maxc) hsize <<= 1;
-  size_t per_warp = sizeof(int) * (2 * (size_t)hsize + 1);
-  int wpb = (int)std::max<size_t>(1, std::min<size_t>(8, (48u << 10) / per_warp));
-  size_t smem = per_warp * wpb;
-  IMPES_REQUIRE(smem <= (200u << 10), IMPES_ERR_ARG, "Galerkin row too wide for the hash table");
+  k_max_narrow<<<grid_for(rows, TB), TB, 0, s>>>(rows, bound.p, kWideBound, h.iflag.p); ::impes::count_launch();
+  IMPES_CHECK_LAUNCH();
+  const int maxc = to_host_int(h, h.iflag.p, s);
+  const int hsize = hash_cap(maxc);
+  const size_t per_warp = sizeof(int) * (2 * (size_t)hsize + 1);
+  const int wpb = (int)std::max<size_t>(1, std::min<size_t>(8, (64u << 10) / per_warp));
+  const size_t smem = per_warp * wpb;
   IMPES_CUDA(cudaFuncSetAttribute(k_union_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   unsigned grid = (unsigned)std::min<long long>((rows + wpb - 1) / wpb, (long long)num_sms() * 32);
-  k_union_rows<<<std::max(1u, grid), 32 * wpb, smem, s>>>(rows, optr, ocol, iptr, icol, hsize,
-                                                          ucnt.p, nullptr, nullptr); ::impes::count_launch();
+  k_union_rows<<<std::max(1u, grid), 32 * wpb, smem, s>>>(rows, optr, ocol, iptr, icol, hsize, bound.p,
+                                                          goff.p, gscratch.p, ucnt.p, nullptr, nullptr); ::impes::count_launch();
   IMPES_CHECK_LAUNCH();
   outptr.alloc(rows + 1);
   int nnz = exclusive_scan_i32(ucnt.p, outptr.p, rows, s);
   outcol.alloc(std::max(nnz, 1));
-  k_union_rows<<<std::max(1u, grid), 32 * wpb, smem, s>>>(rows, optr, ocol, iptr, icol, hsize,
-                                                          nullptr, outptr.p, outcol.p); ::impes::count_launch();
+  k_union_rows<<<std::max(1u, grid), 32 * wpb, smem, s>>>(rows, optr, ocol, iptr, icol, hsize, bound.p,
+                                                          goff.p, gscratch.p, nullptr, outptr.p, outcol.p); ::impes::count_launch();
   IMPES_CHECK_LAUNCH();
   IMPES_CUDA(cudaMemsetAsync(h.iflag.p, 0, sizeof(int), s));
   k_max_i32<<<grid_for(rows, TB), TB, 0, s>>>(rows, ucnt.p, h.iflag.p); ::impes::count_launch();
+  IMPES_CHECK_LAUNCH();
   maxrow = to_host_int(h, h.iflag.p, s);
 }
 

@@ -32,12 +32,18 @@ def _lognormal(rng, shape, mean_md, sigma):
     return np.exp(math.log(mean_md) + sigma * rng.standard_normal(shape)) * MD
 
 
-def pvt_table_black_oil(rows: int = 20, p_lo: float = 5.0, p_hi: float = 40.0) -> dict:
+def pvt_table_black_oil(rows: int = 20, p_lo: float = 5.0, p_hi: float = 40.0,
+                        bo_increasing: bool = False) -> dict:
     """Monotone synthetic black-oil table over ``p_lo..p_hi`` MPa.
 
-    Bo 1.1 -> 1.3, Rs 0 -> 150, mu_o 3 -> 1.5 cP, mu_g 0.012 -> 0.025 cP (all
-    linear in p); Bg 0.02 -> 0.003 as ``a/p + b`` through both end points;
+    Bo spans 1.1..1.3, Rs 0 -> 150, mu_o 3 -> 1.5 cP, mu_g 0.012 -> 0.025 cP
+    (all linear in p); Bg 0.02 -> 0.003 as ``a/p + b`` through both end points;
     water is slightly compressible (Bw 1.02 -> 1.00) with mu_w 0.5 cP; Rv is 0.
+
+    Bo decreases with pressure by default (1.3 at p_lo to 1.1 at p_hi).  The
+    reference's total compressibility c_o = -(1/Bo) dBo/dP (fluid.py:190-222) has
+    no dissolved-gas term, so a Bo that grows with pressure (``bo_increasing``)
+    makes c_t negative and the pressure matrix indefinite.
     """
     p = np.linspace(p_lo, p_hi, rows)
     t = (p - p_lo) / (p_hi - p_lo)
@@ -45,7 +51,7 @@ def pvt_table_black_oil(rows: int = 20, p_lo: float = 5.0, p_hi: float = 40.0) -
     b = 0.02 - a / p_lo
     return {
         "pressure_MPa": p.tolist(),
-        "Bo": (1.1 + 0.2 * t).tolist(),
+        "Bo": ((1.1 + 0.2 * t) if bo_increasing else (1.3 - 0.2 * t)).tolist(),
         "Bw": (1.02 - 0.02 * t).tolist(),
         "Bg": (a / p + b).tolist(),
         "mu_o_cP": (3.0 - 1.5 * t).tolist(),
@@ -111,13 +117,13 @@ def _black_oil_fluid(pvt):
 
 
 def black_oil_5spot(seed: int = 1, nx: int = 100, ny: int = 100, nz: int = 20, steps: int = 50,
-                    inj_rate: float = 200.0, dt_days: float = 5.0):
+                    inj_rate: float = 200.0, dt_days: float = 5.0, bo_increasing: bool = False):
     """Three-phase black oil: ln kx ~ N(ln 200 mD, 0.8^2) per cell, ky=kx, kz=0.1 kx."""
     rng = np.random.default_rng(seed)
     shape = (nx, ny, nz)
     kx = _lognormal(rng, shape, 200.0, 0.8)
     poro = 0.15 + 0.10 * rng.random(shape)
-    pvt = pvt_table_black_oil()
+    pvt = pvt_table_black_oil(bo_increasing=bo_increasing)
     km = nz // 2
     inj = [(0, 0), (nx - 1, 0), (0, ny - 1), (nx - 1, ny - 1)]
     wells = [{"name": f"INJ{n}", "type": "injector", "i": i, "j": j, "k": km, "radius": 0.1,
@@ -157,22 +163,38 @@ def _gaussian_smooth(z, sigma=2.5, radius=5):
 
 def gas_injection_1m(seed: int = 2, nx: int = 200, ny: int = 200, nz: int = 25, steps: int = 20,
                      dt_days: float = 2.0, gas_rate: float = 2.0e5, n_inj_side: int = 3,
-                     n_prod_side: int = 4):
-    """Gas-injection stress case: ln k ~ N(ln 150 mD, 1.0^2) Gaussian-correlated (radius 5)."""
+                     n_prod_side: int = 4, surface_units: bool = False, bo_increasing: bool = False):
+    """Gas-injection stress case: ln k ~ N(ln 150 mD, 1.0^2) Gaussian-correlated (radius 5).
+
+    ``gas_rate`` is in sm3/d.  By default each injector is given the equivalent
+    reservoir rate, gas_rate * Bg(initial pressure), as a ``rate_type:
+    "reservoir"`` well: the reference's pressure step injects a surface-rate
+    well's number unconverted, as reservoir m3/s (simulation.py:1626-1634, while
+    the saturation step converts it with Bg at :1061-1064), which at 2e5 sm3/d
+    drives the explicit saturation update out of range.  ``surface_units=True``
+    keeps the literal surface-rate wells.
+    """
     rng = np.random.default_rng(seed)
     shape = (nx, ny, nz)
     z = _gaussian_smooth(rng.standard_normal(shape))
     kx = np.exp(math.log(150.0) + 1.0 * z) * MD
     poro = 0.15 + 0.10 * rng.random(shape)
-    pvt = pvt_table_black_oil()
+    pvt = pvt_table_black_oil(bo_increasing=bo_increasing)
+    p0 = 25.0
+    bg0 = float(np.interp(p0, pvt["pressure_MPa"], pvt["Bg"]))
     km = nz // 2
     wells = []
     for a in range(n_inj_side):
         for b in range(n_inj_side):
             i = int((a + 0.5) * nx / n_inj_side); j = int((b + 0.5) * ny / n_inj_side)
-            wells.append({"name": f"GI{a}{b}", "type": "injector", "i": i, "j": j, "k": km,
-                          "radius": 0.1, "control_type": "rate", "control_value": gas_rate,
-                          "injected_phase": "gas", "rate_type": "surface"})
+            if surface_units:
+                wells.append({"name": f"GI{a}{b}", "type": "injector", "i": i, "j": j, "k": km,
+                              "radius": 0.1, "control_type": "rate", "control_value": gas_rate,
+                              "injected_phase": "gas", "rate_type": "surface"})
+            else:
+                wells.append({"name": f"GI{a}{b}", "type": "injector", "i": i, "j": j, "k": km,
+                              "radius": 0.1, "control_type": "rate", "control_value": gas_rate * bg0,
+                              "injected_phase": "gas", "rate_type": "reservoir"})
     for a in range(n_prod_side):
         for b in range(n_prod_side):
             i = int(a * (nx - 1) / max(n_prod_side - 1, 1)); j = int(b * (ny - 1) / max(n_prod_side - 1, 1))

@@ -568,6 +568,19 @@ class Simulator:
             w.cell_index_flat = int(c)
         self._wells_stale = False
 
+    def amg_levels(self):
+        """[(n, nnz, p_cols, p_nnz, is_coarsest)] of the pressure hierarchy."""
+        if self._amg_h is None:
+            return []
+        nl = C.c_int(0)
+        check(lib.impes_amg_num_levels(self._amg_h, C.byref(nl)))
+        out = []
+        for l in range(nl.value):
+            d = _lib.LevelDesc()
+            check(lib.impes_amg_level_info(self._amg_h, l, C.byref(d)))
+            out.append((d.n, d.nnz, d.p_cols, d.p_nnz, bool(d.is_coarsest)))
+        return out
+
     # --------------------------------------------------- building blocks
     def csr_pattern(self):
         n, nnz = C.c_int(), C.c_int()

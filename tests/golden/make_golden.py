@@ -30,8 +30,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
 REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-sys.path[:0] = [os.path.join(HERE, "_stubs"), os.path.join(REF, "src"),
-                os.path.join(REPO, "oil-simulator-py_b200"), REPO]
+sys.path[:0] = [os.path.join(HERE, "_stubs"), os.path.join(REF, "src"), REPO]
 
 import torch  # noqa: E402
 import scipy.sparse as sp  # noqa: E402
@@ -47,8 +46,21 @@ from simulator.simulation import Simulator  # noqa: E402
 import solver.pressure_amg as pamg  # noqa: E402
 from solver.classical_amg import ClassicalAMG  # noqa: E402
 
-from impes_b200 import scenarios  # noqa: E402  (input generator only)
 from oracle.amg import tiebreak  # noqa: E402  (the shared tie-break definition)
+
+
+def _load_scenarios():
+    # the input generator, loaded by path: putting the package directory on
+    # sys.path would shadow the reference's namespace package ``solver``
+    import importlib.util
+    path = os.path.join(REPO, "oil-simulator-py_b200", "impes_b200", "scenarios.py")
+    spec = importlib.util.spec_from_file_location("scenarios_for_fixtures", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+scenarios = _load_scenarios()
 
 
 def _eval_pvt64(self, p_tensor, key):
@@ -205,7 +217,7 @@ def main():
     # (the 2e5 sm3/d stress rate makes the reference's own saturation update diverge
     # on small grids, so the trajectory fixture uses a rate its explicit update can carry)
     cfg, f = scenarios.gas_injection_1m(seed=2, nx=12, ny=12, nz=3, steps=4, gas_rate=1.0e2,
-                                        n_inj_side=1, n_prod_side=2)
+                                        n_inj_side=1, n_prod_side=2, surface_units=True)
     cfg["fluid"]["capillary_pressure_og"] = {"pc_scale": 2.0e4, "pc_exponent": 1.5}
     cfg["wells"].append({"name": "PS", "type": "producer", "i": 6, "j": 2, "k": 0, "radius": 0.1,
                          "control_type": "rate", "control_value": 5.0, "rate_type": "surface",

@@ -100,8 +100,10 @@ def test_dropin_modules_and_json_schema(tmp_path):
         "wells": [
             {"name": "I", "type": "injector", "coordinates": [0, 0, 1], "radius": 0.1,
              "control": {"type": "rate", "value": 20.0}, "injected_phase": "water"},
+            # a rate producer: a BHP producer's saturation-step rate WI*lambda*(p - p_bhp)
+            # is the rounding of p when the cell sits at p_bhp (simulation.py:1297)
             {"name": "P", "type": "producer", "i": 7, "j": 5, "k": 1, "radius": 0.1,
-             "control_type": "bhp", "control_value": 18.0},
+             "control_type": "rate", "control_value": 15.0},
         ],
         "simulation": {"solver_type": "impes", "pressure_solver": "gmres_amg",
                        "amg": {"tol": 1e-12, "max_iters": 300}},
