@@ -78,7 +78,9 @@ def run_cpu_reference(steps: int, warmup: int):
     from oracle.impes import Model
     cfg, f = cpu_sample_workload()
     m = Model(cfg, f["kx"], f["ky"], f["kz"], f["poro"], pvt_table=f["pvt"])
-    solver = AMGSolver(tol=1e-6, max_cycles=40, theta=0.25, max_levels=10, coarsest_size=200, seed=0)
+    a = cfg["simulation"]["amg"]
+    solver = AMGSolver(tol=1e-6, max_cycles=40, theta=a["theta"], max_levels=a["max_levels"],
+                       coarsest_size=a["coarsest_size"], seed=0)
     dt = 2 * 86400.0
     for _ in range(max(warmup, 1)):       # the first step builds the hierarchy
         m.step(dt, solve=solver)
@@ -146,12 +148,14 @@ class ClockSampler:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
-def make_sim(cfg, fields, precision, device):
+def make_sim(cfg, fields, precision, device, restart=30, solver="gmres_amg"):
+    """FGMRES + V-cycle (solver="gmres_amg"), or the plain stand-alone V-cycles of
+    the reference (solver="amg"), both stopping at PRESSURE_TOL in the Jacobi norm."""
     from impes_b200.simulator import build_from_config
     c = json.loads(json.dumps(cfg))
-    c["simulation"]["pressure_solver"] = "gmres_amg"
+    c["simulation"]["pressure_solver"] = solver
     c["simulation"]["amg"].update({"tol": PRESSURE_TOL, "norm": "jacobi", "precision": precision,
-                                   "restart": 30, "max_iters": 400, "seed": 0})
+                                   "restart": restart, "max_iters": 600, "max_cycles": 3000, "seed": 0})
     return build_from_config(c, fields, device=device)
 
 
@@ -223,7 +227,11 @@ def run_ours(args, world, rank, local):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=device)
-    cfg, fields = scenarios.gas_injection_1m(seed=2)
+    if args.grid:
+        nx, ny, nz = (int(v) for v in args.grid.lower().split("x"))
+        cfg, fields = scenarios.gas_injection_1m(seed=2, nx=nx, ny=ny, nz=nz)
+    else:
+        cfg, fields = scenarios.gas_injection_1m(seed=2)
     dt = cfg["simulation"]["time_step_days"] * 86400.0
     cells = cfg["reservoir"]["dimensions"][0] * cfg["reservoir"]["dimensions"][1] * cfg["reservoir"]["dimensions"][2]
     stream = torch.cuda.current_stream(device)
@@ -232,7 +240,7 @@ def run_ours(args, world, rank, local):
     results = {}
     precisions = ("fp64", "mixed") if args.precision == "both" else (args.precision,)
     for precision in precisions:
-        _, fl, _, sim = make_sim(cfg, fields, precision, device)
+        _, fl, _, sim = make_sim(cfg, fields, precision, device, restart=args.restart)
         torch.cuda.synchronize()
         t_setup = time.perf_counter()
         for _ in range(args.warmup):           # the first warm-up step builds the hierarchy
@@ -274,6 +282,25 @@ def run_ours(args, world, rank, local):
         torch.cuda.synchronize()
         torch.cuda.empty_cache()
 
+    plain = None
+    if args.precision == "both" and not args.no_plain:
+        # the plain FP64 GPU path: the reference's stand-alone V-cycles, fp64, to the
+        # same 1e-6 Jacobi-scaled residual (fewer timed steps: it is slow)
+        _, flp, _, simp = make_sim(cfg, fields, "fp64", device, solver="amg")
+        for _ in range(args.warmup):
+            simp.run_step(dt)
+        psteps = max(1, min(args.steps, 3))
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ms_p, it_p = time_steps(simp, psteps, dt, flush, stream)
+        tp = torch.tensor([ms_p], dtype=torch.float64, device=device)
+        if dist is not None:
+            dist.all_reduce(tp, op=dist.ReduceOp.MAX)
+        plain = dict(ms=float(tp.item()), iters=it_p, steps=psteps)
+        simp.close()
+        del simp, flp
+        torch.cuda.empty_cache()
     if dist is not None:
         dist.destroy_process_group()
     if rank != 0:
@@ -289,12 +316,15 @@ def run_ours(args, world, rank, local):
     steps = args.steps
     value = world * cells * steps / (mixed["ms"] / 1e3)
     fp64_value = world * cells * steps / (fp64["ms"] / 1e3)
-    # dominant kernel: the level-0 l1-Jacobi sweep of the mixed path
-    n_s, ms_s, by_s = mixed["phases"]["smooth_l0"]
+    # dominant kernel: the warp-per-row l1-Jacobi sweep of the dense coarse levels
+    # (k_csr<float,32,Y_SMOOTH>), timed per launch by the library's CUDA events
+    key = "smooth_wide" if mixed["phases"]["smooth_wide"][0] else "smooth_l0"
+    n_s, ms_s, by_s = mixed["phases"][key]
     avg_ms = ms_s / max(n_s, 1)
     bytes_launch = by_s / max(n_s, 1)
-    achieved = bytes_launch / (avg_ms / 1e3) / 1e9
-    traffic = read_traffic("smooth_l0")
+    achieved = by_s / (ms_s / 1e3) / 1e9
+    traffic = read_traffic(key)
+    n0, ms0, by0 = mixed["phases"]["smooth_l0"]
     share = {k: round(v[1] / mixed["ms"], 4) for k, v in mixed["phases"].items() if k != "solve"}
     drift_sw = float((results["mixed"]["sw"] - results["fp64"]["sw"]).abs().max())
     drift_p = float(((results["mixed"]["p"] - results["fp64"]["p"]).abs().max()
@@ -313,7 +343,7 @@ def run_ours(args, world, rank, local):
         "dtype": "f64 Krylov/assembly/saturation + f32 V-cycle",
         "data": "synthetic (seeded; no dataset)",
         "config": {"workload": WORKLOAD, "cells": cells, "precision": "mixed",
-                   "pressure_solver": "FGMRES(30) + RS-AMG V-cycle", "pressure_tol": PRESSURE_TOL,
+                   "pressure_solver": f"FGMRES({args.restart}) + RS-AMG V-cycle", "pressure_tol": PRESSURE_TOL,
                    "residual_norm": "||D^-1 r|| / ||D^-1 b|| (Jacobi-scaled)",
                    "l2": "flushed before every timed step (512 MiB write)",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
@@ -321,16 +351,24 @@ def run_ours(args, world, rank, local):
         "fp64": {"value": fp64_value, "ms_per_step": fp64["ms"] / steps,
                  "vcycles_per_step": statistics.mean(fp64["iters"]),
                  "mixed_speedup": fp64["ms"] / mixed["ms"]},
+        "plain_fp64_vcycle": None if plain is None else {
+            "value": world * cells * plain["steps"] / (plain["ms"] / 1e3),
+            "ms_per_step": plain["ms"] / plain["steps"], "steps_timed": plain["steps"],
+            "vcycles_per_step": statistics.mean(plain["iters"]),
+            "mixed_speedup": (plain["ms"] / plain["steps"]) / (mixed["ms"] / steps)},
         "mixed_vs_fp64_drift": {"sw_abs_max": drift_sw, "p_rel_max": drift_p},
         "setup_s": {"mixed": mixed["setup_s"], "fp64": fp64["setup_s"]},
         "phase_share": share,
         "e2e": {"value": world * cells * steps / (mixed["e2e_ms"] / 1e3), "unit": "cell-steps/s",
                 "h2d_bytes_per_step": mixed["e2e_bytes"], "d2h_bytes_per_step": mixed["e2e_bytes"]},
-        "roofline": {"kernel": "k_csr<float,1,Y_SMOOTH> (level-0 l1-Jacobi sweep)", "bound": "hbm",
-                     "achieved": achieved, "peak": hbm_peak, "peak_kind": peak_kind, "unit": "GB/s",
-                     "frac": achieved / hbm_peak, "traffic": traffic,
+        "roofline": {"kernel": ("k_csr<float,32,Y_SMOOTH> (l1-Jacobi sweep, levels with > 96 nnz/row)"
+                                if key == "smooth_wide" else "k_csr<float,1,Y_SMOOTH> (level-0 sweep)"),
+                     "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "peak_kind": peak_kind,
+                     "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": traffic,
                      "bytes_per_launch": bytes_launch, "avg_launch_us": avg_ms * 1e3,
-                     "launches_timed": n_s},
+                     "launches_timed": n_s,
+                     "level0_sweep": {"achieved": by0 / max(ms0, 1e-9) * 1e3 / 1e9,
+                                      "avg_launch_us": ms0 / max(n0, 1) * 1e3, "launches_timed": n0}},
         "clocks": mixed["clocks"],
         "gpu_launches": mixed["launches"],
     }
@@ -366,6 +404,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--restart", type=int, default=60, help="FGMRES restart length")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 V-cycle baseline")
+    ap.add_argument("--grid", default=None,
+                    help="NXxNYxNZ: a smaller grid of the same workload (profiling captures only)")
     ap.add_argument("--precision", choices=["both", "mixed", "fp64"], default="both",
                     help="both (the benchmark line) or one path only (profiling runs)")
     args = ap.parse_args()

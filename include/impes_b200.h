@@ -109,9 +109,10 @@ int impes_amg_update(impes_amg* h, const double* val, void* stream);
 
 /* ClassicalAMG.solve (classical_amg.py:1108-1155): stand-alone V-cycles from
  * x0 = 0 until ||r_s||/||b_s|| < tol or max_cycles.  b, x: device, length n.
- * cycles/rel_res: host outputs (may be NULL). */
+ * cycles/rel_res: host outputs (may be NULL).  norm: IMPES_NORM_EQUILIBRATED (the
+ * reference's test) or IMPES_NORM_JACOBI. */
 int impes_amg_solve_vcycles(impes_amg* h, const double* b, double* x, double tol,
-                            int max_cycles, int* cycles, double* rel_res, void* stream);
+                            int max_cycles, int* cycles, double* rel_res, int norm, void* stream);
 
 /* ClassicalAMG.apply (classical_amg.py:1157-1180): `cycles` V-cycles, then
  * continue up to apply_max_cycles while ||r||/||b|| >= apply_tol. */
@@ -260,12 +261,13 @@ enum {
   IMPES_PH_SPMV_L0 = 5,    /* FGMRES operator product on level 0          */
   IMPES_PH_ORTHO = 6,      /* FGMRES Gram-Schmidt of one iteration        */
   IMPES_PH_SOLVE = 7,      /* whole pressure solve                        */
-  IMPES_NUM_PHASES = 8
+  IMPES_PH_SMOOTH_WIDE = 8,/* one l1-Jacobi sweep on a level with > 96 nnz per row (warp per row) */
+  IMPES_NUM_PHASES = 9
 };
 typedef struct {
-  long long count[8];   /* timed launches per phase                     */
-  double ms[8];         /* summed device time per phase                 */
-  double bytes[8];      /* summed algorithmic bytes per phase           */
+  long long count[9];   /* timed launches per phase                     */
+  double ms[9];         /* summed device time per phase                 */
+  double bytes[9];      /* summed algorithmic bytes per phase           */
 } impes_timing;
 int impes_timing_enable(int on);
 int impes_timing_collect(impes_timing* out);

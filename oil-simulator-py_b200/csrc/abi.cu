@@ -81,12 +81,12 @@ int impes_amg_update(impes_amg* h, const double* val, void* stream) {
 }
 
 int impes_amg_solve_vcycles(impes_amg* h, const double* b, double* x, double tol, int max_cycles,
-                            int* cycles, double* rel_res, void* stream) {
+                            int* cycles, double* rel_res, int norm, void* stream) {
   return guarded([&] {
     IMPES_REQUIRE(h && b && x, IMPES_ERR_ARG, "null argument");
     IMPES_REQUIRE(h->a.built, IMPES_ERR_STATE, "solve before setup");
     IMPES_REQUIRE(max_cycles >= 1, IMPES_ERR_ARG, "max_cycles must be >= 1");
-    amg_solve_vcycles(h->a, b, x, tol, max_cycles, cycles, rel_res, S(stream));
+    amg_solve_vcycles(h->a, b, x, tol, max_cycles, cycles, rel_res, S(stream), norm);
   });
 }
 
@@ -367,7 +367,7 @@ int impes_step(impes_model* h, impes_amg* amg, double* p, double* sw, double* sg
       if (solver == 0) {
         int cyc = 0;
         double rel = 0.0;
-        amg_solve_vcycles(a, m.rhs.p, p, kp->tol, std::max(1, max_cycles), &cyc, &rel, s);
+        amg_solve_vcycles(a, m.rhs.p, p, kp->tol, std::max(1, max_cycles), &cyc, &rel, s, kp->norm);
         st.iterations = cyc;
         st.rel_res = rel;
         st.true_rel_res = rel;
@@ -450,6 +450,14 @@ int impes_timing_collect(impes_timing* out) {
     IMPES_REQUIRE(out, IMPES_ERR_ARG, "null argument");
     impes_timing t{};
     PhaseTimers& T = timers();
+    IMPES_CUDA(cudaDeviceSynchronize());
+    T.harvest();
+    for (int q = 0; q < IMPES_NUM_PHASES; ++q) {
+      t.count[q] += T.acc_n[q];
+      t.ms[q] += T.acc_ms[q];
+      t.bytes[q] += T.acc_bytes[q];
+      T.acc_n[q] = 0; T.acc_ms[q] = 0.0; T.acc_bytes[q] = 0.0;
+    }
     for (auto& r : T.recs) {
       IMPES_CUDA(cudaEventSynchronize(r.b));
       float ms = 0.f;

@@ -28,6 +28,11 @@ struct Level {
   DBuf<double> apval;
   int ap_maxrow = 0;               // longest A*P row
   int ac_maxrow = 0;               // longest row of the next level's A (computed here)
+  // Galerkin numeric plans (P is frozen, so both products are fixed maps of
+  // values): AP[o] = sum_t A[ap_e[t]] * P[ap_f[t]] over t in [ap_seg[o], ap_seg[o+1]),
+  // Ac[o] = sum_t P[ac_r[t]] * AP[ac_f[t]] (ac_r indexes P, since R = P^T)
+  bool planned = false;
+  DBuf<int> ap_seg, ap_e, ap_f, ac_seg, ac_r, ac_f;
   // cycle vectors (fp64 and fp32)
   DBuf<double> x, b, r, t;
   DBuf<float> xf, bf, rf, tf;
@@ -55,6 +60,28 @@ struct AMG {
   int krylov_m = 0;
   DBuf<double> V, Z, H, cs, sn, g, y, kw, kb, kx;
   bool krylov_mode = false;        // V-cycles issued by FGMRES
+  // CUDA graphs of a whole V-cycle from level 0, per [fp32][zero start][krylov][timed]
+  struct VGraph {
+    cudaGraphExec_t exec = nullptr;
+    void* out = nullptr;
+    long long kernels = 0;
+    std::vector<PhaseTimers::Rec> timers;
+  };
+  VGraph vgraph[2][2][2][2];
+  cudaStream_t cap_stream = nullptr;
+  bool use_graphs = true;
+  void drop_graphs() {
+    for (auto& a : vgraph) for (auto& b : a) for (auto& c : b) for (auto& g : c) {
+      if (g.exec) cudaGraphExecDestroy(g.exec);
+      g.exec = nullptr;
+      for (auto& r : g.timers) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+      g.timers.clear();
+    }
+  }
+  ~AMG() {
+    drop_graphs();
+    if (cap_stream) cudaStreamDestroy(cap_stream);
+  }
 };
 
 // amg_setup.cu
@@ -64,7 +91,7 @@ void amg_update(AMG& h, const double* val, cudaStream_t s);
 // amg_cycle.cu
 void amg_vcycle(AMG& h, int lvl, bool zero_x, int precision, cudaStream_t s);
 void amg_solve_vcycles(AMG& h, const double* b, double* x, double tol, int max_cycles,
-                       int* cycles, double* rel, cudaStream_t s);
+                       int* cycles, double* rel, cudaStream_t s, int norm = IMPES_NORM_EQUILIBRATED);
 void amg_apply(AMG& h, const double* b, double* x, int cycles, double apply_tol,
                int apply_max_cycles, cudaStream_t s);
 void amg_vcycle_scaled(AMG& h, const double* bs, double* xs, int precision, cudaStream_t s);

@@ -282,8 +282,10 @@ void coarse_factor(AMG& h, Level& L, cudaStream_t s) {
   IMPES_CUDA(cudaMemsetAsync(h.iflag.p + 2, 0, sizeof(int), s));
   k_gauss_jordan<<<1, kGJ, 2 * n * sizeof(double), s>>>(n, L.lu.p, L.piv.p, h.iflag.p + 2); ::impes::count_launch();
   IMPES_CHECK_LAUNCH();
-  if (&L == h.levels[0].get()) {
-    // single-level hierarchy: the pinned solve would freeze x[0] inside FGMRES
+  {
+    // unpinned inverse for FGMRES preconditioning (the pinned solve mirrors the
+    // reference's stand-alone V-cycle; on a single-level hierarchy it would
+    // freeze x[0] inside FGMRES)
     L.lu_free.ensure((size_t)n * n);
     k_dense_pinned<<<grid_for((size_t)n * n, TB), TB, 0, s>>>(n, L.rowptr.p, L.col.p, L.val.p, L.lu_free.p); ::impes::count_launch();
     IMPES_CHECK_LAUNCH();
@@ -309,6 +311,7 @@ double dot_host(AMG& h, const double* a, const double* b, int n, cudaStream_t s)
   IMPES_CHECK_LAUNCH();
   IMPES_CUDA(cudaMemcpyAsync(h.hbuf.p, h.scal.p, sizeof(double), cudaMemcpyDeviceToHost, s));
   IMPES_CUDA(cudaStreamSynchronize(s));
+  timers().harvest();
   return h.hbuf.p[0];
 }
 
@@ -352,7 +355,9 @@ T* smooth(Level& L, T* x, T* spare, const T* b, int nu, bool zero_x, cudaStream_
                                LV<T>::inv(L), x, s);
       continue;
     }
-    const int tid = top ? timers().begin(IMPES_PH_SMOOTH_L0, s) : -1;
+    const bool wide = L.avg_row > 96;   // the warp-per-row instance of k_csr
+    const int tid = top ? timers().begin(IMPES_PH_SMOOTH_L0, s)
+                        : (wide ? timers().begin(IMPES_PH_SMOOTH_WIDE, s) : -1);
     launch_csr<T, Y_SMOOTH>(L.n, L.avg_row, L.rowptr.p, L.col.p, LV<T>::val(L), x, b,
                             LV<T>::inv(L), spare, s);
     timers().end(tid, s, sweep_bytes(sizeof(T), L.nnz, L.n));
@@ -387,7 +392,7 @@ T* vcycle(AMG& h, int l, bool zero_x, cudaStream_t s) {
   if (L.coarsest) {
     if (L.n <= 500) {
       const int n = L.n;
-      const bool free_ = (l == 0) && h.krylov_mode && L.lu_free.p != nullptr;
+      const bool free_ = h.krylov_mode && L.lu_free.p != nullptr;
       k_coarse_apply<T><<<std::max(1, (n + 7) / 8), 256, n * sizeof(double), s>>>(
           n, free_ ? L.lu_free.p : L.lu.p, LV<T>::b(L), LV<T>::x(L), free_ ? 0 : 1); ::impes::count_launch();
       IMPES_CHECK_LAUNCH();
@@ -413,6 +418,43 @@ T* vcycle(AMG& h, int l, bool zero_x, cudaStream_t s) {
   return out;
 }
 
+// One V-cycle from level 0 (input in LV<T>::b(L0), initial iterate in
+// LV<T>::x(L0) unless zero_x), replayed from a CUDA graph captured on first use.
+template <typename T>
+T* vcycle_top(AMG& h, bool zero_x, cudaStream_t s) {
+  if (!h.use_graphs) return vcycle<T>(h, 0, zero_x, s);
+  PhaseTimers& tm = timers();
+  AMG::VGraph& g = h.vgraph[sizeof(T) == 4][zero_x][h.krylov_mode][tm.on];
+  if (!g.exec) {
+    if (!h.cap_stream) IMPES_CUDA(cudaStreamCreateWithFlags(&h.cap_stream, cudaStreamNonBlocking));
+    const unsigned long long before = launches();
+    tm.capture = &g.timers;
+    IMPES_CUDA(cudaStreamBeginCapture(h.cap_stream, cudaStreamCaptureModeThreadLocal));
+    T* out = nullptr;
+    cudaGraph_t graph = nullptr;
+    try {
+      out = vcycle<T>(h, 0, zero_x, h.cap_stream);
+    } catch (...) {
+      tm.capture = nullptr;
+      cudaStreamEndCapture(h.cap_stream, &graph);
+      if (graph) cudaGraphDestroy(graph);
+      throw;
+    }
+    tm.capture = nullptr;
+    IMPES_CUDA(cudaStreamEndCapture(h.cap_stream, &graph));
+    cudaError_t e = cudaGraphInstantiate(&g.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    IMPES_CUDA(e);
+    g.out = out;
+    g.kernels = (long long)(launches() - before);
+    count_launches(-g.kernels);
+  }
+  IMPES_CUDA(cudaGraphLaunch(g.exec, s));
+  count_launches(g.kernels);
+  if (tm.on && !g.timers.empty()) tm.pending = &g.timers;
+  return (T*)g.out;
+}
+
 }  // namespace
 
 // V-cycle on the equilibrated system: xs = V(0, bs)  (FP64 or FP32 inside)
@@ -422,36 +464,40 @@ void amg_vcycle_scaled(AMG& h, const double* bs, double* xs, int precision, cuda
   if (precision == 1) {
     IMPES_REQUIRE(h.prm.mixed_precision, IMPES_ERR_STATE, "fp32 V-cycle needs mixed_precision=1");
     k_convert<double, float><<<grid_for(n, TB), TB, 0, s>>>(n, bs, L0.bf.p); ::impes::count_launch();
-    float* x = vcycle<float>(h, 0, true, s);
+    float* x = vcycle_top<float>(h, true, s);
     k_convert<float, double><<<grid_for(n, TB), TB, 0, s>>>(n, x, xs); ::impes::count_launch();
   } else {
     IMPES_CUDA(cudaMemcpyAsync(L0.b.p, bs, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-    double* x = vcycle<double>(h, 0, true, s);
+    double* x = vcycle_top<double>(h, true, s);
     IMPES_CUDA(cudaMemcpyAsync(xs, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
   }
   IMPES_CHECK_LAUNCH();
 }
 
-// ClassicalAMG.solve (classical_amg.py:1108-1155)
+// ClassicalAMG.solve (classical_amg.py:1108-1155).  norm = IMPES_NORM_JACOBI
+// measures the stopping test in ||D^-1 r|| / ||D^-1 b|| instead.
 void amg_solve_vcycles(AMG& h, const double* b, double* x, double tol, int max_cycles, int* cycles,
-                       double* rel, cudaStream_t s) {
+                       double* rel, cudaStream_t s, int norm) {
   Level& L0 = *h.levels[0];
   const int n = L0.n;
-  DBuf<double> bs(n), r(n);
+  DBuf<double> bs(n), r(n), wb(n);
   k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, h.dhalf_inv.p, b, bs.p); ::impes::count_launch();
   IMPES_CHECK_LAUNCH();
-  const double bn = std::sqrt(dot_host(h, bs.p, bs.p, n, s));
+  const bool jac = norm == IMPES_NORM_JACOBI;
+  if (jac) { k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, h.jac_w.p, bs.p, wb.p); ::impes::count_launch(); }
+  const double bn = std::sqrt(jac ? dot_host(h, wb.p, wb.p, n, s) : dot_host(h, bs.p, bs.p, n, s));
   IMPES_CUDA(cudaMemcpyAsync(L0.b.p, bs.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
   double rr = INFINITY;
   int c = 0;
   double* xs = nullptr;
   for (c = 1; c <= max_cycles; ++c) {
-    xs = vcycle<double>(h, 0, c == 1, s);
+    xs = vcycle_top<double>(h, c == 1, s);
     if (xs != L0.x.p)
       IMPES_CUDA(cudaMemcpyAsync(L0.x.p, xs, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     xs = L0.x.p;
     launch_csr<double, Y_B_MINUS_AX>(n, L0.avg_row, L0.rowptr.p, L0.col.p, L0.val.p, xs, bs.p,
                                      nullptr, r.p, s);
+    if (jac) { k_mul_inplace<<<grid_for(n, TB), TB, 0, s>>>(n, r.p, h.jac_w.p); ::impes::count_launch(); }
     rr = std::sqrt(dot_host(h, r.p, r.p, n, s)) / (bn + 1e-30);
     if (!(rr == rr)) throw Error(IMPES_ERR_NAN, "NaN residual in V-cycle solve");
     if (rr < tol) break;
@@ -474,7 +520,7 @@ void amg_apply(AMG& h, const double* b, double* x, int cycles, double apply_tol,
   const double bn = std::sqrt(dot_host(h, bs.p, bs.p, n, s));
   int c = 0;
   while (c < apply_max_cycles) {
-    double* xs = vcycle<double>(h, 0, c == 0, s);
+    double* xs = vcycle_top<double>(h, c == 0, s);
     if (xs != L0.x.p)
       IMPES_CUDA(cudaMemcpyAsync(L0.x.p, xs, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     ++c;
@@ -625,11 +671,11 @@ void amg_fgmres(AMG& h, const double* b, double* x, const impes_krylov_params& k
       // z_j = V(v_j ./ wt)
       if (prec == 1) {
         k_div_convert<double, float><<<grid_for(n, TB), TB, 0, s>>>(n, vj, wt, L0.bf.p); ::impes::count_launch();
-        float* zf = vcycle<float>(h, 0, true, s);
+        float* zf = vcycle_top<float>(h, true, s);
         k_convert<float, double><<<grid_for(n, TB), TB, 0, s>>>(n, zf, zj); ::impes::count_launch();
       } else {
         k_div_convert<double, double><<<grid_for(n, TB), TB, 0, s>>>(n, vj, wt, L0.b.p); ::impes::count_launch();
-        double* zd = vcycle<double>(h, 0, true, s);
+        double* zd = vcycle_top<double>(h, true, s);
         IMPES_CUDA(cudaMemcpyAsync(zj, zd, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
       }
       // w = wt .* (A_s z_j)
@@ -658,6 +704,7 @@ void amg_fgmres(AMG& h, const double* b, double* x, const impes_krylov_params& k
       ++total;
       IMPES_CUDA(cudaMemcpyAsync(h.hbuf.p, dscal + 1, sizeof(double), cudaMemcpyDeviceToHost, s));
       IMPES_CUDA(cudaStreamSynchronize(s));
+      timers().harvest();
       est_rel = h.hbuf.p[0] / bnorm;
       if (!(est_rel == est_rel)) throw Error(IMPES_ERR_NAN, "NaN in FGMRES");
       if (est_rel < kp.tol) { ++j; break; }

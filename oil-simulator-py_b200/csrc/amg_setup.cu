@@ -571,6 +571,77 @@ __global__ void k_union_rows(int rows, const int* optr, const int* ocol, const i
   }
 }
 
+// --------------------------------------------------- Galerkin product plans
+// Output position of every (outer entry, inner entry) product, enumerated row
+// by row in (outer, inner) order; kbase = exclusive scan of the row bounds.
+__global__ void k_plan_pos(int rows, const int* optr, const int* ocol, const int* iptr,
+                           const int* icol, const int* outptr, const int* outcol,
+                           const long long* kbase, int* ppos) {
+  GRID_LOOP(r, rows) {
+    long long k = kbase[r];
+    const int ob = outptr[r], L = outptr[r + 1] - ob;
+    for (int e = optr[r]; e < optr[r + 1]; ++e) {
+      const int j = ocol[e];
+      for (int f = iptr[j]; f < iptr[j + 1]; ++f, ++k) {
+        const int key = icol[f];
+        int lo = 0, hi = L - 1;
+        while (lo < hi) {
+          int mid = (lo + hi) >> 1;
+          if (outcol[ob + mid] < key) lo = mid + 1; else hi = mid;
+        }
+        ppos[k] = ob + lo;
+      }
+    }
+  }
+}
+__global__ void k_plan_count(long long nprod, const int* ppos, int* cnt) {
+  GRID_LOOP(k, nprod) atomicAdd(&cnt[ppos[k]], 1);
+}
+// Scatter products into their output segments; outer index is remapped by
+// `omap` (R entry -> P entry) when given.
+__global__ void k_plan_fill(int rows, const int* optr, const int* ocol, const int* iptr,
+                            const long long* kbase, const int* ppos, const int* omap, int* fill,
+                            long long* key, int* pe, int* pf) {
+  GRID_LOOP(r, rows) {
+    long long k = kbase[r];
+    for (int e = optr[r]; e < optr[r + 1]; ++e) {
+      const int j = ocol[e];
+      const int eo = omap ? omap[e] : e;
+      for (int f = iptr[j]; f < iptr[j + 1]; ++f, ++k) {
+        const int slot = atomicAdd(&fill[ppos[k]], 1);
+        key[slot] = k;
+        pe[slot] = eo;
+        pf[slot] = f;
+      }
+    }
+  }
+}
+// Order every segment by product index: the sums then run in enumeration order.
+__global__ void k_plan_sort(int nout, const int* seg, long long* key, int* pe, int* pf) {
+  GRID_LOOP(o, nout) {
+    const int a = seg[o], b = seg[o + 1];
+    for (int x = a + 1; x < b; ++x) {
+      long long kk = key[x];
+      int e = pe[x], f = pf[x], y = x - 1;
+      while (y >= a && key[y] > kk) { key[y + 1] = key[y]; pe[y + 1] = pe[y]; pf[y + 1] = pf[y]; --y; }
+      key[y + 1] = kk; pe[y + 1] = e; pf[y + 1] = f;
+    }
+  }
+}
+// out[o] = sum over the segment of a[pe] * b[pf]
+__global__ void __launch_bounds__(256) k_plan_apply(int nout, const int* __restrict__ seg,
+                                                    const int* __restrict__ pe,
+                                                    const int* __restrict__ pf,
+                                                    const double* __restrict__ a,
+                                                    const double* __restrict__ b,
+                                                    double* __restrict__ out) {
+  GRID_LOOP(o, nout) {
+    double acc = 0.0;
+    for (int t = seg[o]; t < seg[o + 1]; ++t) acc += a[pe[t]] * b[pf[t]];
+    out[o] = acc;
+  }
+}
+
 // ------------------------------------------------ union SpGEMM (numeric)
 // out[r, J] = sum_e oval[e] * inner[ocol[e], J]; each output row lives in shared
 // memory; for one outer entry the lanes own distinct columns (deterministic).
@@ -655,6 +726,10 @@ __global__ void k_to_float(long long n, const double* in, float* out) {
 
 // =================================================================== host
 namespace {
+
+void union_numeric(int rows, const int* optr, const int* ocol, const double* oval, const int* iptr,
+                   const int* icol, const double* ival, const int* outptr, const int* outcol,
+                   double* outval, int maxrow, cudaStream_t s);
 
 struct Ctx {
   AMG& h;
@@ -792,6 +867,67 @@ void union_symbolic(AMG& h, int rows, const int* optr, const int* ocol, const in
   maxrow = to_host_int(h, h.iflag.p, s);
 }
 
+// Product plan of out = outer * inner on a known output pattern (see Level).
+// Returns false (no plan) when the product count does not fit the memory budget.
+bool build_plan(int rows, const int* optr, const int* ocol, const int* iptr, const int* icol,
+                const int* outptr, const int* outcol, int nout, const int* omap, DBuf<int>& seg,
+                DBuf<int>& pe, DBuf<int>& pf, cudaStream_t s) {
+  DBuf<int> bound(std::max(rows, 1));
+  k_union_bound<<<grid_for(rows, TB), TB, 0, s>>>(rows, optr, ocol, iptr, bound.p); ::impes::count_launch();
+  IMPES_CHECK_LAUNCH();
+  std::vector<int> hb(rows);
+  IMPES_CUDA(cudaMemcpyAsync(hb.data(), bound.p, sizeof(int) * rows, cudaMemcpyDeviceToHost, s));
+  IMPES_CUDA(cudaStreamSynchronize(s));
+  std::vector<long long> hk(rows + 1, 0);
+  for (int r = 0; r < rows; ++r) hk[r + 1] = hk[r] + hb[r];
+  const long long nprod = hk[rows];
+  if (nprod >= (1LL << 31) - 1) return false;
+  size_t free_b = 0, total_b = 0;
+  IMPES_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  const double keep = 8.0 * nprod + 4.0 * nout, temp = 16.0 * nprod;
+  if (keep + temp > 0.5 * (double)free_b) return false;
+  DBuf<long long> kbase(rows + 1);
+  IMPES_CUDA(cudaMemcpyAsync(kbase.p, hk.data(), sizeof(long long) * (rows + 1), cudaMemcpyHostToDevice, s));
+  DBuf<int> ppos(std::max<long long>(nprod, 1));
+  k_plan_pos<<<grid_for(rows, TB), TB, 0, s>>>(rows, optr, ocol, iptr, icol, outptr, outcol, kbase.p, ppos.p); ::impes::count_launch();
+  IMPES_CHECK_LAUNCH();
+  DBuf<int> cnt(nout + 1), fill(nout + 1);
+  IMPES_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(int) * (nout + 1), s));
+  k_plan_count<<<grid_for(nprod, TB), TB, 0, s>>>(nprod, ppos.p, cnt.p); ::impes::count_launch();
+  IMPES_CHECK_LAUNCH();
+  seg.alloc(nout + 1);
+  exclusive_scan_i32(cnt.p, seg.p, nout, s);
+  IMPES_CUDA(cudaMemcpyAsync(fill.p, seg.p, sizeof(int) * nout, cudaMemcpyDeviceToDevice, s));
+  DBuf<long long> key(std::max<long long>(nprod, 1));
+  pe.alloc(std::max<long long>(nprod, 1));
+  pf.alloc(std::max<long long>(nprod, 1));
+  k_plan_fill<<<grid_for(rows, TB), TB, 0, s>>>(rows, optr, ocol, iptr, kbase.p, ppos.p, omap, fill.p,
+                                                key.p, pe.p, pf.p); ::impes::count_launch();
+  IMPES_CHECK_LAUNCH();
+  k_plan_sort<<<grid_for(nout, TB), TB, 0, s>>>(nout, seg.p, key.p, pe.p, pf.p); ::impes::count_launch();
+  IMPES_CHECK_LAUNCH();
+  IMPES_CUDA(cudaStreamSynchronize(s));
+  return true;
+}
+
+// Galerkin numeric update of level l -> l+1 (plan when available).
+void galerkin_numeric(Level& L, Level& Nc, cudaStream_t s) {
+  if (L.planned) {
+    const int apn = (int)L.apval.n;
+    k_plan_apply<<<grid_for(apn, 256, 16), 256, 0, s>>>(apn, L.ap_seg.p, L.ap_e.p, L.ap_f.p, L.val.p,
+                                                         L.pval.p, L.apval.p); ::impes::count_launch();
+    IMPES_CHECK_LAUNCH();
+    k_plan_apply<<<grid_for(Nc.nnz, 256, 16), 256, 0, s>>>(Nc.nnz, L.ac_seg.p, L.ac_r.p, L.ac_f.p,
+                                                            L.pval.p, L.apval.p, Nc.val.p); ::impes::count_launch();
+    IMPES_CHECK_LAUNCH();
+    return;
+  }
+  union_numeric(L.n, L.rowptr.p, L.col.p, L.val.p, L.prow.p, L.pcol.p, L.pval.p, L.aprow.p,
+                L.apcol.p, L.apval.p, L.ap_maxrow, s);
+  union_numeric(L.nc, L.rrow.p, L.rcol.p, L.rval.p, L.aprow.p, L.apcol.p, L.apval.p, Nc.rowptr.p,
+                Nc.col.p, Nc.val.p, L.ac_maxrow, s);
+}
+
 void union_numeric(int rows, const int* optr, const int* ocol, const double* oval, const int* iptr,
                    const int* icol, const double* ival, const int* outptr, const int* outcol,
                    double* outval, int maxrow, cudaStream_t s) {
@@ -868,6 +1004,11 @@ void level_precision_copies(AMG& h, Level& L, cudaStream_t s) {
 void amg_setup(AMG& h, int n, int nnz, const int* rowptr, const int* col, const double* val,
                cudaStream_t s) {
   IMPES_REQUIRE(n > 0 && nnz > 0, IMPES_ERR_ARG, "empty matrix");
+  h.drop_graphs();
+  {
+    const char* ev = getenv("IMPES_NO_GRAPHS");
+    h.use_graphs = !(ev && ev[0] == '1');
+  }
   h.levels.clear();
   h.built = false;
   h.iflag.ensure(8);
@@ -1001,10 +1142,15 @@ void amg_setup(AMG& h, int n, int nnz, const int* rowptr, const int* col, const 
     IMPES_CUDA(cudaStreamSynchronize(s));
     Nc.nnz = h.hint.p[0];
     Nc.val.alloc(std::max(Nc.nnz, 1));
-    union_numeric(nl, L.rowptr.p, L.col.p, L.val.p, L.prow.p, L.pcol.p, L.pval.p, L.aprow.p,
-                  L.apcol.p, L.apval.p, L.ap_maxrow, s);
-    union_numeric(nc, L.rrow.p, L.rcol.p, L.rval.p, L.aprow.p, L.apcol.p, L.apval.p, Nc.rowptr.p,
-                  Nc.col.p, Nc.val.p, L.ac_maxrow, s);
+    L.planned = build_plan(nl, L.rowptr.p, L.col.p, L.prow.p, L.pcol.p, L.aprow.p, L.apcol.p, apnnz,
+                           nullptr, L.ap_seg, L.ap_e, L.ap_f, s) &&
+                build_plan(nc, L.rrow.p, L.rcol.p, L.aprow.p, L.apcol.p, Nc.rowptr.p, Nc.col.p, Nc.nnz,
+                           L.rsrc.p, L.ac_seg, L.ac_r, L.ac_f, s);
+    if (!L.planned) {
+      L.ap_seg.release(); L.ap_e.release(); L.ap_f.release();
+      L.ac_seg.release(); L.ac_r.release(); L.ac_f.release();
+    }
+    galerkin_numeric(L, Nc, s);
     // coarse basis (classical_amg.py:906-914)
     if (m > 0) {
       DBuf<double> Bc((size_t)std::max(nc, 1) * m);
@@ -1042,11 +1188,7 @@ void amg_update(AMG& h, const double* val, cudaStream_t s) {
     Level& L = *h.levels[l];
     compute_inv_relax(h, L, s);
     if (L.coarsest) break;
-    Level& Nc = *h.levels[l + 1];
-    union_numeric(L.n, L.rowptr.p, L.col.p, L.val.p, L.prow.p, L.pcol.p, L.pval.p, L.aprow.p,
-                  L.apcol.p, L.apval.p, L.ap_maxrow, s);
-    union_numeric(L.nc, L.rrow.p, L.rcol.p, L.rval.p, L.aprow.p, L.apcol.p, L.apval.p,
-                  Nc.rowptr.p, Nc.col.p, Nc.val.p, L.ac_maxrow, s);
+    galerkin_numeric(L, *h.levels[l + 1], s);
   }
   coarse_factor(h, *h.levels.back(), s);
   for (auto& L : h.levels) {

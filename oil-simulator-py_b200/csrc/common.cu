@@ -10,6 +10,7 @@ void set_last_error(const std::string& msg) { g_last_error = msg; }
 
 static std::atomic<unsigned long long> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void count_launches(long long n) { g_launches.fetch_add((unsigned long long)n, std::memory_order_relaxed); }
 unsigned long long launches() { return g_launches.load(std::memory_order_relaxed); }
 const char* last_error_cstr() { return g_last_error.c_str(); }
 

@@ -20,8 +20,10 @@ struct Error : public std::runtime_error {
 
 void set_last_error(const std::string& msg);
 
-// Number of kernel launches issued by this library (every launch site calls it).
+// Number of kernel launches issued by this library (every launch site calls it;
+// graph replays add the kernels they hold).
 void count_launch();
+void count_launches(long long n);
 unsigned long long launches();
 
 #define IMPES_CUDA(call)                                                        \
@@ -155,6 +157,24 @@ struct PhaseTimers {
   bool on = false;
   std::vector<Rec> recs;
   std::vector<cudaEvent_t> pool;
+  // During stream capture, records become external event nodes of the graph,
+  // collected in `capture`; after a replay has completed, harvest() adds them.
+  std::vector<Rec>* capture = nullptr;
+  const std::vector<Rec>* pending = nullptr;
+  long long acc_n[16] = {};
+  double acc_ms[16] = {}, acc_bytes[16] = {};
+  void harvest() {
+    if (!pending) return;
+    for (const Rec& r : *pending) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess && r.phase >= 0 && r.phase < 16) {
+        acc_n[r.phase] += 1;
+        acc_ms[r.phase] += ms;
+        acc_bytes[r.phase] += r.bytes;
+      }
+    }
+    pending = nullptr;
+  }
   cudaEvent_t take() {
     if (pool.empty()) {
       cudaEvent_t e;
@@ -168,12 +188,23 @@ struct PhaseTimers {
   int begin(int phase, cudaStream_t s) {
     if (!on) return -1;
     Rec r{phase, take(), take(), 0.0};
+    if (capture) {
+      IMPES_CUDA(cudaEventRecordWithFlags(r.a, s, cudaEventRecordExternal));
+      capture->push_back(r);
+      return -2 - (int)(capture->size() - 1);
+    }
     IMPES_CUDA(cudaEventRecord(r.a, s));
     recs.push_back(r);
     return (int)recs.size() - 1;
   }
   void end(int idx, cudaStream_t s, double bytes) {
-    if (idx < 0) return;
+    if (idx == -1) return;
+    if (idx <= -2) {
+      Rec& r = (*capture)[-2 - idx];
+      r.bytes = bytes;
+      IMPES_CUDA(cudaEventRecordWithFlags(r.b, s, cudaEventRecordExternal));
+      return;
+    }
     recs[idx].bytes = bytes;
     IMPES_CUDA(cudaEventRecord(recs[idx].b, s));
   }

@@ -88,10 +88,11 @@ class SatStats(C.Structure):
 
 
 class Timing(C.Structure):
-    _fields_ = [("count", C.c_longlong * 8), ("ms", C.c_double * 8), ("bytes", C.c_double * 8)]
+    _fields_ = [("count", C.c_longlong * 9), ("ms", C.c_double * 9), ("bytes", C.c_double * 9)]
 
 
-PHASES = ("assemble", "saturation", "galerkin", "vcycle", "smooth_l0", "spmv_l0", "ortho", "solve")
+PHASES = ("assemble", "saturation", "galerkin", "vcycle", "smooth_l0", "spmv_l0", "ortho", "solve",
+          "smooth_wide")
 
 _P = C.c_void_p
 _I = C.c_int
@@ -105,7 +106,7 @@ _SIGNATURES = {
     "impes_amg_destroy": ([_P], _I),
     "impes_amg_setup": ([_P, _I, _I, _P, _P, _P, _P], _I),
     "impes_amg_update": ([_P, _P, _P], _I),
-    "impes_amg_solve_vcycles": ([_P, _P, _P, _D, _I, C.POINTER(_I), C.POINTER(_D), _P], _I),
+    "impes_amg_solve_vcycles": ([_P, _P, _P, _D, _I, C.POINTER(_I), C.POINTER(_D), _I, _P], _I),
     "impes_amg_apply": ([_P, _P, _P, _I, _D, _I, _P], _I),
     "impes_amg_vcycle_scaled": ([_P, _P, _P, _I, _P], _I),
     "impes_amg_fgmres": ([_P, _P, _P, C.POINTER(KrylovParams), C.POINTER(KrylovStats), _P], _I),

@@ -154,8 +154,10 @@ class ClassicalAMG:
     def _vec(self, b):
         return b.to(self.device, dtype=torch.float64).contiguous().reshape(-1)
 
-    def solve(self, b, x0: Optional[torch.Tensor] = None, tol: float = 1e-6, max_iter: int = 10) -> torch.Tensor:
-        """Stand-alone V-cycles (``solve``, classical_amg.py:1108-1155)."""
+    def solve(self, b, x0: Optional[torch.Tensor] = None, tol: float = 1e-6, max_iter: int = 10,
+              norm: str = "equilibrated") -> torch.Tensor:
+        """Stand-alone V-cycles (``solve``, classical_amg.py:1108-1155); ``norm="jacobi"``
+        stops on ||D^-1 r|| / ||D^-1 b|| instead of the reference's equilibrated norm."""
         if x0 is not None:
             raise ValueError("x0 is not supported by the V-cycle solve; use fgmres(use_x0=...)")
         bb = self._vec(b)
@@ -163,7 +165,8 @@ class ClassicalAMG:
         cyc, rel = C.c_int(0), C.c_double(0.0)
         with torch.cuda.device(self.device):
             check(lib.impes_amg_solve_vcycles(self._h, ptr(bb), ptr(x), float(tol), int(max_iter),
-                                              C.byref(cyc), C.byref(rel), _lib.stream_of(self.device)),
+                                              C.byref(cyc), C.byref(rel), _NORMS[norm],
+                                              _lib.stream_of(self.device)),
                   "impes_amg_solve_vcycles")
         self.last_stats = {"cycles": cyc.value, "rel_res": rel.value}
         return x

@@ -201,12 +201,16 @@ def gas_injection_1m(seed: int = 2, nx: int = 200, ny: int = 200, nz: int = 25, 
             wells.append({"name": f"P{a}{b}", "type": "producer", "i": i, "j": j, "k": km,
                           "radius": 0.1, "control_type": "bhp", "control_value": 15.0})
     fluid = _black_oil_fluid(pvt)
+    sim = _sim(dt_days, steps)
+    # the reference's own AMG settings for its million-cell case
+    # (configs/mega_3phase_million.json:19-25; docs/PERFORMANCE.md:44-46)
+    sim["amg"].update({"theta": 0.2, "max_levels": 20, "coarsest_size": 120})
     cfg = {
         "reservoir": {"dimensions": [nx, ny, nz], "grid_size": [20.0, 20.0, 2.0], "porosity": 0.2,
                       "permeability": 150.0, "k_vertical_fraction": 0.1, "c_rock": 1e-4},
         "fluid": fluid,
         "wells": wells,
-        "simulation": _sim(dt_days, steps),
+        "simulation": sim,
     }
     return cfg, {"kx": kx, "ky": kx.copy(), "kz": 0.1 * kx, "poro": poro, "pvt": pvt}
 

@@ -413,7 +413,8 @@ class Simulator:
         self.amg_max_cycles = int(amg_cfg.get("max_cycles", 20))
         self.amg_max_iters = int(amg_cfg.get("max_iters", 400))
         self.amg_restart = int(amg_cfg.get("restart", 30))
-        self.amg_norm = amg_cfg.get("norm", "jacobi")
+        # the reference's own stopping norm for its stand-alone V-cycles
+        self.amg_norm = amg_cfg.get("norm", "equilibrated" if self.pressure_solver == "amg" else "jacobi")
         self.amg_precision = amg_cfg.get("precision", "fp64")
         kw = dict(device=self.device, dtype=torch.float64)
         kx, ky, kz = (t.to(**kw).contiguous() for t in reservoir.permeability_tensors)

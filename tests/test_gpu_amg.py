@@ -155,3 +155,36 @@ def test_larger_3d_hierarchy_vs_oracle():
     amg = gpu_amg(A, coarsest_size=200, seed=2)
     ref = oa.AMG(A, coarsest_size=200, seed=2)
     compare_hierarchy(amg, ref, pval_rtol=1e-6)
+
+
+def test_graph_replay_matches_direct_launches(golden, monkeypatch):
+    """V-cycles replayed from CUDA graphs give bitwise the same FGMRES iterates as
+    direct launches (IMPES_NO_GRAPHS=1 is read at setup)."""
+    t = golden("two_phase_64x64")
+    n = len(t["A0_crow"]) - 1
+    A = sp.csr_matrix((t["A0_val"], t["A0_col"], t["A0_crow"]), shape=(n, n))
+    b = torch.tensor(t["b0"], device="cuda")
+    outs = []
+    for flag in ("0", "1"):
+        monkeypatch.setenv("IMPES_NO_GRAPHS", flag)
+        amg = gpu_amg(A, coarsest_size=100, seed=3)
+        for prec in ("fp64", "mixed"):
+            outs.append(amg.fgmres(b, tol=1e-10, precision=prec)[0])
+        outs.append(amg.solve(b, tol=1e-30, max_iter=3))
+    for a, c in zip(outs[:3], outs[3:]):
+        assert torch.equal(a, c)
+
+
+def test_phase_timers_inside_graphs(golden):
+    from impes_b200 import _lib
+    t = golden("two_phase_64x64")
+    n = len(t["A0_crow"]) - 1
+    A = sp.csr_matrix((t["A0_val"], t["A0_col"], t["A0_crow"]), shape=(n, n))
+    amg = gpu_amg(A, coarsest_size=100)
+    _lib.timing_enable(True)
+    _lib.timing_collect()
+    _, st = amg.fgmres(torch.tensor(t["b0"], device="cuda"), tol=1e-8, precision="mixed")
+    ph = _lib.timing_collect()
+    _lib.timing_enable(False)
+    assert ph["vcycle"][0] == st["iterations"]
+    assert ph["smooth_l0"][0] >= 4 * st["iterations"] and ph["smooth_l0"][1] > 0
