@@ -114,6 +114,23 @@ int impes_amg_update(impes_amg* h, const double* val, void* stream);
 int impes_amg_solve_vcycles(impes_amg* h, const double* b, double* x, double tol,
                             int max_cycles, int* cycles, double* rel_res, int norm, void* stream);
 
+/* The stand-alone V-cycle solve above, for callers that must not allocate
+ * device memory during a solve -- for example a host that reserves the GPU's
+ * memory up front for its own pool, or one that cannot afford the device-wide
+ * synchronisation that cudaFree implies.  (No counterpart in the reference.)
+ * impes_amg_solve_vcycles allocates and frees three n-vectors on every call;
+ * this variant keeps them in a 6 MiB static device array instead and makes no
+ * allocation, so n is limited to 262144 rows (larger n returns IMPES_ERR_ARG).
+ * Every GPU that loads the library holds that array until the process exits.
+ * Every call on a device shares it: calls that overlap on the GPU (several
+ * streams or threads) race, so serialise them.  Nothing in the array needs to
+ * start at zero (each call writes before it reads).  The first call on each
+ * device looks up the array's device address; make that first call before any
+ * stream capture.  Results equal impes_amg_solve_vcycles'. */
+int impes_amg_solve_vcycles_noalloc(impes_amg* h, const double* b, double* x, double tol,
+                                    int max_cycles, int* cycles, double* rel_res, int norm,
+                                    void* stream);
+
 /* ClassicalAMG.apply (classical_amg.py:1157-1180): `cycles` V-cycles, then
  * continue up to apply_max_cycles while ||r||/||b|| >= apply_tol. */
 int impes_amg_apply(impes_amg* h, const double* b, double* x, int cycles, double apply_tol,

@@ -18,6 +18,9 @@ struct impes_model {
 
 using namespace impes;
 
+bool impes_amg_handle_built(impes_amg* h) { return h && h->a.built; }
+impes::AMG* impes_amg_handle_core(impes_amg* h) { return &h->a; }
+
 namespace {
 
 template <typename F>

@@ -11,6 +11,11 @@
 #include "amg.cuh"
 #include <algorithm>
 #include <cmath>
+#include <mutex>
+
+// handle accessors (abi.cu)
+bool impes_amg_handle_built(impes_amg* h);
+impes::AMG* impes_amg_handle_core(impes_amg* h);
 
 namespace impes {
 namespace {
@@ -723,3 +728,97 @@ void amg_fgmres(AMG& h, const double* b, double* x, const impes_krylov_params& k
 }
 
 }  // namespace impes
+
+// ============================================================ no-alloc solve
+// Work space of impes_amg_solve_vcycles_noalloc: the scaled right-hand side, the
+// residual and the weighted right-hand side (3 vectors of up to
+// kNoAllocMaxRows doubles, 6 MiB).  It is static device storage: every GPU that
+// loads this library holds it until the process exits, and every call on a
+// device shares it.
+namespace impes {
+constexpr int kNoAllocMaxRows = 262144;
+}
+static __device__ __align__(256) double g_solve_scratch[3 * (size_t)impes::kNoAllocMaxRows];
+
+namespace impes {
+namespace {
+std::mutex g_scratch_mu;
+double* g_scratch_dev[128] = {};
+
+// Device address of g_solve_scratch on the current device, looked up once per
+// device with that device current (the host-side symbol is not a device address).
+double* solve_scratch() {
+  int dev = 0;
+  IMPES_CUDA(cudaGetDevice(&dev));
+  IMPES_REQUIRE(dev >= 0 && dev < 128, IMPES_ERR_ARG, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_scratch_mu);
+  if (!g_scratch_dev[dev]) {
+    void* ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_solve_scratch);
+    if (e != cudaSuccess || !ptr)
+      throw Error(IMPES_ERR_CUDA, std::string("cudaGetSymbolAddress(g_solve_scratch): ") +
+                                      cudaGetErrorString(e));
+    g_scratch_dev[dev] = static_cast<double*>(ptr);
+  }
+  return g_scratch_dev[dev];
+}
+
+// The stand-alone V-cycle solve of amg_solve_vcycles with its three vectors in
+// the static array and the V-cycles launched directly (no graph instantiation).
+void solve_vcycles_noalloc(AMG& h, const double* b, double* x, double tol, int max_cycles,
+                           int* cycles, double* rel, int norm, cudaStream_t s) {
+  Level& L0 = *h.levels[0];
+  const int n = L0.n;
+  IMPES_REQUIRE(n <= kNoAllocMaxRows, IMPES_ERR_ARG,
+                "impes_amg_solve_vcycles_noalloc: n exceeds the 262144-row static work space");
+  IMPES_REQUIRE(h.red.n >= (size_t)kMD * kDotBlocks, IMPES_ERR_STATE, "hierarchy not set up");
+  double* base = solve_scratch();
+  double* bs = base;
+  double* r = base + kNoAllocMaxRows;
+  double* wb = base + 2 * (size_t)kNoAllocMaxRows;
+  k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, h.dhalf_inv.p, b, bs); ::impes::count_launch();
+  IMPES_CHECK_LAUNCH();
+  const bool jac = norm == IMPES_NORM_JACOBI;
+  if (jac) { k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, h.jac_w.p, bs, wb); ::impes::count_launch(); }
+  const double bn = std::sqrt(jac ? dot_host(h, wb, wb, n, s) : dot_host(h, bs, bs, n, s));
+  IMPES_CUDA(cudaMemcpyAsync(L0.b.p, bs, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  double rr = INFINITY;
+  int c = 0;
+  for (c = 1; c <= max_cycles; ++c) {
+    double* xs = vcycle<double>(h, 0, c == 1, s);
+    if (xs != L0.x.p)
+      IMPES_CUDA(cudaMemcpyAsync(L0.x.p, xs, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    launch_csr<double, Y_B_MINUS_AX>(n, L0.avg_row, L0.rowptr.p, L0.col.p, L0.val.p, L0.x.p, bs,
+                                     nullptr, r, s);
+    if (jac) { k_mul_inplace<<<grid_for(n, TB), TB, 0, s>>>(n, r, h.jac_w.p); ::impes::count_launch(); }
+    rr = std::sqrt(dot_host(h, r, r, n, s)) / (bn + 1e-30);
+    if (!(rr == rr)) throw Error(IMPES_ERR_NAN, "NaN residual in V-cycle solve");
+    if (rr < tol) break;
+  }
+  if (c > max_cycles) c = max_cycles;
+  k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, h.dhalf_inv.p, L0.x.p, x); ::impes::count_launch();
+  IMPES_CHECK_LAUNCH();
+  if (cycles) *cycles = c;
+  if (rel) *rel = rr;
+}
+}  // namespace
+}  // namespace impes
+
+extern "C" int impes_amg_solve_vcycles_noalloc(impes_amg* h, const double* b, double* x, double tol,
+                                               int max_cycles, int* cycles, double* rel_res, int norm,
+                                               void* stream) {
+  try {
+    IMPES_REQUIRE(h && b && x, IMPES_ERR_ARG, "null argument");
+    IMPES_REQUIRE(impes_amg_handle_built(h), IMPES_ERR_STATE, "solve before setup");
+    IMPES_REQUIRE(max_cycles >= 1, IMPES_ERR_ARG, "max_cycles must be >= 1");
+    impes::solve_vcycles_noalloc(*impes_amg_handle_core(h), b, x, tol, max_cycles, cycles, rel_res, norm,
+                                 reinterpret_cast<cudaStream_t>(stream));
+    return IMPES_OK;
+  } catch (const impes::Error& e) {
+    impes::set_last_error(e.what());
+    return e.code;
+  } catch (const std::exception& e) {
+    impes::set_last_error(e.what());
+    return IMPES_ERR_ARG;
+  }
+}

@@ -107,6 +107,7 @@ _SIGNATURES = {
     "impes_amg_setup": ([_P, _I, _I, _P, _P, _P, _P], _I),
     "impes_amg_update": ([_P, _P, _P], _I),
     "impes_amg_solve_vcycles": ([_P, _P, _P, _D, _I, C.POINTER(_I), C.POINTER(_D), _I, _P], _I),
+    "impes_amg_solve_vcycles_noalloc": ([_P, _P, _P, _D, _I, C.POINTER(_I), C.POINTER(_D), _I, _P], _I),
     "impes_amg_apply": ([_P, _P, _P, _I, _D, _I, _P], _I),
     "impes_amg_vcycle_scaled": ([_P, _P, _P, _I, _P], _I),
     "impes_amg_fgmres": ([_P, _P, _P, C.POINTER(KrylovParams), C.POINTER(KrylovStats), _P], _I),
