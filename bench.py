@@ -42,7 +42,8 @@ METRIC = "IMPES cell-steps/s, mixed vs FP64 AMG at 1e-6 residual; adjoint/forwar
 WORKLOAD = ("gas_injection_1m: 200x200x25 = 1,000,000 cells, ln k ~ N(ln 150 mD, 1.0^2) "
             "Gaussian-correlated (radius 5), 20-row black-oil PVT (Bo 1.3->1.1 with p), Stone II, "
             "gravity, capillarity, 9 gas injectors at 2e5 sm3/d given as reservoir rate "
-            "(x Bg at 25 MPa), 16 BHP producers (15 MPa), dt 2 d")
+            "(x Bg at 25 MPa) with global_rate_scale 0.05 and max_substeps 20 (the reference's "
+            "million-cell settings), 16 BHP producers (15 MPa), dt 2 d")
 PRESSURE_TOL = 1e-6
 L2_FLUSH_BYTES = 512 << 20
 CPU_SAMPLE = (100, 100, 25)     # spatial sample of the workload for the CPU legs
@@ -252,12 +253,8 @@ def run_ours(args, world, rank, local):
             dist.barrier()
         torch.cuda.synchronize()
         launches0 = _lib.kernel_launches()
-        _lib.timing_enable(True)
-        _lib.timing_collect()
         with ClockSampler(local) as clk:
             ms, iters = time_steps(sim, args.steps, dt, flush, stream)
-        phases = _lib.timing_collect()
-        _lib.timing_enable(False)
         launches = _lib.kernel_launches() - launches0
         torch.cuda.synchronize()
         if dist is not None:
@@ -266,6 +263,14 @@ def run_ours(args, world, rank, local):
         if dist is not None:
             dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
         ms_max = float(tmax.item())
+        # phase timers (CUDA events around every phase and every wide-level sweep,
+        # recorded inside the V-cycle graphs) run on K further steps, kept out of the
+        # headline region because their event records lengthen each V-cycle
+        _lib.timing_enable(True)
+        _lib.timing_collect()
+        ms_inst, iters_inst = time_steps(sim, args.steps, dt, flush, stream)
+        phases = _lib.timing_collect()
+        _lib.timing_enable(False)
         e2e_ms, e2e_bytes = time_e2e(sim, fl, args.steps, dt, flush, stream)
         te = torch.tensor([e2e_ms], dtype=torch.float64, device=device)
         if dist is not None:
@@ -274,7 +279,11 @@ def run_ours(args, world, rank, local):
             print(f"[bench] {precision}: levels (n, nnz, nc, p_nnz, coarsest) = {sim.amg_levels()}",
                   file=sys.stderr)
             print(f"[bench] {precision}: phases {phases}", file=sys.stderr)
+        state = {"sw": [float(fl.s_w.min()), float(fl.s_w.max())],
+                 "sg": [float(fl.s_g.min()), float(fl.s_g.max())],
+                 "p_MPa": [float(fl.pressure.min()) / 1e6, float(fl.pressure.max()) / 1e6]}
         results[precision] = dict(ms=ms_max, iters=iters, phases=phases, clocks=clk.summary(),
+                                  ms_inst=ms_inst, iters_inst=iters_inst, state=state,
                                   launches=launches, e2e_ms=float(te.item()), e2e_bytes=e2e_bytes,
                                   setup_s=setup_s, p=fl.pressure.clone(), sw=fl.s_w.clone())
         sim.close()
@@ -325,7 +334,7 @@ def run_ours(args, world, rank, local):
     achieved = by_s / (ms_s / 1e3) / 1e9
     traffic = read_traffic(key)
     n0, ms0, by0 = mixed["phases"]["smooth_l0"]
-    share = {k: round(v[1] / mixed["ms"], 4) for k, v in mixed["phases"].items() if k != "solve"}
+    share = {k: round(v[1] / mixed["ms_inst"], 4) for k, v in mixed["phases"].items() if k != "solve"}
     drift_sw = float((results["mixed"]["sw"] - results["fp64"]["sw"]).abs().max())
     drift_p = float(((results["mixed"]["p"] - results["fp64"]["p"]).abs().max()
                      / results["fp64"]["p"].abs().max()))
@@ -359,6 +368,11 @@ def run_ours(args, world, rank, local):
         "mixed_vs_fp64_drift": {"sw_abs_max": drift_sw, "p_rel_max": drift_p},
         "setup_s": {"mixed": mixed["setup_s"], "fp64": fp64["setup_s"]},
         "phase_share": share,
+        "instrumented": {"note": "phase shares and roofline come from K further steps with the "
+                                 "library's per-phase CUDA events on; the headline region runs without them",
+                         "ms_per_step": mixed["ms_inst"] / steps,
+                         "vcycles_per_step": statistics.mean(mixed["iters_inst"])},
+        "state_after": {"mixed": mixed["state"], "fp64": fp64["state"]},
         "e2e": {"value": world * cells * steps / (mixed["e2e_ms"] / 1e3), "unit": "cell-steps/s",
                 "h2d_bytes_per_step": mixed["e2e_bytes"], "d2h_bytes_per_step": mixed["e2e_bytes"]},
         "roofline": {"kernel": ("k_csr<float,32,Y_SMOOTH> (l1-Jacobi sweep, levels with > 96 nnz/row)"

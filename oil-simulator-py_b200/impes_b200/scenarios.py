@@ -163,7 +163,8 @@ def _gaussian_smooth(z, sigma=2.5, radius=5):
 
 def gas_injection_1m(seed: int = 2, nx: int = 200, ny: int = 200, nz: int = 25, steps: int = 20,
                      dt_days: float = 2.0, gas_rate: float = 2.0e5, n_inj_side: int = 3,
-                     n_prod_side: int = 4, surface_units: bool = False, bo_increasing: bool = False):
+                     n_prod_side: int = 4, surface_units: bool = False, bo_increasing: bool = False,
+                     rate_scale: float = 0.05):
     """Gas-injection stress case: ln k ~ N(ln 150 mD, 1.0^2) Gaussian-correlated (radius 5).
 
     ``gas_rate`` is in sm3/d.  By default each injector is given the equivalent
@@ -172,7 +173,8 @@ def gas_injection_1m(seed: int = 2, nx: int = 200, ny: int = 200, nz: int = 25, 
     well's number unconverted, as reservoir m3/s (simulation.py:1626-1634, while
     the saturation step converts it with Bg at :1061-1064), which at 2e5 sm3/d
     drives the explicit saturation update out of range.  ``surface_units=True``
-    keeps the literal surface-rate wells.
+    keeps the literal surface-rate wells.  ``rate_scale`` is the simulation's
+    ``global_rate_scale``.
     """
     rng = np.random.default_rng(seed)
     shape = (nx, ny, nz)
@@ -205,6 +207,10 @@ def gas_injection_1m(seed: int = 2, nx: int = 200, ny: int = 200, nz: int = 25, 
     # the reference's own AMG settings for its million-cell case
     # (configs/mega_3phase_million.json:19-25; docs/PERFORMANCE.md:44-46)
     sim["amg"].update({"theta": 0.2, "max_levels": 20, "coarsest_size": 120})
+    # and its rate scale and substep cap (configs/mega_3phase_million.json:13-14): at the
+    # unscaled 2e5 sm3/d an injector cell takes ~20 pore volumes per 2-day step and the
+    # explicit update leaves [0, 1] (Sw -8, Sg 9 after four steps, reference semantics)
+    sim.update({"global_rate_scale": rate_scale, "max_substeps": 20})
     cfg = {
         "reservoir": {"dimensions": [nx, ny, nz], "grid_size": [20.0, 20.0, 2.0], "porosity": 0.2,
                       "permeability": 150.0, "k_vertical_fraction": 0.1, "c_rock": 1e-4},
