@@ -216,6 +216,39 @@ def read_traffic(kernel: str):
     return None
 
 
+ADJOINT_WORKLOAD = ("adjoint_case: 64x64x8 oil-water, ln k ~ N(ln 100 mD, 0.7^2), 50 steps of 2 d, "
+                    "J = sum (q_o - q_target)^2 at the producer (flux-balance rate), targets from a "
+                    "second seeded k field, gradient w.r.t. ln k and porosity, checkpoints every 10 steps, "
+                    "FGMRES to 1e-10 (Jacobi norm) in the forward and adjoint solves")
+
+
+def run_adjoint(device):
+    """Forward run and adjoint gradient of the history-matching objective; device
+    times come from the library's own CUDA events (forward run; reverse sweep
+    with the recomputation of the checkpointed segments)."""
+    from impes_b200 import scenarios
+    from impes_b200.adjoint import misfit_gradient, producer_rates
+    steps = 50
+    cfg, f = scenarios.adjoint_case(seed=3, steps=steps)
+    _, f2 = scenarios.adjoint_case(seed=5, steps=steps)
+    dt = cfg["simulation"]["time_step_days"] * 86400.0
+    target = producer_rates(cfg, dict(f2, poro=f["poro"]), steps, dt, tol=1e-10, device=device)
+    runs = []
+    for _ in range(3):          # the first call is a warm-up
+        out = misfit_gradient(cfg, f, target, steps, dt, checkpoint_every=10, tol=1e-10,
+                              adjoint_tol=1e-10, device=device)
+        runs.append(out["stats"])
+    st = runs[-1]
+    fwd = statistics.median(r["forward_ms"] for r in runs[1:])
+    rev = statistics.median(r["reverse_ms"] for r in runs[1:])
+    return {"workload": ADJOINT_WORKLOAD, "cells": 64 * 64 * 8, "steps": steps,
+            "forward_ms": fwd, "reverse_ms": rev, "adjoint_over_forward": rev / fwd,
+            "gradient_over_forward": (fwd + rev) / fwd, "J": st["J"],
+            "forward_fgmres_iterations": st["forward_iterations"],
+            "adjoint_fgmres_iterations": st["adjoint_iterations"],
+            "recomputed_steps": st["recomputed_steps"]}
+
+
 def run_ours(args, world, rank, local):
     import torch
     from impes_b200 import _lib, scenarios
@@ -310,6 +343,9 @@ def run_ours(args, world, rank, local):
         simp.close()
         del simp, flp
         torch.cuda.empty_cache()
+    adjoint = None
+    if args.precision == "both" and not args.no_adjoint:
+        adjoint = run_adjoint(device)
     if dist is not None:
         dist.destroy_process_group()
     if rank != 0:
@@ -365,6 +401,7 @@ def run_ours(args, world, rank, local):
             "ms_per_step": plain["ms"] / plain["steps"], "steps_timed": plain["steps"],
             "vcycles_per_step": statistics.mean(plain["iters"]),
             "mixed_speedup": (plain["ms"] / plain["steps"]) / (mixed["ms"] / steps)},
+        "adjoint": adjoint,
         "mixed_vs_fp64_drift": {"sw_abs_max": drift_sw, "p_rel_max": drift_p},
         "setup_s": {"mixed": mixed["setup_s"], "fp64": fp64["setup_s"]},
         "phase_share": share,
@@ -420,6 +457,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--restart", type=int, default=60, help="FGMRES restart length")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 V-cycle baseline")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward measurement")
     ap.add_argument("--grid", default=None,
                     help="NXxNYxNZ: a smaller grid of the same workload (profiling captures only)")
     ap.add_argument("--precision", choices=["both", "mixed", "fp64"], default="both",

@@ -291,6 +291,49 @@ int impes_timing_collect(impes_timing* out);
 /* Kernel launches issued by the library since load. */
 unsigned long long impes_kernel_launches(void);
 
+/* ------------------------------------------------------------------ adjoint
+ * Discrete adjoint of the IMPES step (no counterpart in the reference).
+ * Objective J = sum over steps and producers of (q_o - q_target)^2, q_o the
+ * producer oil rate (m3/day) from the flux balance of its pressure row,
+ *   q = sum_f c_f (p_nb - p_c) - PV ct/dt (p_c - p_prev) + Qg_c,
+ * times the oil fractional flow at the step's starting saturation.  This is
+ * the well's WI*lambda_t*(p - p_bhp) (simulation.py:1297) written without its
+ * round-off.  Gradients are with respect to ln k (kx, ky, kz of a cell scaled
+ * together) and porosity.  Scope: oil-water (s_g = 0) without PVT tables or
+ * capillarity, Corey relative permeability, no bhp_min switching; other models
+ * return IMPES_ERR_ARG.  The runs step internal copies of the state (the
+ * caller's p, sw are not touched by impes_adjoint_gradient) and use the model's
+ * and the AMG handle's work space: the model's mass balances are restored, the
+ * hierarchy is left holding the values of some step's matrix. */
+typedef struct {
+  double J;                       /* objective of the forward run                 */
+  long long forward_iterations;   /* FGMRES iterations, forward run + recomputation */
+  long long adjoint_iterations;   /* FGMRES iterations of the adjoint solves       */
+  double forward_ms;              /* device time of the forward run                */
+  double reverse_ms;              /* device time of the reverse sweep (recomputation included) */
+  int checkpoints;                /* state checkpoints kept                        */
+  int recomputed_steps;           /* forward steps recomputed from checkpoints     */
+} impes_adjoint_stats;
+/* Producers observed by the objective (wells of type producer, in well order). */
+int impes_adjoint_num_producers(impes_model* m, int* n);
+/* Forward run of `steps` steps from (p, sw) in place (s_g = 0), writing the
+ * producer oil rates to rates_host[steps * nprod] (may be NULL). */
+int impes_adjoint_rates(impes_model* m, impes_amg* amg, double* p, double* sw, int steps,
+                        double dt, const impes_krylov_params* kp, double* rates_host,
+                        void* stream);
+/* J and dJ/dln k, dJ/dphi (device arrays of N) for the run of `steps` steps
+ * from (p0, sw0).  States are checkpointed every `checkpoint_every` steps
+ * (0: keep all) and recomputed segment by segment in the reverse sweep; the
+ * adjoint pressure solve reuses the forward hierarchy (A is symmetric).
+ * kx, ky, kz are the model's permeabilities (m^2, device).  target_host and
+ * rates_host (may be NULL) hold steps * nprod rates in m3/day. */
+int impes_adjoint_gradient(impes_model* m, impes_amg* amg, const double* p0, const double* sw0,
+                           const double* kx, const double* ky, const double* kz, int steps,
+                           int checkpoint_every, double dt, const impes_krylov_params* forward,
+                           const impes_krylov_params* adjoint, const double* target_host,
+                           double* rates_host, double* g_lnk, double* g_poro,
+                           impes_adjoint_stats* stats, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

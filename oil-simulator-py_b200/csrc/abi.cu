@@ -21,6 +21,19 @@ using namespace impes;
 bool impes_amg_handle_built(impes_amg* h) { return h && h->a.built; }
 impes::AMG* impes_amg_handle_core(impes_amg* h) { return &h->a; }
 
+namespace impes {
+void adjoint_check_model(const Model& m);
+int adjoint_num_producers(const Model& m);
+void adjoint_rates(Model& m, AMG& a, double* p, double* sw, int steps, double dt,
+                   const impes_krylov_params& kp, double* rates_host, long long& iters,
+                   cudaStream_t s);
+void adjoint_gradient(Model& m, AMG& a, const double* p0, const double* sw0, const double* kx,
+                      const double* ky, const double* kz, int steps, int ckpt, double dt,
+                      const impes_krylov_params& kf, const impes_krylov_params& ka,
+                      const double* target_host, double* rates_host, double* g_lnk,
+                      double* g_poro, impes_adjoint_stats& out, cudaStream_t s);
+}  // namespace impes
+
 namespace {
 
 template <typename F>
@@ -481,3 +494,36 @@ int impes_timing_collect(impes_timing* out) {
 unsigned long long impes_kernel_launches(void) { return launches(); }
 
 }  // extern "C"
+
+int impes_adjoint_num_producers(impes_model* h, int* n) {
+  return guarded([&] {
+    IMPES_REQUIRE(h && n, IMPES_ERR_ARG, "null argument");
+    *n = adjoint_num_producers(h->m);
+  });
+}
+
+int impes_adjoint_rates(impes_model* h, impes_amg* amg, double* p, double* sw, int steps, double dt,
+                        const impes_krylov_params* kp, double* rates_host, void* stream) {
+  return guarded([&] {
+    IMPES_REQUIRE(h && amg && p && sw && kp, IMPES_ERR_ARG, "null argument");
+    long long iters = 0;
+    adjoint_rates(h->m, amg->a, p, sw, steps, dt, *kp, rates_host, iters, S(stream));
+  });
+}
+
+int impes_adjoint_gradient(impes_model* h, impes_amg* amg, const double* p0, const double* sw0,
+                           const double* kx, const double* ky, const double* kz, int steps,
+                           int checkpoint_every, double dt, const impes_krylov_params* forward,
+                           const impes_krylov_params* adjoint, const double* target_host,
+                           double* rates_host, double* g_lnk, double* g_poro,
+                           impes_adjoint_stats* stats, void* stream) {
+  return guarded([&] {
+    IMPES_REQUIRE(h && amg && p0 && sw0 && kx && ky && kz && forward && adjoint && target_host &&
+                      g_lnk && g_poro,
+                  IMPES_ERR_ARG, "null argument");
+    impes_adjoint_stats st{};
+    adjoint_gradient(h->m, amg->a, p0, sw0, kx, ky, kz, steps, checkpoint_every, dt, *forward,
+                     *adjoint, target_host, rates_host, g_lnk, g_poro, st, S(stream));
+    if (stats) *stats = st;
+  });
+}

@@ -27,6 +27,7 @@ SOURCES = {
     "physics.cu": ["-fmad=false"],
     "amg_setup.cu": [],
     "amg_cycle.cu": [],
+    "adjoint.cu": [],
     "abi.cu": [],
 }
 HEADERS = ["common.cuh", "model.cuh", "amg.cuh", os.path.join(REPO, "include", "impes_b200.h")]

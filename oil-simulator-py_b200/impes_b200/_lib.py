@@ -87,6 +87,12 @@ class SatStats(C.Structure):
                 ("component", C.c_double * 6)]
 
 
+class AdjointStats(C.Structure):
+    _fields_ = [("J", C.c_double), ("forward_iterations", C.c_longlong),
+                ("adjoint_iterations", C.c_longlong), ("forward_ms", C.c_double),
+                ("reverse_ms", C.c_double), ("checkpoints", C.c_int), ("recomputed_steps", C.c_int)]
+
+
 class Timing(C.Structure):
     _fields_ = [("count", C.c_longlong * 9), ("ms", C.c_double * 9), ("bytes", C.c_double * 9)]
 
@@ -107,6 +113,10 @@ _SIGNATURES = {
     "impes_amg_setup": ([_P, _I, _I, _P, _P, _P, _P], _I),
     "impes_amg_update": ([_P, _P, _P], _I),
     "impes_amg_solve_vcycles": ([_P, _P, _P, _D, _I, C.POINTER(_I), C.POINTER(_D), _I, _P], _I),
+    "impes_adjoint_num_producers": ([_P, C.POINTER(_I)], _I),
+    "impes_adjoint_rates": ([_P, _P, _P, _P, _I, _D, C.POINTER(KrylovParams), _P, _P], _I),
+    "impes_adjoint_gradient": ([_P, _P, _P, _P, _P, _P, _P, _I, _I, _D, C.POINTER(KrylovParams),
+                                C.POINTER(KrylovParams), _P, _P, _P, _P, C.POINTER(AdjointStats), _P], _I),
     "impes_amg_solve_vcycles_noalloc": ([_P, _P, _P, _D, _I, C.POINTER(_I), C.POINTER(_D), _I, _P], _I),
     "impes_amg_apply": ([_P, _P, _P, _I, _D, _I, _P], _I),
     "impes_amg_vcycle_scaled": ([_P, _P, _P, _I, _P], _I),

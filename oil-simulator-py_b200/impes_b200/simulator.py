@@ -639,10 +639,14 @@ def build_from_config(cfg: dict, fields: Optional[dict] = None, device=None):
     res = Reservoir(cfg["reservoir"], device)
     if fields is not None:
         kw = dict(device=res.device, dtype=torch.float64)
-        res.permeability_x = torch.as_tensor(np.asarray(fields["kx"]), **kw).reshape(res.nx, res.ny, res.nz)
-        res.permeability_y = torch.as_tensor(np.asarray(fields["ky"]), **kw).reshape(res.nx, res.ny, res.nz)
-        res.permeability_z = torch.as_tensor(np.asarray(fields["kz"]), **kw).reshape(res.nx, res.ny, res.nz)
-        res.porosity = torch.as_tensor(np.asarray(fields["poro"]), **kw).reshape(res.nx, res.ny, res.nz)
+
+        def field(v):
+            t = v.detach().to(**kw) if torch.is_tensor(v) else torch.as_tensor(np.asarray(v), **kw)
+            return t.reshape(res.nx, res.ny, res.nz)
+        res.permeability_x = field(fields["kx"])
+        res.permeability_y = field(fields["ky"])
+        res.permeability_z = field(fields["kz"])
+        res.porosity = field(fields["poro"])
         res.porous_volume = res.cell_volume * res.porosity
     wm = WellManager(cfg.get("wells", []), res)
     fl = Fluid(cfg["fluid"], res, device)
