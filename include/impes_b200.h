@@ -291,6 +291,30 @@ int impes_timing_collect(impes_timing* out);
 /* Kernel launches issued by the library since load. */
 unsigned long long impes_kernel_launches(void);
 
+/* ----------------------------------------------------------------- ensemble
+ * Independent realisations stepped concurrently (no counterpart in the
+ * reference, whose callers loop over Simulator.run_step).  Member m has its own
+ * model and AMG handle and its own state arrays; each member's numerics are
+ * those of impes_step on that member alone (FGMRES solver with *kp).  A pool of
+ * `workers` host threads, each with its own CUDA stream on the calling thread's
+ * device, takes members largest first (cells[m]) and runs all `steps` steps of
+ * dt seconds.  Returns IMPES_OK, or the status of the first failing member
+ * (impes_last_error names it); per-member results are in stats[members].
+ * span_ms (may be NULL) receives the device time from before the first
+ * member's first kernel to after the last member's last kernel.
+ * Handles of different members must be distinct. */
+typedef struct {
+  int status;            /* IMPES_OK or this member's error                 */
+  int steps_done;
+  long long iterations;  /* FGMRES iterations over its steps                */
+  double device_ms;      /* device time of its steps on its worker's stream */
+  int worker;            /* host thread that ran it                         */
+} impes_ensemble_member_stats;
+int impes_ensemble_run(impes_model** models, impes_amg** amgs, double** p, double** sw,
+                       double** sg, double** so, const int* cells, int members, int steps,
+                       double dt, const impes_krylov_params* kp, int workers,
+                       impes_ensemble_member_stats* stats, double* span_ms);
+
 /* ------------------------------------------------------------------ adjoint
  * Discrete adjoint of the IMPES step (no counterpart in the reference).
  * Objective J = sum over steps and producers of (q_o - q_target)^2, q_o the

@@ -8,6 +8,7 @@ namespace impes {
 struct Level {
   int n = 0, nnz = 0;
   DBuf<int> rowptr, col;
+  DBuf<unsigned short> col16;      // col as 16-bit indices (wide levels of <= 65536 rows)
   DBuf<double> val;
   DBuf<float> valf;
   DBuf<double> inv_relax;

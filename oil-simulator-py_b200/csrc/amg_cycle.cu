@@ -56,9 +56,84 @@ __global__ void __launch_bounds__(TB) k_csr(int n, const int* __restrict__ rowpt
   }
 }
 
+// Four consecutive matrix values starting at a 4-element boundary (16-byte
+// loads: one float4, or two double2).
+__device__ __forceinline__ void load4(const float* p, float& a, float& b, float& c, float& d) {
+  const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+  a = v.x; b = v.y; c = v.z; d = v.w;
+}
+__device__ __forceinline__ void load4(const double* p, double& a, double& b, double& c, double& d) {
+  const double2 v0 = __ldg(reinterpret_cast<const double2*>(p));
+  const double2 v1 = __ldg(reinterpret_cast<const double2*>(p) + 1);
+  a = v0.x; b = v0.y; c = v1.x; d = v1.y;
+}
+
+// Four consecutive column indices starting at a 4-element boundary.
+__device__ __forceinline__ void load4c(const int* p, int& a, int& b, int& c, int& d) {
+  const int4 v = __ldg(reinterpret_cast<const int4*>(p));
+  a = v.x; b = v.y; c = v.z; d = v.w;
+}
+__device__ __forceinline__ void load4c(const unsigned short* p, int& a, int& b, int& c, int& d) {
+  const ushort4 v = __ldg(reinterpret_cast<const ushort4*>(p));
+  a = v.x; b = v.y; c = v.z; d = v.w;
+}
+
+// Warp per row for wide rows (coarse Galerkin levels, hundreds to thousands of
+// entries per row): the aligned body of each row is read as vectors of 4
+// columns and 4 values per lane with four independent partial sums, so each
+// lane keeps 24-32 bytes of matrix in flight instead of 8.  CT is int, or
+// unsigned short on levels of at most 65536 rows (6 bytes per entry instead of
+// 8 in fp32).  col and val must be 16-byte aligned (device allocations are).
+// Same epilogues as k_csr.
+template <typename T, typename CT, int MODE>
+__global__ void __launch_bounds__(TB) k_csr_warp(int n, const int* __restrict__ rowptr,
+                                                 const CT* __restrict__ col, const T* __restrict__ val,
+                                                 const T* __restrict__ x, const T* __restrict__ b,
+                                                 const T* __restrict__ inv, T* __restrict__ y) {
+  const int lane = threadIdx.x & 31;
+  constexpr int kWarps = TB / 32;
+  for (long long row = (long long)blockIdx.x * kWarps + (threadIdx.x >> 5); row < n;
+       row += (long long)gridDim.x * kWarps) {
+    const int a = rowptr[row], e = rowptr[row + 1];
+    int a4 = (a + 3) & ~3;
+    if (a4 > e) a4 = e;
+    const int nv = (e - a4) >> 2;             // whole 4-element vectors
+    const int t0 = a4 + (nv << 2);            // tail start
+    T s0 = T(0), s1 = T(0), s2 = T(0), s3 = T(0);
+    if (a + lane < a4) s0 = val[a + lane] * x[col[a + lane]];
+    if (t0 + lane < e) s1 = val[t0 + lane] * x[col[t0 + lane]];
+    const CT* c4 = col + a4;
+    const T* v4 = val + a4;
+#pragma unroll 2
+    for (int q = lane; q < nv; q += 32) {
+      int ca, cb, cc, cd;
+      load4c(c4 + 4 * q, ca, cb, cc, cd);
+      T va, vb, vc, vd;
+      load4(v4 + 4 * q, va, vb, vc, vd);
+      s0 += va * x[ca];
+      s1 += vb * x[cb];
+      s2 += vc * x[cc];
+      s3 += vd * x[cd];
+    }
+    T acc = (s0 + s1) + (s2 + s3);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (lane == 0) {
+      if (MODE == Y_AX) y[row] = acc;
+      else if (MODE == Y_B_MINUS_AX) y[row] = b[row] - acc;
+      else if (MODE == Y_SMOOTH) y[row] = x[row] + T(kOmega) * inv[row] * (b[row] - acc);
+      else if (MODE == Y_ADD_AX) y[row] = y[row] + acc;
+      else if (MODE == Y_W_AX) y[row] = inv[row] * acc;
+    }
+  }
+}
+
+// col16: the same column indices as unsigned short (levels of at most 65536
+// rows), or null; used by the warp-per-row kernel only.
 template <typename T, int MODE>
 void launch_csr(int n, int avg, const int* rowptr, const int* col, const T* val, const T* x,
-                const T* b, const T* inv, T* y, cudaStream_t s) {
+                const T* b, const T* inv, T* y, cudaStream_t s,
+                const unsigned short* col16 = nullptr) {
   if (n <= 0) return;
   int lpr = avg <= 8 ? 1 : avg <= 16 ? 4 : avg <= 48 ? 8 : avg <= 96 ? 16 : 32;
   if (MODE == Y_SMOOTH0) lpr = 1;
@@ -68,7 +143,10 @@ void launch_csr(int n, int avg, const int* rowptr, const int* col, const T* val,
     case 4: k_csr<T, 4, MODE><<<grid(4), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y); ::impes::count_launch(); break;
     case 8: k_csr<T, 8, MODE><<<grid(8), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y); ::impes::count_launch(); break;
     case 16: k_csr<T, 16, MODE><<<grid(16), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y); ::impes::count_launch(); break;
-    default: k_csr<T, 32, MODE><<<grid(32), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y); ::impes::count_launch(); break;
+    default:
+      if (col16) { k_csr_warp<T, unsigned short, MODE><<<grid(32), TB, 0, s>>>(n, rowptr, col16, val, x, b, inv, y); ::impes::count_launch(); }
+      else { k_csr_warp<T, int, MODE><<<grid(32), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y); ::impes::count_launch(); }
+      break;
   }
   IMPES_CHECK_LAUNCH();
 }
@@ -348,7 +426,10 @@ template <> struct LV<float> {
 inline double spmv_bytes(double sv, double sx, double nnz, double rows, double cols) {
   return (sv + 4.0) * nnz + 4.0 * (rows + 1) + sx * cols + sx * rows;
 }
-inline double sweep_bytes(double s, double nnz, double n) { return (s + 4.0) * nnz + 4.0 * n + 4.0 * s * n; }
+// l1-Jacobi sweep: values, column indices (si bytes each), row pointers, x, b, inv, y.
+inline double sweep_bytes(double s, double nnz, double n, double si = 4.0) {
+  return (s + si) * nnz + 4.0 * n + 4.0 * s * n;
+}
 
 // nu l1-Jacobi sweeps (classical_amg.py:1016-1035); returns the buffer holding x.
 // Level-0 sweeps with a non-zero iterate are timed as IMPES_PH_SMOOTH_L0.
@@ -364,8 +445,8 @@ T* smooth(Level& L, T* x, T* spare, const T* b, int nu, bool zero_x, cudaStream_
     const int tid = top ? timers().begin(IMPES_PH_SMOOTH_L0, s)
                         : (wide ? timers().begin(IMPES_PH_SMOOTH_WIDE, s) : -1);
     launch_csr<T, Y_SMOOTH>(L.n, L.avg_row, L.rowptr.p, L.col.p, LV<T>::val(L), x, b,
-                            LV<T>::inv(L), spare, s);
-    timers().end(tid, s, sweep_bytes(sizeof(T), L.nnz, L.n));
+                            LV<T>::inv(L), spare, s, L.col16.p);
+    timers().end(tid, s, sweep_bytes(sizeof(T), L.nnz, L.n, L.col16.p ? 2.0 : 4.0));
     std::swap(x, spare);
   }
   return x;
@@ -413,7 +494,7 @@ T* vcycle(AMG& h, int l, bool zero_x, cudaStream_t s) {
   T* spare = (x == LV<T>::x(L)) ? LV<T>::t(L) : LV<T>::x(L);
   Level& Nc = *h.levels[l + 1];
   launch_csr<T, Y_B_MINUS_AX>(L.n, L.avg_row, L.rowptr.p, L.col.p, LV<T>::val(L), x, LV<T>::b(L),
-                              nullptr, LV<T>::r(L), s);
+                              nullptr, LV<T>::r(L), s, L.col16.p);
   launch_csr<T, Y_AX>(L.nc, L.r_avg, L.rrow.p, L.rcol.p, LV<T>::rval(L), LV<T>::r(L), nullptr,
                       nullptr, LV<T>::b(Nc), s);
   T* ec = vcycle<T>(h, l + 1, true, s);
@@ -432,8 +513,8 @@ T* vcycle_top(AMG& h, bool zero_x, cudaStream_t s) {
   AMG::VGraph& g = h.vgraph[sizeof(T) == 4][zero_x][h.krylov_mode][tm.on];
   if (!g.exec) {
     if (!h.cap_stream) IMPES_CUDA(cudaStreamCreateWithFlags(&h.cap_stream, cudaStreamNonBlocking));
-    const unsigned long long before = launches();
-    tm.capture = &g.timers;
+    const unsigned long long before = thread_launches();
+    if (tm.on) tm.capture = &g.timers;   // timer nodes only in the timed variant
     IMPES_CUDA(cudaStreamBeginCapture(h.cap_stream, cudaStreamCaptureModeThreadLocal));
     T* out = nullptr;
     cudaGraph_t graph = nullptr;
@@ -451,7 +532,7 @@ T* vcycle_top(AMG& h, bool zero_x, cudaStream_t s) {
     cudaGraphDestroy(graph);
     IMPES_CUDA(e);
     g.out = out;
-    g.kernels = (long long)(launches() - before);
+    g.kernels = (long long)(thread_launches() - before);
     count_launches(-g.kernels);
   }
   IMPES_CUDA(cudaGraphLaunch(g.exec, s));

@@ -62,6 +62,11 @@ __global__ void k_nonfinite(const double* v, long long n, int* flag) {
 
 // ------------------------------------------------------- diag / scaling
 // _extract_diag (classical_amg.py:940-955): value of the diagonal entry, 0 if none.
+__global__ void k_narrow_cols(int nnz, const int* col, unsigned short* col16) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nnz;
+       e += (long long)gridDim.x * blockDim.x)
+    col16[e] = (unsigned short)col[e];
+}
 __global__ void k_diag(int n, const int* rowptr, const int* col, const double* val, double* d) {
   GRID_LOOP(i, n) {
     double v = 0.0;
@@ -850,7 +855,7 @@ void union_symbolic(AMG& h, int rows, const int* optr, const int* ocol, const in
   const size_t per_warp = sizeof(int) * (2 * (size_t)hsize + 1);
   const int wpb = (int)std::max<size_t>(1, std::min<size_t>(8, (64u << 10) / per_warp));
   const size_t smem = per_warp * wpb;
-  IMPES_CUDA(cudaFuncSetAttribute(k_union_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  raise_smem_limit((const void*)k_union_rows, smem);
   unsigned grid = (unsigned)std::min<long long>((rows + wpb - 1) / wpb, (long long)num_sms() * 32);
   k_union_rows<<<std::max(1u, grid), 32 * wpb, smem, s>>>(rows, optr, ocol, iptr, icol, hsize, bound.p,
                                                           goff.p, gscratch.p, ucnt.p, nullptr, nullptr); ::impes::count_launch();
@@ -937,7 +942,7 @@ void union_numeric(int rows, const int* optr, const int* ocol, const double* ova
   if (per_warp * 8 + 16 <= (96u << 10)) {
     constexpr int W = 8;
     size_t smem = per_warp * W + 16;
-    IMPES_CUDA(cudaFuncSetAttribute(k_union_numeric<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    raise_smem_limit((const void*)k_union_numeric<W>, smem);
     unsigned grid = (unsigned)std::min<long long>((rows + W - 1) / W, (long long)num_sms() * 16);
     k_union_numeric<W><<<grid, 32 * W, smem, s>>>(rows, optr, ocol, oval, iptr, icol, ival, outptr,
                                                    outcol, outval, maxrow); ::impes::count_launch();
@@ -945,7 +950,7 @@ void union_numeric(int rows, const int* optr, const int* ocol, const double* ova
     constexpr int W = 1;
     size_t smem = per_warp * W + 16;
     IMPES_REQUIRE(smem <= (220u << 10), IMPES_ERR_ARG, "Galerkin row too wide for shared memory");
-    IMPES_CUDA(cudaFuncSetAttribute(k_union_numeric<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    raise_smem_limit((const void*)k_union_numeric<W>, smem);
     unsigned grid = (unsigned)std::min<long long>(rows, (long long)num_sms() * 32);
     k_union_numeric<W><<<grid, 32 * W, smem, s>>>(rows, optr, ocol, oval, iptr, icol, ival, outptr,
                                                    outcol, outval, maxrow); ::impes::count_launch();
@@ -1171,6 +1176,17 @@ void amg_setup(AMG& h, int n, int nnz, const int* rowptr, const int* col, const 
   }
   coarse_factor(h, Lc, s);
   for (auto& L : h.levels) level_precision_copies(h, *L, s);
+  // 16-bit column indices for the warp-per-row levels that fit (the pattern is
+  // fixed from here on: update_matrix only changes values)
+  for (auto& L : h.levels) {
+    if (L->n <= 65536 && L->avg_row > 96 && L->nnz > 0) {
+      L->col16.alloc(L->nnz);
+      k_narrow_cols<<<grid_for(L->nnz, 256), 256, 0, s>>>(L->nnz, L->col.p, L->col16.p); ::impes::count_launch();
+      IMPES_CHECK_LAUNCH();
+    } else {
+      L->col16 = DBuf<unsigned short>();
+    }
+  }
   IMPES_CUDA(cudaStreamSynchronize(s));
   h.built = true;
 }

@@ -28,6 +28,7 @@ SOURCES = {
     "amg_setup.cu": [],
     "amg_cycle.cu": [],
     "adjoint.cu": [],
+    "ensemble.cu": [],
     "abi.cu": [],
 }
 HEADERS = ["common.cuh", "model.cuh", "amg.cuh", os.path.join(REPO, "include", "impes_b200.h")]

@@ -1,6 +1,8 @@
 // Shared host utilities: thread-local error text and a device exclusive scan.
 #include "common.cuh"
 #include <atomic>
+#include <map>
+#include <mutex>
 
 namespace impes {
 
@@ -9,9 +11,28 @@ static thread_local std::string g_last_error;
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 
 static std::atomic<unsigned long long> g_launches{0};
-void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
-void count_launches(long long n) { g_launches.fetch_add((unsigned long long)n, std::memory_order_relaxed); }
+static thread_local unsigned long long t_launches = 0;   // this host thread's launches
+void count_launch() {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  ++t_launches;
+}
+void count_launches(long long n) {
+  g_launches.fetch_add((unsigned long long)n, std::memory_order_relaxed);
+  t_launches += (unsigned long long)n;
+}
 unsigned long long launches() { return g_launches.load(std::memory_order_relaxed); }
+unsigned long long thread_launches() { return t_launches; }
+
+void raise_smem_limit(const void* kernel, size_t bytes) {
+  static std::mutex mu;
+  static std::map<const void*, size_t> current;
+  std::lock_guard<std::mutex> lock(mu);
+  size_t& c = current[kernel];
+  if (bytes > c) {
+    IMPES_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    c = bytes;
+  }
+}
 const char* last_error_cstr() { return g_last_error.c_str(); }
 
 PhaseTimers& timers() {

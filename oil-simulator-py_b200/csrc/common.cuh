@@ -25,6 +25,11 @@ void set_last_error(const std::string& msg);
 void count_launch();
 void count_launches(long long n);
 unsigned long long launches();
+unsigned long long thread_launches();   // launches issued by the calling host thread
+// Raise a kernel's dynamic shared-memory limit to at least `bytes`; never
+// lowers it, so host threads launching the same kernel with different sizes
+// do not undo each other's setting.
+void raise_smem_limit(const void* kernel, size_t bytes);
 
 #define IMPES_CUDA(call)                                                        \
   do {                                                                          \

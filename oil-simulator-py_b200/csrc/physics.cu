@@ -18,6 +18,7 @@
 #include "model.cuh"
 #include <algorithm>
 #include <math.h>
+#include <mutex>
 
 namespace impes {
 
@@ -214,8 +215,10 @@ Brick make_brick(const ModelParams& P) {
 // Raise a kernel's dynamic shared-memory limit when a launch needs more.
 template <typename K>
 void ensure_smem(K kernel, size_t bytes, size_t& current) {
+  static std::mutex mu;   // several host threads may step different models
+  std::lock_guard<std::mutex> lock(mu);
   if (bytes > current) {
-    IMPES_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    raise_smem_limit((const void*)kernel, bytes);
     current = bytes;
   }
 }

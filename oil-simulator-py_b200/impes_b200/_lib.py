@@ -93,6 +93,11 @@ class AdjointStats(C.Structure):
                 ("reverse_ms", C.c_double), ("checkpoints", C.c_int), ("recomputed_steps", C.c_int)]
 
 
+class EnsembleMemberStats(C.Structure):
+    _fields_ = [("status", C.c_int), ("steps_done", C.c_int), ("iterations", C.c_longlong),
+                ("device_ms", C.c_double), ("worker", C.c_int)]
+
+
 class Timing(C.Structure):
     _fields_ = [("count", C.c_longlong * 9), ("ms", C.c_double * 9), ("bytes", C.c_double * 9)]
 
@@ -113,6 +118,8 @@ _SIGNATURES = {
     "impes_amg_setup": ([_P, _I, _I, _P, _P, _P, _P], _I),
     "impes_amg_update": ([_P, _P, _P], _I),
     "impes_amg_solve_vcycles": ([_P, _P, _P, _D, _I, C.POINTER(_I), C.POINTER(_D), _I, _P], _I),
+    "impes_ensemble_run": ([_P, _P, _P, _P, _P, _P, _P, _I, _I, _D, C.POINTER(KrylovParams), _I,
+                            _P, C.POINTER(_D)], _I),
     "impes_adjoint_num_producers": ([_P, C.POINTER(_I)], _I),
     "impes_adjoint_rates": ([_P, _P, _P, _P, _I, _D, C.POINTER(KrylovParams), _P, _P], _I),
     "impes_adjoint_gradient": ([_P, _P, _P, _P, _P, _P, _P, _I, _I, _D, C.POINTER(KrylovParams),

@@ -192,7 +192,7 @@ class ClassicalAMG:
                                               _lib.stream_of(self.device)), "impes_amg_vcycle_scaled")
         return x
 
-    def fgmres(self, b, tol: float = 1e-6, restart: int = 30, max_iters: int = 300,
+    def fgmres(self, b, tol: float = 1e-6, restart: int = 60, max_iters: int = 300,
                norm: str = "jacobi", precision: str = "fp64", x0: Optional[torch.Tensor] = None):
         """FGMRES with one V-cycle per iteration.  Returns (x, stats dict)."""
         bb = self._vec(b)
@@ -273,7 +273,7 @@ _AMG_CACHE: Dict[Tuple[Any, ...], ClassicalAMG] = {}
 def amg_solve(A, b: torch.Tensor, *, tol: float = 1e-6, max_cycles: int = 20, theta: float = 0.25,
               max_levels: int = 10, coarsest_size: int = 200, device: Optional[str] = "auto",
               enable_equilibration: Optional[bool] = None, method: str = "vcycle",
-              norm: str = "equilibrated", precision: str = "fp64", restart: int = 30,
+              norm: str = "equilibrated", precision: str = "fp64", restart: int = 60,
               max_iters: Optional[int] = None, seed: int = 0) -> torch.Tensor:
     """Solve A x = b (``amg_solve``, pressure_amg.py:35-89).
 

@@ -412,7 +412,7 @@ class Simulator:
         self.amg_tol = float(amg_cfg.get("tol", sim_params.get("cg_tolerance", 1e-6)))
         self.amg_max_cycles = int(amg_cfg.get("max_cycles", 20))
         self.amg_max_iters = int(amg_cfg.get("max_iters", 400))
-        self.amg_restart = int(amg_cfg.get("restart", 30))
+        self.amg_restart = int(amg_cfg.get("restart", 60))
         # the reference's own stopping norm for its stand-alone V-cycles
         self.amg_norm = amg_cfg.get("norm", "equilibrated" if self.pressure_solver == "amg" else "jacobi")
         self.amg_precision = amg_cfg.get("precision", "fp64")
