@@ -253,11 +253,23 @@ int impes_saturation(impes_model* m, const double* p_new, double* sw, double* sg
 /* One full IMPES step, _impes_step (simulation.py:822-865): assemble, AMG
  * setup on first use / update_matrix afterwards, pressure solve
  * (solver = 0: stand-alone V-cycles to kp->tol in the equilibrated norm, the
- * reference's "amg" branch; solver = 1: FGMRES per kp), then the saturation
- * update.  p is replaced by the new pressure.  kstats/sstats may be NULL. */
+ * reference's "amg" branch; solver = 1: FGMRES per kp; solver = 2: the
+ * reference's default Jacobi-PCG from zero to sqrt(r.M^-1 r) < kp->tol within
+ * kp->max_iters, then once more with 10x the tolerance and 4x the iterations,
+ * simulation.py:931-966 -- amg may be NULL), then the saturation update.  p is
+ * replaced by the new pressure; on a missed tolerance p is restored and
+ * IMPES_ERR_NOT_CONVERGED returned.  kstats/sstats may be NULL. */
 int impes_step(impes_model* m, impes_amg* amg, double* p, double* sw, double* sg, double* so,
                double dt, int solver, const impes_krylov_params* kp, int max_cycles,
                impes_krylov_stats* kstats, impes_sat_stats* sstats, void* stream);
+
+/* Simulator._solve_pressure_cg_pytorch (simulation.py:1662-1697): Jacobi-
+ * preconditioned CG on a CSR matrix (device arrays, n rows) from x = 0, stopping
+ * when sqrt(r . D^-1 r) < tol (absolute) or after max_iter iterations.  x is
+ * written; iterations, converged and the last r . D^-1 r (rz) may be NULL. */
+int impes_pcg_solve(int n, const int* rowptr, const int* col, const double* val, const double* b,
+                    double* x, double tol, int max_iter, int* iterations, int* converged,
+                    double* rz, void* stream);
 
 /* Running balances and per-well diagnostics (host outputs; syncs the stream). */
 int impes_model_balances(impes_model* m, impes_sat_stats* stats, void* stream);
@@ -278,7 +290,7 @@ enum {
   IMPES_PH_SPMV_L0 = 5,    /* FGMRES operator product on level 0          */
   IMPES_PH_ORTHO = 6,      /* FGMRES Gram-Schmidt of one iteration        */
   IMPES_PH_SOLVE = 7,      /* whole pressure solve                        */
-  IMPES_PH_SMOOTH_WIDE = 8,/* one l1-Jacobi sweep on a level with > 96 nnz per row (warp per row) */
+  IMPES_PH_SMOOTH_WIDE = 8,/* one l1-Jacobi sweep on a level with > 96 nnz per row (warps per row) */
   IMPES_NUM_PHASES = 9
 };
 typedef struct {

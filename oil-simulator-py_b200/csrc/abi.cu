@@ -22,6 +22,9 @@ bool impes_amg_handle_built(impes_amg* h) { return h && h->a.built; }
 impes::AMG* impes_amg_handle_core(impes_amg* h) { return &h->a; }
 
 namespace impes {
+void pcg_solve(int n, const int* rowptr, const int* col, const double* val, const double* b,
+               double* x, double tol, int max_iter, int& iters, bool& converged, double& rs_out,
+               cudaStream_t s);
 void adjoint_check_model(const Model& m);
 int adjoint_num_producers(const Model& m);
 void adjoint_rates(Model& m, AMG& a, double* p, double* sw, int steps, double dt,
@@ -361,16 +364,20 @@ int impes_step(impes_model* h, impes_amg* amg, double* p, double* sw, double* sg
                double dt, int solver, const impes_krylov_params* kp, int max_cycles,
                impes_krylov_stats* kstats, impes_sat_stats* sstats, void* stream) {
   return guarded([&] {
-    IMPES_REQUIRE(h && amg && p && sw && sg && so && kp, IMPES_ERR_ARG, "null argument");
+    IMPES_REQUIRE(h && p && sw && sg && so && kp, IMPES_ERR_ARG, "null argument");
     IMPES_REQUIRE(dt > 0, IMPES_ERR_ARG, "dt must be positive");
+    IMPES_REQUIRE(solver >= 0 && solver <= 2, IMPES_ERR_ARG, "solver must be 0, 1 or 2");
     Model& m = h->m;
     cudaStream_t s = S(stream);
     model_assemble(m, p, sw, sg, dt, m.csr_val.p, m.rhs.p, s);
-    AMG& a = amg->a;
-    if (!a.built || a.levels[0]->n != m.P.N)
-      amg_setup(a, m.P.N, m.nnz, m.rowptr.p, m.col.p, m.csr_val.p, s);
-    else
-      amg_update(a, m.csr_val.p, s);
+    IMPES_REQUIRE(solver == 2 || amg, IMPES_ERR_ARG, "null AMG handle");
+    if (solver != 2) {
+      AMG& a = amg->a;
+      if (!a.built || a.levels[0]->n != m.P.N)
+        amg_setup(a, m.P.N, m.nnz, m.rowptr.p, m.col.p, m.csr_val.p, s);
+      else
+        amg_update(a, m.csr_val.p, s);
+    }
     impes_krylov_stats st{};
     // a failed pressure solve leaves the state as it was (the caller may retry
     // with a smaller dt, as _impes_step does at simulation.py:833-862)
@@ -380,7 +387,25 @@ int impes_step(impes_model* h, impes_amg* amg, double* p, double* sw, double* sg
       cudaStreamSynchronize(s);
     };
     try {
-      if (solver == 0) {
+      if (solver == 2) {
+        // _impes_pressure_step's CG and its one relaxed retry (simulation.py:931-966)
+        int it = 0;
+        bool conv = false;
+        double rz = 0.0;
+        pcg_solve(m.P.N, m.rowptr.p, m.col.p, m.csr_val.p, m.rhs.p, p, kp->tol, kp->max_iters, it,
+                  conv, rz, s);
+        st.iterations = it;
+        if (!conv) {
+          pcg_solve(m.P.N, m.rowptr.p, m.col.p, m.csr_val.p, m.rhs.p, p, kp->tol * 10.0,
+                    kp->max_iters * 4, it, conv, rz, s);
+          st.iterations += it;
+          st.restarts = 1;
+        }
+        st.rel_res = std::sqrt(std::max(rz, 0.0));
+        st.true_rel_res = st.rel_res;
+        st.converged = conv;
+      } else if (solver == 0) {
+        AMG& a = amg->a;
         int cyc = 0;
         double rel = 0.0;
         amg_solve_vcycles(a, m.rhs.p, p, kp->tol, std::max(1, max_cycles), &cyc, &rel, s, kp->norm);
@@ -390,7 +415,7 @@ int impes_step(impes_model* h, impes_amg* amg, double* p, double* sw, double* sg
         st.converged = rel < kp->tol;
       } else {
         impes_krylov_params k = *kp;
-        amg_fgmres(a, m.rhs.p, p, k, st, s);
+        amg_fgmres(amg->a, m.rhs.p, p, k, st, s);
       }
     } catch (...) {
       restore();
@@ -399,7 +424,8 @@ int impes_step(impes_model* h, impes_amg* amg, double* p, double* sw, double* sg
     if (kstats) *kstats = st;
     if (solver != 0 && !st.converged) {
       restore();
-      throw Error(IMPES_ERR_NOT_CONVERGED, "FGMRES did not reach the pressure tolerance");
+      throw Error(IMPES_ERR_NOT_CONVERGED, solver == 2 ? "CG did not reach the pressure tolerance"
+                                                       : "FGMRES did not reach the pressure tolerance");
     }
     model_saturation(m, p, sw, sg, so, dt, s);
     if (sstats) {
@@ -525,5 +551,20 @@ int impes_adjoint_gradient(impes_model* h, impes_amg* amg, const double* p0, con
     adjoint_gradient(h->m, amg->a, p0, sw0, kx, ky, kz, steps, checkpoint_every, dt, *forward,
                      *adjoint, target_host, rates_host, g_lnk, g_poro, st, S(stream));
     if (stats) *stats = st;
+  });
+}
+
+int impes_pcg_solve(int n, const int* rowptr, const int* col, const double* val, const double* b,
+                    double* x, double tol, int max_iter, int* iterations, int* converged,
+                    double* rz, void* stream) {
+  return guarded([&] {
+    IMPES_REQUIRE(rowptr && col && val && b && x, IMPES_ERR_ARG, "null argument");
+    int it = 0;
+    bool conv = false;
+    double r = 0.0;
+    pcg_solve(n, rowptr, col, val, b, x, tol, max_iter, it, conv, r, S(stream));
+    if (iterations) *iterations = it;
+    if (converged) *converged = conv ? 1 : 0;
+    if (rz) *rz = r;
   });
 }

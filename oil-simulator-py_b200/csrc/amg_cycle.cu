@@ -56,80 +56,75 @@ __global__ void __launch_bounds__(TB) k_csr(int n, const int* __restrict__ rowpt
   }
 }
 
-// Four consecutive matrix values starting at a 4-element boundary (16-byte
-// loads: one float4, or two double2).
-__device__ __forceinline__ void load4(const float* p, float& a, float& b, float& c, float& d) {
-  const float4 v = __ldg(reinterpret_cast<const float4*>(p));
-  a = v.x; b = v.y; c = v.z; d = v.w;
-}
-__device__ __forceinline__ void load4(const double* p, double& a, double& b, double& c, double& d) {
-  const double2 v0 = __ldg(reinterpret_cast<const double2*>(p));
-  const double2 v1 = __ldg(reinterpret_cast<const double2*>(p) + 1);
-  a = v0.x; b = v0.y; c = v1.x; d = v1.y;
-}
-
-// Four consecutive column indices starting at a 4-element boundary.
-__device__ __forceinline__ void load4c(const int* p, int& a, int& b, int& c, int& d) {
-  const int4 v = __ldg(reinterpret_cast<const int4*>(p));
-  a = v.x; b = v.y; c = v.z; d = v.w;
-}
-__device__ __forceinline__ void load4c(const unsigned short* p, int& a, int& b, int& c, int& d) {
-  const ushort4 v = __ldg(reinterpret_cast<const ushort4*>(p));
-  a = v.x; b = v.y; c = v.z; d = v.w;
-}
-
-// Warp per row for wide rows (coarse Galerkin levels, hundreds to thousands of
-// entries per row): the aligned body of each row is read as vectors of 4
-// columns and 4 values per lane with four independent partial sums, so each
-// lane keeps 24-32 bytes of matrix in flight instead of 8.  CT is int, or
-// unsigned short on levels of at most 65536 rows (6 bytes per entry instead of
-// 8 in fp32).  col and val must be 16-byte aligned (device allocations are).
-// Same epilogues as k_csr.
-template <typename T, typename CT, int MODE>
-__global__ void __launch_bounds__(TB) k_csr_warp(int n, const int* __restrict__ rowptr,
+// Wide rows (coarse Galerkin levels, hundreds to thousands of entries per row):
+// WPR warps per row, chosen by the mean row length.  Thread t of the row group
+// takes entries a+t, a+t+G, ... (G = 32*WPR), so each warp's value and column
+// loads are coalesced and its gathers of x hit adjacent columns.  CT is int, or
+// unsigned short on levels of at most 65536 rows (6 bytes per fp32 entry
+// instead of 8).  With WPR > 1 the row's first warp adds the group's partial
+// sums in a fixed order.  Same epilogues as k_csr.
+template <typename T, typename CT, int MODE, int WPR>
+__global__ void __launch_bounds__(TB) k_csr_rows(int n, const int* __restrict__ rowptr,
                                                  const CT* __restrict__ col, const T* __restrict__ val,
                                                  const T* __restrict__ x, const T* __restrict__ b,
                                                  const T* __restrict__ inv, T* __restrict__ y) {
-  const int lane = threadIdx.x & 31;
-  constexpr int kWarps = TB / 32;
-  for (long long row = (long long)blockIdx.x * kWarps + (threadIdx.x >> 5); row < n;
-       row += (long long)gridDim.x * kWarps) {
-    const int a = rowptr[row], e = rowptr[row + 1];
-    int a4 = (a + 3) & ~3;
-    if (a4 > e) a4 = e;
-    const int nv = (e - a4) >> 2;             // whole 4-element vectors
-    const int t0 = a4 + (nv << 2);            // tail start
-    T s0 = T(0), s1 = T(0), s2 = T(0), s3 = T(0);
-    if (a + lane < a4) s0 = val[a + lane] * x[col[a + lane]];
-    if (t0 + lane < e) s1 = val[t0 + lane] * x[col[t0 + lane]];
-    const CT* c4 = col + a4;
-    const T* v4 = val + a4;
-#pragma unroll 2
-    for (int q = lane; q < nv; q += 32) {
-      int ca, cb, cc, cd;
-      load4c(c4 + 4 * q, ca, cb, cc, cd);
-      T va, vb, vc, vd;
-      load4(v4 + 4 * q, va, vb, vc, vd);
-      s0 += va * x[ca];
-      s1 += vb * x[cb];
-      s2 += vc * x[cc];
-      s3 += vd * x[cd];
-    }
-    T acc = (s0 + s1) + (s2 + s3);
+  constexpr int kWarps = TB / 32, kRows = kWarps / WPR, G = 32 * WPR;
+  __shared__ T part[kWarps];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int grp = warp / WPR, sub = warp % WPR;
+  const int tid = sub * 32 + lane;
+  for (long long base = (long long)blockIdx.x * kRows; base < n; base += (long long)gridDim.x * kRows) {
+    const long long row = base + grp;
+    T acc = T(0);
+    if (row < n) {
+      const int a = rowptr[row], e = rowptr[row + 1];
+      for (int k = a + tid; k < e; k += G) acc += val[k] * x[col[k]];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-    if (lane == 0) {
-      if (MODE == Y_AX) y[row] = acc;
-      else if (MODE == Y_B_MINUS_AX) y[row] = b[row] - acc;
-      else if (MODE == Y_SMOOTH) y[row] = x[row] + T(kOmega) * inv[row] * (b[row] - acc);
-      else if (MODE == Y_ADD_AX) y[row] = y[row] + acc;
-      else if (MODE == Y_W_AX) y[row] = inv[row] * acc;
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
     }
+    if (WPR == 1) {
+      if (lane == 0 && row < n) {
+        if (MODE == Y_AX) y[row] = acc;
+        else if (MODE == Y_B_MINUS_AX) y[row] = b[row] - acc;
+        else if (MODE == Y_SMOOTH) y[row] = x[row] + T(kOmega) * inv[row] * (b[row] - acc);
+        else if (MODE == Y_ADD_AX) y[row] = y[row] + acc;
+        else if (MODE == Y_W_AX) y[row] = inv[row] * acc;
+      }
+      continue;
+    }
+    if (lane == 0) part[warp] = acc;
+    __syncthreads();
+    if (sub == 0 && lane == 0 && row < n) {
+      T t = part[warp];
+#pragma unroll
+      for (int w = 1; w < WPR; ++w) t += part[warp + w];
+      if (MODE == Y_AX) y[row] = t;
+      else if (MODE == Y_B_MINUS_AX) y[row] = b[row] - t;
+      else if (MODE == Y_SMOOTH) y[row] = x[row] + T(kOmega) * inv[row] * (b[row] - t);
+      else if (MODE == Y_ADD_AX) y[row] = y[row] + t;
+      else if (MODE == Y_W_AX) y[row] = inv[row] * t;
+    }
+    __syncthreads();
+  }
+}
+
+template <typename T, typename CT, int MODE>
+void launch_wide(int n, int avg, const int* rowptr, const CT* col, const T* val, const T* x,
+                 const T* b, const T* inv, T* y, cudaStream_t s) {
+  auto grid = [&](int rows_per_block) {
+    return grid_for(((size_t)(n + rows_per_block - 1) / rows_per_block) * TB, TB, 16);
+  };
+  if (avg <= 512) {
+    k_csr_rows<T, CT, MODE, 1><<<grid(8), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y); ::impes::count_launch();
+  } else if (avg <= 1536) {
+    k_csr_rows<T, CT, MODE, 2><<<grid(4), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y); ::impes::count_launch();
+  } else {
+    k_csr_rows<T, CT, MODE, 4><<<grid(2), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y); ::impes::count_launch();
   }
 }
 
 // col16: the same column indices as unsigned short (levels of at most 65536
-// rows), or null; used by the warp-per-row kernel only.
+// rows), or null; used by the wide-row kernels only.
 template <typename T, int MODE>
 void launch_csr(int n, int avg, const int* rowptr, const int* col, const T* val, const T* x,
                 const T* b, const T* inv, T* y, cudaStream_t s,
@@ -144,8 +139,8 @@ void launch_csr(int n, int avg, const int* rowptr, const int* col, const T* val,
     case 8: k_csr<T, 8, MODE><<<grid(8), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y); ::impes::count_launch(); break;
     case 16: k_csr<T, 16, MODE><<<grid(16), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y); ::impes::count_launch(); break;
     default:
-      if (col16) { k_csr_warp<T, unsigned short, MODE><<<grid(32), TB, 0, s>>>(n, rowptr, col16, val, x, b, inv, y); ::impes::count_launch(); }
-      else { k_csr_warp<T, int, MODE><<<grid(32), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y); ::impes::count_launch(); }
+      if (col16) launch_wide<T, unsigned short, MODE>(n, avg, rowptr, col16, val, x, b, inv, y, s);
+      else launch_wide<T, int, MODE>(n, avg, rowptr, col, val, x, b, inv, y, s);
       break;
   }
   IMPES_CHECK_LAUNCH();

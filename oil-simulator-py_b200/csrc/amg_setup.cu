@@ -633,7 +633,8 @@ __global__ void k_plan_sort(int nout, const int* seg, long long* key, int* pe, i
     }
   }
 }
-// out[o] = sum over the segment of a[pe] * b[pf]
+// out[o] = sum over the segment of a[pe] * b[pf]; one thread per output walks
+// its own run of the plan (consecutive terms share cache lines).
 __global__ void __launch_bounds__(256) k_plan_apply(int nout, const int* __restrict__ seg,
                                                     const int* __restrict__ pe,
                                                     const int* __restrict__ pf,
@@ -645,6 +646,13 @@ __global__ void __launch_bounds__(256) k_plan_apply(int nout, const int* __restr
     for (int t = seg[o]; t < seg[o + 1]; ++t) acc += a[pe[t]] * b[pf[t]];
     out[o] = acc;
   }
+}
+
+void plan_apply(int nout, const int* seg, const int* pe, const int* pf, const double* a,
+                const double* b, double* out, cudaStream_t s) {
+  if (nout <= 0) return;
+  k_plan_apply<<<grid_for(nout, 256, 16), 256, 0, s>>>(nout, seg, pe, pf, a, b, out); ::impes::count_launch();
+  IMPES_CHECK_LAUNCH();
 }
 
 // ------------------------------------------------ union SpGEMM (numeric)
@@ -919,12 +927,8 @@ bool build_plan(int rows, const int* optr, const int* ocol, const int* iptr, con
 void galerkin_numeric(Level& L, Level& Nc, cudaStream_t s) {
   if (L.planned) {
     const int apn = (int)L.apval.n;
-    k_plan_apply<<<grid_for(apn, 256, 16), 256, 0, s>>>(apn, L.ap_seg.p, L.ap_e.p, L.ap_f.p, L.val.p,
-                                                         L.pval.p, L.apval.p); ::impes::count_launch();
-    IMPES_CHECK_LAUNCH();
-    k_plan_apply<<<grid_for(Nc.nnz, 256, 16), 256, 0, s>>>(Nc.nnz, L.ac_seg.p, L.ac_r.p, L.ac_f.p,
-                                                            L.pval.p, L.apval.p, Nc.val.p); ::impes::count_launch();
-    IMPES_CHECK_LAUNCH();
+    plan_apply(apn, L.ap_seg.p, L.ap_e.p, L.ap_f.p, L.val.p, L.pval.p, L.apval.p, s);
+    plan_apply(Nc.nnz, L.ac_seg.p, L.ac_r.p, L.ac_f.p, L.pval.p, L.apval.p, Nc.val.p, s);
     return;
   }
   union_numeric(L.n, L.rowptr.p, L.col.p, L.val.p, L.prow.p, L.pcol.p, L.pval.p, L.aprow.p,

@@ -29,6 +29,7 @@ SOURCES = {
     "amg_cycle.cu": [],
     "adjoint.cu": [],
     "ensemble.cu": [],
+    "pcg.cu": [],
     "abi.cu": [],
 }
 HEADERS = ["common.cuh", "model.cuh", "amg.cuh", os.path.join(REPO, "include", "impes_b200.h")]

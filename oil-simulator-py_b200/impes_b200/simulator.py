@@ -21,6 +21,10 @@ stand-alone V-cycles with its stopping rule; ``"gmres_amg"`` (also the default)
 runs FGMRES with one V-cycle per iteration, ``simulation.amg.norm`` selecting
 ``"jacobi"`` (default) or ``"equilibrated"``, ``simulation.amg.precision``
 ``"fp64"`` or ``"mixed"`` (fp32 V-cycle), ``simulation.amg.max_iters`` the cap.
+Any other value (``"cg"``, the reference's default) runs the reference's
+Jacobi-PCG (``cg_tolerance``, ``cg_max_iter``, absolute stopping test, one
+relaxed retry).  The default here is ``"gmres_amg"``: with a BHP well the CG's
+absolute test on sqrt(r . D^-1 r) is dominated by the well row and is not met.
 """
 from __future__ import annotations
 
@@ -496,18 +500,26 @@ class Simulator:
                 setattr(fl, name, t.to(device=self.device, dtype=torch.float64).contiguous())
         if fl.s_o.dtype != torch.float64 or fl.s_o.device != self.device or not fl.s_o.is_contiguous():
             fl.s_o = torch.empty_like(fl.s_w)
-        kp = self.krylov_params()
         ks = _lib.KrylovStats()
-        solver = 0 if self.pressure_solver == "amg" else 1
-        if self.pressure_solver not in ("amg", "gmres_amg", "cg", "cg_amg"):
-            raise ValueError(f"unknown pressure_solver {self.pressure_solver!r}")
+        # "amg": the reference's stand-alone V-cycles; "gmres_amg": FGMRES with the
+        # AMG V-cycle; any other value: the reference's Jacobi-PCG, as in
+        # _impes_pressure_step (simulation.py:905-966)
+        if self.pressure_solver == "amg":
+            solver, kp = 0, self.krylov_params()
+        elif self.pressure_solver == "gmres_amg":
+            solver, kp = 1, self.krylov_params()
+        else:
+            solver = 2
+            kp = _lib.KrylovParams(float(self.sim_params.get("cg_tolerance", 1e-6)), 0,
+                                   int(self.sim_params.get("cg_max_iter", 500)), 0, 0, 0)
         max_attempts = int(self.sim_params.get("max_time_step_attempts", 5))
         factor = float(self.sim_params.get("dt_reduction_factor", 2.0))
         current_dt = float(dt)
         self._set_well_cells()
         for _ in range(max(1, max_attempts)):
             with torch.cuda.device(self.device):
-                st = lib.impes_step(self._h, self._amg_h, ptr(fl.pressure), ptr(fl.s_w), ptr(fl.s_g),
+                st = lib.impes_step(self._h, self._amg_h if solver != 2 else None, ptr(fl.pressure),
+                                    ptr(fl.s_w), ptr(fl.s_g),
                                     ptr(fl.s_o), current_dt, solver, C.byref(kp), self.amg_max_cycles,
                                     C.byref(ks), None, _lib.stream_of(self.device))
             self.last_krylov = {"iterations": ks.iterations, "restarts": ks.restarts,

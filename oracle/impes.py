@@ -709,13 +709,52 @@ class Model:
 
     # ------------------------------------------------------------------- step
     def step(self, dt, solve="direct"):
-        """One ``_impes_step`` attempt (simulation.py:822-865): pressure, then saturation."""
+        """One ``_impes_step`` attempt (simulation.py:822-865): pressure, then saturation.
+
+        ``solve`` is "direct", "cg" (the reference's Jacobi-PCG with its retry,
+        simulation.py:931-966; returns (None, 0) when both attempts miss) or a
+        callable (A, b) -> x."""
         A, b, _ = self.assemble(dt)
         if solve == "direct":
             p_new = spla.spsolve(A.tocsc(), b)
+        elif solve == "cg":
+            tol = float(self.sim_params.get("cg_tolerance", 1e-6))
+            it = int(self.sim_params.get("cg_max_iter", 500))
+            diag = A.diagonal()
+            p_new, ok, _ = pcg_solve(A, b, diag, tol, it)
+            if not ok:
+                p_new, ok, _ = pcg_solve(A, b, diag, tol * 10.0, it * 4)
+            if not ok:
+                return None, 0
         else:
             p_new = solve(A, b)
         p_new = np.asarray(p_new, dtype=np.float64)
         self.p = p_new
         n_sub = self.saturation(p_new, dt)
         return p_new, n_sub
+
+
+def pcg_solve(A, b, m_diag, tol=1e-6, max_iter=500):
+    """``_solve_pressure_cg_pytorch`` (simulation.py:1662-1697): Jacobi-preconditioned
+    CG from x = 0, stopping when sqrt(r . M^-1 r) < tol (absolute).  Returns
+    (x, converged, iterations)."""
+    b = np.asarray(b, dtype=np.float64)
+    x = np.zeros_like(b)
+    r = b - A @ x
+    z = r / m_diag
+    p = z.copy()
+    rs_old = float(r @ z)
+    if rs_old < 1e-10:
+        return x, True, 0
+    for i in range(max_iter):
+        Ap = A @ p
+        alpha = rs_old / float(p @ Ap)
+        x += alpha * p
+        r -= alpha * Ap
+        z = r / m_diag
+        rs_new = float(r @ z)
+        if math.sqrt(rs_new) < tol:
+            return x, True, i + 1
+        p = z + (rs_new / rs_old) * p
+        rs_old = rs_new
+    return x, False, max_iter

@@ -1,6 +1,6 @@
 """Generate the golden fixtures by running the reference itself (build container only).
 
-Usage:  python tests/golden/make_golden.py [REFERENCE_ROOT]
+Usage:  python tests/golden/make_golden.py [REFERENCE_ROOT] [--pcg-only]
 
 REFERENCE_ROOT defaults to /root/reference (researchim-ai/oil-simulator-py).
 The reference is imported unmodified; the harness only
@@ -29,7 +29,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+_ARGS = [a for a in sys.argv[1:] if not a.startswith("--")]
+REF = _ARGS[0] if _ARGS else "/root/reference"
 sys.path[:0] = [os.path.join(HERE, "_stubs"), os.path.join(REF, "src"), REPO]
 
 import torch  # noqa: E402
@@ -97,7 +98,10 @@ def build_reference(cfg, fields, tmpdir):
     return sim, fl, wm
 
 
-def run_trajectory(name, cfg, fields, steps, dt_days):
+def run_trajectory(name, cfg, fields, steps, dt_days, solver="direct"):
+    """The reference's trajectory with amg_solve replaced by a direct solve of its
+    own (A, b); with solver="cg" the reference's own Jacobi-PCG path runs
+    unpatched (pressure_solver "cg")."""
     rec = {"A": [], "b": []}
 
     def direct(A, b, **kw):
@@ -109,6 +113,25 @@ def run_trajectory(name, cfg, fields, steps, dt_days):
         return torch.from_numpy(spla.spsolve(M.tocsc(), b.numpy()))
 
     pamg.amg_solve = direct
+    if solver == "cg":
+        cfg = json.loads(json.dumps(cfg))
+        cfg["simulation"]["pressure_solver"] = "cg"
+        orig = Simulator._build_pressure_matrix_vectorized
+
+        def record(self, *a, **kw):
+            A, A_diag = orig(self, *a, **kw)
+            C = A.coalesce().to_sparse_csr()
+            rec["A"].append((C.crow_indices().numpy().copy(), C.col_indices().numpy().copy(),
+                             C.values().numpy().copy()))
+            return A, A_diag
+        Simulator._build_pressure_matrix_vectorized = record
+        orig_rhs = Simulator._build_pressure_rhs
+
+        def record_rhs(self, *a, **kw):
+            Q = orig_rhs(self, *a, **kw)
+            rec["b"].append(Q.numpy().copy())
+            return Q
+        Simulator._build_pressure_rhs = record_rhs
     out = {}
     with tempfile.TemporaryDirectory() as td:
         sim, fl, wm = build_reference(cfg, fields, td)
@@ -137,10 +160,37 @@ def run_trajectory(name, cfg, fields, steps, dt_days):
         well_cells=np.array([w[0] for w in wells], dtype=np.int64),
         well_last_q=np.array([w[1] for w in wells]),
     )
+    if solver == "cg":
+        Simulator._build_pressure_matrix_vectorized = orig
+        Simulator._build_pressure_rhs = orig_rhs
     np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
     print(name, "N", fields["kx"].size, "steps", steps, "p range", ps[-1].min(), ps[-1].max(),
           "sw max", sws[-1].max(), "sg max", sgs[-1].max())
     return out
+
+
+def pcg_fixture(name, traj, cases):
+    """The reference's _solve_pressure_cg_pytorch (simulation.py:1662-1697) on a
+    recorded first-step system, for (tol, max_iter) pairs."""
+    crow, col, val = (traj["A0_crow"].astype(np.int64), traj["A0_col"].astype(np.int64),
+                      traj["A0_val"])
+    n = len(crow) - 1
+    Acsr = torch.sparse_csr_tensor(torch.from_numpy(crow), torch.from_numpy(col), torch.from_numpy(val),
+                                   size=(n, n))
+    A = Acsr.to_sparse_coo().coalesce()
+    diag = torch.from_numpy(sp.csr_matrix((val, col, crow), shape=(n, n)).diagonal().copy())
+    b = torch.from_numpy(traj["b0"])
+    out = {"A0_crow": traj["A0_crow"], "A0_col": traj["A0_col"], "A0_val": val, "b0": traj["b0"],
+           "tol": np.array([c[0] for c in cases]), "max_iter": np.array([c[1] for c in cases])}
+    with tempfile.TemporaryDirectory() as td:
+        cfg = json.loads(str(traj["cfg"]))
+        sim, _, _ = build_reference(cfg, {k: traj[k] for k in ("kx", "ky", "kz", "poro")}, td)
+        for q, (tol, it) in enumerate(cases):
+            x, conv = sim._solve_pressure_cg_pytorch(A, b.clone(), M_diag=diag, tol=tol, max_iter=it)
+            out[f"x{q}"] = x.numpy().copy()
+            out[f"converged{q}"] = np.array(bool(conv))
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+    print(name, [(c, bool(out[f"converged{q}"])) for q, c in enumerate(cases)])
 
 
 def amg_fixture(name, traj, seed=7, coarsest=50):
@@ -217,13 +267,40 @@ def main():
     # (the 2e5 sm3/d stress rate makes the reference's own saturation update diverge
     # on small grids, so the trajectory fixture uses a rate its explicit update can carry)
     cfg, f = scenarios.gas_injection_1m(seed=2, nx=12, ny=12, nz=3, steps=4, gas_rate=1.0e2,
-                                        n_inj_side=1, n_prod_side=2, surface_units=True)
+                                        n_inj_side=1, n_prod_side=2, surface_units=True,
+                                        rate_scale=1.0)
     cfg["fluid"]["capillary_pressure_og"] = {"pc_scale": 2.0e4, "pc_exponent": 1.5}
     cfg["wells"].append({"name": "PS", "type": "producer", "i": 6, "j": 2, "k": 0, "radius": 0.1,
                          "control_type": "rate", "control_value": 5.0, "rate_type": "surface",
                          "surface_phase": "oil", "limits": {"wopr": 3.0}})
     run_trajectory("gas_injection_12x12x3", cfg, f, steps=4, dt_days=2.0)
+    # the reference's default pressure solver (Jacobi-PCG): solves of a recorded
+    # system, and a whole trajectory on a case where its absolute tolerance is met
+    # (a rate producer; with a BHP producer the well row keeps sqrt(r.M^-1 r) large)
+    pcg_fixture("pcg_two_phase_32x32", t0, [(1e-6, 25), (1e-6, 120)])
+    cfg, f = scenarios.two_phase_2d(seed=5, nx=20, ny=16, nz=2, steps=3)
+    cfg["wells"][1] = {"name": "PROD", "type": "producer", "i": 19, "j": 15, "k": 0, "radius": 0.1,
+                       "control_type": "rate", "control_value": 40.0}
+    cfg["simulation"]["cg_tolerance"] = 1e-9
+    cfg["simulation"]["cg_max_iter"] = 3000
+    run_trajectory("cg_two_phase_20x16x2", cfg, f, steps=3, dt_days=1.0, solver="cg")
+
+
+def main_pcg_only():
+    """Regenerate only the Jacobi-PCG fixtures (the others are unchanged)."""
+    cfg, f = scenarios.two_phase_2d(seed=0, nx=32, ny=32, nz=1, steps=4)
+    t0 = dict(np.load(os.path.join(HERE, "two_phase_32x32.npz")))
+    pcg_fixture("pcg_two_phase_32x32", t0, [(1e-6, 25), (1e-6, 120)])
+    cfg, f = scenarios.two_phase_2d(seed=5, nx=20, ny=16, nz=2, steps=3)
+    cfg["wells"][1] = {"name": "PROD", "type": "producer", "i": 19, "j": 15, "k": 0, "radius": 0.1,
+                       "control_type": "rate", "control_value": 40.0}
+    cfg["simulation"]["cg_tolerance"] = 1e-9
+    cfg["simulation"]["cg_max_iter"] = 3000
+    run_trajectory("cg_two_phase_20x16x2", cfg, f, steps=3, dt_days=1.0, solver="cg")
 
 
 if __name__ == "__main__":
+    if "--pcg-only" in sys.argv:
+        main_pcg_only()
+        sys.exit(0)
     main()

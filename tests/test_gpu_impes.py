@@ -164,3 +164,42 @@ def test_bhp_min_autoswitch_and_limits():
     _, _, wm3, s3 = build_from_config(cfg3, device="cuda")
     s3.run_step(86400.0)
     assert wm3.get_wells()[0].last_surface_rates["oil"] <= 100.0 * 1.10
+
+
+def test_reference_cg_solver_matches_reference(golden):
+    """pressure_solver "cg": the reference's own Jacobi-PCG path end to end
+    (simulation.py:931-966, 1662-1697), against the trajectory the reference
+    produced with it."""
+    g = golden("cg_two_phase_20x16x2")
+    cfg, f = cfg_fields(g)
+    assert cfg["simulation"]["pressure_solver"] == "cg"
+    _, fl, _, sim = gpu_sim(cfg, f)
+    for s in range(g["p"].shape[0]):
+        assert sim.run_step(float(g["dt"]))
+        assert sim.last_krylov["converged"]
+        assert np.abs(to_np(fl.pressure) - g["p"][s]).max() <= 1e-9 * np.abs(g["p"][s]).max()
+        assert np.abs(to_np(fl.s_w) - g["sw"][s]).max() <= 1e-9
+
+
+def test_pcg_entry_point_matches_reference_iterates(golden):
+    """impes_pcg_solve after a fixed number of iterations equals the reference's
+    _solve_pressure_cg_pytorch iterate (a BHP system: the absolute tolerance is
+    not met, so both stop at max_iter)."""
+    import ctypes as C
+    from impes_b200 import _lib
+    g = golden("pcg_two_phase_32x32")
+    n = len(g["A0_crow"]) - 1
+    dev = torch.device("cuda")
+    rowptr = torch.tensor(g["A0_crow"], dtype=torch.int32, device=dev)
+    col = torch.tensor(g["A0_col"], dtype=torch.int32, device=dev)
+    val = torch.tensor(g["A0_val"], device=dev)
+    b = torch.tensor(g["b0"], device=dev)
+    for q, (tol, it) in enumerate(zip(g["tol"], g["max_iter"])):
+        x = torch.full((n,), 3.0, dtype=torch.float64, device=dev)
+        iters, conv, rz = C.c_int(), C.c_int(), C.c_double()
+        st = _lib.lib.impes_pcg_solve(n, _lib.ptr(rowptr), _lib.ptr(col), _lib.ptr(val), _lib.ptr(b),
+                                      _lib.ptr(x), float(tol), int(it), C.byref(iters), C.byref(conv),
+                                      C.byref(rz), _lib.stream_of(dev))
+        assert st == 0 and iters.value == int(it) and bool(conv.value) == bool(g[f"converged{q}"])
+        ref = g[f"x{q}"]
+        assert np.abs(to_np(x) - ref).max() <= 1e-9 * np.abs(ref).max()

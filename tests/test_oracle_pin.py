@@ -131,3 +131,31 @@ def test_tiebreak_stream_is_uniform_and_deterministic():
     assert 0.0 <= a.min() and a.max() < 1.0
     assert abs(a.mean() - 0.5) < 0.01
     assert not np.array_equal(a, oa.tiebreak(3, 2, 100000))
+
+
+def test_oracle_pcg_matches_reference_solver(golden):
+    """pcg_solve against the reference's _solve_pressure_cg_pytorch on a recorded
+    system (a BHP producer: its absolute tolerance is not reached, so the iterate
+    after max_iter is what the reference returns)."""
+    from oracle.impes import pcg_solve
+    g = golden("pcg_two_phase_32x32")
+    n = len(g["A0_crow"]) - 1
+    A = sp.csr_matrix((g["A0_val"], g["A0_col"], g["A0_crow"]), shape=(n, n))
+    for q, (tol, it) in enumerate(zip(g["tol"], g["max_iter"])):
+        x, ok, iters = pcg_solve(A, g["b0"], A.diagonal(), float(tol), int(it))
+        assert ok == bool(g[f"converged{q}"]) and iters == int(it)
+        ref = g[f"x{q}"]
+        assert np.abs(x - ref).max() <= 1e-9 * np.abs(ref).max()
+
+
+def test_oracle_cg_trajectory_matches_reference(golden):
+    """The reference's default pressure solver end to end (pressure_solver "cg")."""
+    from oracle.impes import Model
+    g = golden("cg_two_phase_20x16x2")
+    cfg = json.loads(str(g["cfg"]))
+    m = Model(cfg, g["kx"], g["ky"], g["kz"], g["poro"])
+    for s in range(g["p"].shape[0]):
+        p, _ = m.step(float(g["dt"]), solve="cg")
+        assert p is not None
+        assert np.abs(m.p - g["p"][s]).max() <= 1e-9 * np.abs(g["p"][s]).max()
+        assert np.abs(m.sw - g["sw"][s]).max() <= 1e-9
