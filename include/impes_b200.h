@@ -234,6 +234,10 @@ int impes_model_nnz(impes_model* m, int* n, int* nnz);
 int impes_csr_pattern(impes_model* m, int* rowptr, int* col, void* stream);
 /* Flat cell index of each well, (i*ny + j)*nz + k (simulation.py:1629-1630). */
 int impes_well_cells(impes_model* m, int* cells_host);
+/* New control values of the wells (rate m3/day or BHP MPa, in well order, host
+ * array of nwells), as when a caller assigns Well.control_value between steps
+ * (rl_env.py:127-140).  Takes effect from the next assembly. */
+int impes_model_set_well_values(impes_model* m, const double* values, int nwells, void* stream);
 /* Device transmissibilities (F face values, x then y then z) and pore volume. */
 int impes_model_export_static(impes_model* m, double* tx, double* ty, double* tz, double* pv,
                               void* stream);

@@ -315,6 +315,23 @@ int impes_well_cells(impes_model* h, int* cells_host) {
   });
 }
 
+int impes_model_set_well_values(impes_model* h, const double* values, int nwells, void* stream) {
+  return guarded([&] {
+    IMPES_REQUIRE(h && (values || nwells == 0), IMPES_ERR_ARG, "null argument");
+    Model& m = h->m;
+    IMPES_REQUIRE(nwells == m.P.nwells, IMPES_ERR_ARG, "well count differs from the model's");
+    if (nwells == 0) return;
+    for (int w = 0; w < nwells; ++w) {
+      IMPES_REQUIRE(std::isfinite(values[w]), IMPES_ERR_NAN, "non-finite well control value");
+      m.wells_host[w].value = values[w];
+    }
+    cudaStream_t s = S(stream);
+    IMPES_CUDA(cudaMemcpyAsync(m.wells.p, m.wells_host.data(), sizeof(WellDev) * nwells,
+                               cudaMemcpyHostToDevice, s));
+    IMPES_CUDA(cudaStreamSynchronize(s));   // wells_host is pageable and may change again
+  });
+}
+
 int impes_model_export_static(impes_model* h, double* tx, double* ty, double* tz, double* pv,
                               void* stream) {
   return guarded([&] {

@@ -118,6 +118,7 @@ _SIGNATURES = {
     "impes_amg_setup": ([_P, _I, _I, _P, _P, _P, _P], _I),
     "impes_amg_update": ([_P, _P, _P], _I),
     "impes_amg_solve_vcycles": ([_P, _P, _P, _D, _I, C.POINTER(_I), C.POINTER(_D), _I, _P], _I),
+    "impes_model_set_well_values": ([_P, _P, _I, _P], _I),
     "impes_pcg_solve": ([_I, _P, _P, _P, _P, _P, _D, _I, C.POINTER(_I), C.POINTER(_I), C.POINTER(_D), _P], _I),
     "impes_ensemble_run": ([_P, _P, _P, _P, _P, _P, _P, _I, _I, _D, C.POINTER(KrylovParams), _I,
                             _P, C.POINTER(_D)], _I),

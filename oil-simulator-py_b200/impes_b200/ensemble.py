@@ -83,6 +83,8 @@ class Ensemble:
             self.last_stats = []
             self.last_span_ms = 0.0
             return []
+        for s in self.sims:
+            s._sync_well_controls()
         P = C.c_void_p * n
         models = P(*[s._h.value for s in self.sims])
         amgs = P(*[s._amg_h.value for s in self.sims])

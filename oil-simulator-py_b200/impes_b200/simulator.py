@@ -436,6 +436,7 @@ class Simulator:
                                          ptr(kx), ptr(ky), ptr(kz), ptr(poro),
                                          _lib.stream_of(self.device)), "impes_model_create")
         self._h = h
+        self._well_values = [float(w.control_value) for w in wells]
         # porous volume as the library forms it (cell volume * porosity)
         self.porous_volume = reservoir.cell_volume * poro
         for n, w in enumerate(wells):
@@ -488,6 +489,17 @@ class Simulator:
         for w in self.well_manager.get_wells():
             w.cell_index_flat = (w.i * r.ny + w.j) * r.nz + w.k
 
+    def _sync_well_controls(self):
+        """Upload Well.control_value when a caller changed it between steps (the
+        reference reads it afresh every step, e.g. after rl_env.py:127-140)."""
+        wells = self.well_manager.get_wells()
+        vals = [float(w.control_value) for w in wells]
+        if vals != self._well_values:
+            arr = (C.c_double * max(len(vals), 1))(*vals)
+            check(lib.impes_model_set_well_values(self._h, arr, len(vals), _lib.stream_of(self.device)),
+                  "impes_model_set_well_values")
+            self._well_values = vals
+
     def _impes_step(self, dt):
         """``_impes_step`` (simulation.py:822-865).  A pressure solve that misses its
         tolerance leaves the state untouched and is retried with dt divided by
@@ -516,6 +528,7 @@ class Simulator:
         factor = float(self.sim_params.get("dt_reduction_factor", 2.0))
         current_dt = float(dt)
         self._set_well_cells()
+        self._sync_well_controls()
         for _ in range(max(1, max_attempts)):
             with torch.cuda.device(self.device):
                 st = lib.impes_step(self._h, self._amg_h if solver != 2 else None, ptr(fl.pressure),
@@ -629,6 +642,37 @@ class Simulator:
         self.last_substeps = st.substeps
         self._wells_stale = True
         return st.substeps
+
+    def run(self, output_filename, save_vtk=False, results_root="results"):
+        """Full run (simulation.py:2121-2260): total_time_days / time_step_days steps
+        of run_step, intermediate states every save_interval steps, then the
+        summary text and the npz of the final fields in
+        results/<output_filename>_<timestamp>/.  Returns that directory."""
+        from . import results as res
+        total_days = self.sim_params.get("total_time_days", 100)
+        step_days = self.sim_params.get("time_step_days", 1.0)
+        save_interval = self.sim_params.get("save_interval", 10)
+        num_steps = int(total_days / step_days)
+        out_dir = res.results_dir(output_filename, results_root)
+        inter = os.path.join(out_dir, "intermediate")
+        if save_interval < num_steps:
+            os.makedirs(inter, exist_ok=True)
+        fl = self.fluid
+        for i in range(num_steps):
+            if not self.run_step(step_days * 86400):
+                break
+            if (i + 1) % save_interval == 0 and save_interval < num_steps:
+                res.write_snapshot(os.path.join(inter, f"{output_filename}_step_{i+1}.npz"),
+                                   fl.pressure.cpu().numpy(), fl.s_w.cpu().numpy(), fl.s_g.cpu().numpy())
+        p, sw, sg = fl.pressure.cpu().numpy(), fl.s_w.cpu().numpy(), fl.s_g.cpu().numpy()
+        so = fl.s_o.cpu().numpy().reshape(p.shape)
+        res.write_summary(os.path.join(out_dir, f"{output_filename}.txt"), p, sw, sg, so, self.mass_balance,
+                          bool(self.sim_params.get("write_full_arrays_txt", False)))
+        if self.sim_params.get("save_npz", True):
+            res.write_npz(os.path.join(out_dir, f"{output_filename}.npz"), p, sw, sg, so)
+        if save_vtk:
+            print("VTK output is not part of this package; the npz holds the final fields.")
+        return out_dir
 
     def static_fields(self):
         """(Tx, Ty, Tz, PV) device tensors as the library computed them."""

@@ -203,3 +203,26 @@ def test_pcg_entry_point_matches_reference_iterates(golden):
         assert st == 0 and iters.value == int(it) and bool(conv.value) == bool(g[f"converged{q}"])
         ref = g[f"x{q}"]
         assert np.abs(to_np(x) - ref).max() <= 1e-9 * np.abs(ref).max()
+
+
+def test_run_writes_reference_result_files(tmp_path):
+    """Simulator.run: the reference's results directory, txt summary and npz keys
+    (simulation.py:2121-2248), intermediate states at its save_interval cadence."""
+    import glob
+    import os
+    from impes_b200 import scenarios
+    from impes_b200.simulator import build_from_config
+    cfg, f = scenarios.two_phase_2d(seed=2, nx=10, ny=8, nz=1, steps=4)
+    cfg["simulation"].update({"total_time_days": 4.0, "time_step_days": 1.0, "save_interval": 2})
+    _, fl, _, sim = build_from_config(cfg, f, device="cuda")
+    out = sim.run("case", results_root=str(tmp_path))
+    assert os.path.basename(out).startswith("case_")
+    snaps = sorted(glob.glob(os.path.join(out, "intermediate", "case_step_*.npz")))
+    assert [os.path.basename(s) for s in snaps] == ["case_step_2.npz", "case_step_4.npz"]
+    z = np.load(os.path.join(out, "case.npz"))
+    assert sorted(z.files) == ["pressure", "sg", "so", "sw"]
+    assert np.array_equal(z["pressure"], fl.pressure.cpu().numpy())
+    txt = open(os.path.join(out, "case.txt")).read()
+    assert txt.startswith("=== SUMMARY (final) ===\nPressure MPa: min=")
+    assert "=== MASS BALANCE (kg) ===" in txt and "total net=" in txt
+    assert sim.step_count == 4
