@@ -149,14 +149,15 @@ class ClockSampler:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
-def make_sim(cfg, fields, precision, device, restart=30, solver="gmres_amg"):
+def make_sim(cfg, fields, precision, device, restart=30, solver="gmres_amg", warm_start=True):
     """FGMRES + V-cycle (solver="gmres_amg"), or the plain stand-alone V-cycles of
     the reference (solver="amg"), both stopping at PRESSURE_TOL in the Jacobi norm."""
     from impes_b200.simulator import build_from_config
     c = json.loads(json.dumps(cfg))
     c["simulation"]["pressure_solver"] = solver
     c["simulation"]["amg"].update({"tol": PRESSURE_TOL, "norm": "jacobi", "precision": precision,
-                                   "restart": restart, "max_iters": 600, "max_cycles": 3000, "seed": 0})
+                                   "restart": restart, "max_iters": 600, "max_cycles": 3000, "seed": 0,
+                                   "warm_start": warm_start})
     return build_from_config(c, fields, device=device)
 
 
@@ -309,7 +310,8 @@ def run_ours(args, world, rank, local):
     results = {}
     precisions = ("fp64", "mixed") if args.precision == "both" else (args.precision,)
     for precision in precisions:
-        _, fl, _, sim = make_sim(cfg, fields, precision, device, restart=args.restart)
+        _, fl, _, sim = make_sim(cfg, fields, precision, device, restart=args.restart,
+                                 warm_start=not args.no_warm_start)
         torch.cuda.synchronize()
         t_setup = time.perf_counter()
         for _ in range(args.warmup):           # the first warm-up step builds the hierarchy
@@ -499,6 +501,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 V-cycle baseline")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward measurement")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-member ensemble measurement")
+    ap.add_argument("--no-warm-start", action="store_true",
+                    help="start each FGMRES solve from zero instead of the previous pressure")
     ap.add_argument("--grid", default=None,
                     help="NXxNYxNZ: a smaller grid of the same workload (profiling captures only)")
     ap.add_argument("--precision", choices=["both", "mixed", "fp64"], default="both",

@@ -20,7 +20,8 @@ Pressure solvers (``simulation.pressure_solver``): ``"amg"`` runs the reference'
 stand-alone V-cycles with its stopping rule; ``"gmres_amg"`` (also the default)
 runs FGMRES with one V-cycle per iteration, ``simulation.amg.norm`` selecting
 ``"jacobi"`` (default) or ``"equilibrated"``, ``simulation.amg.precision``
-``"fp64"`` or ``"mixed"`` (fp32 V-cycle), ``simulation.amg.max_iters`` the cap.
+``"fp64"`` or ``"mixed"`` (fp32 V-cycle), ``simulation.amg.max_iters`` the cap,
+``simulation.amg.warm_start`` (default true) the previous pressure as first iterate.
 Any other value (``"cg"``, the reference's default) runs the reference's
 Jacobi-PCG (``cg_tolerance``, ``cg_max_iter``, absolute stopping test, one
 relaxed retry).  The default here is ``"gmres_amg"``: with a BHP well the CG's
@@ -420,6 +421,8 @@ class Simulator:
         # the reference's own stopping norm for its stand-alone V-cycles
         self.amg_norm = amg_cfg.get("norm", "equilibrated" if self.pressure_solver == "amg" else "jacobi")
         self.amg_precision = amg_cfg.get("precision", "fp64")
+        # FGMRES starts from the previous pressure (the test stays ||r|| / ||b||)
+        self.amg_warm_start = bool(amg_cfg.get("warm_start", True))
         kw = dict(device=self.device, dtype=torch.float64)
         kx, ky, kz = (t.to(**kw).contiguous() for t in reservoir.permeability_tensors)
         poro = reservoir.porosity.to(**kw).contiguous()
@@ -477,7 +480,8 @@ class Simulator:
     def krylov_params(self) -> _lib.KrylovParams:
         norm = {"jacobi": _lib.NORM_JACOBI, "equilibrated": _lib.NORM_EQUILIBRATED}[self.amg_norm]
         prec = 1 if self.amg_precision in ("mixed", "fp32") else 0
-        return _lib.KrylovParams(self.amg_tol, self.amg_restart, self.amg_max_iters, norm, prec, 0)
+        return _lib.KrylovParams(self.amg_tol, self.amg_restart, self.amg_max_iters, norm, prec,
+                                 1 if self.amg_warm_start else 0)
 
     def run_step(self, dt):
         """One time step (simulation.py:126-135)."""
