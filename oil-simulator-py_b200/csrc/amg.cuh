@@ -38,10 +38,10 @@ struct Level {
   DBuf<double> x, b, r, t;
   DBuf<float> xf, bf, rf, tf;
   // coarsest level (n <= 500): inverse of the dense matrix with DOF 0 pinned
-  // (the reference's coarse solve), row-major; when the coarsest level is also
-  // level 0, lu_free holds the unpinned inverse used as FGMRES preconditioner
+  // (the reference's coarse solve), row-major, and lu_free, the inverse of the
+  // unpinned matrix used inside FGMRES unless it was singular (device flag)
   DBuf<double> lu, lu_free;
-  DBuf<int> piv;
+  DBuf<int> piv;                   // two permutations of n
 };
 
 struct AMG {

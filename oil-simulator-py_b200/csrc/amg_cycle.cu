@@ -250,88 +250,106 @@ __global__ void k_dense_fill(int n, const int* rowptr, const int* col, const dou
     if (pin && i == 0) M[0] = 1.0;
   }
 }
-// In-place Gauss-Jordan inversion with partial pivoting, one block.
+// In-place Gauss-Jordan inversion with partial pivoting: block b inverts M[b]
+// (the pinned and the unpinned coarsest matrix in one launch).  With SMEM the
+// n x n matrix lives in shared memory for the whole elimination (n <= 168 in
+// 227 KB); otherwise it stays in global memory.  Pivot ties go to the lower row.
 constexpr int kGJ = 1024;
-__global__ void __launch_bounds__(kGJ) k_gauss_jordan(int n, double* M, int* perm, int* singular) {
+struct GJArgs {
+  double* M[2];
+  int* perm[2];
+  int* singular[2];
+};
+template <bool SMEM>
+__global__ void __launch_bounds__(kGJ) k_gauss_jordan(int n, GJArgs args) {
   __shared__ double s_val[kGJ / 32];
   __shared__ int s_idx[kGJ / 32];
   __shared__ int s_p;
   __shared__ double s_inv;
-  extern __shared__ double s_row[];  // n (pivot row) + n (pivot column)
-  double* s_col = s_row + n;
+  extern __shared__ double s_dyn[];
+  double* s_row = s_dyn;             // n (pivot row)
+  double* s_col = s_row + n;         // n (pivot column)
+  double* G = args.M[blockIdx.x];
+  int* perm = args.perm[blockIdx.x];
+  double* M = SMEM ? s_col + n : G;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (SMEM) {
+    for (int t = threadIdx.x; t < n * n; t += blockDim.x) M[t] = G[t];
+    __syncthreads();
+  }
   for (int k = 0; k < n; ++k) {
-    // pivot: first index of max |M[i][k]|, i >= k
     double best = -1.0;
     int bi = k;
     for (int i = k + threadIdx.x; i < n; i += blockDim.x) {
-      double v = fabs(M[(long long)i * n + k]);
+      const double v = fabs(M[i * n + k]);
       if (v > best) { best = v; bi = i; }
     }
     for (int o = 16; o > 0; o >>= 1) {
-      double ov = __shfl_down_sync(0xffffffffu, best, o);
-      int oi = __shfl_down_sync(0xffffffffu, bi, o);
+      const double ov = __shfl_down_sync(0xffffffffu, best, o);
+      const int oi = __shfl_down_sync(0xffffffffu, bi, o);
       if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
     }
-    if ((threadIdx.x & 31) == 0) { s_val[threadIdx.x >> 5] = best; s_idx[threadIdx.x >> 5] = bi; }
+    if (lane == 0) { s_val[warp] = best; s_idx[warp] = bi; }
     __syncthreads();
     if (threadIdx.x == 0) {
-      double bv = -1.0; int b = k;
-      for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
+      double bv = -1.0;
+      int b = k;
+      for (int w = 0; w < nw; ++w)
         if (s_val[w] > bv || (s_val[w] == bv && s_idx[w] < b)) { bv = s_val[w]; b = s_idx[w]; }
       s_p = b;
       perm[k] = b;
-      if (!(bv > 0.0)) *singular = 1;
-    }
-    __syncthreads();
-    const int p = s_p;
-    if (p != k)
-      for (int j = threadIdx.x; j < n; j += blockDim.x) {
-        double a = M[(long long)k * n + j];
-        M[(long long)k * n + j] = M[(long long)p * n + j];
-        M[(long long)p * n + j] = a;
-      }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double piv = M[(long long)k * n + k];
+      if (!(bv > 0.0)) *args.singular[blockIdx.x] = 1;
+      const double piv = M[b * n + k];
       s_inv = piv != 0.0 ? 1.0 / piv : 0.0;
     }
     __syncthreads();
+    const int p = s_p;
     const double inv = s_inv;
+    // swap rows k and p, scale the pivot row, keep it and the pivot column
     for (int j = threadIdx.x; j < n; j += blockDim.x) {
-      double v = (j == k) ? inv : M[(long long)k * n + j] * inv;
-      M[(long long)k * n + j] = v;
+      const double rk = M[k * n + j], rp = M[p * n + j];
+      if (p != k) M[p * n + j] = rk;
+      const double v = (j == k) ? inv : rp * inv;
+      M[k * n + j] = v;
       s_row[j] = v;
     }
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      s_col[i] = M[(long long)i * n + k];
-    }
     __syncthreads();
-    for (long long t = threadIdx.x; t < (long long)n * n; t += blockDim.x) {
-      int i = (int)(t / n), j = (int)(t % n);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s_col[i] = M[i * n + k];
+    __syncthreads();
+    for (int i = warp; i < n; i += nw) {
       if (i == k) continue;
-      double f = s_col[i];
-      if (j == k) M[t] = -f * s_row[k];
-      else M[t] -= f * s_row[j];
+      const double f = s_col[i];
+      for (int j = lane; j < n; j += 32) {
+        if (j == k) M[i * n + j] = -f * s_row[k];
+        else M[i * n + j] -= f * s_row[j];
+      }
     }
     __syncthreads();
   }
   // undo the row interchanges as column interchanges, last first
   for (int k = n - 1; k >= 0; --k) {
-    int p = perm[k];
+    const int p = perm[k];
     if (p != k)
       for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        double a = M[(long long)i * n + k];
-        M[(long long)i * n + k] = M[(long long)i * n + p];
-        M[(long long)i * n + p] = a;
+        const double a = M[i * n + k];
+        M[i * n + k] = M[i * n + p];
+        M[i * n + p] = a;
       }
     __syncthreads();
   }
+  if (SMEM)
+    for (int t = threadIdx.x; t < n * n; t += blockDim.x) G[t] = M[t];
 }
-// x = Ainv * b (b[0] pinned to 0 when pin); one warp per row group
+// x = Ainv * b with b[0] pinned to 0 (the reference's coarsest solve), or, in
+// Krylov mode while the unpinned matrix was invertible, x = Afree^-1 * b.
 template <typename T>
-__global__ void k_coarse_apply(int n, const double* __restrict__ Ainv, const T* __restrict__ b,
-                               T* __restrict__ x, int pin) {
+__global__ void k_coarse_apply(int n, const double* __restrict__ Apin, const double* __restrict__ Afree,
+                               const int* __restrict__ free_singular, int krylov,
+                               const T* __restrict__ b, T* __restrict__ x) {
   extern __shared__ double s_b[];
+  const bool use_free = krylov && Afree != nullptr && *free_singular == 0;
+  const double* Ainv = use_free ? Afree : Apin;
+  const int pin = use_free ? 0 : 1;
   for (int i = threadIdx.x; i < n; i += blockDim.x) s_b[i] = (pin && i == 0) ? 0.0 : (double)b[i];
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
@@ -351,31 +369,27 @@ __global__ void k_pin_copy(int n, const T* b, T* out) { GRID_LOOP(i, n) out[i] =
 void coarse_factor(AMG& h, Level& L, cudaStream_t s) {
   if (L.n > 500 || L.n == 0) return;
   const int n = L.n;
+  // the reference's pinned matrix (row/column 0 replaced by e_0) and the
+  // unpinned one used inside FGMRES (the pinned solve would freeze x[0] there)
   L.lu.ensure((size_t)n * n);
-  L.piv.ensure(n);
-  k_dense_pinned<<<grid_for((size_t)n * n, TB), TB, 0, s>>>(n, L.rowptr.p, L.col.p, L.val.p, L.lu.p); ::impes::count_launch();
-  IMPES_CHECK_LAUNCH();
-  k_dense_fill<<<grid_for(n, TB), TB, 0, s>>>(n, L.rowptr.p, L.col.p, L.val.p, L.lu.p, 1); ::impes::count_launch();
-  IMPES_CHECK_LAUNCH();
-  IMPES_CUDA(cudaMemsetAsync(h.iflag.p + 2, 0, sizeof(int), s));
-  k_gauss_jordan<<<1, kGJ, 2 * n * sizeof(double), s>>>(n, L.lu.p, L.piv.p, h.iflag.p + 2); ::impes::count_launch();
-  IMPES_CHECK_LAUNCH();
-  {
-    // unpinned inverse for FGMRES preconditioning (the pinned solve mirrors the
-    // reference's stand-alone V-cycle; on a single-level hierarchy it would
-    // freeze x[0] inside FGMRES)
-    L.lu_free.ensure((size_t)n * n);
-    k_dense_pinned<<<grid_for((size_t)n * n, TB), TB, 0, s>>>(n, L.rowptr.p, L.col.p, L.val.p, L.lu_free.p); ::impes::count_launch();
-    IMPES_CHECK_LAUNCH();
-    k_dense_fill<<<grid_for(n, TB), TB, 0, s>>>(n, L.rowptr.p, L.col.p, L.val.p, L.lu_free.p, 0); ::impes::count_launch();
-    IMPES_CHECK_LAUNCH();
-    IMPES_CUDA(cudaMemsetAsync(h.iflag.p + 3, 0, sizeof(int), s));
-    k_gauss_jordan<<<1, kGJ, 2 * n * sizeof(double), s>>>(n, L.lu_free.p, L.piv.p, h.iflag.p + 3); ::impes::count_launch();
-    IMPES_CHECK_LAUNCH();
-    IMPES_CUDA(cudaMemcpyAsync(h.hint.p + 3, h.iflag.p + 3, sizeof(int), cudaMemcpyDeviceToHost, s));
-    IMPES_CUDA(cudaStreamSynchronize(s));
-    if (h.hint.p[3]) L.lu_free.release();  // singular without the pin: keep the pinned solve
+  L.lu_free.ensure((size_t)n * n);
+  L.piv.ensure(2 * (size_t)n);
+  double* mats[2] = {L.lu.p, L.lu_free.p};
+  for (int q = 0; q < 2; ++q) {
+    k_dense_pinned<<<grid_for((size_t)n * n, TB), TB, 0, s>>>(n, L.rowptr.p, L.col.p, L.val.p, mats[q]); ::impes::count_launch();
+    k_dense_fill<<<grid_for(n, TB), TB, 0, s>>>(n, L.rowptr.p, L.col.p, L.val.p, mats[q], q == 0 ? 1 : 0); ::impes::count_launch();
   }
+  IMPES_CHECK_LAUNCH();
+  IMPES_CUDA(cudaMemsetAsync(h.iflag.p + 2, 0, 2 * sizeof(int), s));
+  GJArgs args{{L.lu.p, L.lu_free.p}, {L.piv.p, L.piv.p + n}, {h.iflag.p + 2, h.iflag.p + 3}};
+  const size_t smem_full = sizeof(double) * ((size_t)n * n + 2 * (size_t)n);
+  if (smem_full <= (size_t)(224u << 10)) {
+    raise_smem_limit((const void*)k_gauss_jordan<true>, smem_full);
+    k_gauss_jordan<true><<<2, kGJ, smem_full, s>>>(n, args); ::impes::count_launch();
+  } else {
+    k_gauss_jordan<false><<<2, kGJ, 2 * n * sizeof(double), s>>>(n, args); ::impes::count_launch();
+  }
+  IMPES_CHECK_LAUNCH();
 }
 
 void spmv(const Level& L, const double* x, double* y, cudaStream_t s) {
@@ -473,9 +487,8 @@ T* vcycle(AMG& h, int l, bool zero_x, cudaStream_t s) {
   if (L.coarsest) {
     if (L.n <= 500) {
       const int n = L.n;
-      const bool free_ = h.krylov_mode && L.lu_free.p != nullptr;
       k_coarse_apply<T><<<std::max(1, (n + 7) / 8), 256, n * sizeof(double), s>>>(
-          n, free_ ? L.lu_free.p : L.lu.p, LV<T>::b(L), LV<T>::x(L), free_ ? 0 : 1); ::impes::count_launch();
+          n, L.lu.p, L.lu_free.p, h.iflag.p + 3, h.krylov_mode ? 1 : 0, LV<T>::b(L), LV<T>::x(L)); ::impes::count_launch();
       IMPES_CHECK_LAUNCH();
       return LV<T>::x(L);
     }

@@ -121,6 +121,31 @@ __global__ void k_inv_relax(int n, const int* rowptr, const int* col, const doub
   }
 }
 
+// The same, one warp per row (coarse levels with hundreds to thousands of
+// entries per row): the diagonal comes from the lane that holds it, the
+// absolute row sum from a fixed-order warp reduction.
+__global__ void k_inv_relax_warp(int n, const int* __restrict__ rowptr, const int* __restrict__ col,
+                                 const double* __restrict__ val, double* __restrict__ inv) {
+  const int lane = threadIdx.x & 31;
+  for (long long i = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); i < n;
+       i += (long long)gridDim.x * (blockDim.x >> 5)) {
+    double d = 0.0, ra = 0.0;
+    for (int e = rowptr[i] + lane; e < rowptr[i + 1]; e += 32) {
+      const double v = val[e];
+      if (col[e] == i) d = v;
+      ra += fabs(v);
+    }
+    ra = warp_sum(ra);
+    d = warp_sum(d);                 // one lane holds the diagonal (rows are unique)
+    if (lane == 0) {
+      double denom = fmax(fabs(d), 0.3 * ra);
+      denom = denom < 1e-30 ? 1e-30 : denom;
+      const double r = 1.0 / denom;
+      inv[i] = r > 1e2 ? 1e2 : r;
+    }
+  }
+}
+
 // --------------------------------------------------------------- strength
 // find_strong_connections (classical_amg.py:34-82)
 __global__ void k_strength(int n, const int* rowptr, const int* col, const double* val,
@@ -964,7 +989,12 @@ void union_numeric(int rows, const int* optr, const int* ocol, const double* ova
 
 void compute_inv_relax(AMG& h, Level& L, cudaStream_t s) {
   L.inv_relax.ensure(std::max(L.n, 1));
-  k_inv_relax<<<grid_for(L.n, TB), TB, 0, s>>>(L.n, L.rowptr.p, L.col.p, L.val.p, L.inv_relax.p); ::impes::count_launch();
+  if (L.n > 0 && L.nnz / L.n > 32) {
+    k_inv_relax_warp<<<grid_for((size_t)L.n * 32, TB, 16), TB, 0, s>>>(L.n, L.rowptr.p, L.col.p, L.val.p,
+                                                                     L.inv_relax.p); ::impes::count_launch();
+  } else {
+    k_inv_relax<<<grid_for(L.n, TB), TB, 0, s>>>(L.n, L.rowptr.p, L.col.p, L.val.p, L.inv_relax.p); ::impes::count_launch();
+  }
   IMPES_CHECK_LAUNCH();
 }
 
