@@ -149,7 +149,7 @@ class ClockSampler:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
-def make_sim(cfg, fields, precision, device, restart=30, solver="gmres_amg", warm_start=True):
+def make_sim(cfg, fields, precision, device, restart=30, solver="gmres_amg", warm_start="extrapolate"):
     """FGMRES + V-cycle (solver="gmres_amg"), or the plain stand-alone V-cycles of
     the reference (solver="amg"), both stopping at PRESSURE_TOL in the Jacobi norm."""
     from impes_b200.simulator import build_from_config
@@ -311,7 +311,7 @@ def run_ours(args, world, rank, local):
     precisions = ("fp64", "mixed") if args.precision == "both" else (args.precision,)
     for precision in precisions:
         _, fl, _, sim = make_sim(cfg, fields, precision, device, restart=args.restart,
-                                 warm_start=not args.no_warm_start)
+                                 warm_start=False if args.warm_start == "zero" else args.warm_start)
         torch.cuda.synchronize()
         t_setup = time.perf_counter()
         for _ in range(args.warmup):           # the first warm-up step builds the hierarchy
@@ -501,8 +501,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 V-cycle baseline")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward measurement")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-member ensemble measurement")
-    ap.add_argument("--no-warm-start", action="store_true",
-                    help="start each FGMRES solve from zero instead of the previous pressure")
+    ap.add_argument("--warm-start", default="extrapolate", choices=["extrapolate", "previous", "zero"],
+                    help="FGMRES first iterate: extrapolated pressure, previous pressure, or zero")
     ap.add_argument("--grid", default=None,
                     help="NXxNYxNZ: a smaller grid of the same workload (profiling captures only)")
     ap.add_argument("--precision", choices=["both", "mixed", "fp64"], default="both",

@@ -83,7 +83,9 @@ typedef struct {
   int max_iters;      /* total iteration cap                        */
   int norm;           /* IMPES_NORM_*                               */
   int precision;      /* 0: fp64 V-cycle, 1: fp32 V-cycle (mixed)   */
-  int use_x0;         /* 1: x holds an initial guess                */
+  int use_x0;         /* 1: x holds an initial guess; 2 (impes_step only): the
+                         pressure extrapolated linearly in time from the last
+                         two accepted steps (the current one on the first)    */
 } impes_krylov_params;
 
 typedef struct {

@@ -39,6 +39,14 @@ void adjoint_gradient(Model& m, AMG& a, const double* p0, const double* sw0, con
 
 namespace {
 
+// x0 = p + r (p - p_prev): the pressure extrapolated linearly in time
+__global__ void k_extrapolate(int n, const double* __restrict__ p, const double* __restrict__ p_prev,
+                              double r, double* __restrict__ x0) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    x0[i] = p[i] + r * (p[i] - p_prev[i]);
+}
+
 template <typename F>
 int guarded(F&& f) {
   try {
@@ -432,6 +440,16 @@ int impes_step(impes_model* h, impes_amg* amg, double* p, double* sw, double* sg
         st.converged = rel < kp->tol;
       } else {
         impes_krylov_params k = *kp;
+        if (k.use_x0 == 2) {
+          // first iterate extrapolated from the last two accepted pressures
+          // (p_save holds p^n; the assembly has already used it)
+          if (m.have_prev && m.dt_prev > 0) {
+            k_extrapolate<<<grid_for(m.P.N, 256), 256, 0, s>>>(m.P.N, m.p_save.p, m.p_prev.p,
+                                                               dt / m.dt_prev, p); ::impes::count_launch();
+            IMPES_CHECK_LAUNCH();
+          }
+          k.use_x0 = 1;
+        }
         amg_fgmres(amg->a, m.rhs.p, p, k, st, s);
       }
     } catch (...) {
@@ -444,6 +462,11 @@ int impes_step(impes_model* h, impes_amg* amg, double* p, double* sw, double* sg
       throw Error(IMPES_ERR_NOT_CONVERGED, solver == 2 ? "CG did not reach the pressure tolerance"
                                                        : "FGMRES did not reach the pressure tolerance");
     }
+    // the accepted step's starting pressure, for the next extrapolated iterate
+    m.p_prev.ensure(m.P.N);
+    IMPES_CUDA(cudaMemcpyAsync(m.p_prev.p, m.p_save.p, sizeof(double) * m.P.N, cudaMemcpyDeviceToDevice, s));
+    m.dt_prev = dt;
+    m.have_prev = true;
     model_saturation(m, p, sw, sg, so, dt, s);
     if (sstats) {
       double hb[12];

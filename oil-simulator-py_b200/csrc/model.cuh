@@ -57,6 +57,9 @@ struct Model {
   DBuf<double> well_rates;             // per well 4 surface rates (NaN unset)
   DBuf<double> csr_val, rhs;           // assembled system (owned for impes_step)
   DBuf<double> p_save;                 // pressure before the solve (restored on failure)
+  DBuf<double> p_prev;                 // pressure before the last accepted step
+  double dt_prev = 0.0;                // and that step's dt (extrapolated first iterate)
+  bool have_prev = false;
   DBuf<int> rowptr, col;               // static pattern
   int red_blocks = 0;
 };

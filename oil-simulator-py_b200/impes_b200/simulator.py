@@ -21,7 +21,8 @@ stand-alone V-cycles with its stopping rule; ``"gmres_amg"`` (also the default)
 runs FGMRES with one V-cycle per iteration, ``simulation.amg.norm`` selecting
 ``"jacobi"`` (default) or ``"equilibrated"``, ``simulation.amg.precision``
 ``"fp64"`` or ``"mixed"`` (fp32 V-cycle), ``simulation.amg.max_iters`` the cap,
-``simulation.amg.warm_start`` (default true) the previous pressure as first iterate.
+``simulation.amg.warm_start`` the first iterate: ``"extrapolate"`` (default, linear
+in time from the last two steps), ``"previous"`` or ``false`` (zero).
 Any other value (``"cg"``, the reference's default) runs the reference's
 Jacobi-PCG (``cg_tolerance``, ``cg_max_iter``, absolute stopping test, one
 relaxed retry).  The default here is ``"gmres_amg"``: with a BHP well the CG's
@@ -421,8 +422,11 @@ class Simulator:
         # the reference's own stopping norm for its stand-alone V-cycles
         self.amg_norm = amg_cfg.get("norm", "equilibrated" if self.pressure_solver == "amg" else "jacobi")
         self.amg_precision = amg_cfg.get("precision", "fp64")
-        # FGMRES starts from the previous pressure (the test stays ||r|| / ||b||)
-        self.amg_warm_start = bool(amg_cfg.get("warm_start", True))
+        # FGMRES's first iterate: the pressure extrapolated in time from the last
+        # two steps ("extrapolate"), the previous one (True / "previous") or zero
+        # (False); the test stays ||r|| / ||b||
+        ws = amg_cfg.get("warm_start", "extrapolate")
+        self.amg_warm_start = ws if ws in ("extrapolate", "previous") else bool(ws)
         kw = dict(device=self.device, dtype=torch.float64)
         kx, ky, kz = (t.to(**kw).contiguous() for t in reservoir.permeability_tensors)
         poro = reservoir.porosity.to(**kw).contiguous()
@@ -480,8 +484,8 @@ class Simulator:
     def krylov_params(self) -> _lib.KrylovParams:
         norm = {"jacobi": _lib.NORM_JACOBI, "equilibrated": _lib.NORM_EQUILIBRATED}[self.amg_norm]
         prec = 1 if self.amg_precision in ("mixed", "fp32") else 0
-        return _lib.KrylovParams(self.amg_tol, self.amg_restart, self.amg_max_iters, norm, prec,
-                                 1 if self.amg_warm_start else 0)
+        x0 = {False: 0, True: 1, "previous": 1, "extrapolate": 2}[self.amg_warm_start]
+        return _lib.KrylovParams(self.amg_tol, self.amg_restart, self.amg_max_iters, norm, prec, x0)
 
     def run_step(self, dt):
         """One time step (simulation.py:126-135)."""
