@@ -48,6 +48,7 @@ struct Model {
   // per-step scratch
   DBuf<double> dsw, dsg;               // saturation increments
   DBuf<double> wq;                     // 3 x nwc well sources (q_w, q_g, q_o)
+  DBuf<double> wsub;                   // per (substep, well) component-balance addends
   DBuf<double> red;                    // block partials for reductions
   DBuf<unsigned> counter;              // last-block counters
   DBuf<int> nsub;                      // substep count (device)

@@ -756,21 +756,31 @@ __global__ void __launch_bounds__(256) k_saturation_flux(
     s_last = (done == gridDim.x - 1);
   }
   __syncthreads();
-  if (s_last && threadIdx.x == 0) {
+  if (s_last) {   // the whole last block reduces the block maxima
     __threadfence();
     double a = 0, b = 0, c = 0;
-    for (unsigned q = 0; q < gridDim.x; ++q) {
+    for (unsigned q = threadIdx.x; q < gridDim.x; q += blockDim.x) {
       a = fmax(a, ((volatile double*)red)[3 * q]);
       b = fmax(b, ((volatile double*)red)[3 * q + 1]);
       c = fmax(c, ((volatile double*)red)[3 * q + 2]);
     }
-    double rat_max = (b > 0 || c > 0) ? 0.0 : a;  // nan_to_num(nan=0, posinf=0)
-    double n = ceil(rat_max);
-    int N = n > 2.0e9 ? 2000000000 : (int)n;
-    if (N < 1) N = 1;
-    if (N > P.max_substeps) N = P.max_substeps;
-    *nsub_out = N;
-    *counter = 0u;
+    a = warp_max(a); b = warp_max(b); c = warp_max(c);
+    __syncthreads();
+    if (lane == 0) { s_red[wid] = a; s_red[8 + wid] = b; s_red[16 + wid] = c; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      a = 0; b = 0; c = 0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+        a = fmax(a, s_red[w]); b = fmax(b, s_red[8 + w]); c = fmax(c, s_red[16 + w]);
+      }
+      double rat_max = (b > 0 || c > 0) ? 0.0 : a;  // nan_to_num(nan=0, posinf=0)
+      double n = ceil(rat_max);
+      int N = n > 2.0e9 ? 2000000000 : (int)n;
+      if (N < 1) N = 1;
+      if (N > P.max_substeps) N = P.max_substeps;
+      *nsub_out = N;
+      *counter = 0u;
+    }
   }
 }
 
@@ -780,24 +790,27 @@ __global__ void k_well_substeps(ModelParams P, const double* __restrict__ pvt_g,
                                 const WellDev* __restrict__ wells, const double* __restrict__ p_new,
                                 const double* __restrict__ sw, const double* __restrict__ sg,
                                 const double* __restrict__ dsw, const double* __restrict__ dsg,
-                                const int* __restrict__ nsub, double dt, double* bal) {
+                                const int* __restrict__ nsub, double dt, double* __restrict__ contrib,
+                                double* bal) {
+  // contrib[(s * nwells + w) * 4 + q]: the addend of bal[6 + {0, 1, 3, 4}[q]] for
+  // substep s and well w (never negative), -1 where the reference adds nothing
   __shared__ double s_col[kPvtCols * kMaxPvtRows];
   __shared__ double s_slope[(kPvtCols - 1) * kMaxPvtRows];
   PvtSmem T{P.pvt_rows, s_col, s_slope};
   pvt_stage(pvt_g, P.pvt_rows, s_col, s_slope);
-  if (threadIdx.x != 0) return;
   const int N = *nsub;
   const double dt_sub = dt / N;
   const double so_r = P.so_r;
-  // substep state per well cell (recomputed from the same increments as K4b)
-  for (int s = 0; s < N; ++s) {
-    for (int w = 0; w < P.nwells; ++w) {
-      const WellDev W = wells[w];
-      const int c = W.cell;
-      if (c < 0) continue;
+  const int items = N * P.nwells;
+  for (int it = threadIdx.x; it < items; it += blockDim.x) {
+    const int s = it / P.nwells, w = it % P.nwells;
+    double add[4] = {-1.0, -1.0, -1.0, -1.0};   // bal[6+0], bal[6+1], bal[6+3], bal[6+4]
+    const WellDev W = wells[w];
+    const int c = W.cell;
+    if (c >= 0) {
       double swc = sw[c], sgc = sg[c];
       const double dws = dsw[c] / N, dgs = dsg[c] / N;
-      for (int q = 0; q <= s; ++q) {
+      for (int q = 0; q <= s; ++q) {   // the cell's state after substep s (as K4b)
         swc = swc + dws;
         sgc = sgc + dgs;
         swc = tclamp(swc, P.sw_cr, 1.0 - so_r - sgc);
@@ -817,8 +830,8 @@ __global__ void k_well_substeps(ModelParams P, const double* __restrict__ pvt_g,
           double q_sub = W.surface_rate ? q_base * (W.injected_phase == 1 ? Bg : Bw) : q_base;
           if (W.injected_phase == 1) {
             double qg_surf = fmax(q_sub, 0.0) / fmax(Bg, 1e-12) * 86400.0;
-            bal[6 + 3] += qg_surf * (dt_sub / 86400.0);
-            bal[6 + 0] += Rv * qg_surf * (dt_sub / 86400.0);
+            add[2] = qg_surf * (dt_sub / 86400.0);
+            add[0] = Rv * qg_surf * (dt_sub / 86400.0);
           }
         } else {
           double q_sub;
@@ -835,25 +848,39 @@ __global__ void k_well_substeps(ModelParams P, const double* __restrict__ pvt_g,
             q_sub = -q_base;
           }
           double qo_res = fmax(-q_sub * fo_, 0.0), qg_res = fmax(-q_sub * fg_, 0.0);
-          bal[6 + 1] += dt_sub * (qo_res / fmax(Bo, 1e-12) + Rv * qg_res / fmax(Bg, 1e-12));
-          bal[6 + 4] += dt_sub * (qg_res / fmax(Bg, 1e-12) + Rs * qo_res / fmax(Bo, 1e-12));
+          add[1] = dt_sub * (qo_res / fmax(Bo, 1e-12) + Rv * qg_res / fmax(Bg, 1e-12));
+          add[3] = dt_sub * (qg_res / fmax(Bg, 1e-12) + Rs * qo_res / fmax(Bo, 1e-12));
         }
       } else {
         double q_sub = W.well_index * mt * (p - W.value * 1e6);
         if (W.is_injector) {
           if (W.injected_phase == 1) {
             double qg_surf = fmax(-q_sub, 0.0) / fmax(Bg, 1e-12) * 86400.0;
-            bal[6 + 3] += qg_surf * (dt_sub / 86400.0);
-            bal[6 + 0] += Rv * qg_surf * (dt_sub / 86400.0);
+            add[2] = qg_surf * (dt_sub / 86400.0);
+            add[0] = Rv * qg_surf * (dt_sub / 86400.0);
           }
         } else {
           double qabs = fabs(q_sub);
           double qo_res = qabs * fo_, qg_res = qabs * fg_;
-          bal[6 + 1] += dt_sub * (qo_res / fmax(Bo, 1e-12) + Rv * qg_res / fmax(Bg, 1e-12));
-          bal[6 + 4] += dt_sub * (qg_res / fmax(Bg, 1e-12) + Rs * qo_res / fmax(Bo, 1e-12));
+          add[1] = dt_sub * (qo_res / fmax(Bo, 1e-12) + Rv * qg_res / fmax(Bg, 1e-12));
+          add[3] = dt_sub * (qg_res / fmax(Bg, 1e-12) + Rs * qo_res / fmax(Bo, 1e-12));
         }
       }
     }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) contrib[(size_t)it * 4 + q] = add[q];
+  }
+  __syncthreads();
+  // the reference's accumulation order: substeps outer, wells inner (simulation.py:1396-1505)
+  if (threadIdx.x < 4) {
+    const int q = threadIdx.x;
+    const int slot = q == 0 ? 0 : q == 1 ? 1 : q == 2 ? 3 : 4;
+    double acc = bal[6 + slot];
+    for (int it = 0; it < items; ++it) {
+      const double v = contrib[(size_t)it * 4 + q];
+      if (!(v < 0.0)) acc += v;   // NaN propagates as before
+    }
+    bal[6 + slot] = acc;
   }
 }
 
@@ -908,17 +935,21 @@ __global__ void __launch_bounds__(kSatBlock) k_saturation_substeps(
     s_last = (done == gridDim.x - 1);
   }
   __syncthreads();
-  if (s_last && threadIdx.x == 0) {
+  if (s_last) {   // the whole last block sums the block partials (fixed order)
     __threadfence();
     double tot[6] = {0, 0, 0, 0, 0, 0};
-    for (unsigned b = 0; b < gridDim.x; ++b)
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
       for (int q = 0; q < 6; ++q) tot[q] += ((volatile double*)red)[6 * b + q];
-    // mass_balance[water/oil/gas][in/out] (simulation.py:1521-1526)
-    for (int q = 0; q < 6; ++q) bal[q] += tot[q];
-    // component accum = in - out (simulation.py:1529-1530)
-    bal[6 + 2] = bal[6 + 0] - bal[6 + 1];
-    bal[6 + 5] = bal[6 + 3] - bal[6 + 4];
-    *counter = 0u;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) tot[q] = block_sum<kSatBlock>(tot[q], s_w);
+    if (threadIdx.x == 0) {
+      // mass_balance[water/oil/gas][in/out] (simulation.py:1521-1526)
+      for (int q = 0; q < 6; ++q) bal[q] += tot[q];
+      // component accum = in - out (simulation.py:1529-1530)
+      bal[6 + 2] = bal[6 + 0] - bal[6 + 1];
+      bal[6 + 5] = bal[6 + 3] - bal[6 + 4];
+      *counter = 0u;
+    }
   }
 }
 
@@ -955,6 +986,7 @@ void model_build_static(Model& m, const double* kx, const double* ky, const doub
   m.dsw.alloc(P.N);
   m.dsg.alloc(P.N);
   m.wq.alloc(std::max(1, 3 * P.nwc));
+  m.wsub.alloc(std::max<size_t>(1, (size_t)4 * std::max(P.max_substeps, 1) * std::max(P.nwells, 1)));
 }
 
 void model_pattern(Model& m, int* rowptr, int* col, cudaStream_t s) {
@@ -993,8 +1025,8 @@ void model_saturation(Model& m, const double* p_new, double* sw, double* sg, dou
       m.dsw.p, m.dsg.p, m.red.p, m.counter.p, m.nsub.p); ::impes::count_launch();
   IMPES_CHECK_LAUNCH();
   if (P.pvt_rows > 0 && P.nwells > 0) {
-    k_well_substeps<<<1, 128, 0, s>>>(P, m.pvt.p, m.wells.p, p_new, sw, sg, m.dsw.p, m.dsg.p,
-                                      m.nsub.p, dt, m.balances.p); ::impes::count_launch();
+    k_well_substeps<<<1, 256, 0, s>>>(P, m.pvt.p, m.wells.p, p_new, sw, sg, m.dsw.p, m.dsg.p,
+                                      m.nsub.p, dt, m.wsub.p, m.balances.p); ::impes::count_launch();
     IMPES_CHECK_LAUNCH();
   }
   unsigned g = grid_for(P.N, kSatBlock);
