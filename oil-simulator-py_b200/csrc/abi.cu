@@ -171,6 +171,7 @@ int impes_amg_level_export(impes_amg* h, int lvl, int* A_rowptr, int* A_col, dou
                            double* inv_relax, int* P_rowptr, int* P_col, double* P_val,
                            void* stream) {
   return guarded([&] {
+    if (h) amg_ensure_fp64(h->a, S(stream));
     IMPES_REQUIRE(h, IMPES_ERR_ARG, "null argument");
     IMPES_REQUIRE(lvl >= 0 && lvl < (int)h->a.levels.size(), IMPES_ERR_ARG, "level out of range");
     const Level& L = *h->a.levels[lvl];

@@ -27,6 +27,7 @@ struct Level {
   // Galerkin helper: pattern of A*P (n x nc)
   DBuf<int> aprow, apcol;
   DBuf<double> apval;
+  DBuf<float> apvalf;              // A*P values of the fp32 Galerkin chain
   int ap_maxrow = 0;               // longest A*P row
   int ac_maxrow = 0;               // longest row of the next level's A (computed here)
   // Galerkin numeric plans (P is frozen, so both products are fixed maps of
@@ -49,6 +50,9 @@ struct AMG {
   std::vector<std::unique_ptr<Level>> levels;
   bool built = false;
   bool equilibrated = false;
+  // mixed AMG: update_matrix runs the Galerkin chain in fp32 (all the V-cycle
+  // of the mixed path reads); the fp64 coarse levels are rebuilt on demand
+  bool fp64_stale = false;
   DBuf<double> dhalf_inv;          // D^-1/2 when equilibrated
   DBuf<double> jac_w;              // Jacobi weights in the scaled space
   DBuf<double> diag_tmp;
@@ -102,7 +106,9 @@ void amg_fgmres(AMG& h, const double* b, double* x, const impes_krylov_params& k
 // shared kernels (amg_cycle.cu)
 void spmv(const Level& L, const double* x, double* y, cudaStream_t s);
 double dot_host(AMG& h, const double* a, const double* b, int n, cudaStream_t s);
-void coarse_factor(AMG& h, Level& L, cudaStream_t s);
+void coarse_factor(AMG& h, Level& L, cudaStream_t s, bool from_fp32 = false);
+// Brings the fp64 coarse levels up to date after an fp32 update (no-op otherwise).
+void amg_ensure_fp64(AMG& h, cudaStream_t s);
 void level_precision_copies(AMG& h, Level& L, cudaStream_t s);
 
 }  // namespace impes

@@ -239,7 +239,8 @@ __global__ void k_scale_by_inv_sqrt(long long n, const double* in, double* out, 
 __global__ void k_dense_pinned(int n, const int* rowptr, const int* col, const double* val, double* M) {
   GRID_LOOP(t, (long long)n * n) M[t] = 0.0;
 }
-__global__ void k_dense_fill(int n, const int* rowptr, const int* col, const double* val, double* M,
+template <typename TV>
+__global__ void k_dense_fill(int n, const int* rowptr, const int* col, const TV* val, double* M,
                              int pin) {
   GRID_LOOP(i, n) {
     for (int e = rowptr[i]; e < rowptr[i + 1]; ++e) {
@@ -366,7 +367,7 @@ __global__ void k_pin_copy(int n, const T* b, T* out) { GRID_LOOP(i, n) out[i] =
 }  // namespace
 
 // =================================================================== host
-void coarse_factor(AMG& h, Level& L, cudaStream_t s) {
+void coarse_factor(AMG& h, Level& L, cudaStream_t s, bool from_fp32) {
   if (L.n > 500 || L.n == 0) return;
   const int n = L.n;
   // the reference's pinned matrix (row/column 0 replaced by e_0) and the
@@ -377,7 +378,11 @@ void coarse_factor(AMG& h, Level& L, cudaStream_t s) {
   double* mats[2] = {L.lu.p, L.lu_free.p};
   for (int q = 0; q < 2; ++q) {
     k_dense_pinned<<<grid_for((size_t)n * n, TB), TB, 0, s>>>(n, L.rowptr.p, L.col.p, L.val.p, mats[q]); ::impes::count_launch();
-    k_dense_fill<<<grid_for(n, TB), TB, 0, s>>>(n, L.rowptr.p, L.col.p, L.val.p, mats[q], q == 0 ? 1 : 0); ::impes::count_launch();
+    if (from_fp32) {
+      k_dense_fill<float><<<grid_for(n, TB), TB, 0, s>>>(n, L.rowptr.p, L.col.p, L.valf.p, mats[q], q == 0 ? 1 : 0); ::impes::count_launch();
+    } else {
+      k_dense_fill<double><<<grid_for(n, TB), TB, 0, s>>>(n, L.rowptr.p, L.col.p, L.val.p, mats[q], q == 0 ? 1 : 0); ::impes::count_launch();
+    }
   }
   IMPES_CHECK_LAUNCH();
   IMPES_CUDA(cudaMemsetAsync(h.iflag.p + 2, 0, 2 * sizeof(int), s));
@@ -553,6 +558,7 @@ T* vcycle_top(AMG& h, bool zero_x, cudaStream_t s) {
 
 // V-cycle on the equilibrated system: xs = V(0, bs)  (FP64 or FP32 inside)
 void amg_vcycle_scaled(AMG& h, const double* bs, double* xs, int precision, cudaStream_t s) {
+  if (precision == 0) amg_ensure_fp64(h, s);
   Level& L0 = *h.levels[0];
   const int n = L0.n;
   if (precision == 1) {
@@ -572,6 +578,7 @@ void amg_vcycle_scaled(AMG& h, const double* bs, double* xs, int precision, cuda
 // measures the stopping test in ||D^-1 r|| / ||D^-1 b|| instead.
 void amg_solve_vcycles(AMG& h, const double* b, double* x, double tol, int max_cycles, int* cycles,
                        double* rel, cudaStream_t s, int norm) {
+  amg_ensure_fp64(h, s);
   Level& L0 = *h.levels[0];
   const int n = L0.n;
   DBuf<double> bs(n), r(n), wb(n);
@@ -606,6 +613,7 @@ void amg_solve_vcycles(AMG& h, const double* b, double* x, double tol, int max_c
 // ClassicalAMG.apply (classical_amg.py:1157-1180)
 void amg_apply(AMG& h, const double* b, double* x, int cycles, double apply_tol,
                int apply_max_cycles, cudaStream_t s) {
+  amg_ensure_fp64(h, s);
   Level& L0 = *h.levels[0];
   const int n = L0.n;
   DBuf<double> bs(n), r(n);
@@ -695,6 +703,7 @@ struct KrylovModeGuard {
 
 void amg_fgmres(AMG& h, const double* b, double* x, const impes_krylov_params& kp,
                 impes_krylov_stats& st, cudaStream_t s) {
+  if (kp.precision == 0) amg_ensure_fp64(h, s);
   KrylovModeGuard guard(h);
   struct SolveTimer {
     cudaStream_t s;
@@ -861,6 +870,7 @@ void solve_vcycles_noalloc(AMG& h, const double* b, double* x, double tol, int m
   IMPES_REQUIRE(n <= kNoAllocMaxRows, IMPES_ERR_ARG,
                 "impes_amg_solve_vcycles_noalloc: n exceeds the 262144-row static work space");
   IMPES_REQUIRE(h.red.n >= (size_t)kMD * kDotBlocks, IMPES_ERR_STATE, "hierarchy not set up");
+  amg_ensure_fp64(h, s);
   double* base = solve_scratch();
   double* bs = base;
   double* r = base + kNoAllocMaxRows;

@@ -105,8 +105,8 @@ __global__ void k_equilibrate(int n, const int* rowptr, const int* col, const do
 }
 
 // l1-Jacobi weights (classical_amg.py:885-889, 1298-1306)
-__global__ void k_inv_relax(int n, const int* rowptr, const int* col, const double* val,
-                            double* inv) {
+template <typename TV, typename TO>
+__global__ void k_inv_relax(int n, const int* rowptr, const int* col, const TV* val, TO* inv) {
   GRID_LOOP(i, n) {
     double d = 0.0, ra = 0.0;
     for (int e = rowptr[i]; e < rowptr[i + 1]; ++e) {
@@ -117,15 +117,16 @@ __global__ void k_inv_relax(int n, const int* rowptr, const int* col, const doub
     double denom = fmax(fabs(d), 0.3 * ra);
     denom = denom < 1e-30 ? 1e-30 : denom;
     double r = 1.0 / denom;
-    inv[i] = r > 1e2 ? 1e2 : r;
+    inv[i] = (TO)(r > 1e2 ? 1e2 : r);
   }
 }
 
 // The same, one warp per row (coarse levels with hundreds to thousands of
 // entries per row): the diagonal comes from the lane that holds it, the
 // absolute row sum from a fixed-order warp reduction.
+template <typename TV, typename TO>
 __global__ void k_inv_relax_warp(int n, const int* __restrict__ rowptr, const int* __restrict__ col,
-                                 const double* __restrict__ val, double* __restrict__ inv) {
+                                 const TV* __restrict__ val, TO* __restrict__ inv) {
   const int lane = threadIdx.x & 31;
   for (long long i = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); i < n;
        i += (long long)gridDim.x * (blockDim.x >> 5)) {
@@ -141,7 +142,7 @@ __global__ void k_inv_relax_warp(int n, const int* __restrict__ rowptr, const in
       double denom = fmax(fabs(d), 0.3 * ra);
       denom = denom < 1e-30 ? 1e-30 : denom;
       const double r = 1.0 / denom;
-      inv[i] = r > 1e2 ? 1e2 : r;
+      inv[i] = (TO)(r > 1e2 ? 1e2 : r);
     }
   }
 }
@@ -660,23 +661,25 @@ __global__ void k_plan_sort(int nout, const int* seg, long long* key, int* pe, i
 }
 // out[o] = sum over the segment of a[pe] * b[pf]; one thread per output walks
 // its own run of the plan (consecutive terms share cache lines).
+template <typename T>
 __global__ void __launch_bounds__(256) k_plan_apply(int nout, const int* __restrict__ seg,
                                                     const int* __restrict__ pe,
                                                     const int* __restrict__ pf,
-                                                    const double* __restrict__ a,
-                                                    const double* __restrict__ b,
-                                                    double* __restrict__ out) {
+                                                    const T* __restrict__ a,
+                                                    const T* __restrict__ b,
+                                                    T* __restrict__ out) {
   GRID_LOOP(o, nout) {
-    double acc = 0.0;
+    T acc = T(0);
     for (int t = seg[o]; t < seg[o + 1]; ++t) acc += a[pe[t]] * b[pf[t]];
     out[o] = acc;
   }
 }
 
-void plan_apply(int nout, const int* seg, const int* pe, const int* pf, const double* a,
-                const double* b, double* out, cudaStream_t s) {
+template <typename T>
+void plan_apply(int nout, const int* seg, const int* pe, const int* pf, const T* a, const T* b,
+                T* out, cudaStream_t s) {
   if (nout <= 0) return;
-  k_plan_apply<<<grid_for(nout, 256, 16), 256, 0, s>>>(nout, seg, pe, pf, a, b, out); ::impes::count_launch();
+  k_plan_apply<T><<<grid_for(nout, 256, 16), 256, 0, s>>>(nout, seg, pe, pf, a, b, out); ::impes::count_launch();
   IMPES_CHECK_LAUNCH();
 }
 
@@ -952,8 +955,8 @@ bool build_plan(int rows, const int* optr, const int* ocol, const int* iptr, con
 void galerkin_numeric(Level& L, Level& Nc, cudaStream_t s) {
   if (L.planned) {
     const int apn = (int)L.apval.n;
-    plan_apply(apn, L.ap_seg.p, L.ap_e.p, L.ap_f.p, L.val.p, L.pval.p, L.apval.p, s);
-    plan_apply(Nc.nnz, L.ac_seg.p, L.ac_r.p, L.ac_f.p, L.pval.p, L.apval.p, Nc.val.p, s);
+    plan_apply<double>(apn, L.ap_seg.p, L.ap_e.p, L.ap_f.p, L.val.p, L.pval.p, L.apval.p, s);
+    plan_apply<double>(Nc.nnz, L.ac_seg.p, L.ac_r.p, L.ac_f.p, L.pval.p, L.apval.p, Nc.val.p, s);
     return;
   }
   union_numeric(L.n, L.rowptr.p, L.col.p, L.val.p, L.prow.p, L.pcol.p, L.pval.p, L.aprow.p,
@@ -987,15 +990,26 @@ void union_numeric(int rows, const int* optr, const int* ocol, const double* ova
   IMPES_CHECK_LAUNCH();
 }
 
-void compute_inv_relax(AMG& h, Level& L, cudaStream_t s) {
-  L.inv_relax.ensure(std::max(L.n, 1));
+template <typename TV, typename TO>
+void launch_inv_relax(const Level& L, const TV* val, TO* out, cudaStream_t s) {
   if (L.n > 0 && L.nnz / L.n > 32) {
-    k_inv_relax_warp<<<grid_for((size_t)L.n * 32, TB, 16), TB, 0, s>>>(L.n, L.rowptr.p, L.col.p, L.val.p,
-                                                                     L.inv_relax.p); ::impes::count_launch();
+    k_inv_relax_warp<TV, TO><<<grid_for((size_t)L.n * 32, TB, 16), TB, 0, s>>>(L.n, L.rowptr.p, L.col.p, val,
+                                                                             out); ::impes::count_launch();
   } else {
-    k_inv_relax<<<grid_for(L.n, TB), TB, 0, s>>>(L.n, L.rowptr.p, L.col.p, L.val.p, L.inv_relax.p); ::impes::count_launch();
+    k_inv_relax<TV, TO><<<grid_for(L.n, TB), TB, 0, s>>>(L.n, L.rowptr.p, L.col.p, val, out); ::impes::count_launch();
   }
   IMPES_CHECK_LAUNCH();
+}
+
+void compute_inv_relax(AMG& h, Level& L, cudaStream_t s) {
+  L.inv_relax.ensure(std::max(L.n, 1));
+  launch_inv_relax<double, double>(L, L.val.p, L.inv_relax.p, s);
+}
+
+// l1 weights of the fp32 chain, from the fp32 values
+void compute_inv_relax_f(Level& L, cudaStream_t s) {
+  L.inv_relaxf.ensure(std::max(L.n, 1));
+  launch_inv_relax<float, float>(L, L.valf.p, L.inv_relaxf.p, s);
 }
 
 void alloc_level_vectors(Level& L) {
@@ -1050,6 +1064,7 @@ void amg_setup(AMG& h, int n, int nnz, const int* rowptr, const int* col, const 
   }
   h.levels.clear();
   h.built = false;
+  h.fp64_stale = false;
   h.iflag.ensure(8);
   h.red.ensure(4096);
   h.scal.ensure(256);
@@ -1225,15 +1240,59 @@ void amg_setup(AMG& h, int n, int nnz, const int* rowptr, const int* col, const 
   h.built = true;
 }
 
+// The fp32 Galerkin chain of a mixed AMG (every level planned): the V-cycle of
+// the mixed path reads only fp32 coarse values, so A*P and P^T(AP) gather 4-byte
+// values.  The coarsest inverses come from the fp32 coarsest matrix.
+void update_fp32_chain(AMG& h, cudaStream_t s) {
+  Level& L0 = *h.levels[0];
+  compute_inv_relax(h, L0, s);
+  k_to_float<<<grid_for(L0.nnz, TB), TB, 0, s>>>(L0.nnz, L0.val.p, L0.valf.p); ::impes::count_launch();
+  k_to_float<<<grid_for(L0.n, TB), TB, 0, s>>>(L0.n, L0.inv_relax.p, L0.inv_relaxf.p); ::impes::count_launch();
+  IMPES_CHECK_LAUNCH();
+  for (size_t l = 0; l < h.levels.size(); ++l) {
+    Level& L = *h.levels[l];
+    if (L.coarsest) break;
+    Level& Nc = *h.levels[l + 1];
+    const int apn = (int)L.apval.n;
+    L.apvalf.ensure(std::max(apn, 1));
+    Nc.valf.ensure(std::max(Nc.nnz, 1));
+    plan_apply<float>(apn, L.ap_seg.p, L.ap_e.p, L.ap_f.p, L.valf.p, L.pvalf.p, L.apvalf.p, s);
+    plan_apply<float>(Nc.nnz, L.ac_seg.p, L.ac_r.p, L.ac_f.p, L.pvalf.p, L.apvalf.p, Nc.valf.p, s);
+    compute_inv_relax_f(Nc, s);
+  }
+  coarse_factor(h, *h.levels.back(), s, true);
+  h.fp64_stale = true;
+}
+
+void amg_ensure_fp64(AMG& h, cudaStream_t s) {
+  if (!h.fp64_stale) return;
+  for (size_t l = 0; l < h.levels.size(); ++l) {
+    Level& L = *h.levels[l];
+    compute_inv_relax(h, L, s);
+    if (L.coarsest) break;
+    galerkin_numeric(L, *h.levels[l + 1], s);
+  }
+  coarse_factor(h, *h.levels.back(), s);
+  h.fp64_stale = false;
+}
+
 void amg_update(AMG& h, const double* val, cudaStream_t s) {
   IMPES_REQUIRE(h.built, IMPES_ERR_STATE, "update before setup");
   const int tid = timers().begin(IMPES_PH_GALERKIN, s);
   double bytes = 0.0;
+  bool all_planned = true;
   for (size_t l = 0; l + 1 < h.levels.size(); ++l) {
     const Level& L = *h.levels[l];
     bytes += 12.0 * L.nnz + 24.0 * L.pnnz + 8.0 * h.levels[l + 1]->nnz;
+    if (!L.coarsest && !L.planned) all_planned = false;
   }
   equilibrate_level0(h, val, s);
+  if (h.prm.mixed_precision && all_planned && h.levels.size() > 1) {
+    update_fp32_chain(h, s);
+    timers().end(tid, s, bytes * 0.6);   // 4-byte values instead of 8
+    return;
+  }
+  h.fp64_stale = false;
   for (size_t l = 0; l < h.levels.size(); ++l) {
     Level& L = *h.levels[l];
     compute_inv_relax(h, L, s);
