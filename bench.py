@@ -401,8 +401,8 @@ def run_ours(args, world, rank, local):
     steps = args.steps
     value = world * cells * steps / (mixed["ms"] / 1e3)
     fp64_value = world * cells * steps / (fp64["ms"] / 1e3)
-    # dominant kernel: the l1-Jacobi sweep of the wide coarse levels (k_csr_rows,
-    # Y_SMOOTH), timed per launch by the library's CUDA events
+    # dominant kernel: the l1-Jacobi sweep of the wide coarse levels (k_csr_stream
+    # and k_csr_rows, Y_SMOOTH), timed per launch by the library's CUDA events
     key = "smooth_wide" if mixed["phases"]["smooth_wide"][0] else "smooth_l0"
     n_s, ms_s, by_s = mixed["phases"][key]
     avg_ms = ms_s / max(n_s, 1)
@@ -453,7 +453,8 @@ def run_ours(args, world, rank, local):
         "state_after": {"mixed": mixed["state"], "fp64": fp64["state"]},
         "e2e": {"value": world * cells * steps / (mixed["e2e_ms"] / 1e3), "unit": "cell-steps/s",
                 "h2d_bytes_per_step": mixed["e2e_bytes"], "d2h_bytes_per_step": mixed["e2e_bytes"]},
-        "roofline": {"kernel": ("k_csr_rows<float,u16|int,Y_SMOOTH,1|2|4 warps/row> (l1-Jacobi sweep, "
+        "roofline": {"kernel": ("k_csr_stream<u16|int,Y_SMOOTH> (rows > 512 on levels >= 48 MB) and "
+                                "k_csr_rows<float,u16|int,Y_SMOOTH,1|2|4 warps/row> (l1-Jacobi sweep, "
                                 "levels with > 96 nnz/row)"
                                 if key == "smooth_wide" else "k_csr<float,1,Y_SMOOTH> (level-0 sweep)"),
                      "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "peak_kind": peak_kind,

@@ -108,12 +108,113 @@ __global__ void __launch_bounds__(TB) k_csr_rows(int n, const int* __restrict__ 
   }
 }
 
+// 16-byte asynchronous global -> shared copy; src_bytes < 16 zero-fills the rest
+// (only src_bytes are read from global memory).
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes) {
+  const unsigned saddr = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(saddr), "l"(gmem), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+
+// Wide rows, streamed: each warp walks its rows in chunks of kCh entries that
+// cp.async brings into shared memory (two stages, the next chunk -- of this row
+// or of the warp's next row -- in flight while the current one is consumed), so
+// HBM sees many outstanding 16-byte requests per warp instead of one load per
+// lane per step.  Chunks start at 8-entry boundaries (16-byte aligned for fp32
+// values and 16-bit columns); the last piece of a row is clamped to the row end,
+// so nothing past it is read.  Entries of a chunk outside the row are skipped.
+// fp32 values only (the mixed V-cycle).  Same epilogues as k_csr.  Chunks are
+// 512 entries with 16-bit columns and 384 with int columns.
+template <typename CT, int MODE>
+__global__ void __launch_bounds__(TB) k_csr_stream(int n, const int* __restrict__ rowptr,
+                                                   const CT* __restrict__ col, const float* __restrict__ val,
+                                                   const float* __restrict__ x, const float* __restrict__ b,
+                                                   const float* __restrict__ inv, float* __restrict__ y) {
+  constexpr int kWarps = TB / 32;
+  constexpr int kCh = sizeof(CT) == 2 ? 512 : 384;   // 48 KB of stages per block
+  __shared__ __align__(16) float s_val[kWarps][2][kCh];
+  __shared__ __align__(16) CT s_col[kWarps][2][kCh];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long long stride = (long long)gridDim.x * kWarps;
+  long long row = (long long)blockIdx.x * kWarps + warp;
+  if (row >= n) return;                       // warp-uniform
+  constexpr int VP = 16 / sizeof(float);      // values per 16-byte piece
+  constexpr int CP = 16 / sizeof(CT);         // columns per piece
+  // issue the copies of chunk [g0, g0 + kCh) of a row ending at e into stage st
+  auto fetch = [&](int g0, int e, int st) {
+    for (int q = lane; q < kCh / VP; q += 32) {
+      const int gi = g0 + q * VP;
+      const int valid = e - gi;
+      if (valid > 0) cp_async16(&s_val[warp][st][q * VP], val + gi, (valid >= VP ? VP : valid) * 4);
+    }
+    for (int q = lane; q < kCh / CP; q += 32) {
+      const int gi = g0 + q * CP;
+      const int valid = e - gi;
+      if (valid > 0)
+        cp_async16(&s_col[warp][st][q * CP], col + gi, (valid >= CP ? CP : valid) * (int)sizeof(CT));
+    }
+  };
+  int a = rowptr[row], e = rowptr[row + 1];
+  int g = a & ~7;                             // current chunk start
+  int st = 0;
+  fetch(g, e, st);
+  cp_async_commit();
+  float acc = 0.0f;
+  while (true) {
+    // the task after this chunk: the next chunk of this row, or the next row
+    long long nrow = row;
+    int na = a, ne = e, ng = g + kCh;
+    if (ng >= e) {
+      nrow = row + stride;
+      if (nrow < n) { na = rowptr[nrow]; ne = rowptr[nrow + 1]; ng = na & ~7; }
+    }
+    if (nrow < n) fetch(ng, ne, st ^ 1);
+    cp_async_commit();
+    cp_async_wait1();
+    __syncwarp();
+    const int lo = a > g ? a - g : 0;
+    const int hi = e - g < kCh ? e - g : kCh;
+    for (int j = lo + lane; j < hi; j += 32) acc += s_val[warp][st][j] * x[s_col[warp][st][j]];
+    __syncwarp();                             // stage st is refilled two chunks on
+    if (g + kCh >= e) {                       // row done
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+      if (lane == 0) {
+        if (MODE == Y_AX) y[row] = acc;
+        else if (MODE == Y_B_MINUS_AX) y[row] = b[row] - acc;
+        else if (MODE == Y_SMOOTH) y[row] = x[row] + float(kOmega) * inv[row] * (b[row] - acc);
+        else if (MODE == Y_ADD_AX) y[row] = y[row] + acc;
+        else if (MODE == Y_W_AX) y[row] = inv[row] * acc;
+      }
+      acc = 0.0f;
+    }
+    if (nrow >= n) break;
+    row = nrow; a = na; e = ne; g = ng;
+    st ^= 1;
+  }
+}
+
 template <typename T, typename CT, int MODE>
 void launch_wide(int n, int avg, const int* rowptr, const CT* col, const T* val, const T* x,
                  const T* b, const T* inv, T* y, cudaStream_t s) {
   auto grid = [&](int rows_per_block) {
     return grid_for(((size_t)(n + rows_per_block - 1) / rows_per_block) * TB, TB, 16);
   };
+  // fp32 rows longer than 512 entries on levels of 48 MB or more: streamed
+  // through shared memory (A/B on the 1e6-cell case, ~100 MB levels: 28 us
+  // against 30 us per wide sweep).  Shorter rows are faster with the direct
+  // kernel, and so are levels that stay in L2: on 64 models of <= 262,144 cells
+  // stepped concurrently, streaming their <= 30 MB levels cost 20-35 % of the
+  // run (the 48 KB of shared memory per block crowds out the other models).
+  if constexpr (sizeof(T) == 4) {
+    constexpr double kStreamMinBytes = 48.0 * (1 << 20);
+    if (avg > 512 && (double)n * avg * (sizeof(T) + sizeof(CT)) >= kStreamMinBytes) {
+      k_csr_stream<CT, MODE><<<grid(8), TB, 0, s>>>(n, rowptr, col, (const float*)val, (const float*)x,
+                                                    (const float*)b, (const float*)inv, (float*)y); ::impes::count_launch();
+      return;
+    }
+  }
   if (avg <= 512) {
     k_csr_rows<T, CT, MODE, 1><<<grid(8), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y); ::impes::count_launch();
   } else if (avg <= 1536) {

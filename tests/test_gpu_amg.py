@@ -188,3 +188,44 @@ def test_phase_timers_inside_graphs(golden):
     _lib.timing_enable(False)
     assert ph["vcycle"][0] == st["iterations"]
     assert ph["smooth_l0"][0] >= 4 * st["iterations"] and ph["smooth_l0"][1] > 0
+
+
+def test_mixed_vcycle_on_wide_levels_matches_fp64():
+    """A hierarchy (640,000 cells) whose coarse levels have rows of more than 512
+    entries and more than 48 MB of values and columns (the fp32 sweep streams
+    those through shared memory), updated through the fp32 Galerkin chain: one
+    fp32 V-cycle agrees with the fp64 one to fp32 rounding, and the fp64 levels
+    exported afterwards are those of the updated matrix."""
+    from impes_b200 import scenarios
+    from impes_b200.simulator import build_from_config
+    cfg, f = scenarios.gas_injection_1m(seed=2, nx=160, ny=160, nz=25)
+    _, fl, _, sim = build_from_config(cfg, f, device="cuda")
+    rowptr, col, val, rhs = sim.assemble(2 * 86400.0)
+    n = rhs.numel()
+    A = torch.sparse_csr_tensor(rowptr.long(), col.long(), val, size=(n, n))
+    amg = gpu_amg(A, theta=0.2, max_levels=20, coarsest_size=120, mixed_precision=True)
+    rng = np.random.default_rng(3)
+    # keep the symmetric pattern: scale each row and column by the same factors
+    d = torch.tensor(1.0 + 0.01 * rng.random(n), device="cuda")
+    r = torch.repeat_interleave(torch.arange(n, device="cuda"), rowptr[1:] - rowptr[:-1])
+    val2 = val * d[r] * d[col.long()]
+    A2 = torch.sparse_csr_tensor(rowptr.long(), col.long(), val2, size=(n, n))
+    amg.update_matrix(A2)
+    b = torch.tensor(rng.standard_normal(n), device="cuda")
+    x32 = amg.vcycle_scaled(b, precision="fp32")
+    x64 = amg.vcycle_scaled(b, precision="fp64")
+    assert torch.linalg.norm(x32 - x64) <= 1e-4 * torch.linalg.norm(x64)
+    levels = amg.levels
+    def streamed(lv):
+        nnz = lv["A"].values().numel()
+        col_bytes = 2 if lv["n"] <= 65536 else 4
+        return nnz > 512 * lv["n"] and nnz * (4 + col_bytes) >= 48 * 2**20
+    assert any(streamed(lv) for lv in levels if not lv["is_coarsest"])
+    A0 = csr_from(levels[0]["A"].crow_indices(), levels[0]["A"].col_indices(), levels[0]["A"].values(), n)
+    P0 = levels[0]["P"]
+    P0 = sp.csr_matrix((to_np(P0.values()), to_np(P0.col_indices()), to_np(P0.crow_indices())),
+                       shape=(n, P0.shape[1]))
+    Ac = (P0.T @ A0 @ P0).tocsr()
+    A1 = csr_from(levels[1]["A"].crow_indices(), levels[1]["A"].col_indices(), levels[1]["A"].values(),
+                  levels[1]["n"])
+    assert abs(A1 - Ac).max() <= 1e-10 * abs(Ac).max()
