@@ -346,7 +346,7 @@ def run_ours(args, world, rank, local):
         if dist is not None:
             dist.all_reduce(te, op=dist.ReduceOp.MAX)
         if rank == 0:
-            print(f"[bench] {precision}: levels (n, nnz, nc, p_nnz, coarsest) = {sim.amg_levels()}",
+            print(f"[bench] {precision}: levels (n, nnz, nc, p_nnz, coarsest, columns) = {sim.amg_levels()}",
                   file=sys.stderr)
             print(f"[bench] {precision}: phases {phases}", file=sys.stderr)
         state = {"sw": [float(fl.s_w.min()), float(fl.s_w.max())],

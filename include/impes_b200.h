@@ -69,6 +69,8 @@ typedef struct {
   int p_cols;      /* coarse size (0 on the coarsest level) */
   int p_nnz;
   int is_coarsest;
+  int col_index_bytes;   /* 2 or 4: column storage of the smoothing/residual passes */
+  int col_row_relative;  /* 1: 16-bit columns hold col - row + 32768              */
 } impes_amg_level_desc;
 
 /* Norms for Krylov stopping tests. */

@@ -164,6 +164,8 @@ int impes_amg_level_info(impes_amg* h, int lvl, impes_amg_level_desc* info) {
     info->p_cols = L.coarsest ? 0 : L.nc;
     info->p_nnz = L.coarsest ? 0 : L.pnnz;
     info->is_coarsest = L.coarsest ? 1 : 0;
+    info->col_index_bytes = L.col16.p ? 2 : 4;
+    info->col_row_relative = L.col16.p ? L.col16_rel : 0;
   });
 }
 

@@ -8,7 +8,8 @@ namespace impes {
 struct Level {
   int n = 0, nnz = 0;
   DBuf<int> rowptr, col;
-  DBuf<unsigned short> col16;      // col as 16-bit indices (wide levels of <= 65536 rows)
+  DBuf<unsigned short> col16;      // col as 16-bit indices, or empty (int columns only)
+  int col16_rel = 0;               // 1: column = row - 32768 + col16 (levels of > 65536 rows)
   DBuf<double> val;
   DBuf<float> valf;
   DBuf<double> inv_relax;

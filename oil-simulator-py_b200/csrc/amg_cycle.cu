@@ -29,11 +29,19 @@ enum CsrMode { Y_AX = 0, Y_B_MINUS_AX = 1, Y_SMOOTH = 2, Y_ADD_AX = 3, Y_SMOOTH0
 //  Y_AX: y = A x;  Y_B_MINUS_AX: y = b - A x;  Y_SMOOTH: y = x + w*inv*(b - A x);
 //  Y_ADD_AX: y += A x (prolongation);  Y_SMOOTH0: y = w*inv*b (x = 0);
 //  Y_W_AX: y = wt .* (A x) (weighted operator of FGMRES, wt passed as inv).
-template <typename T, int LPR, int MODE>
+// CT is int, or unsigned short with the column of entry k at
+// col[k] + (rel ? row - 32768 : 0): plain 16-bit indices on levels of at most
+// 65536 rows, row-relative ones on larger levels whose bandwidth fits.
+template <typename CT>
+__device__ __forceinline__ int col_base(long long row, int rel) {
+  return (sizeof(CT) == 2 && rel) ? (int)row - 32768 : 0;
+}
+
+template <typename T, typename CT, int LPR, int MODE>
 __global__ void __launch_bounds__(TB) k_csr(int n, const int* __restrict__ rowptr,
-                                            const int* __restrict__ col, const T* __restrict__ val,
+                                            const CT* __restrict__ col, const T* __restrict__ val,
                                             const T* __restrict__ x, const T* __restrict__ b,
-                                            const T* __restrict__ inv, T* __restrict__ y) {
+                                            const T* __restrict__ inv, T* __restrict__ y, int rel) {
   const int g = threadIdx.x / LPR, lane = threadIdx.x % LPR;
   const int rows_per_block = TB / LPR;
   for (long long row = (long long)blockIdx.x * rows_per_block + g; row < n;
@@ -41,7 +49,8 @@ __global__ void __launch_bounds__(TB) k_csr(int n, const int* __restrict__ rowpt
     T acc = T(0);
     if (MODE != Y_SMOOTH0) {
       const int a = rowptr[row], e = rowptr[row + 1];
-      for (int k = a + lane; k < e; k += LPR) acc += val[k] * x[col[k]];
+      const int cb = col_base<CT>(row, rel);
+      for (int k = a + lane; k < e; k += LPR) acc += val[k] * x[cb + (int)col[k]];
 #pragma unroll
       for (int o = LPR / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, LPR);
     }
@@ -59,15 +68,15 @@ __global__ void __launch_bounds__(TB) k_csr(int n, const int* __restrict__ rowpt
 // Wide rows (coarse Galerkin levels, hundreds to thousands of entries per row):
 // WPR warps per row, chosen by the mean row length.  Thread t of the row group
 // takes entries a+t, a+t+G, ... (G = 32*WPR), so each warp's value and column
-// loads are coalesced and its gathers of x hit adjacent columns.  CT is int, or
-// unsigned short on levels of at most 65536 rows (6 bytes per fp32 entry
-// instead of 8).  With WPR > 1 the row's first warp adds the group's partial
-// sums in a fixed order.  Same epilogues as k_csr.
+// loads are coalesced and its gathers of x hit adjacent columns.  CT and rel as
+// in k_csr (16-bit columns: 6 bytes per fp32 entry instead of 8).  With WPR > 1
+// the row's first warp adds the group's partial sums in a fixed order.  Same
+// epilogues as k_csr.
 template <typename T, typename CT, int MODE, int WPR>
 __global__ void __launch_bounds__(TB) k_csr_rows(int n, const int* __restrict__ rowptr,
                                                  const CT* __restrict__ col, const T* __restrict__ val,
                                                  const T* __restrict__ x, const T* __restrict__ b,
-                                                 const T* __restrict__ inv, T* __restrict__ y) {
+                                                 const T* __restrict__ inv, T* __restrict__ y, int rel) {
   constexpr int kWarps = TB / 32, kRows = kWarps / WPR, G = 32 * WPR;
   __shared__ T part[kWarps];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -78,7 +87,8 @@ __global__ void __launch_bounds__(TB) k_csr_rows(int n, const int* __restrict__ 
     T acc = T(0);
     if (row < n) {
       const int a = rowptr[row], e = rowptr[row + 1];
-      for (int k = a + tid; k < e; k += G) acc += val[k] * x[col[k]];
+      const int cb = col_base<CT>(row, rel);
+      for (int k = a + tid; k < e; k += G) acc += val[k] * x[cb + (int)col[k]];
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
     }
@@ -124,13 +134,14 @@ __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_g
 // lane per step.  Chunks start at 8-entry boundaries (16-byte aligned for fp32
 // values and 16-bit columns); the last piece of a row is clamped to the row end,
 // so nothing past it is read.  Entries of a chunk outside the row are skipped.
-// fp32 values only (the mixed V-cycle).  Same epilogues as k_csr.  Chunks are
-// 512 entries with 16-bit columns and 384 with int columns.
+// fp32 values only (the mixed V-cycle).  CT and rel as in k_csr; same epilogues.
+// Chunks are 512 entries with 16-bit columns and 384 with int columns.
 template <typename CT, int MODE>
 __global__ void __launch_bounds__(TB) k_csr_stream(int n, const int* __restrict__ rowptr,
                                                    const CT* __restrict__ col, const float* __restrict__ val,
                                                    const float* __restrict__ x, const float* __restrict__ b,
-                                                   const float* __restrict__ inv, float* __restrict__ y) {
+                                                   const float* __restrict__ inv, float* __restrict__ y,
+                                                   int rel) {
   constexpr int kWarps = TB / 32;
   constexpr int kCh = sizeof(CT) == 2 ? 512 : 384;   // 48 KB of stages per block
   __shared__ __align__(16) float s_val[kWarps][2][kCh];
@@ -175,7 +186,8 @@ __global__ void __launch_bounds__(TB) k_csr_stream(int n, const int* __restrict_
     __syncwarp();
     const int lo = a > g ? a - g : 0;
     const int hi = e - g < kCh ? e - g : kCh;
-    for (int j = lo + lane; j < hi; j += 32) acc += s_val[warp][st][j] * x[s_col[warp][st][j]];
+    const int cb = col_base<CT>(row, rel);
+    for (int j = lo + lane; j < hi; j += 32) acc += s_val[warp][st][j] * x[cb + (int)s_col[warp][st][j]];
     __syncwarp();                             // stage st is refilled two chunks on
     if (g + kCh >= e) {                       // row done
 #pragma unroll
@@ -197,7 +209,7 @@ __global__ void __launch_bounds__(TB) k_csr_stream(int n, const int* __restrict_
 
 template <typename T, typename CT, int MODE>
 void launch_wide(int n, int avg, const int* rowptr, const CT* col, const T* val, const T* x,
-                 const T* b, const T* inv, T* y, cudaStream_t s) {
+                 const T* b, const T* inv, T* y, int rel, cudaStream_t s) {
   auto grid = [&](int rows_per_block) {
     return grid_for(((size_t)(n + rows_per_block - 1) / rows_per_block) * TB, TB, 16);
   };
@@ -211,38 +223,47 @@ void launch_wide(int n, int avg, const int* rowptr, const CT* col, const T* val,
     constexpr double kStreamMinBytes = 48.0 * (1 << 20);
     if (avg > 512 && (double)n * avg * (sizeof(T) + sizeof(CT)) >= kStreamMinBytes) {
       k_csr_stream<CT, MODE><<<grid(8), TB, 0, s>>>(n, rowptr, col, (const float*)val, (const float*)x,
-                                                    (const float*)b, (const float*)inv, (float*)y); ::impes::count_launch();
+                                                    (const float*)b, (const float*)inv, (float*)y, rel); ::impes::count_launch();
       return;
     }
   }
   if (avg <= 512) {
-    k_csr_rows<T, CT, MODE, 1><<<grid(8), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y); ::impes::count_launch();
+    k_csr_rows<T, CT, MODE, 1><<<grid(8), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y, rel); ::impes::count_launch();
   } else if (avg <= 1536) {
-    k_csr_rows<T, CT, MODE, 2><<<grid(4), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y); ::impes::count_launch();
+    k_csr_rows<T, CT, MODE, 2><<<grid(4), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y, rel); ::impes::count_launch();
   } else {
-    k_csr_rows<T, CT, MODE, 4><<<grid(2), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y); ::impes::count_launch();
+    k_csr_rows<T, CT, MODE, 4><<<grid(2), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y, rel); ::impes::count_launch();
   }
 }
 
-// col16: the same column indices as unsigned short (levels of at most 65536
-// rows), or null; used by the wide-row kernels only.
+template <typename T, typename CT, int MODE>
+void launch_lanes(int lpr, int n, const int* rowptr, const CT* col, const T* val, const T* x,
+                  const T* b, const T* inv, T* y, int rel, cudaStream_t s) {
+  auto grid = [&](int l) { return grid_for(((size_t)n * l + TB - 1) / TB * TB, TB, 16); };
+  switch (lpr) {
+    case 1: k_csr<T, CT, 1, MODE><<<grid(1), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y, rel); break;
+    case 4: k_csr<T, CT, 4, MODE><<<grid(4), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y, rel); break;
+    case 8: k_csr<T, CT, 8, MODE><<<grid(8), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y, rel); break;
+    default: k_csr<T, CT, 16, MODE><<<grid(16), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y, rel); break;
+  }
+  ::impes::count_launch();
+}
+
+// col16 / rel: the level's columns as 16-bit indices (absolute when rel is 0,
+// row - 32768 + col16 when rel is 1), or null for the int columns.
 template <typename T, int MODE>
 void launch_csr(int n, int avg, const int* rowptr, const int* col, const T* val, const T* x,
                 const T* b, const T* inv, T* y, cudaStream_t s,
-                const unsigned short* col16 = nullptr) {
+                const unsigned short* col16 = nullptr, int rel = 0) {
   if (n <= 0) return;
   int lpr = avg <= 8 ? 1 : avg <= 16 ? 4 : avg <= 48 ? 8 : avg <= 96 ? 16 : 32;
   if (MODE == Y_SMOOTH0) lpr = 1;
-  auto grid = [&](int l) { return grid_for(((size_t)n * l + TB - 1) / TB * TB, TB, 16); };
-  switch (lpr) {
-    case 1: k_csr<T, 1, MODE><<<grid(1), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y); ::impes::count_launch(); break;
-    case 4: k_csr<T, 4, MODE><<<grid(4), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y); ::impes::count_launch(); break;
-    case 8: k_csr<T, 8, MODE><<<grid(8), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y); ::impes::count_launch(); break;
-    case 16: k_csr<T, 16, MODE><<<grid(16), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y); ::impes::count_launch(); break;
-    default:
-      if (col16) launch_wide<T, unsigned short, MODE>(n, avg, rowptr, col16, val, x, b, inv, y, s);
-      else launch_wide<T, int, MODE>(n, avg, rowptr, col, val, x, b, inv, y, s);
-      break;
+  if (lpr < 32) {
+    if (col16) launch_lanes<T, unsigned short, MODE>(lpr, n, rowptr, col16, val, x, b, inv, y, rel, s);
+    else launch_lanes<T, int, MODE>(lpr, n, rowptr, col, val, x, b, inv, y, 0, s);
+  } else {
+    if (col16) launch_wide<T, unsigned short, MODE>(n, avg, rowptr, col16, val, x, b, inv, y, rel, s);
+    else launch_wide<T, int, MODE>(n, avg, rowptr, col, val, x, b, inv, y, 0, s);
   }
   IMPES_CHECK_LAUNCH();
 }
@@ -538,8 +559,8 @@ template <> struct LV<float> {
 };
 
 // Algorithmic bytes of CSR products (value size sv, vector size sx).
-inline double spmv_bytes(double sv, double sx, double nnz, double rows, double cols) {
-  return (sv + 4.0) * nnz + 4.0 * (rows + 1) + sx * cols + sx * rows;
+inline double spmv_bytes(double sv, double sx, double nnz, double rows, double cols, double si = 4.0) {
+  return (sv + si) * nnz + 4.0 * (rows + 1) + sx * cols + sx * rows;
 }
 // l1-Jacobi sweep: values, column indices (si bytes each), row pointers, x, b, inv, y.
 inline double sweep_bytes(double s, double nnz, double n, double si = 4.0) {
@@ -560,15 +581,16 @@ T* smooth(Level& L, T* x, T* spare, const T* b, int nu, bool zero_x, cudaStream_
     const int tid = top ? timers().begin(IMPES_PH_SMOOTH_L0, s)
                         : (wide ? timers().begin(IMPES_PH_SMOOTH_WIDE, s) : -1);
     launch_csr<T, Y_SMOOTH>(L.n, L.avg_row, L.rowptr.p, L.col.p, LV<T>::val(L), x, b,
-                            LV<T>::inv(L), spare, s, L.col16.p);
+                            LV<T>::inv(L), spare, s, L.col16.p, L.col16_rel);
     timers().end(tid, s, sweep_bytes(sizeof(T), L.nnz, L.n, L.col16.p ? 2.0 : 4.0));
     std::swap(x, spare);
   }
   return x;
 }
 
-// Algorithmic bytes of one V-cycle from level l down (5 sweeps, residual,
-// restriction, prolongation, vector updates; dense coarsest apply).
+// Algorithmic bytes of one V-cycle from level l down, started from zero (5
+// sweeps, residual, restriction, prolongation, vector updates; dense coarsest
+// apply).
 template <typename T>
 double vcycle_bytes(const AMG& h, int l) {
   const double sz = sizeof(T);
@@ -579,7 +601,9 @@ double vcycle_bytes(const AMG& h, int l) {
       tot += L.n <= 500 ? 8.0 * L.n * (double)L.n + 2.0 * sz * L.n : 50.0 * sweep_bytes(sz, L.nnz, L.n);
       break;
     }
-    tot += 5.0 * sweep_bytes(sz, L.nnz, L.n) + spmv_bytes(sz, sz, L.nnz, L.n, L.n) +
+    // first sweep from zero (b, inv, y), four full sweeps, the residual
+    const double si = L.col16.p ? 2.0 : 4.0;
+    tot += 3.0 * sz * L.n + 4.0 * sweep_bytes(sz, L.nnz, L.n, si) + spmv_bytes(sz, sz, L.nnz, L.n, L.n, si) +
            spmv_bytes(sz, sz, L.pnnz, L.nc, L.n) + spmv_bytes(sz, sz, L.pnnz, L.n, L.nc) + 2.0 * sz * L.n;
   }
   return tot;
@@ -608,7 +632,7 @@ T* vcycle(AMG& h, int l, bool zero_x, cudaStream_t s) {
   T* spare = (x == LV<T>::x(L)) ? LV<T>::t(L) : LV<T>::x(L);
   Level& Nc = *h.levels[l + 1];
   launch_csr<T, Y_B_MINUS_AX>(L.n, L.avg_row, L.rowptr.p, L.col.p, LV<T>::val(L), x, LV<T>::b(L),
-                              nullptr, LV<T>::r(L), s, L.col16.p);
+                              nullptr, LV<T>::r(L), s, L.col16.p, L.col16_rel);
   launch_csr<T, Y_AX>(L.nc, L.r_avg, L.rrow.p, L.rcol.p, LV<T>::rval(L), LV<T>::r(L), nullptr,
                       nullptr, LV<T>::b(Nc), s);
   T* ec = vcycle<T>(h, l + 1, true, s);
@@ -884,8 +908,9 @@ void amg_fgmres(AMG& h, const double* b, double* x, const impes_krylov_params& k
       }
       // w = wt .* (A_s z_j)
       const int tsp = timers().begin(IMPES_PH_SPMV_L0, s);
-      launch_csr<double, Y_W_AX>(n, L0.avg_row, L0.rowptr.p, L0.col.p, L0.val.p, zj, nullptr, wt, w, s);
-      timers().end(tsp, s, spmv_bytes(8.0, 8.0, L0.nnz, n, n) + 8.0 * n);
+      launch_csr<double, Y_W_AX>(n, L0.avg_row, L0.rowptr.p, L0.col.p, L0.val.p, zj, nullptr, wt, w, s,
+                                 L0.col16.p, L0.col16_rel);
+      timers().end(tsp, s, spmv_bytes(8.0, 8.0, L0.nnz, n, n, L0.col16.p ? 2.0 : 4.0) + 8.0 * n);
       const int tor = timers().begin(IMPES_PH_ORTHO, s);
       double* hcol = h.H.p + (size_t)j * ldh;
       for (int pass = 0; pass < 2; ++pass) {

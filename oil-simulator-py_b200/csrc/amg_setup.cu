@@ -67,6 +67,22 @@ __global__ void k_narrow_cols(int nnz, const int* col, unsigned short* col16) {
        e += (long long)gridDim.x * blockDim.x)
     col16[e] = (unsigned short)col[e];
 }
+// flag = 1 when some entry lies more than 32768 columns left or 32767 right of
+// its row (the row-relative 16-bit form cannot hold it)
+__global__ void k_rel16_check(int n, const int* rowptr, const int* col, int* flag) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n;
+       r += (long long)gridDim.x * blockDim.x) {
+    for (int e = rowptr[r]; e < rowptr[r + 1]; ++e) {
+      const long long d = (long long)col[e] - r;
+      if (d < -32768 || d > 32767) { atomicOr(flag, 1); break; }
+    }
+  }
+}
+__global__ void k_narrow_cols_rel(int n, const int* rowptr, const int* col, unsigned short* col16) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n;
+       r += (long long)gridDim.x * blockDim.x)
+    for (int e = rowptr[r]; e < rowptr[r + 1]; ++e) col16[e] = (unsigned short)(col[e] - r + 32768);
+}
 __global__ void k_diag(int n, const int* rowptr, const int* col, const double* val, double* d) {
   GRID_LOOP(i, n) {
     double v = 0.0;
@@ -660,7 +676,11 @@ __global__ void k_plan_sort(int nout, const int* seg, long long* key, int* pe, i
   }
 }
 // out[o] = sum over the segment of a[pe] * b[pf]; one thread per output walks
-// its own run of the plan (consecutive terms share cache lines).
+// its own run of the plan (consecutive terms share cache lines).  Interleaving
+// the runs of 32 outputs so that a warp's index loads coalesce was slower on the
+// 1e6-cell hierarchy (update 10.9 -> 13.0 ms per step): the padding to each
+// group's longest run grows the index stream, while the runs' L1 reuse (~80 %
+// hits) already absorbs the uncoalesced pattern.
 template <typename T>
 __global__ void __launch_bounds__(256) k_plan_apply(int nout, const int* __restrict__ seg,
                                                     const int* __restrict__ pe,
@@ -1225,16 +1245,33 @@ void amg_setup(AMG& h, int n, int nnz, const int* rowptr, const int* col, const 
   }
   coarse_factor(h, Lc, s);
   for (auto& L : h.levels) level_precision_copies(h, *L, s);
-  // 16-bit column indices for the warp-per-row levels that fit (the pattern is
-  // fixed from here on: update_matrix only changes values)
+  // 16-bit column indices for the smoothing and residual passes (the pattern is
+  // fixed from here on: update_matrix only changes values): absolute on levels
+  // of <= 65536 rows, row-relative on larger levels whose entries all lie within
+  // [row - 32768, row + 32767] (banded by the grid ordering, which coarsening
+  // keeps: C-points are numbered in fine order); int columns otherwise.
+  DBuf<int> rel_flag(1);
   for (auto& L : h.levels) {
-    if (L->n <= 65536 && L->avg_row > 96 && L->nnz > 0) {
+    L->col16 = DBuf<unsigned short>();
+    L->col16_rel = 0;
+    if (L->nnz <= 0) continue;
+    if (L->n <= 65536) {
       L->col16.alloc(L->nnz);
       k_narrow_cols<<<grid_for(L->nnz, 256), 256, 0, s>>>(L->nnz, L->col.p, L->col16.p); ::impes::count_launch();
       IMPES_CHECK_LAUNCH();
-    } else {
-      L->col16 = DBuf<unsigned short>();
+      continue;
     }
+    IMPES_CUDA(cudaMemsetAsync(rel_flag.p, 0, sizeof(int), s));
+    k_rel16_check<<<grid_for(L->n, 256), 256, 0, s>>>(L->n, L->rowptr.p, L->col.p, rel_flag.p); ::impes::count_launch();
+    IMPES_CHECK_LAUNCH();
+    int out_of_band = 1;
+    IMPES_CUDA(cudaMemcpyAsync(&out_of_band, rel_flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    IMPES_CUDA(cudaStreamSynchronize(s));
+    if (out_of_band) continue;
+    L->col16.alloc(L->nnz);
+    L->col16_rel = 1;
+    k_narrow_cols_rel<<<grid_for(L->n, 256), 256, 0, s>>>(L->n, L->rowptr.p, L->col.p, L->col16.p); ::impes::count_launch();
+    IMPES_CHECK_LAUNCH();
   }
   IMPES_CUDA(cudaStreamSynchronize(s));
   h.built = true;

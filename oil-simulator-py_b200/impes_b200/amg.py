@@ -224,7 +224,9 @@ class ClassicalAMG:
 
     @property
     def levels(self):
-        """List of level dicts with keys A, n, P, inv_relax, diag, is_coarsest."""
+        """List of level dicts with keys A, n, P, inv_relax, diag, is_coarsest, and the
+        column storage of the level's sweeps: col_index_bytes (2 or 4) and
+        col_row_relative (16-bit offsets from the row)."""
         if self._levels_cache is not None:
             return self._levels_cache
         nl = C.c_int(0)
@@ -257,7 +259,9 @@ class ClassicalAMG:
             d = torch.zeros(info.n, dtype=torch.float64, device=dev)
             d[idx[0][dmask]] = diag.values()[dmask]
             out.append({"A": A, "n": info.n, "P": P, "inv_relax": ir, "diag": d.abs(),
-                        "is_coarsest": bool(info.is_coarsest)})
+                        "is_coarsest": bool(info.is_coarsest),
+                        "col_index_bytes": info.col_index_bytes,
+                        "col_row_relative": bool(info.col_row_relative)})
         self._levels_cache = out
         return out
 

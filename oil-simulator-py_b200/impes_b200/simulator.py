@@ -603,7 +603,9 @@ class Simulator:
         self._wells_stale = False
 
     def amg_levels(self):
-        """[(n, nnz, p_cols, p_nnz, is_coarsest)] of the pressure hierarchy."""
+        """[(n, nnz, p_cols, p_nnz, is_coarsest, columns)] of the pressure hierarchy;
+        columns is the index storage of the level's sweeps: "i32", "u16" or
+        "u16rel" (16-bit offsets from the row)."""
         if self._amg_h is None:
             return []
         nl = C.c_int(0)
@@ -612,7 +614,8 @@ class Simulator:
         for l in range(nl.value):
             d = _lib.LevelDesc()
             check(lib.impes_amg_level_info(self._amg_h, l, C.byref(d)))
-            out.append((d.n, d.nnz, d.p_cols, d.p_nnz, bool(d.is_coarsest)))
+            cols = "i32" if d.col_index_bytes == 4 else ("u16rel" if d.col_row_relative else "u16")
+            out.append((d.n, d.nnz, d.p_cols, d.p_nnz, bool(d.is_coarsest), cols))
         return out
 
     # --------------------------------------------------- building blocks

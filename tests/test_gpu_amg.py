@@ -229,3 +229,65 @@ def test_mixed_vcycle_on_wide_levels_matches_fp64():
     A1 = csr_from(levels[1]["A"].crow_indices(), levels[1]["A"].col_indices(), levels[1]["A"].values(),
                   levels[1]["n"])
     assert abs(A1 - Ac).max() <= 1e-10 * abs(Ac).max()
+
+
+def _laplacian_3d(nx, ny, nz, az=0.1, shift=1e-3):
+    def d1(m, a):
+        return sp.diags([-a * np.ones(m - 1), 2 * a * np.ones(m), -a * np.ones(m - 1)], [-1, 0, 1])
+    ix, iy, iz = sp.identity(nx), sp.identity(ny), sp.identity(nz)
+    A = (sp.kron(sp.kron(d1(nx, 1.0), iy), iz) + sp.kron(sp.kron(ix, d1(ny, 1.0)), iz)
+         + sp.kron(sp.kron(ix, iy), d1(nz, az)))
+    return (A + shift * sp.identity(nx * ny * nz)).tocsr()
+
+
+def _host_hierarchy(amg):
+    """The oracle's V-cycle over the GPU's exported levels (scipy, float64)."""
+    ref = oa.AMG.__new__(oa.AMG)
+    ref.levels = []
+    for lv in amg.levels:
+        n = lv["n"]
+        A = csr_from(lv["A"].crow_indices(), lv["A"].col_indices(), lv["A"].values(), n)
+        P = None
+        if not lv["is_coarsest"]:
+            Pt = lv["P"]
+            P = sp.csr_matrix((to_np(Pt.values()), to_np(Pt.col_indices()), to_np(Pt.crow_indices())),
+                              shape=(n, Pt.shape[1]))
+        ref.levels.append(dict(A=A, n=n, P=P, inv_relax=to_np(lv["inv_relax"]), is_coarsest=lv["is_coarsest"]))
+    return ref
+
+
+@pytest.mark.parametrize("far", [False, True])
+def test_vcycle_with_16bit_row_relative_columns_vs_host(far):
+    """Levels of more than 65,536 rows keep their columns as 16-bit offsets from
+    the row when every entry lies within 32K of the diagonal (the 3-D grid
+    ordering: 64x64x40, bandwidth 2,560), and as int columns when some entry
+    does not (far=True adds symmetric couplings 100,000 columns apart).  The
+    fp64 V-cycle equals the oracle's V-cycle over the same exported levels."""
+    A = _laplacian_3d(64, 64, 40)
+    n = A.shape[0]
+    assert n > 65536
+    if far:
+        i = np.arange(0, n - 100000, 997)
+        C = sp.coo_matrix((np.full(i.size, -0.05), (i, i + 100000)), shape=(n, n))
+        A = (A + C + C.T + sp.diags(np.asarray(abs(C + C.T).sum(axis=1)).ravel())).tocsr()
+    amg = gpu_amg(A, coarsest_size=200, seed=1, mixed_precision=True)
+    lv0 = amg.levels[0]
+    assert lv0["col_index_bytes"] == (4 if far else 2)
+    assert lv0["col_row_relative"] == (not far)
+    for lv in amg.levels:
+        if lv["n"] <= 65536:
+            assert lv["col_index_bytes"] == 2 and not lv["col_row_relative"]
+    ref = _host_hierarchy(amg)
+    rng = np.random.default_rng(5)
+    for _ in range(2):
+        bs = rng.standard_normal(n)
+        v = to_np(amg.vcycle_scaled(torch.tensor(bs, device="cuda"), precision="fp64"))
+        v_ref = ref.vcycle(0, np.zeros_like(bs), bs)
+        assert np.linalg.norm(v - v_ref) <= 1e-10 * np.linalg.norm(v_ref)
+        v32 = to_np(amg.vcycle_scaled(torch.tensor(bs, device="cuda"), precision="fp32"))
+        assert np.linalg.norm(v32 - v_ref) <= 1e-4 * np.linalg.norm(v_ref)
+    # FGMRES to a true residual checked on the host against the original matrix
+    b = rng.standard_normal(n)
+    x, st = amg.fgmres(torch.tensor(b, device="cuda"), tol=1e-10, norm="equilibrated", precision="mixed")
+    assert st["converged"]
+    assert np.linalg.norm(A @ to_np(x) - b) <= 1e-8 * np.linalg.norm(b)
