@@ -36,6 +36,10 @@ struct Level {
   // Ac[o] = sum_t P[ac_r[t]] * AP[ac_f[t]] (ac_r indexes P, since R = P^T)
   bool planned = false;
   DBuf<int> ap_seg, ap_e, ap_f, ac_seg, ac_r, ac_f;
+  long long ap_terms = 0, ac_terms = 0;
+  // the fp32 P factor of every term (P[ap_f[t]], P[ac_r[t]]), copied once since
+  // P is frozen: the fp32 chain then gathers only A (or AP) values
+  DBuf<float> ap_cf, ac_cf;
   // cycle vectors (fp64 and fp32)
   DBuf<double> x, b, r, t;
   DBuf<float> xf, bf, rf, tf;

@@ -695,6 +695,32 @@ __global__ void __launch_bounds__(256) k_plan_apply(int nout, const int* __restr
   }
 }
 
+// out[o] = sum over the segment of v[idx] * cf, cf the term's frozen P factor
+// (same products and order as k_plan_apply, one gather fewer per term).
+template <typename T>
+__global__ void __launch_bounds__(256) k_plan_apply_cf(int nout, const int* __restrict__ seg,
+                                                       const int* __restrict__ idx,
+                                                       const T* __restrict__ cf,
+                                                       const T* __restrict__ v,
+                                                       T* __restrict__ out) {
+  GRID_LOOP(o, nout) {
+    T acc = T(0);
+    for (int t = seg[o]; t < seg[o + 1]; ++t) acc += v[idx[t]] * cf[t];
+    out[o] = acc;
+  }
+}
+__global__ void k_gather_f(long long n, const int* src, const float* in, float* out) {
+  GRID_LOOP(i, n) out[i] = in[src[i]];
+}
+
+template <typename T>
+void plan_apply_cf(int nout, const int* seg, const int* idx, const T* cf, const T* v, T* out,
+                   cudaStream_t s) {
+  if (nout <= 0) return;
+  k_plan_apply_cf<T><<<grid_for(nout, 256, 16), 256, 0, s>>>(nout, seg, idx, cf, v, out); ::impes::count_launch();
+  IMPES_CHECK_LAUNCH();
+}
+
 template <typename T>
 void plan_apply(int nout, const int* seg, const int* pe, const int* pf, const T* a, const T* b,
                 T* out, cudaStream_t s) {
@@ -932,7 +958,8 @@ void union_symbolic(AMG& h, int rows, const int* optr, const int* ocol, const in
 // Returns false (no plan) when the product count does not fit the memory budget.
 bool build_plan(int rows, const int* optr, const int* ocol, const int* iptr, const int* icol,
                 const int* outptr, const int* outcol, int nout, const int* omap, DBuf<int>& seg,
-                DBuf<int>& pe, DBuf<int>& pf, cudaStream_t s) {
+                DBuf<int>& pe, DBuf<int>& pf, long long& nterms, cudaStream_t s) {
+  nterms = 0;
   DBuf<int> bound(std::max(rows, 1));
   k_union_bound<<<grid_for(rows, TB), TB, 0, s>>>(rows, optr, ocol, iptr, bound.p); ::impes::count_launch();
   IMPES_CHECK_LAUNCH();
@@ -968,6 +995,7 @@ bool build_plan(int rows, const int* optr, const int* ocol, const int* iptr, con
   k_plan_sort<<<grid_for(nout, TB), TB, 0, s>>>(nout, seg.p, key.p, pe.p, pf.p); ::impes::count_launch();
   IMPES_CHECK_LAUNCH();
   IMPES_CUDA(cudaStreamSynchronize(s));
+  nterms = nprod;
   return true;
 }
 
@@ -1217,9 +1245,9 @@ void amg_setup(AMG& h, int n, int nnz, const int* rowptr, const int* col, const 
     Nc.nnz = h.hint.p[0];
     Nc.val.alloc(std::max(Nc.nnz, 1));
     L.planned = build_plan(nl, L.rowptr.p, L.col.p, L.prow.p, L.pcol.p, L.aprow.p, L.apcol.p, apnnz,
-                           nullptr, L.ap_seg, L.ap_e, L.ap_f, s) &&
+                           nullptr, L.ap_seg, L.ap_e, L.ap_f, L.ap_terms, s) &&
                 build_plan(nc, L.rrow.p, L.rcol.p, L.aprow.p, L.apcol.p, Nc.rowptr.p, Nc.col.p, Nc.nnz,
-                           L.rsrc.p, L.ac_seg, L.ac_r, L.ac_f, s);
+                           L.rsrc.p, L.ac_seg, L.ac_r, L.ac_f, L.ac_terms, s);
     if (!L.planned) {
       L.ap_seg.release(); L.ap_e.release(); L.ap_f.release();
       L.ac_seg.release(); L.ac_r.release(); L.ac_f.release();
@@ -1245,6 +1273,24 @@ void amg_setup(AMG& h, int n, int nnz, const int* rowptr, const int* col, const 
   }
   coarse_factor(h, Lc, s);
   for (auto& L : h.levels) level_precision_copies(h, *L, s);
+  // frozen fp32 P factors of the plan terms (mixed precision, while memory allows)
+  for (auto& L : h.levels) {
+    L->ap_cf.release();
+    L->ac_cf.release();
+    if (!h.prm.mixed_precision || L->coarsest || !L->planned || !L->pvalf.p) continue;
+    size_t free_b = 0, total_b = 0;
+    IMPES_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    if (4.0 * (double)(L->ap_terms + L->ac_terms) > 0.5 * (double)free_b) continue;
+    if (L->ap_terms > 0) {
+      L->ap_cf.alloc(L->ap_terms);
+      k_gather_f<<<grid_for(L->ap_terms, TB), TB, 0, s>>>(L->ap_terms, L->ap_f.p, L->pvalf.p, L->ap_cf.p); ::impes::count_launch();
+    }
+    if (L->ac_terms > 0) {
+      L->ac_cf.alloc(L->ac_terms);
+      k_gather_f<<<grid_for(L->ac_terms, TB), TB, 0, s>>>(L->ac_terms, L->ac_r.p, L->pvalf.p, L->ac_cf.p); ::impes::count_launch();
+    }
+    IMPES_CHECK_LAUNCH();
+  }
   // 16-bit column indices for the smoothing and residual passes (the pattern is
   // fixed from here on: update_matrix only changes values): absolute on levels
   // of <= 65536 rows, row-relative on larger levels whose entries all lie within
@@ -1293,8 +1339,14 @@ void update_fp32_chain(AMG& h, cudaStream_t s) {
     const int apn = (int)L.apval.n;
     L.apvalf.ensure(std::max(apn, 1));
     Nc.valf.ensure(std::max(Nc.nnz, 1));
-    plan_apply<float>(apn, L.ap_seg.p, L.ap_e.p, L.ap_f.p, L.valf.p, L.pvalf.p, L.apvalf.p, s);
-    plan_apply<float>(Nc.nnz, L.ac_seg.p, L.ac_r.p, L.ac_f.p, L.pvalf.p, L.apvalf.p, Nc.valf.p, s);
+    if (L.ap_terms == 0 || L.ap_cf.p)
+      plan_apply_cf<float>(apn, L.ap_seg.p, L.ap_e.p, L.ap_cf.p, L.valf.p, L.apvalf.p, s);
+    else
+      plan_apply<float>(apn, L.ap_seg.p, L.ap_e.p, L.ap_f.p, L.valf.p, L.pvalf.p, L.apvalf.p, s);
+    if (L.ac_terms == 0 || L.ac_cf.p)
+      plan_apply_cf<float>(Nc.nnz, L.ac_seg.p, L.ac_f.p, L.ac_cf.p, L.apvalf.p, Nc.valf.p, s);
+    else
+      plan_apply<float>(Nc.nnz, L.ac_seg.p, L.ac_r.p, L.ac_f.p, L.pvalf.p, L.apvalf.p, Nc.valf.p, s);
     compute_inv_relax_f(Nc, s);
   }
   coarse_factor(h, *h.levels.back(), s, true);
