@@ -40,6 +40,10 @@ struct Level {
   // the fp32 P factor of every term (P[ap_f[t]], P[ac_r[t]]), copied once since
   // P is frozen: the fp32 chain then gathers only A (or AP) values
   DBuf<float> ap_cf, ac_cf;
+  // A*P terms of the fp32 chain as 16-bit offsets into their output's A row:
+  // ap_e[t] = ap_ebase[o] + ap_e16[t] (empty when a row is longer than 65536)
+  DBuf<unsigned short> ap_e16;
+  DBuf<int> ap_ebase;
   // cycle vectors (fp64 and fp32)
   DBuf<double> x, b, r, t;
   DBuf<float> xf, bf, rf, tf;

@@ -712,6 +712,37 @@ __global__ void __launch_bounds__(256) k_plan_apply_cf(int nout, const int* __re
 __global__ void k_gather_f(long long n, const int* src, const float* in, float* out) {
   GRID_LOOP(i, n) out[i] = in[src[i]];
 }
+// out[o] = sum over the segment of v[base[o] + idx16] * cf (k_plan_apply_cf with
+// the A*P term indices stored as offsets into the output's A row)
+template <typename T>
+__global__ void __launch_bounds__(256) k_plan_apply_cf16(int nout, const int* __restrict__ seg,
+                                                         const int* __restrict__ base,
+                                                         const unsigned short* __restrict__ idx16,
+                                                         const T* __restrict__ cf,
+                                                         const T* __restrict__ v,
+                                                         T* __restrict__ out) {
+  GRID_LOOP(o, nout) {
+    T acc = T(0);
+    const T* __restrict__ vr = v + base[o];
+    for (int t = seg[o]; t < seg[o + 1]; ++t) acc += vr[idx16[t]] * cf[t];
+    out[o] = acc;
+  }
+}
+// base[o] = rowptr[i] for every output o of A*P row i
+__global__ void k_ap_ebase(int n, const int* aprow, const int* rowptr, int* base) {
+  GRID_LOOP(i, n) for (int o = aprow[i]; o < aprow[i + 1]; ++o) base[o] = rowptr[i];
+}
+// e16[t] = pe[t] - base[o]; flag = 1 when an offset does not fit 16 bits
+__global__ void k_ap_e16(int nout, const int* seg, const int* pe, const int* base,
+                         unsigned short* e16, int* flag) {
+  GRID_LOOP(o, nout) {
+    for (int t = seg[o]; t < seg[o + 1]; ++t) {
+      const int d = pe[t] - base[o];
+      if (d < 0 || d > 65535) { atomicOr(flag, 1); return; }
+      e16[t] = (unsigned short)d;
+    }
+  }
+}
 
 template <typename T>
 void plan_apply_cf(int nout, const int* seg, const int* idx, const T* cf, const T* v, T* out,
@@ -1277,6 +1308,8 @@ void amg_setup(AMG& h, int n, int nnz, const int* rowptr, const int* col, const 
   for (auto& L : h.levels) {
     L->ap_cf.release();
     L->ac_cf.release();
+    L->ap_e16.release();
+    L->ap_ebase.release();
     if (!h.prm.mixed_precision || L->coarsest || !L->planned || !L->pvalf.p) continue;
     size_t free_b = 0, total_b = 0;
     IMPES_CUDA(cudaMemGetInfo(&free_b, &total_b));
@@ -1284,6 +1317,18 @@ void amg_setup(AMG& h, int n, int nnz, const int* rowptr, const int* col, const 
     if (L->ap_terms > 0) {
       L->ap_cf.alloc(L->ap_terms);
       k_gather_f<<<grid_for(L->ap_terms, TB), TB, 0, s>>>(L->ap_terms, L->ap_f.p, L->pvalf.p, L->ap_cf.p); ::impes::count_launch();
+      const int apn = (int)L->apval.n;
+      L->ap_ebase.alloc(apn);
+      L->ap_e16.alloc(L->ap_terms);
+      DBuf<int> flag(1);
+      IMPES_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(int), s));
+      k_ap_ebase<<<grid_for(L->n, TB), TB, 0, s>>>(L->n, L->aprow.p, L->rowptr.p, L->ap_ebase.p); ::impes::count_launch();
+      k_ap_e16<<<grid_for(apn, TB), TB, 0, s>>>(apn, L->ap_seg.p, L->ap_e.p, L->ap_ebase.p, L->ap_e16.p, flag.p); ::impes::count_launch();
+      IMPES_CHECK_LAUNCH();
+      int wide = 1;
+      IMPES_CUDA(cudaMemcpyAsync(&wide, flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+      IMPES_CUDA(cudaStreamSynchronize(s));
+      if (wide) { L->ap_e16.release(); L->ap_ebase.release(); }
     }
     if (L->ac_terms > 0) {
       L->ac_cf.alloc(L->ac_terms);
@@ -1339,7 +1384,11 @@ void update_fp32_chain(AMG& h, cudaStream_t s) {
     const int apn = (int)L.apval.n;
     L.apvalf.ensure(std::max(apn, 1));
     Nc.valf.ensure(std::max(Nc.nnz, 1));
-    if (L.ap_terms == 0 || L.ap_cf.p)
+    if (L.ap_e16.p) {
+      k_plan_apply_cf16<float><<<grid_for(apn, 256, 16), 256, 0, s>>>(apn, L.ap_seg.p, L.ap_ebase.p, L.ap_e16.p,
+                                                                      L.ap_cf.p, L.valf.p, L.apvalf.p); ::impes::count_launch();
+      IMPES_CHECK_LAUNCH();
+    } else if (L.ap_terms == 0 || L.ap_cf.p)
       plan_apply_cf<float>(apn, L.ap_seg.p, L.ap_e.p, L.ap_cf.p, L.valf.p, L.apvalf.p, s);
     else
       plan_apply<float>(apn, L.ap_seg.p, L.ap_e.p, L.ap_f.p, L.valf.p, L.pvalf.p, L.apvalf.p, s);
