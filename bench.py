@@ -99,10 +99,14 @@ def run_cpu_reference(steps: int, warmup: int):
 
 # ------------------------------------------------------------------ GPU legs
 class ClockSampler:
-    def __init__(self, index: int):
+    """nvidia-smi clock and throttle-reason samples every 200 ms while the timed
+    region runs; the raw samples go to `directory` (a temporary one by default)."""
+
+    def __init__(self, index: int, directory: str | None = None):
+        import tempfile
         self.index = index
         self.proc = None
-        self.path = os.path.join(REPO, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+        self.path = os.path.join(directory or tempfile.gettempdir(), f"clocks_bench_{os.getpid()}.csv")
 
     def __enter__(self):
         os.makedirs(os.path.dirname(self.path), exist_ok=True)
@@ -328,7 +332,7 @@ def run_ours(args, world, rank, local):
             dist.barrier()
         torch.cuda.synchronize()
         launches0 = _lib.kernel_launches()
-        with ClockSampler(local) as clk:
+        with ClockSampler(local, args.clocks_dir) as clk:
             ms, iters = time_steps(sim, args.steps, dt, flush, stream)
         launches = _lib.kernel_launches() - launches0
         torch.cuda.synchronize()
@@ -503,6 +507,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--clocks-dir", default=None,
+                    help="directory for the raw nvidia-smi clock samples (default: a temporary one)")
     ap.add_argument("--restart", type=int, default=60, help="FGMRES restart length")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 V-cycle baseline")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward measurement")
