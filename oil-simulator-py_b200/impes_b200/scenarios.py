@@ -14,6 +14,9 @@ Workloads (sizes as named):
                         capillarity, 4 rate injectors + 1 BHP producer, 50 x 5 d
 * ``gas_injection_1m``  200x200x25 = 1e6 cells, correlated log-normal k,
                         9 surface-rate gas injectors + 16 BHP producers, 20 x 2 d
+* ``three_phase``       16x16x3 oil-water-gas without PVT (constant
+                        compressibilities), initial free gas above Sgc, a gas
+                        and a water injector, two rate producers, 10 x 1 d
 * ``adjoint_case``      64x64x8 with the two-phase fluids, 50 x 2 d
 * ``ensemble``          64 uneven realisations (nx, ny in {32..128}, nz in {4,8,16})
 
@@ -101,6 +104,54 @@ def two_phase_2d(seed: int = 0, nx: int = 64, ny: int = 64, nz: int = 1, steps: 
         "simulation": _sim(dt_days, steps),
     }
     return cfg, {"kx": k, "ky": k.copy(), "kz": k.copy(), "poro": poro}
+
+
+def three_phase(seed: int = 6, nx: int = 16, ny: int = 16, nz: int = 3, steps: int = 10,
+                dt_days: float = 1.0, rate: float = 10.0):
+    """Three phases without PVT: ln k ~ N(ln 120 mD, 0.6^2) i.i.d., kz = 0.1 kx,
+    phi ~ U[0.2, 0.25]; Sw = 0.2, Sg = 0.04 (Sgc 0.02) at 22 MPa; c_gas = 1e-3
+    1/MPa; Corey with ng = 2.5; a gas and a water injector and two producers,
+    all rate-controlled at ``rate`` m3/d, in the middle layer.
+
+    The producers are rate wells on purpose.  A BHP producer's cell sits at the
+    well pressure to within rounding, so its saturation-step rate
+    WI*lambda*(p - p_bhp) (simulation.py:1297) is rounding noise; with mobile gas
+    that noise decides the trajectory within a few steps (the reference's own
+    run of this case with BHP producers reaches Sw = -0.6 at the fifth step).
+    Near the substep cap of 20 the explicit update is fragile too: on the
+    reference's configs/gas_injection_3phase.json, run in float64, a gas
+    injector's cell passes Sg > 1 - Sor - Swc at the third step and the clamp
+    order (Sw to [Swc, 1 - Sor - Sg] first) takes Sw below Swc."""
+    rng = np.random.default_rng(seed)
+    shape = (nx, ny, nz)
+    k = _lognormal(rng, shape, 120.0, 0.6)
+    poro = 0.2 + 0.05 * rng.random(shape)
+    km = nz // 2
+    cfg = {
+        "reservoir": {"dimensions": [nx, ny, nz], "grid_size": [10.0, 10.0, 5.0], "porosity": 0.22,
+                      "permeability": 120.0, "k_vertical_fraction": 0.1, "c_rock": 1e-5},
+        "fluid": {
+            "pressure": 22.0, "s_w": 0.2, "s_g": 0.04,
+            "mu_oil": 1.8, "mu_water": 0.5, "mu_gas": 0.02,
+            "rho_oil": 840.0, "rho_water": 1000.0, "rho_gas": 1.1,
+            "c_oil": 1e-5, "c_water": 5e-6, "c_gas": 1e-3, "c_rock": 1e-5,
+            "relative_permeability": {"nw": 2.0, "no": 2.0, "ng": 2.5, "sw_cr": 0.15, "so_r": 0.2,
+                                      "sg_cr": 0.02},
+            "capillary_pressure": {"pc_scale": 0.0},
+        },
+        "wells": [
+            {"name": "GI", "type": "injector", "i": 2, "j": ny // 2, "k": km, "radius": 0.1,
+             "control_type": "rate", "control_value": rate, "injected_phase": "gas"},
+            {"name": "WI", "type": "injector", "i": nx - 3, "j": ny // 2, "k": km, "radius": 0.1,
+             "control_type": "rate", "control_value": rate, "injected_phase": "water"},
+            {"name": "P1", "type": "producer", "i": nx // 2, "j": 3, "k": km, "radius": 0.1,
+             "control_type": "rate", "control_value": rate},
+            {"name": "P2", "type": "producer", "i": nx // 2, "j": ny - 4, "k": km, "radius": 0.1,
+             "control_type": "rate", "control_value": rate},
+        ],
+        "simulation": _sim(dt_days, steps),
+    }
+    return cfg, {"kx": k, "ky": k.copy(), "kz": 0.1 * k, "poro": poro}
 
 
 def _black_oil_fluid(pvt):

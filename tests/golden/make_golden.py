@@ -1,6 +1,6 @@
 """Generate the golden fixtures by running the reference itself (build container only).
 
-Usage:  python tests/golden/make_golden.py [REFERENCE_ROOT] [--pcg-only]
+Usage:  python tests/golden/make_golden.py [REFERENCE_ROOT] [--pcg-only | --three-phase-only]
 
 REFERENCE_ROOT defaults to /root/reference (researchim-ai/oil-simulator-py).
 The reference is imported unmodified; the harness only
@@ -284,6 +284,15 @@ def main():
     cfg["simulation"]["cg_tolerance"] = 1e-9
     cfg["simulation"]["cg_max_iter"] = 3000
     run_trajectory("cg_two_phase_20x16x2", cfg, f, steps=3, dt_days=1.0, solver="cg")
+    three_phase_fixture()
+
+
+def three_phase_fixture():
+    """Three phases without PVT (initial free gas above Sgc, a gas and a water
+    injector, two rate producers): the reference's constant-compressibility gas
+    path, which the black-oil fixtures do not reach."""
+    cfg, f = scenarios.three_phase(seed=6, steps=5)
+    run_trajectory("three_phase_16x16x3", cfg, f, steps=5, dt_days=1.0)
 
 
 def main_pcg_only():
@@ -302,5 +311,8 @@ def main_pcg_only():
 if __name__ == "__main__":
     if "--pcg-only" in sys.argv:
         main_pcg_only()
+        sys.exit(0)
+    if "--three-phase-only" in sys.argv:
+        three_phase_fixture()
         sys.exit(0)
     main()

@@ -9,7 +9,7 @@ from gpu_util import cfg_fields, gpu_sim, oracle_model, rel_max, to_np
 pytestmark = pytest.mark.gpu
 
 CASES = ["two_phase_32x32", "two_phase_64x64", "two_phase_16x16x2", "black_oil_10x10x4",
-         "gas_injection_12x12x3"]
+         "gas_injection_12x12x3", "three_phase_16x16x3"]
 
 
 @pytest.mark.parametrize("name", CASES)

@@ -1,0 +1,67 @@
+"""The reference's own known-answer tests restated against the oracle: Stone II
+(tests/test_relperm_stone2.py:11-57) and the three-phase IMPES smoke and mass
+balance checks (tests/test_impes_3phase.py:16-110).  The three-phase checks run
+on this package's seeded three_phase scenario, whose first five steps the oracle
+reproduces to 1e-13 (tests/golden/three_phase_16x16x3.npz)."""
+import numpy as np
+
+from impes_b200 import scenarios
+from oracle.impes import Model
+
+
+def _stone_model(**rp):
+    cfg = {"reservoir": {"dimensions": [4, 4, 1], "grid_size": [10.0, 10.0, 10.0], "porosity": 0.2,
+                         "permeability": 100.0, "k_vertical_fraction": 1.0},
+           "fluid": {"pressure": 20.0, "s_w": 0.3, "s_g": 0.0,
+                     "relative_permeability": dict(model="stone2", **rp)},
+           "wells": [], "simulation": {}}
+    return Model(cfg)
+
+
+def test_stone2_reduces_to_corey_when_sg_is_zero():
+    """test_relperm_stone2.py:11-43, over the whole Sw range instead of Sw = 0.6."""
+    m = _stone_model(nw=2.0, no=2.0, ng=2.0, ko_end_w=1.0, ko_end_g=1.0)
+    sw = np.linspace(0.0, 1.0, 101)
+    kro, _, _ = m.relperms(sw, np.zeros_like(sw))
+    s_norm = (sw - m.sw_cr) / (1 - m.sw_cr - m.so_r)
+    kro_corey = np.clip(1 - s_norm, 0.0, 1.0) ** m.no
+    np.testing.assert_allclose(kro, kro_corey, atol=1e-6)
+
+
+def test_stone2_oil_relperm_vanishes_at_residual_oil():
+    """test_relperm_stone2.py:46-57: kro <= 1e-3 at Sw = 1 - Sor - 1e-6, Sg = 0."""
+    m = _stone_model()
+    sw = np.full(16, 1.0 - m.so_r - 1e-6)
+    kro, _, _ = m.relperms(sw, np.zeros_like(sw))
+    assert (kro <= 1e-3).all()
+
+
+def _total_mass(m):
+    """_compute_total_masses (test_impes_3phase.py:16-30): sum of phi S rho V."""
+    rw, ro, rg = m.densities(m.p)
+    return float(np.sum(m.pv * (m.sw * rw + m.so * ro + m.sg * rg)))
+
+
+def test_three_phase_bounds_and_mass_balance():
+    """test_impes_3phase.py:60-110, 10 steps of 1 day: finite fields,
+    saturations within their clamps, Sw + Sg + So = 1 to 1e-6, gas moved, and
+    the change of total mass equal to the recorded net inflow within the
+    reference's 5 * max(1e-6, 1e-3 * M0) (here it agrees to rounding, since the
+    densities depend on pressure only weakly)."""
+    cfg, f = scenarios.three_phase(seed=6, steps=10)
+    m = Model(cfg, f["kx"], f["ky"], f["kz"], f["poro"])
+    m0 = _total_mass(m)
+    sg0 = m.sg.copy()
+    for _ in range(10):
+        p, _ = m.step(86400.0)
+        assert p is not None
+    assert np.isfinite(m.p).all() and np.isfinite(m.sw).all() and np.isfinite(m.sg).all()
+    assert (m.sw >= m.sw_cr).all() and (m.sw <= 1.0 - m.so_r).all()
+    assert (m.sg >= m.sg_cr).all() and (m.sg <= 1.0 - m.so_r - m.sw + 1e-8).all()
+    np.testing.assert_allclose(m.sw + m.sg + m.so, 1.0, atol=1e-6)
+    assert np.abs(m.sg - sg0).max() > 0.1
+    net = sum(m.mass_balance[ph]["in"] - m.mass_balance[ph]["out"] for ph in ("water", "oil", "gas"))
+    d_mass = _total_mass(m) - m0
+    atol = max(1e-6, 1e-3 * max(abs(m0), 1.0))
+    assert abs(d_mass - net) <= 5 * atol, (d_mass, net, m0)
+    assert abs(d_mass - net) <= 1e-6 * abs(m0)
