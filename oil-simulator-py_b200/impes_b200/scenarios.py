@@ -36,12 +36,14 @@ def _lognormal(rng, shape, mean_md, sigma):
 
 
 def pvt_table_black_oil(rows: int = 20, p_lo: float = 5.0, p_hi: float = 40.0,
-                        bo_increasing: bool = False) -> dict:
+                        bo_increasing: bool = False, rv_max: float = 0.0) -> dict:
     """Monotone synthetic black-oil table over ``p_lo..p_hi`` MPa.
 
     Bo spans 1.1..1.3, Rs 0 -> 150, mu_o 3 -> 1.5 cP, mu_g 0.012 -> 0.025 cP
     (all linear in p); Bg 0.02 -> 0.003 as ``a/p + b`` through both end points;
-    water is slightly compressible (Bw 1.02 -> 1.00) with mu_w 0.5 cP; Rv is 0.
+    water is slightly compressible (Bw 1.02 -> 1.00) with mu_w 0.5 cP.  Rv
+    (vaporised oil, ``Rv_m3m3``) rises linearly from 0 to ``rv_max``; with the
+    default 0 the column is left out, as the reference's loader allows.
 
     Bo decreases with pressure by default (1.3 at p_lo to 1.1 at p_hi).  The
     reference's total compressibility c_o = -(1/Bo) dBo/dP (fluid.py:190-222) has
@@ -61,6 +63,7 @@ def pvt_table_black_oil(rows: int = 20, p_lo: float = 5.0, p_hi: float = 40.0,
         "mu_w_cP": np.full(rows, 0.5).tolist(),
         "mu_g_cP": (0.012 + 0.013 * t).tolist(),
         "Rs_m3m3": (150.0 * t).tolist(),
+        **({"Rv_m3m3": (rv_max * t).tolist()} if rv_max > 0.0 else {}),
     }
 
 

@@ -1,6 +1,6 @@
 """Generate the golden fixtures by running the reference itself (build container only).
 
-Usage:  python tests/golden/make_golden.py [REFERENCE_ROOT] [--pcg-only | --three-phase-only]
+Usage:  python tests/golden/make_golden.py [REFERENCE_ROOT] [--pcg-only | --three-phase-only | --wells-only]
 
 REFERENCE_ROOT defaults to /root/reference (researchim-ai/oil-simulator-py).
 The reference is imported unmodified; the harness only
@@ -285,6 +285,7 @@ def main():
     cfg["simulation"]["cg_max_iter"] = 3000
     run_trajectory("cg_two_phase_20x16x2", cfg, f, steps=3, dt_days=1.0, solver="cg")
     three_phase_fixture()
+    well_fixtures()
 
 
 def three_phase_fixture():
@@ -293,6 +294,52 @@ def three_phase_fixture():
     path, which the black-oil fixtures do not reach."""
     cfg, f = scenarios.three_phase(seed=6, steps=5)
     run_trajectory("three_phase_16x16x3", cfg, f, steps=5, dt_days=1.0)
+
+
+def _well_case(nx, ny, wells, s_w, s_g, rv_max=0.0, k_md=150.0, poro=0.22):
+    """A small homogeneous black-oil grid (10 x 10 x 8 m cells, Stone II) around
+    a handful of surface-rate wells."""
+    pvt = scenarios.pvt_table_black_oil(rv_max=rv_max)
+    shape = (nx, ny, 1)
+    k = np.full(shape, k_md * scenarios.MD)
+    cfg = {
+        "reservoir": {"dimensions": [nx, ny, 1], "grid_size": [10.0, 10.0, 8.0], "porosity": poro,
+                      "permeability": k_md, "k_vertical_fraction": 1.0, "c_rock": 1e-5},
+        "fluid": {"pressure": 21.0, "s_w": s_w, "s_g": s_g, "pvt": {"table": pvt},
+                  "rho_oil": 850.0, "rho_water": 1000.0, "rho_gas": 1.0,
+                  "relative_permeability": {"model": "stone2", "nw": 2.0, "no": 2.0, "ng": 2.0,
+                                            "sw_cr": 0.2, "so_r": 0.2, "sg_cr": 0.0}},
+        "wells": wells,
+        "simulation": {"solver_type": "impes", "time_step_days": 1.0, "total_time_days": 3.0},
+    }
+    return cfg, {"kx": k, "ky": k.copy(), "kz": k.copy(), "poro": np.full(shape, poro)}
+
+
+def well_fixtures():
+    """Surface-rate wells as the reference's own tests place them
+    (tests/test_surface_*.py, tests/test_component_balance_rv.py): a surface oil
+    producer beside a water injector, a surface gas producer in free gas, a
+    surface gas injector with a surface liquid producer on a table with Rv, and
+    a surface water injector beside a reservoir-rate producer; 3 steps of 1 day."""
+    w = lambda name, typ, i, j, **kw: dict(name=name, type=typ, i=i, j=j, k=0, radius=0.1,
+                                            control_type="rate", **kw)
+    cases = {
+        "wells_surface_oil_6x6": _well_case(6, 6, [
+            w("PO", "producer", 4, 4, control_value=60.0, rate_type="surface", surface_phase="oil"),
+            w("WI", "injector", 1, 1, control_value=50.0, injected_phase="water")], 0.3, 0.0),
+        "wells_surface_gas_6x6": _well_case(6, 6, [
+            w("PG", "producer", 3, 3, control_value=25.0, rate_type="surface", surface_phase="gas")],
+            0.3, 0.06),
+        "wells_rv_liquid_6x6": _well_case(6, 6, [
+            w("GI", "injector", 1, 1, control_value=300.0, rate_type="surface", injected_phase="gas"),
+            w("PL", "producer", 4, 4, control_value=150.0, rate_type="surface", surface_phase="liquid")],
+            0.25, 0.05, rv_max=1.0e-4),
+        "wells_surface_water_6x6": _well_case(6, 6, [
+            w("WI", "injector", 2, 2, control_value=80.0, rate_type="surface", injected_phase="water"),
+            w("PR", "producer", 4, 4, control_value=70.0)], 0.2, 0.0),
+    }
+    for name, (cfg, f) in cases.items():
+        run_trajectory(name, cfg, f, steps=3, dt_days=1.0)
 
 
 def main_pcg_only():
@@ -314,5 +361,8 @@ if __name__ == "__main__":
         sys.exit(0)
     if "--three-phase-only" in sys.argv:
         three_phase_fixture()
+        sys.exit(0)
+    if "--wells-only" in sys.argv:
+        well_fixtures()
         sys.exit(0)
     main()

@@ -65,3 +65,54 @@ def test_three_phase_bounds_and_mass_balance():
     atol = max(1e-6, 1e-3 * max(abs(m0), 1.0))
     assert abs(d_mass - net) <= 5 * atol, (d_mass, net, m0)
     assert abs(d_mass - net) <= 1e-6 * abs(m0)
+
+
+def _black_oil_5x5(wells, s_w, s_g, rv_max=0.0, k_md=150.0, poro=0.2):
+    pvt = scenarios.pvt_table_black_oil(rv_max=rv_max)
+    cfg = {"reservoir": {"dimensions": [5, 5, 1], "grid_size": [10.0, 10.0, 10.0], "porosity": poro,
+                         "permeability": k_md, "k_vertical_fraction": 1.0},
+           "fluid": {"pressure": 20.0, "s_w": s_w, "s_g": s_g, "pvt": {"table": pvt}},
+           "wells": wells, "simulation": {"solver_type": "impes", "time_step_days": 1.0}}
+    return Model(cfg)
+
+
+def test_component_balance_closes_with_rv():
+    """test_component_balance_rv.py:12-45: a surface gas injector and a surface
+    liquid producer on a table with vaporised oil; after one day each
+    component's (in - out) - accumulation is below 1e-2 (1 + |accumulation|)."""
+    m = _black_oil_5x5([
+        {"name": "GI", "type": "injector", "i": 1, "j": 1, "k": 0, "radius": 0.1, "control_type": "rate",
+         "control_value": 400.0, "rate_type": "surface", "injected_phase": "gas"},
+        {"name": "PL", "type": "producer", "i": 3, "j": 3, "k": 0, "radius": 0.1, "control_type": "rate",
+         "control_value": 250.0, "rate_type": "surface", "surface_phase": "liquid"}], 0.25, 0.05,
+        rv_max=1.0e-4, k_md=200.0, poro=0.25)
+    p, _ = m.step(86400.0)
+    assert p is not None
+    cb = m.component_balance
+    for comp in ("oil", "gas"):
+        resid = (cb[comp]["in"] - cb[comp]["out"]) - cb[comp]["accum"]
+        assert abs(resid) < 1e-2 * (1.0 + abs(cb[comp]["accum"])), (comp, cb[comp])
+    assert cb["gas"]["in"] > 0.0 and cb["oil"]["out"] > 0.0
+
+
+def test_surface_water_injection_adds_its_mass():
+    """test_surface_rate_conversion.py:13-70: a lone surface water injector; the
+    water mass gained in one day is positive and within 35 % of
+    min(q_surf Bw rho_w dt, the mass the availability window admits)."""
+    m = _black_oil_5x5([
+        {"name": "WI", "type": "injector", "i": 2, "j": 2, "k": 0, "radius": 0.1, "control_type": "rate",
+         "control_value": 100.0, "injected_phase": "water", "rate_type": "surface"}], 0.2, 0.0)
+    c = 2 * 5 + 2
+    rho_w0 = m.densities(m.p)[0]
+    mw0 = float(np.sum(m.pv * m.sw * rho_w0))
+    sw0 = m.sw.copy()
+    dt = 86400.0
+    p, _ = m.step(dt)
+    assert p is not None
+    rho_w1 = m.densities(m.p)[0]
+    bw = float(m.ev(m.p, "Bw")[c])
+    expected = 100.0 / 86400.0 * bw * float(rho_w1[c]) * dt
+    cap = float(np.sum(m.pv * np.maximum(1.0 - m.so_r - sw0, 0.0) * rho_w0))
+    delta = float(np.sum(m.pv * m.sw * rho_w1)) - mw0
+    assert delta > 0.0
+    assert abs(delta - min(expected, cap)) / max(min(expected, cap), 1e-6) < 0.35
