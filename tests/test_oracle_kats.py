@@ -67,11 +67,11 @@ def test_three_phase_bounds_and_mass_balance():
     assert abs(d_mass - net) <= 1e-6 * abs(m0)
 
 
-def _black_oil_5x5(wells, s_w, s_g, rv_max=0.0, k_md=150.0, poro=0.2):
+def _black_oil_5x5(wells, s_w, s_g, rv_max=0.0, k_md=150.0, poro=0.2, p_mpa=20.0):
     pvt = scenarios.pvt_table_black_oil(rv_max=rv_max)
     cfg = {"reservoir": {"dimensions": [5, 5, 1], "grid_size": [10.0, 10.0, 10.0], "porosity": poro,
                          "permeability": k_md, "k_vertical_fraction": 1.0},
-           "fluid": {"pressure": 20.0, "s_w": s_w, "s_g": s_g, "pvt": {"table": pvt}},
+           "fluid": {"pressure": p_mpa, "s_w": s_w, "s_g": s_g, "pvt": {"table": pvt}},
            "wells": wells, "simulation": {"solver_type": "impes", "time_step_days": 1.0}}
     return Model(cfg)
 
@@ -116,3 +116,84 @@ def test_surface_water_injection_adds_its_mass():
     delta = float(np.sum(m.pv * m.sw * rho_w1)) - mw0
     assert delta > 0.0
     assert abs(delta - min(expected, cap)) / max(min(expected, cap), 1e-6) < 0.35
+
+
+def _rv_table():
+    return {"pressure_MPa": [8.0, 18.0, 35.0, 55.0], "Bo": [1.25, 1.12, 1.06, 1.04],
+            "Bw": [1.02, 1.01, 1.0, 0.99], "Bg": [0.012, 0.006, 0.0035, 0.0025],
+            "mu_o_cP": [2.2, 1.6, 1.35, 1.25], "mu_w_cP": [0.5, 0.51, 0.52, 0.53],
+            "mu_g_cP": [0.018, 0.022, 0.028, 0.033], "Rs_m3m3": [70.0, 110.0, 140.0, 155.0],
+            "Rv_m3m3": [0.0, 0.008, 0.014, 0.018]}
+
+
+def test_pvt_rv_column_and_gas_density():
+    """test_pvt_rv.py:32-55: a table with vaporised oil evaluates Rv >= 0 inside
+    and outside its range (flat extrapolation), and the gas density
+    (rho_g,sc + Rv rho_o,sc) / Bg (fluid.py:129-158) is finite and positive."""
+    from oracle.impes import PVT
+    pvt = PVT(_rv_table())
+    rv = pvt.eval(np.array([5.0e6, 15.0e6, 45.0e6, 80.0e6]), "Rv")
+    assert (rv >= 0.0).all() and rv[0] == 0.0 and rv[-1] == 0.018
+    np.testing.assert_allclose(rv[1], 0.008 * 0.7, rtol=1e-15)
+    cfg = {"reservoir": {"dimensions": [2, 2, 1], "grid_size": [10.0, 10.0, 10.0], "porosity": 0.2,
+                         "permeability": 100.0, "k_vertical_fraction": 1.0},
+           "fluid": {"pressure": 40.0, "s_w": 0.2, "s_g": 0.1, "pvt": {"table": _rv_table()}},
+           "wells": [], "simulation": {}}
+    m = Model(cfg)
+    _, _, rho_g = m.densities(m.p)
+    assert np.isfinite(rho_g).all() and (rho_g > 0.0).all()
+    bg, rvp = m.ev(m.p, "Bg"), m.ev(m.p, "Rv")
+    np.testing.assert_allclose(rho_g, (m.rho_gas_ref + rvp * m.rho_oil_ref) / (bg + 1e-12), rtol=1e-15)
+    assert (rvp > 0.0).all()
+
+
+def test_wopr_limit_throttles_a_surface_oil_producer():
+    """test_phase_limits_and_autoswitch.py:12-34: a surface oil producer asked
+    for far more than its WOPR limit produces at most 110 % of the limit."""
+    m = _black_oil_5x5([
+        {"name": "PO", "type": "producer", "i": 2, "j": 2, "k": 0, "radius": 0.1, "control_type": "rate",
+         "control_value": 30000.0, "rate_type": "surface", "surface_phase": "oil",
+         "limits": {"wopr": 80.0}}], 0.3, 0.02)
+    p, _ = m.step(86400.0)
+    assert p is not None
+    rates = m.wells[0].last_surface_rates
+    assert 0.0 < rates.get("oil", 0.0) <= 80.0 * 1.10
+
+
+def _rate_producer_step(s_w, s_g, rate, extra=None):
+    well = {"name": "P", "type": "producer", "i": 2, "j": 2, "k": 0, "radius": 0.1,
+            "control_type": "rate", "control_value": rate, **(extra or {})}
+    m = _black_oil_5x5([well], s_w, s_g, p_mpa=10.0)
+    p, _ = m.step(86400.0)
+    assert p is not None
+    return m
+
+
+def test_bhp_min_autoswitch_does_not_raise_outflow():
+    """test_phase_limits_and_autoswitch.py:37-70: the same rate producer with a
+    bhp_min produces no more than without one.  The switch
+    (simulation.py:1636-1650) compares the BHP a producer needs,
+    p + |q|/(WI lambda), with bhp_min, so it never fires for a producer: the two
+    total rates are equal and the well stays on rate control.  The cell here
+    holds water above Swc and free gas, so the producer is not choked (see the
+    next test); the reference's own case starts at Sw = Swc, Sg = 0, where both
+    rates are 0."""
+    with_min = _rate_producer_step(0.3, 0.03, 50.0, {"bhp_min": 9.5})
+    free = _rate_producer_step(0.3, 0.03, 50.0)
+    q_min, q_free = abs(with_min.wells[0].last_q_total), abs(free.wells[0].last_q_total)
+    assert q_min <= q_free + 1e-9
+    assert q_min == q_free and q_free > 0.0 and with_min.wells[0].last_mode == "rate"
+
+
+def test_rate_producer_at_connate_water_is_choked_in_the_saturation_step():
+    """simulation.py:1161-1170: a phase whose well-driven change dS is exactly 0
+    takes the 'falling' branch, alpha = min(alpha, room / max(|dS|, 1e-12)), so a
+    cell at Swc (or at Sgc, e.g. without free gas when Sgc = 0) gives alpha = 0
+    and the producer removes nothing in the saturation step, while its sink in
+    the pressure step still draws the pressure down."""
+    choked = _rate_producer_step(0.2, 0.0, 50.0)           # Sw = Swc = 0.2, Sg = Sgc = 0
+    assert choked.wells[0].last_q_total == 0.0
+    assert choked.p.min() < 10.0e6 - 1.0e6                  # the pressure sink acted
+    np.testing.assert_array_equal(choked.sw, 0.2)
+    flowing = _rate_producer_step(0.3, 0.03, 50.0)
+    assert flowing.wells[0].last_q_total < 0.0
