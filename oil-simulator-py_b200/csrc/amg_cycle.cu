@@ -317,12 +317,10 @@ __global__ void __launch_bounds__(TB) k_multidot(long long n, const double* __re
 // out[q] (+)= sum of partials, fixed order
 __global__ void k_dot_finalize(int k, const double* partial, double* out, int accumulate) {
   const int q = blockIdx.x;
-  __shared__ double s[32];
   double t = 0.0;
   for (int b = threadIdx.x; b < kDotBlocks; b += 32) t += partial[q * kDotBlocks + b];
   t = warp_sum(t);
   if (threadIdx.x == 0) out[q] = accumulate ? out[q] + t : t;
-  (void)s;
   (void)k;
 }
 // w -= sum_q h[q] V[q]; optionally partial norms of the result

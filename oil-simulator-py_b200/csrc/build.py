@@ -50,6 +50,8 @@ def _compile(src, extra, debug):
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         return obj, f"{' '.join(cmd)}\n{r.stdout}\n{r.stderr}"
+    if "warning" in r.stderr:
+        sys.stderr.write(f"{src}: compiler warnings\n{r.stderr}")
     return obj, None
 
 

@@ -71,7 +71,6 @@ __global__ void __launch_bounds__(TBP) k_pcg_spmv(int n, const int* __restrict__
 // out = sum of kBlocks partials in a fixed order; mode 0: p.Ap -> alpha,
 // mode 1: r.z -> rs_new and beta (rs_old then takes rs_new)
 __global__ void k_pcg_scalar(const double* __restrict__ part, double* scal, int mode) {
-  __shared__ double sh[32];
   double t = 0.0;
   for (int q = threadIdx.x; q < kBlocks; q += 32) t += part[q];
   t = warp_sum(t);
@@ -88,7 +87,6 @@ __global__ void k_pcg_scalar(const double* __restrict__ part, double* scal, int 
       scal[1] = t;
     }
   }
-  (void)sh;
 }
 
 // x += alpha p; r -= alpha Ap; z = r / d; partial r.z
