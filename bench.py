@@ -66,18 +66,33 @@ def dist_env():
 
 
 # ------------------------------------------------------------------ CPU legs
-def cpu_sample_workload(seed=2):
+def cpu_sample_workload(dims=CPU_SAMPLE, seed=2):
     from impes_b200 import scenarios
-    nx, ny, nz = CPU_SAMPLE
+    nx, ny, nz = dims
     return scenarios.gas_injection_1m(seed=seed, nx=nx, ny=ny, nz=nz)
 
 
-def run_cpu_reference(steps: int, warmup: int):
-    """The oracle's restatement of the reference step on the host cores.
+def reference_sample_dims(steps: int, warmup: int, full_steps: int = 8):
+    """The spatial sample of the reference arm: CPU_SAMPLE while the run has at
+    most `full_steps` steps, otherwise a laterally smaller piece (nz kept) whose
+    steps take about as long in total, so a long --steps run still ends within
+    a few minutes (a 100x100x25 step takes ~15 s on one core)."""
+    total = max(steps, 0) + max(warmup, 1)
+    if total <= full_steps:
+        return CPU_SAMPLE
+    scale = (full_steps / total) ** 0.5
+    nx = max(32, int(round(CPU_SAMPLE[0] * scale)))
+    ny = max(32, int(round(CPU_SAMPLE[1] * scale)))
+    return (nx, ny, CPU_SAMPLE[2])
+
+
+def run_cpu_reference(steps: int, warmup: int, dims=CPU_SAMPLE):
+    """The oracle's restatement of the reference step on the host cores, on a
+    `dims` spatial sample of the workload.
     Returns (cell-steps/s, seconds timed, cells, threads, description)."""
     from oracle.amg import AMGSolver
     from oracle.impes import Model
-    cfg, f = cpu_sample_workload()
+    cfg, f = cpu_sample_workload(dims)
     m = Model(cfg, f["kx"], f["ky"], f["kz"], f["poro"], pvt_table=f["pvt"])
     a = cfg["simulation"]["amg"]
     solver = AMGSolver(tol=1e-6, max_cycles=40, theta=a["theta"], max_levels=a["max_levels"],
@@ -91,7 +106,7 @@ def run_cpu_reference(steps: int, warmup: int):
     secs = time.perf_counter() - t0
     cells = m.N
     desc = (f"oracle restatement of the reference IMPES step (stand-alone RS-AMG V-cycles, tol 1e-6 "
-            f"equilibrated, max 40 cycles) on a {CPU_SAMPLE[0]}x{CPU_SAMPLE[1]}x{CPU_SAMPLE[2]} sample "
+            f"equilibrated, max 40 cycles) on a {dims[0]}x{dims[1]}x{dims[2]} sample "
             f"of the workload, {steps} timed steps after {max(warmup, 1)} warm-up (setup excluded); "
             f"numpy/scipy, single-threaded sparse kernels")
     return cells * steps / secs, secs, cells, 1, desc
@@ -485,13 +500,14 @@ def run_ours(args, world, rank, local):
 def run_reference(args, world, rank, local):
     if rank != 0:
         return
-    v, secs, cells, cores, desc = run_cpu_reference(steps=args.steps, warmup=args.warmup)
+    dims = reference_sample_dims(args.steps, args.warmup)
+    v, secs, cells, cores, desc = run_cpu_reference(steps=args.steps, warmup=args.warmup, dims=dims)
     line = {
         "metric": METRIC, "impl": "reference", "value": v, "unit": "cell-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded; no dataset)",
-        "config": {"workload": WORKLOAD, "cells": cells, "sample": list(CPU_SAMPLE),
+        "config": {"workload": WORKLOAD, "cells": cells, "sample": list(dims),
                    "pressure_solver": "stand-alone RS-AMG V-cycles (reference semantics)",
                    "pressure_tol": PRESSURE_TOL, "residual_norm": "||D^-1/2 r|| / ||D^-1/2 b||"},
         "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": cores, "kind": "port", "sample": desc},
