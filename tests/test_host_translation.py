@@ -1,0 +1,84 @@
+"""The host layer's translation of a reference-schema config into the C ABI's
+model and well descriptors, checked field by field against the oracle's own
+parse of the same config, for every recorded fixture.  Runs on the CPU: the
+package's Reservoir and Fluid are built on CPU tensors here by patching the
+device resolver of the module under test (the product path itself refuses
+anything but CUDA)."""
+import json
+
+import pytest
+import torch
+
+from oracle.impes import Model
+
+CASES = ["two_phase_32x32", "two_phase_64x64", "two_phase_16x16x2", "black_oil_10x10x4",
+         "gas_injection_12x12x3", "three_phase_16x16x3", "wells_surface_oil_6x6",
+         "wells_surface_gas_6x6", "wells_rv_liquid_6x6", "wells_surface_water_6x6",
+         "cg_two_phase_20x16x2"]
+
+
+@pytest.fixture
+def sim_module(monkeypatch):
+    from impes_b200 import simulator
+    monkeypatch.setattr(simulator, "_cuda_device", lambda device=None: torch.device("cpu"))
+    return simulator
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_model_descriptor_matches_oracle_parse(golden, sim_module, name):
+    g = golden(name)
+    cfg = json.loads(str(g["cfg"]))
+    res = sim_module.Reservoir(cfg["reservoir"])
+    fl = sim_module.Fluid(cfg["fluid"], res)
+    d = sim_module.model_desc(res, fl, cfg["simulation"])
+    m = Model(cfg, g["kx"], g["ky"], g["kz"], g["poro"])
+    assert (d.nx, d.ny, d.nz) == (m.nx, m.ny, m.nz)
+    assert (d.dx, d.dy, d.dz) == (m.dx, m.dy, m.dz)
+    assert (d.mu_o, d.mu_w, d.mu_g) == (m.mu_oil, m.mu_water, m.mu_gas)
+    assert (d.rho_o_ref, d.rho_w_ref, d.rho_g_ref) == (m.rho_oil_ref, m.rho_water_ref, m.rho_gas_ref)
+    assert (d.c_o, d.c_w, d.c_g, d.c_r) == (m.c_o, m.c_w, m.c_g, m.c_r)
+    assert d.cf == m.cf
+    assert d.relperm_model == (1 if m.relperm_model == "stone2" else 0)
+    assert (d.nw, d.no, d.ng, d.now, d.nog) == tuple(float(v) for v in (m.nw, m.no, m.ng, m.now, m.nog))
+    assert (d.ko_end_w, d.ko_end_g) == (m.ko_end_w, m.ko_end_g)
+    assert (d.sw_cr, d.so_r, d.sg_cr) == (m.sw_cr, m.so_r, m.sg_cr)
+    assert (d.pc_scale, d.pc_exponent) == (float(m.pc_scale), float(m.pc_exponent))
+    assert (d.pc_og_scale, d.pc_og_exponent) == (float(m.pc_og_scale), float(m.pc_og_exponent))
+    sp = m.sim_params
+    assert d.global_rate_scale == float(sp.get("global_rate_scale", 1.0))
+    assert d.max_saturation_change == float(sp.get("max_saturation_change", 0.05))
+    assert d.max_substeps == int(sp.get("max_substeps", 20))
+    assert d.pvt_rows == (0 if m.pvt is None else len(m.pvt.P))
+    # initial state as the oracle sets it
+    assert float(fl.pressure.reshape(-1)[0]) == m.p[0]
+    assert float(fl.s_w.reshape(-1)[0]) == m.sw[0] and float(fl.s_g.reshape(-1)[0]) == m.sg[0]
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_well_descriptors_match_oracle_parse(golden, sim_module, name):
+    g = golden(name)
+    cfg = json.loads(str(g["cfg"]))
+    res = sim_module.Reservoir(cfg["reservoir"])
+    wells = sim_module.WellManager(cfg["wells"], res).get_wells()
+    arr = sim_module.well_descs(wells)
+    m = Model(cfg, g["kx"], g["ky"], g["kz"], g["poro"])
+    assert len(wells) == len(m.wells)
+    for n, (d, w) in enumerate(zip(arr, m.wells)):
+        assert (d.i, d.j, d.k) == (w.i, w.j, w.k)
+        assert d.is_injector == (w.type == "injector")
+        assert d.control_bhp == (w.control_type == "bhp")
+        assert d.value == float(w.control_value)
+        assert d.well_index == w.well_index
+        assert d.injected_phase == (1 if w.injected_phase == "gas" else 0)
+        assert d.surface_rate == (1 if w.rate_type == "surface" else 0)
+        assert d.surface_phase == {"oil": 0, "water": 1, "gas": 2, "liquid": 3}[(w.surface_phase or "liquid").lower()]
+        lims = w.limits or {}
+        for q, (key, bit) in enumerate((("wopr", 1), ("wlpr", 2), ("wgpr", 4), ("liqr", 8))):
+            assert bool(d.limit_mask & bit) == (key in lims)
+            if key in lims:
+                assert d.limits[q] == float(lims[key])
+        assert d.has_bhp_min == (w.bhp_min is not None)
+        if w.bhp_min is not None:
+            assert d.bhp_min == float(w.bhp_min)
+    # the flat cell index the step uses (simulation.py:1629-1630)
+    assert [(w.i * res.ny + w.j) * res.nz + w.k for w in wells] == list(g["well_cells"])
