@@ -45,9 +45,11 @@ def to_csr32(A, device) -> Tuple[torch.Tensor, torch.Tensor, torch.Tensor, Tuple
     (``_to_csr_double``, pressure_amg.py:11-32)."""
     if isinstance(A, tuple) and len(A) == 4:
         return A
-    if hasattr(A, "indptr") and hasattr(A, "tocsr"):
-        A = A.tocsr()
-        A.sort_indices()
+    if not isinstance(A, torch.Tensor) and hasattr(A, "tocsr"):
+        # scipy sparse, any format: a private CSR copy with duplicates summed and
+        # columns sorted (the caller's matrix is left as it was)
+        A = A.tocsr(copy=True)
+        A.sum_duplicates()
         return (torch.as_tensor(A.indptr, dtype=torch.int32, device=device),
                 torch.as_tensor(A.indices, dtype=torch.int32, device=device),
                 torch.as_tensor(A.data, dtype=torch.float64, device=device), tuple(A.shape))

@@ -82,3 +82,50 @@ def test_well_descriptors_match_oracle_parse(golden, sim_module, name):
             assert d.bhp_min == float(w.bhp_min)
     # the flat cell index the step uses (simulation.py:1629-1630)
     assert [(w.i * res.ny + w.j) * res.nz + w.k for w in wells] == list(g["well_cells"])
+
+
+def test_matrix_conversion_follows_the_reference_coalesce_then_cast():
+    """to_csr32 against _to_csr_double's steps (pressure_amg.py:11-32):
+    duplicates of a COO input are summed in the input's dtype by coalesce(), the
+    CSR is cast to float64 afterwards; dense inputs drop their zeros; scipy
+    inputs of any format sum duplicates and sort columns without touching the
+    caller's matrix; a (rowptr, col, val, shape) tuple passes through."""
+    import numpy as np
+    import scipy.sparse as sp
+    from impes_b200.amg import to_csr32
+    cpu = torch.device("cpu")
+    rng = np.random.default_rng(4)
+    n, m = 40, 300
+    r = torch.tensor(rng.integers(0, n, m)); c = torch.tensor(rng.integers(0, n, m))
+    v = torch.tensor(rng.standard_normal(m), dtype=torch.float32)
+    A = torch.sparse_coo_tensor(torch.stack([r, c]), v, (n, n))
+    ref = A.coalesce().to_sparse_csr()
+    rowptr, col, val, shape = to_csr32(A, cpu)
+    assert shape == (n, n) and rowptr.dtype == torch.int32 and col.dtype == torch.int32
+    assert torch.equal(rowptr, ref.crow_indices().int()) and torch.equal(col, ref.col_indices().int())
+    assert val.dtype == torch.float64 and torch.equal(val, ref.values().double())
+    # same matrix given as CSR
+    r2 = to_csr32(ref, cpu)
+    assert all(torch.equal(a, b) for a, b in zip(r2[:3], (rowptr, col, val)))
+    # dense input: explicit zeros are not stored
+    D = torch.zeros(n, n, dtype=torch.float64)
+    D[3, 5], D[7, 7], D[39, 0] = 1.5, -2.0, 0.25
+    rp, cl, vl, _ = to_csr32(D, cpu)
+    assert vl.tolist() == [1.5, -2.0, 0.25] and cl.tolist() == [5, 7, 0]
+    assert rp[-1].item() == 3
+    # scipy COO with duplicates
+    S = sp.coo_matrix((v.double().numpy(), (r.numpy(), c.numpy())), shape=(n, n))
+    rp, cl, vl, _ = to_csr32(S, cpu)
+    T = S.tocsr(); T.sum_duplicates(); T.sort_indices()
+    assert np.array_equal(rp.numpy(), T.indptr) and np.array_equal(cl.numpy(), T.indices)
+    assert np.array_equal(vl.numpy(), T.data)
+    # scipy CSR with unsorted and repeated columns: summed and sorted in a copy
+    U = sp.csr_matrix((np.array([1.0, 2.0, 4.0, 8.0]), np.array([3, 1, 3, 0]), np.array([0, 3, 4])),
+                      shape=(2, 4))
+    before = (U.indices.copy(), U.data.copy())
+    rp, cl, vl, _ = to_csr32(U, cpu)
+    assert rp.tolist() == [0, 2, 3] and cl.tolist() == [1, 3, 0] and vl.tolist() == [2.0, 5.0, 8.0]
+    assert np.array_equal(U.indices, before[0]) and np.array_equal(U.data, before[1])
+    # pass-through
+    tup = (rowptr, col, val, shape)
+    assert to_csr32(tup, cpu) is tup
