@@ -7,7 +7,8 @@ from conftest import REPO
 
 
 def declared_functions():
-    src = open(os.path.join(REPO, "include", "impes_b200.h")).read()
+    with open(os.path.join(REPO, "include", "impes_b200.h")) as f:
+        src = f.read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
     return sorted(set(re.findall(r"^\s*(?:const\s+|unsigned\s+|long\s+)*\w+\s*\*?\s*(impes_\w+)\s*\(",
                                  src, flags=re.M)))
@@ -89,7 +90,8 @@ def test_ctypes_layouts_match_the_c_header(tmp_path):
         seen += 1
     assert seen == sum(1 + len(getattr(_lib, py)._fields_) for py in STRUCTS)
     # and the header declares no field the binding leaves out
-    hdr = open(os.path.join(REPO, "include", "impes_b200.h")).read()
+    with open(os.path.join(REPO, "include", "impes_b200.h")) as f:
+        hdr = f.read()
     hdr = re.sub(r"/\*.*?\*/", "", hdr, flags=re.S)
     for py, c in STRUCTS.items():
         body = re.search(r"typedef struct \{([^}]*)\}\s*" + c + r";", hdr).group(1)

@@ -55,7 +55,7 @@ def _free_port():
 
 def test_gather_over_gloo_world_two():
     cells = [4096, 262144, 16384, 65536, 8192, 131072, 32768]
-    with mp.Manager() as man:
+    with mp.get_context("spawn").Manager() as man:
         out = man.dict()
         mp.spawn(_rank_main, args=(2, _free_port(), cells, out), nprocs=2, join=True)
         res = dict(out)

@@ -34,9 +34,11 @@ def test_summary_and_npz_layout(tmp_path):
     d = results_dir("case", root=str(tmp_path), stamp="20260101_000000")
     assert d == os.path.join(str(tmp_path), "case_20260101_000000") and os.path.isdir(d)
     write_summary(os.path.join(d, "case.txt"), p, sw, sg, so, mb)
-    assert open(os.path.join(d, "case.txt")).read() == _expected(p, sw, sg, so, mb)
+    with open(os.path.join(d, "case.txt")) as f:
+        assert f.read() == _expected(p, sw, sg, so, mb)
     write_summary(os.path.join(d, "full.txt"), p, sw, sg, so, mb, full_arrays=True)
-    txt = open(os.path.join(d, "full.txt")).read()
+    with open(os.path.join(d, "full.txt")) as f:
+        txt = f.read()
     assert txt.startswith(_expected(p, sw, sg, so, mb)) and "Final Oil Saturation:" in txt
     write_npz(os.path.join(d, "case.npz"), p, sw, sg, so)
     z = np.load(os.path.join(d, "case.npz"))
