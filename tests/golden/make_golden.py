@@ -1,6 +1,6 @@
 """Generate the golden fixtures by running the reference itself (build container only).
 
-Usage:  python tests/golden/make_golden.py [REFERENCE_ROOT] [--pcg-only | --three-phase-only | --wells-only]
+Usage:  python tests/golden/make_golden.py [REFERENCE_ROOT] [--pcg-only | --three-phase-only | --wells-only | --amg-3d-only]
 
 REFERENCE_ROOT defaults to /root/reference (researchim-ai/oil-simulator-py).
 The reference is imported unmodified; the harness only
@@ -286,6 +286,7 @@ def main():
     run_trajectory("cg_two_phase_20x16x2", cfg, f, steps=3, dt_days=1.0, solver="cg")
     three_phase_fixture()
     well_fixtures()
+    amg_3d_fixtures()
 
 
 def three_phase_fixture():
@@ -342,6 +343,14 @@ def well_fixtures():
         run_trajectory(name, cfg, f, steps=3, dt_days=1.0)
 
 
+def amg_3d_fixtures():
+    """ClassicalAMG hierarchies of 3-D pressure matrices: black-oil 10x10x4
+    (PVT, gravity, capillarity, anisotropic kz) and the three-phase 16x16x3."""
+    for name, traj, seed, coarsest in (("amg_black_oil_10x10x4", "black_oil_10x10x4", 7, 20),
+                                       ("amg_three_phase_16x16x3", "three_phase_16x16x3", 11, 40)):
+        amg_fixture(name, dict(np.load(os.path.join(HERE, f"{traj}.npz"))), seed=seed, coarsest=coarsest)
+
+
 def main_pcg_only():
     """Regenerate only the Jacobi-PCG fixtures (the others are unchanged)."""
     cfg, f = scenarios.two_phase_2d(seed=0, nx=32, ny=32, nz=1, steps=4)
@@ -364,5 +373,8 @@ if __name__ == "__main__":
         sys.exit(0)
     if "--wells-only" in sys.argv:
         well_fixtures()
+        sys.exit(0)
+    if "--amg-3d-only" in sys.argv:
+        amg_3d_fixtures()
         sys.exit(0)
     main()

@@ -54,11 +54,18 @@ def test_trajectory_matches_reference(golden, name):
     assert np.all(np.abs(bal - ref) <= 1e-10 * np.maximum(np.abs(ref), 1e-30) + 1e-300)
 
 
-def test_amg_hierarchy_matches_reference(golden):
+AMG_CASES = [("amg_two_phase_32x32", "two_phase_32x32"),
+             ("amg_black_oil_10x10x4", "black_oil_10x10x4"),
+             ("amg_three_phase_16x16x3", "three_phase_16x16x3")]
+
+
+@pytest.mark.parametrize("amg_name,traj_name", AMG_CASES)
+def test_amg_hierarchy_matches_reference(golden, amg_name, traj_name):
     """Same tie-break -> identical level sizes and interpolation patterns; values
-    to 1e-8 (the energy-blend least squares is ill-conditioned, ~1e-10 spread)."""
-    g = golden("amg_two_phase_32x32")
-    t = golden("two_phase_32x32")
+    to 1e-8 (the energy-blend least squares is ill-conditioned, ~1e-10 spread).
+    A 2-D two-phase matrix and two 3-D ones (gravity, capillarity, kz = 0.1 kx)."""
+    g = golden(amg_name)
+    t = golden(traj_name)
     n = len(t["A0_crow"]) - 1
     A = sp.csr_matrix((t["A0_val"], t["A0_col"], t["A0_crow"]), shape=(n, n))
     m = oa.AMG(A, theta=0.25, max_levels=10, coarsest_size=int(g["coarsest"]), seed=int(g["seed"]))
