@@ -1,6 +1,6 @@
 """Build libimpes_b200.so for sm_100a with nvcc (in-tree).
 
-Usage: python oil-simulator-py_b200/csrc/build.py [--force] [--debug]
+Usage: python oil-simulator-py_b200/csrc/build.py [--force]
 
 physics.cu is compiled with -fmad=false so the assembly and saturation
 arithmetic rounds operation by operation like the reference's CPU evaluation;
@@ -39,14 +39,12 @@ def _mtime(p):
     return os.path.getmtime(p) if os.path.exists(p) else 0.0
 
 
-def _compile(src, extra, debug):
+def _compile(src, extra):
     obj = os.path.join(BUILD, src.replace(".cu", ".o"))
     deps = [os.path.join(HERE, src)] + [h if os.path.isabs(h) else os.path.join(HERE, h) for h in HEADERS]
     if _mtime(obj) >= max(_mtime(d) for d in deps):
         return obj, None
     cmd = [NVCC, *ARCH, *COMMON, *extra, "-c", os.path.join(HERE, src), "-o", obj]
-    if debug:
-        cmd += ["-DIMPES_DEBUG=1"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         return obj, f"{' '.join(cmd)}\n{r.stdout}\n{r.stderr}"
@@ -55,13 +53,13 @@ def _compile(src, extra, debug):
     return obj, None
 
 
-def build(force: bool = False, debug: bool = False) -> str:
+def build(force: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     if force:
         for f in os.listdir(BUILD):
             os.remove(os.path.join(BUILD, f))
     with cf.ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
-        results = list(ex.map(lambda kv: _compile(kv[0], kv[1], debug), SOURCES.items()))
+        results = list(ex.map(lambda kv: _compile(kv[0], kv[1]), SOURCES.items()))
     errs = [e for _, e in results if e]
     if errs:
         raise RuntimeError("nvcc failed:\n" + "\n".join(errs))
@@ -75,4 +73,4 @@ def build(force: bool = False, debug: bool = False) -> str:
 
 
 if __name__ == "__main__":
-    print(build(force="--force" in sys.argv, debug="--debug" in sys.argv))
+    print(build(force="--force" in sys.argv))
