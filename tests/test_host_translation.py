@@ -129,3 +129,32 @@ def test_matrix_conversion_follows_the_reference_coalesce_then_cast():
     # pass-through
     tup = (rowptr, col, val, shape)
     assert to_csr32(tup, cpu) is tup
+
+
+@pytest.mark.parametrize("source", ["pvt_path", "pvt.path", "pvt.table"])
+def test_pvt_sources_give_the_same_table(sim_module, tmp_path, source):
+    """fluid.py:52-58: a PVT table given by ``pvt_path``, by ``pvt.path`` or
+    inline as ``pvt.table`` packs to the same rows for the C ABI and evaluates
+    like the oracle's table (np.interp with flat ends, pvt.py:48-64)."""
+    import numpy as np
+    from impes_b200 import scenarios
+    from oracle.impes import PVT
+    table = scenarios.pvt_table_black_oil(rv_max=2.0e-4)
+    path = tmp_path / "pvt.json"
+    path.write_text(json.dumps(table))
+    fluid_cfg = {"pressure": 20.0, "s_w": 0.2, "s_g": 0.0}
+    fluid_cfg.update({"pvt_path": {"pvt_path": str(path)}, "pvt.path": {"pvt": {"path": str(path)}},
+                      "pvt.table": {"pvt": {"table": table}}}[source])
+    res = sim_module.Reservoir({"dimensions": [2, 2, 1]})
+    fl = sim_module.Fluid(fluid_cfg, res)
+    packed = fl.pvt.packed()
+    assert packed.shape == (20, 9)
+    ref = PVT(table)
+    cols = ("Bo", "Bw", "Bg", "mu_o", "mu_w", "mu_g", "Rs", "Rv")
+    np.testing.assert_array_equal(packed[:, 0], ref.P)
+    for q, key in enumerate(cols, start=1):
+        np.testing.assert_array_equal(packed[:, q], ref.cols[key])
+    p_mpa = np.array([1.0, 5.0, 12.345, 27.5, 40.0, 60.0])
+    ours = fl.pvt.eval(p_mpa)
+    for key in cols:
+        np.testing.assert_array_equal(ours[key], ref.eval(p_mpa * 1e6, key))
