@@ -158,3 +158,31 @@ def test_pvt_sources_give_the_same_table(sim_module, tmp_path, source):
     ours = fl.pvt.eval(p_mpa)
     for key in cols:
         np.testing.assert_array_equal(ours[key], ref.eval(p_mpa * 1e6, key))
+
+
+def test_alternative_well_and_capillary_schemas(sim_module):
+    """well.py:77-92 accepts wells as coordinates/control or as i, j, k /
+    control_type, control_value; fluid.py:97-105 accepts capillarity as a
+    capillary_pressure section or as top-level keys.  Both forms give the same
+    descriptors."""
+    res = sim_module.Reservoir({"dimensions": [6, 5, 3]})
+    flat = [{"name": "I", "type": "injector", "i": 1, "j": 2, "k": 0, "radius": 0.1,
+             "control_type": "rate", "control_value": 40.0, "injected_phase": "water"},
+            {"name": "P", "type": "producer", "i": 4, "j": 3, "k": 2, "radius": 0.12,
+             "control_type": "bhp", "control_value": 15.0}]
+    nested = [{"name": "I", "type": "injector", "coordinates": [1, 2, 0], "radius": 0.1,
+               "control": {"type": "rate", "value": 40.0}, "injected_phase": "water"},
+              {"name": "P", "type": "producer", "coordinates": [4, 3, 2], "radius": 0.12,
+               "control": {"type": "bhp", "value": 15.0}}]
+    a = sim_module.well_descs(sim_module.WellManager(flat, res).get_wells())
+    b = sim_module.well_descs(sim_module.WellManager(nested, res).get_wells())
+    fields = [name for name, _ in a[0]._fields_ if name != "limits"]
+    for x, y in zip(a, b):
+        assert [getattr(x, f) for f in fields] == [getattr(y, f) for f in fields]
+    with pytest.raises(ValueError):
+        sim_module.WellManager([{"name": "X", "type": "producer", "radius": 0.1,
+                                 "control_type": "bhp", "control_value": 1.0}], res)
+    sect = sim_module.Fluid({"capillary_pressure": {"pc_scale": 3.0e4, "pc_exponent": 0.7}}, res)
+    top = sim_module.Fluid({"pc_scale": 3.0e4, "pc_exponent": 0.7}, res)
+    da, db = sim_module.model_desc(res, sect, {}), sim_module.model_desc(res, top, {})
+    assert (da.pc_scale, da.pc_exponent) == (db.pc_scale, db.pc_exponent) == (3.0e4, 0.7)
