@@ -292,9 +292,14 @@ def main():
 def three_phase_fixture():
     """Three phases without PVT (initial free gas above Sgc, a gas and a water
     injector, two rate producers): the reference's constant-compressibility gas
-    path, which the black-oil fixtures do not reach."""
+    path, which the black-oil fixtures do not reach.  Also its trajectory under
+    the reference's own Jacobi-PCG (pressure_solver "cg")."""
     cfg, f = scenarios.three_phase(seed=6, steps=5)
     run_trajectory("three_phase_16x16x3", cfg, f, steps=5, dt_days=1.0)
+    cfg, f = scenarios.three_phase(seed=6, steps=3)
+    cfg["simulation"]["cg_tolerance"] = 1e-9
+    cfg["simulation"]["cg_max_iter"] = 3000
+    run_trajectory("cg_three_phase_16x16x3", cfg, f, steps=3, dt_days=1.0, solver="cg")
 
 
 def _well_case(nx, ny, wells, s_w, s_g, rv_max=0.0, k_md=150.0, poro=0.22):

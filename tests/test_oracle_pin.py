@@ -156,10 +156,12 @@ def test_oracle_pcg_matches_reference_solver(golden):
         assert np.abs(x - ref).max() <= 1e-9 * np.abs(ref).max()
 
 
-def test_oracle_cg_trajectory_matches_reference(golden):
-    """The reference's default pressure solver end to end (pressure_solver "cg")."""
+@pytest.mark.parametrize("name", ["cg_two_phase_20x16x2", "cg_three_phase_16x16x3"])
+def test_oracle_cg_trajectory_matches_reference(golden, name):
+    """The reference's default pressure solver end to end (pressure_solver "cg"),
+    two-phase and three-phase."""
     from oracle.impes import Model
-    g = golden("cg_two_phase_20x16x2")
+    g = golden(name)
     cfg = json.loads(str(g["cfg"]))
     m = Model(cfg, g["kx"], g["ky"], g["kz"], g["poro"])
     for s in range(g["p"].shape[0]):
@@ -167,3 +169,4 @@ def test_oracle_cg_trajectory_matches_reference(golden):
         assert p is not None
         assert np.abs(m.p - g["p"][s]).max() <= 1e-9 * np.abs(g["p"][s]).max()
         assert np.abs(m.sw - g["sw"][s]).max() <= 1e-9
+        assert np.abs(m.sg - g["sg"][s]).max() <= 1e-9
