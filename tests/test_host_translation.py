@@ -14,7 +14,7 @@ from oracle.impes import Model
 CASES = ["two_phase_32x32", "two_phase_64x64", "two_phase_16x16x2", "black_oil_10x10x4",
          "gas_injection_12x12x3", "three_phase_16x16x3", "wells_surface_oil_6x6",
          "wells_surface_gas_6x6", "wells_rv_liquid_6x6", "wells_surface_water_6x6",
-         "cg_two_phase_20x16x2"]
+         "cg_two_phase_20x16x2", "cg_three_phase_16x16x3"]
 
 
 @pytest.fixture
