@@ -186,3 +186,32 @@ def test_alternative_well_and_capillary_schemas(sim_module):
     top = sim_module.Fluid({"pc_scale": 3.0e4, "pc_exponent": 0.7}, res)
     da, db = sim_module.model_desc(res, sect, {}), sim_module.model_desc(res, top, {})
     assert (da.pc_scale, da.pc_exponent) == (db.pc_scale, db.pc_exponent) == (3.0e4, 0.7)
+
+
+def test_apply_reference_fix_pins_one_dof():
+    """_apply_reference_fix (classical_amg.py:660-686): the anchor's row and
+    column are dropped and its diagonal becomes 1, added when the matrix has no
+    stored diagonal there; every other entry is kept, including explicit
+    zeros."""
+    import numpy as np
+    import scipy.sparse as sp
+    from impes_b200.amg import _apply_reference_fix
+    from test_oracle_pin import laplacian_2d, pin
+    A = laplacian_2d(5)
+    for k in (0, 7, 24):
+        T = torch.sparse_csr_tensor(torch.tensor(A.indptr), torch.tensor(A.indices), torch.tensor(A.data),
+                                    size=A.shape)
+        F = _apply_reference_fix(T, k)
+        got = sp.csr_matrix((F.values().numpy(), F.col_indices().numpy(), F.crow_indices().numpy()), shape=A.shape)
+        assert abs(got - pin(A, k)).max() == 0.0
+    # no stored diagonal at the anchor, and an explicit zero elsewhere
+    r = torch.tensor([[0, 0, 1, 1, 1, 2, 2], [1, 2, 0, 1, 2, 2, 1]])
+    v = torch.tensor([-1.0, 0.0, -1.0, 0.0, -2.0, 3.0, 0.5], dtype=torch.float64)
+    T = torch.sparse_coo_tensor(r, v, (3, 3)).coalesce().to_sparse_csr()
+    Fs = _apply_reference_fix(T, 0)
+    F = Fs.to_dense().numpy()
+    np.testing.assert_array_equal(F, [[1.0, 0.0, 0.0], [0.0, 0.0, -2.0], [0.0, 0.5, 3.0]])
+    assert F.dtype == np.float64
+    # stored pattern: (0,0) added, (1,1) kept as an explicit zero, row/column 0 dropped
+    pattern = list(zip(np.repeat(np.arange(3), np.diff(Fs.crow_indices().numpy())), Fs.col_indices().tolist()))
+    assert pattern == [(0, 0), (1, 1), (1, 2), (2, 1), (2, 2)]
