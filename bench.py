@@ -44,8 +44,12 @@ WORKLOAD = ("gas_injection_1m: 200x200x25 = 1,000,000 cells, ln k ~ N(ln 150 mD,
             "gravity, capillarity, 9 gas injectors at 2e5 sm3/d given as reservoir rate "
             "(x Bg at 25 MPa) with global_rate_scale 0.05 and max_substeps 20 (the reference's "
             "million-cell settings), 16 BHP producers (15 MPa), dt 2 d")
+WORKLOAD_SHORT = ("gas_injection_1m: 200x200x25 cells, correlated log-normal k, 20-row black-oil PVT, "
+                  "Stone II, gravity, Pc, 9 gas injectors (2e5 sm3/d as reservoir rate, rate scale 0.05), "
+                  "16 BHP producers, dt 2 d")
 PRESSURE_TOL = 1e-6
 L2_FLUSH_BYTES = 512 << 20
+DEFAULT_P_MAX = 0               # interpolation row cap of the headline hierarchy
 CPU_SAMPLE = (100, 100, 25)     # spatial sample of the workload for the CPU legs
 
 
@@ -86,13 +90,15 @@ def reference_sample_dims(steps: int, warmup: int, full_steps: int = 8):
     return (nx, ny, CPU_SAMPLE[2])
 
 
-def run_cpu_reference(steps: int, warmup: int, dims=CPU_SAMPLE):
-    """The oracle's restatement of the reference step on the host cores, on a
-    `dims` spatial sample of the workload.
-    Returns (cell-steps/s, seconds timed, cells, threads, description)."""
+def _cpu_reference_worker(args):
+    """One replica of the CPU sample (runs in a spawned process with one thread)."""
+    steps, warmup, dims, seed, barrier = args
+    for _p in (os.path.join(REPO, "oil-simulator-py_b200"), REPO):
+        if _p not in sys.path:
+            sys.path.insert(0, _p)
     from oracle.amg import AMGSolver
     from oracle.impes import Model
-    cfg, f = cpu_sample_workload(dims)
+    cfg, f = cpu_sample_workload(dims, seed=seed)
     m = Model(cfg, f["kx"], f["ky"], f["kz"], f["poro"], pvt_table=f["pvt"])
     a = cfg["simulation"]["amg"]
     solver = AMGSolver(tol=1e-6, max_cycles=40, theta=a["theta"], max_levels=a["max_levels"],
@@ -100,16 +106,59 @@ def run_cpu_reference(steps: int, warmup: int, dims=CPU_SAMPLE):
     dt = 2 * 86400.0
     for _ in range(max(warmup, 1)):       # the first step builds the hierarchy
         m.step(dt, solve=solver)
+    if barrier is not None:
+        barrier.wait()
     t0 = time.perf_counter()
     for _ in range(steps):
         m.step(dt, solve=solver)
-    secs = time.perf_counter() - t0
-    cells = m.N
+    return m.N, time.perf_counter() - t0
+
+
+def cpu_workers() -> int:
+    """Host cores used by the CPU legs: every core this process may run on, up to
+    16 (each replica holds its own AMG hierarchy, ~1 GB for the 100x100x25 sample)."""
+    try:
+        n = len(os.sched_getaffinity(0))
+    except AttributeError:
+        n = os.cpu_count() or 1
+    return max(1, min(16, n))
+
+
+def run_cpu_reference(steps: int, warmup: int, dims=CPU_SAMPLE):
+    """The oracle's restatement of the reference step on the host cores: one
+    replica of a `dims` spatial sample of the workload per core (scipy's sparse
+    kernels are single-threaded, so the cores are used the way the GPU arm uses
+    GPUs: independent replicas), timed from a common start.
+    Returns (cell-steps/s over all replicas, seconds, cells per replica, cores,
+    description)."""
+    import multiprocessing as mp
+    workers = cpu_workers()
+    env_threads = {k: os.environ.get(k) for k in ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS")}
+    for k in env_threads:
+        os.environ[k] = "1"
+    try:
+        if workers == 1:
+            results = [_cpu_reference_worker((steps, warmup, dims, 2, None))]
+        else:
+            ctx = mp.get_context("spawn")
+            with ctx.Manager() as mgr:
+                bar = mgr.Barrier(workers)
+                with ctx.Pool(workers) as pool:
+                    results = pool.map(_cpu_reference_worker,
+                                       [(steps, warmup, dims, 2, bar) for _ in range(workers)])
+    finally:
+        for k, v in env_threads.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+    cells = results[0][0]
+    secs = max(r[1] for r in results)
     desc = (f"oracle restatement of the reference IMPES step (stand-alone RS-AMG V-cycles, tol 1e-6 "
-            f"equilibrated, max 40 cycles) on a {dims[0]}x{dims[1]}x{dims[2]} sample "
-            f"of the workload, {steps} timed steps after {max(warmup, 1)} warm-up (setup excluded); "
-            f"numpy/scipy, single-threaded sparse kernels")
-    return cells * steps / secs, secs, cells, 1, desc
+            f"equilibrated, max 40 cycles) on a {dims[0]}x{dims[1]}x{dims[2]} sample of the "
+            f"workload, {workers} replicas (one per core, one thread each), {steps} timed steps after "
+            f"{max(warmup, 1)} warm-up (setup excluded)")
+    return workers * cells * steps / secs, secs, cells, workers, desc
 
 
 # ------------------------------------------------------------------ GPU legs
@@ -168,15 +217,17 @@ class ClockSampler:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
-def make_sim(cfg, fields, precision, device, restart=30, solver="gmres_amg", warm_start="extrapolate"):
+def make_sim(cfg, fields, precision, device, restart=30, solver="gmres_amg", warm_start="extrapolate",
+             trunc=0):
     """FGMRES + V-cycle (solver="gmres_amg"), or the plain stand-alone V-cycles of
-    the reference (solver="amg"), both stopping at PRESSURE_TOL in the Jacobi norm."""
+    the reference (solver="amg"), both stopping at PRESSURE_TOL in the Jacobi norm;
+    `trunc` caps the interpolation's row length (0: the reference's interpolation)."""
     from impes_b200.simulator import build_from_config
     c = json.loads(json.dumps(cfg))
     c["simulation"]["pressure_solver"] = solver
     c["simulation"]["amg"].update({"tol": PRESSURE_TOL, "norm": "jacobi", "precision": precision,
                                    "restart": restart, "max_iters": 600, "max_cycles": 3000, "seed": 0,
-                                   "warm_start": warm_start})
+                                   "warm_start": warm_start, "p_max_elements": int(trunc)})
     return build_from_config(c, fields, device=device)
 
 
@@ -204,6 +255,7 @@ def time_e2e(sim, fl, steps, dt, flush, stream):
     import torch
     host = [t.detach().cpu().pin_memory() for t in (fl.pressure, fl.s_w, fl.s_g)]
     total = 0.0
+    iters = []
     for _ in range(steps):
         flush.zero_()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -219,8 +271,22 @@ def time_e2e(sim, fl, steps, dt, flush, stream):
         b.record(stream)
         b.synchronize()
         total += a.elapsed_time(b)
+        iters.append(sim.last_krylov["iterations"])
     nbytes = sum(h.numel() * h.element_size() for h in host)
-    return total, nbytes
+    return total, nbytes, iters
+
+
+def total_mass(fl, pv):
+    """Mass in place, sum of PV * S * rho(p) over the phases (kg), as the
+    reference's mass-balance test forms it (tests/test_impes_3phase.py:16-30)."""
+    return float((pv * (fl.s_w * fl.rho_w + fl.s_o * fl.rho_o + fl.s_g * fl.rho_g)).sum())
+
+
+def net_inflow(sim):
+    """Cumulative net mass inflow (kg) of the run, sim.mass_balance (in - out)
+    summed over the phases (simulation.py:1511-1525)."""
+    mb = sim.mass_balance
+    return sum(mb[ph]["in"] - mb[ph]["out"] for ph in ("water", "oil", "gas"))
 
 
 def read_traffic(kernel: str):
@@ -275,21 +341,26 @@ ENSEMBLE_WORKLOAD = ("ensemble: 64 oil-water realisations (seed 4), nx, ny in {3
                      "members sharded across ranks by cell count")
 
 
-def run_ensemble(device, rank, world, dist, steps=30, workers=8, warmup=3):
+def run_ensemble(device, rank, world, dist, steps=30, workers=8, warmup=3, loop_steps=3):
     """All members advanced `steps` steps after `warmup` untimed ones; the time is
     the device span of the library's run (max over ranks).  The warm-up builds
     every member's hierarchy and reaches the paths the first step does not (the
     time-extrapolated iterate and its kernels, further V-cycle graphs): after a
     single warm-up step the first timed run took 4.5-6.0 s, after three 3.9 s,
-    and later runs 3.1-3.4 s."""
+    and later runs 3.1-3.4 s.
+
+    Beside it: the same members looped one at a time through the single-instance
+    path (Simulator.run_step per member per step, as the reference's callers do,
+    simulation.py:126-135, rl_env.py:90-108) for `loop_steps` steps, and the
+    mixed-precision members' final states against an all-fp64 run of the same
+    members and steps."""
     import torch
     from impes_b200 import scenarios
     from impes_b200.ensemble import Ensemble, gather
     cases = scenarios.ensemble(seed=4, members=64, steps=steps)
     dt = cases[0][0]["simulation"]["time_step_days"] * 86400.0
-    ens = Ensemble(cases, device=device, rank=rank, world=world, workers=workers,
-                   amg={"tol": PRESSURE_TOL, "norm": "jacobi", "precision": "mixed", "restart": 60,
-                        "max_iters": 1000})
+    amg = {"tol": PRESSURE_TOL, "norm": "jacobi", "precision": "mixed", "restart": 60, "max_iters": 1000}
+    ens = Ensemble(cases, device=device, rank=rank, world=world, workers=workers, amg=amg)
     ens.run(max(1, warmup), dt)
     if dist is not None:
         dist.barrier()
@@ -299,19 +370,130 @@ def run_ensemble(device, rank, world, dist, steps=30, workers=8, warmup=3):
     if dist is not None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     summ = gather(ens.summary(), world)
+    final = [(s.fluid.pressure.clone(), s.fluid.s_w.clone(), s.fluid.s_g.clone()) for s in ens.sims]
+    # the single-instance loop, on the same members (their trajectories go on)
+    stream = torch.cuda.current_stream(device)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(device)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(loop_steps):
+        for sim in ens.sims:
+            if not sim.run_step(dt):
+                raise RuntimeError("ensemble member failed to converge in the loop baseline")
+    b.record(stream)
+    b.synchronize()
+    tl = torch.tensor([a.elapsed_time(b)], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(tl, op=dist.ReduceOp.MAX)
     ens.close()
+    # all-fp64 run of the same members and steps
+    ens64 = Ensemble(cases, device=device, rank=rank, world=world, workers=workers,
+                     amg=dict(amg, precision="fp64"))
+    ens64.run(max(1, warmup), dt)
+    ens64.run(steps, dt)
+    ds, dp = 0.0, 0.0
+    for (p, sw, sg), s64 in zip(final, ens64.sims):
+        fl = s64.fluid
+        ds = max(ds, float((sw - fl.s_w).abs().max()), float((sg - fl.s_g).abs().max()))
+        dp = max(dp, float((p - fl.pressure).abs().max() / fl.pressure.abs().max()))
+    ens64.close()
+    drift = torch.tensor([ds, dp], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(drift, op=dist.ReduceOp.MAX)
     total = sum(ens.cells)
     ms = float(t.item())
+    loop_cs = total * loop_steps / (float(tl.item()) / 1e3)
+    cs = total * steps / (ms / 1e3)
     return {"workload": ENSEMBLE_WORKLOAD, "members": len(ens.cells), "cells": total, "steps": steps,
-            "ms": ms, "cell_steps_per_s": total * steps / (ms / 1e3), "workers_per_gpu": workers,
+            "ms": ms, "cell_steps_per_s": cs, "workers_per_gpu": workers,
             "warmup_steps": max(1, warmup),
+            "loop_steps": loop_steps, "loop_ms": float(tl.item()), "loop_cell_steps_per_s": loop_cs,
+            "speedup_vs_loop": cs / loop_cs,
+            "drift_s_abs_vs_fp64": float(drift[0]), "drift_p_rel_vs_fp64": float(drift[1]),
             "fgmres_iterations": int(sum(s["iterations"] for s in summ)),
             "all_converged": all(s["status"] == 0 for s in summ), "scaling": "strong"}
 
 
+def sig(x, n=4):
+    """x rounded to n significant digits (floats), for the compact result line."""
+    if x is None or isinstance(x, (bool, int, str)):
+        return x
+    return float(f"{x:.{n}g}")
+
+
+def run_variant(args, cfg, fields, precision, device, dt, flush, stream, dist, rank, local, trunc,
+                label):
+    """Setup + W warm-up steps, K device-timed steps (headline protocol), K steps
+    with the library's phase timers, K steps end to end through run_step with
+    host state.  Returns the measurements of this (precision, interpolation)."""
+    import torch
+    from impes_b200 import _lib
+    _, fl, _, sim = make_sim(cfg, fields, precision, device, restart=args.restart,
+                             warm_start=False if args.warm_start == "zero" else args.warm_start,
+                             trunc=trunc)
+    pv = sim.porous_volume.reshape(fl.s_w.shape)
+    m0 = total_mass(fl, pv)
+    torch.cuda.synchronize()
+    t_setup = time.perf_counter()
+    for _ in range(args.warmup):           # the first warm-up step builds the hierarchy
+        if not sim.run_step(dt):
+            raise RuntimeError("warm-up step failed to converge")
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t_setup
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = _lib.kernel_launches()
+    with ClockSampler(local, args.clocks_dir) as clk:
+        ms, iters = time_steps(sim, args.steps, dt, flush, stream)
+    launches = _lib.kernel_launches() - launches0
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    tmax = torch.tensor([ms], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    # phase timers (CUDA events around every phase and every wide-level sweep,
+    # recorded inside the V-cycle graphs) run on K further steps, kept out of the
+    # headline region because their event records lengthen each V-cycle
+    _lib.timing_enable(True)
+    _lib.timing_collect()
+    ms_inst, iters_inst = time_steps(sim, args.steps, dt, flush, stream)
+    phases = _lib.timing_collect()
+    _lib.timing_enable(False)
+    e2e_ms, e2e_bytes, e2e_iters = time_e2e(sim, fl, args.steps, dt, flush, stream)
+    te = torch.tensor([e2e_ms], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    levels = sim.amg_levels()
+    nnz = [lv[1] for lv in levels]
+    oc = sum(nnz) / max(nnz[0], 1) if nnz else None
+    m1 = total_mass(fl, pv)
+    inflow = net_inflow(sim)
+    if rank == 0:
+        print(f"[bench] {label}: levels (n, nnz, nc, p_nnz, coarsest, columns) = {levels}", file=sys.stderr)
+        print(f"[bench] {label}: phases {phases}", file=sys.stderr)
+    out = dict(ms=float(tmax.item()), iters=iters, phases=phases, clocks=clk.summary(), ms_inst=ms_inst,
+               iters_inst=iters_inst, launches=launches, e2e_ms=float(te.item()), e2e_bytes=e2e_bytes,
+               e2e_iters=e2e_iters, setup_s=setup_s, p=fl.pressure.clone(), sw=fl.s_w.clone(),
+               sg=fl.s_g.clone(), oc=oc, levels=len(levels),
+               mass_err=abs((m1 - m0) - inflow) / max(abs(m0), 1e-300),
+               steps_run=args.warmup + 3 * args.steps,
+               state={"sw": [float(fl.s_w.min()), float(fl.s_w.max())],
+                      "sg": [float(fl.s_g.min()), float(fl.s_g.max())],
+                      "p_MPa": [float(fl.pressure.min()) / 1e6, float(fl.pressure.max()) / 1e6]})
+    sim.close()
+    del sim, fl
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_ours(args, world, rank, local):
     import torch
-    from impes_b200 import _lib, scenarios
+    from impes_b200 import scenarios
 
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
@@ -331,65 +513,28 @@ def run_ours(args, world, rank, local):
     stream = torch.cuda.current_stream(device)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=device)
 
-    results = {}
+    # (precision, interpolation cap) variants; the headline is the mixed path on
+    # the --p-max-elements hierarchy, and the reference's own interpolation (cap 0)
+    # is measured beside it when the headline truncates
+    trunc = args.p_max_elements
+    variants = []
     precisions = ("fp64", "mixed") if args.precision == "both" else (args.precision,)
     for precision in precisions:
-        _, fl, _, sim = make_sim(cfg, fields, precision, device, restart=args.restart,
-                                 warm_start=False if args.warm_start == "zero" else args.warm_start)
-        torch.cuda.synchronize()
-        t_setup = time.perf_counter()
-        for _ in range(args.warmup):           # the first warm-up step builds the hierarchy
-            if not sim.run_step(dt):
-                raise RuntimeError("warm-up step failed to converge")
-        torch.cuda.synchronize()
-        setup_s = time.perf_counter() - t_setup
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
-        launches0 = _lib.kernel_launches()
-        with ClockSampler(local, args.clocks_dir) as clk:
-            ms, iters = time_steps(sim, args.steps, dt, flush, stream)
-        launches = _lib.kernel_launches() - launches0
-        torch.cuda.synchronize()
-        if dist is not None:
-            dist.barrier()
-        tmax = torch.tensor([ms], dtype=torch.float64, device=device)
-        if dist is not None:
-            dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-        ms_max = float(tmax.item())
-        # phase timers (CUDA events around every phase and every wide-level sweep,
-        # recorded inside the V-cycle graphs) run on K further steps, kept out of the
-        # headline region because their event records lengthen each V-cycle
-        _lib.timing_enable(True)
-        _lib.timing_collect()
-        ms_inst, iters_inst = time_steps(sim, args.steps, dt, flush, stream)
-        phases = _lib.timing_collect()
-        _lib.timing_enable(False)
-        e2e_ms, e2e_bytes = time_e2e(sim, fl, args.steps, dt, flush, stream)
-        te = torch.tensor([e2e_ms], dtype=torch.float64, device=device)
-        if dist is not None:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        if rank == 0:
-            print(f"[bench] {precision}: levels (n, nnz, nc, p_nnz, coarsest, columns) = {sim.amg_levels()}",
-                  file=sys.stderr)
-            print(f"[bench] {precision}: phases {phases}", file=sys.stderr)
-        state = {"sw": [float(fl.s_w.min()), float(fl.s_w.max())],
-                 "sg": [float(fl.s_g.min()), float(fl.s_g.max())],
-                 "p_MPa": [float(fl.pressure.min()) / 1e6, float(fl.pressure.max()) / 1e6]}
-        results[precision] = dict(ms=ms_max, iters=iters, phases=phases, clocks=clk.summary(),
-                                  ms_inst=ms_inst, iters_inst=iters_inst, state=state,
-                                  launches=launches, e2e_ms=float(te.item()), e2e_bytes=e2e_bytes,
-                                  setup_s=setup_s, p=fl.pressure.clone(), sw=fl.s_w.clone())
-        sim.close()
-        del sim, fl
-        torch.cuda.synchronize()
-        torch.cuda.empty_cache()
+        variants.append((precision, trunc))
+    if args.precision == "both" and trunc > 0 and not args.no_reference_hierarchy:
+        variants += [("fp64", 0), ("mixed", 0)]
+    results = {}
+    for precision, tr in variants:
+        label = f"{precision}/trunc{tr}"
+        results[(precision, tr)] = run_variant(args, cfg, fields, precision, device, dt, flush, stream, dist,
+                                               rank, local, tr, label)
 
     plain = None
     if args.precision == "both" and not args.no_plain:
-        # the plain FP64 GPU path: the reference's stand-alone V-cycles, fp64, to the
-        # same 1e-6 Jacobi-scaled residual (fewer timed steps: it is slow)
-        _, flp, _, simp = make_sim(cfg, fields, "fp64", device, solver="amg")
+        # the plain FP64 GPU path: the reference's stand-alone V-cycles on the
+        # reference's hierarchy, fp64, to the same 1e-6 Jacobi-scaled residual
+        # (fewer timed steps: it is slow)
+        _, flp, _, simp = make_sim(cfg, fields, "fp64", device, solver="amg", trunc=0)
         for _ in range(args.warmup):
             simp.run_step(dt)
         psteps = max(1, min(args.steps, 3))
@@ -409,35 +554,35 @@ def run_ours(args, world, rank, local):
         adjoint = run_adjoint(device)
     ensemble = None
     if args.precision == "both" and not args.no_ensemble:
-        ensemble = run_ensemble(device, rank, world, dist, warmup=max(3, args.warmup))
+        ensemble = run_ensemble(device, rank, world, dist, warmup=max(3, args.warmup),
+                                loop_steps=args.ensemble_loop_steps)
     if dist is not None:
         dist.destroy_process_group()
     if rank != 0:
         return
     hbm_peak, peak_kind = read_peaks()
+    steps = args.steps
     if args.precision != "both":
-        r = results[args.precision]
-        print(json.dumps({"precision": args.precision, "ms_per_step": r["ms"] / args.steps,
-                          "vcycles_per_step": statistics.mean(r["iters"]),
+        r = results[(args.precision, trunc)]
+        print(json.dumps({"precision": args.precision, "p_max_elements": trunc,
+                          "ms_per_step": r["ms"] / steps, "vcycles_per_step": statistics.mean(r["iters"]),
+                          "operator_complexity": r["oc"], "levels": r["levels"],
                           "phases": r["phases"], "gpu_launches": r["launches"]}), flush=True)
         return
-    mixed, fp64 = results["mixed"], results["fp64"]
-    steps = args.steps
+    mixed, fp64 = results[("mixed", trunc)], results[("fp64", trunc)]
     value = world * cells * steps / (mixed["ms"] / 1e3)
     fp64_value = world * cells * steps / (fp64["ms"] / 1e3)
     # dominant kernel: the l1-Jacobi sweep of the wide coarse levels (k_csr_stream
-    # and k_csr_rows, Y_SMOOTH), timed per launch by the library's CUDA events
+    # and k_csr_rows, Y_SMOOTH) when the hierarchy has such levels, else the
+    # level-0 sweep; timed per launch by the library's CUDA events
     key = "smooth_wide" if mixed["phases"]["smooth_wide"][0] else "smooth_l0"
     n_s, ms_s, by_s = mixed["phases"][key]
-    avg_ms = ms_s / max(n_s, 1)
-    bytes_launch = by_s / max(n_s, 1)
     achieved = by_s / (ms_s / 1e3) / 1e9
     traffic = read_traffic(key)
-    n0, ms0, by0 = mixed["phases"]["smooth_l0"]
     share = {k: round(v[1] / mixed["ms_inst"], 4) for k, v in mixed["phases"].items() if k != "solve"}
-    drift_sw = float((results["mixed"]["sw"] - results["fp64"]["sw"]).abs().max())
-    drift_p = float(((results["mixed"]["p"] - results["fp64"]["p"]).abs().max()
-                     / results["fp64"]["p"].abs().max()))
+    drift_sw = float(max((mixed["sw"] - fp64["sw"]).abs().max(), (mixed["sg"] - fp64["sg"]).abs().max()))
+    drift_p = float((mixed["p"] - fp64["p"]).abs().max() / fp64["p"].abs().max())
+    vps = statistics.mean(mixed["iters"])
     line = {
         "metric": METRIC,
         "value": value,
@@ -451,49 +596,66 @@ def run_ours(args, world, rank, local):
         "vs_baseline": None,
         "dtype": "f64 Krylov/assembly/saturation + f32 V-cycle",
         "data": "synthetic (seeded; no dataset)",
-        "config": {"workload": WORKLOAD, "cells": cells, "precision": "mixed",
-                   "pressure_solver": f"FGMRES({args.restart}) + RS-AMG V-cycle", "pressure_tol": PRESSURE_TOL,
-                   "residual_norm": "||D^-1 r|| / ||D^-1 b|| (Jacobi-scaled)",
-                   "l2": "flushed before every timed step (512 MiB write)",
+        "config": {"workload": WORKLOAD_SHORT, "cells": cells, "precision": "mixed",
+                   "solver": f"FGMRES({args.restart}) + RS-AMG V-cycle, P capped at {trunc}/row"
+                             if trunc else f"FGMRES({args.restart}) + RS-AMG V-cycle",
+                   "tol": PRESSURE_TOL, "norm": "Jacobi-scaled", "l2": "flushed before each step",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
-        "vcycles_per_step": statistics.mean(mixed["iters"]),
-        "fp64": {"value": fp64_value, "ms_per_step": fp64["ms"] / steps,
-                 "vcycles_per_step": statistics.mean(fp64["iters"]),
-                 "mixed_speedup": fp64["ms"] / mixed["ms"]},
-        "plain_fp64_vcycle": None if plain is None else {
-            "value": world * cells * plain["steps"] / (plain["ms"] / 1e3),
-            "ms_per_step": plain["ms"] / plain["steps"], "steps_timed": plain["steps"],
-            "vcycles_per_step": statistics.mean(plain["iters"]),
-            "mixed_speedup": (plain["ms"] / plain["steps"]) / (mixed["ms"] / steps)},
-        "adjoint": adjoint,
-        "ensemble": ensemble,
-        "mixed_vs_fp64_drift": {"sw_abs_max": drift_sw, "p_rel_max": drift_p},
-        "setup_s": {"mixed": mixed["setup_s"], "fp64": fp64["setup_s"]},
-        "phase_share": share,
-        "instrumented": {"note": "phase shares and roofline come from K further steps with the "
-                                 "library's per-phase CUDA events on; the headline region runs without them",
-                         "ms_per_step": mixed["ms_inst"] / steps,
-                         "vcycles_per_step": statistics.mean(mixed["iters_inst"])},
-        "state_after": {"mixed": mixed["state"], "fp64": fp64["state"]},
-        "e2e": {"value": world * cells * steps / (mixed["e2e_ms"] / 1e3), "unit": "cell-steps/s",
-                "h2d_bytes_per_step": mixed["e2e_bytes"], "d2h_bytes_per_step": mixed["e2e_bytes"]},
-        "roofline": {"kernel": ("k_csr_stream<u16|int,Y_SMOOTH> (rows > 512 on levels >= 48 MB) and "
-                                "k_csr_rows<float,u16|int,Y_SMOOTH,1|2|4 warps/row> (l1-Jacobi sweep, "
-                                "levels with > 96 nnz/row)"
-                                if key == "smooth_wide" else "k_csr<float,1,Y_SMOOTH> (level-0 sweep)"),
-                     "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "peak_kind": peak_kind,
-                     "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": traffic,
-                     "bytes_per_launch": bytes_launch, "avg_launch_us": avg_ms * 1e3,
-                     "launches_timed": n_s,
-                     "level0_sweep": {"achieved": by0 / max(ms0, 1e-9) * 1e3 / 1e9,
-                                      "avg_launch_us": ms0 / max(n0, 1) * 1e3, "launches_timed": n0}},
+        "roofline": {"kernel": "wide-level l1-Jacobi sweep" if key == "smooth_wide" else "level-0 l1-Jacobi sweep",
+                     "bound": "hbm", "achieved": sig(achieved), "peak": hbm_peak, "peak_kind": peak_kind,
+                     "unit": "GB/s", "frac": sig(achieved / hbm_peak, 3), "traffic": traffic},
+        "e2e": {"value": sig(world * cells * steps / (mixed["e2e_ms"] / 1e3)), "unit": "cell-steps/s",
+                "h2d_bytes_per_step": mixed["e2e_bytes"], "d2h_bytes_per_step": mixed["e2e_bytes"],
+                "vcycles_per_step": sig(statistics.mean(mixed["e2e_iters"]), 3)},
         "clocks": mixed["clocks"],
         "gpu_launches": mixed["launches"],
+        "vcycles_per_step": sig(vps, 3),
+        "operator_complexity": sig(mixed["oc"], 3),
+        "fp64": {"value": sig(fp64_value), "ms_per_step": sig(fp64["ms"] / steps),
+                 "vcycles_per_step": sig(statistics.mean(fp64["iters"]), 3),
+                 "mixed_speedup": sig(fp64["ms"] / mixed["ms"], 3)},
+        "drift_vs_fp64": {"s_abs": sig(drift_sw, 2), "p_rel": sig(drift_p, 2)},
+        "mass_balance_error": sig(mixed["mass_err"], 2),
     }
+    if ("mixed", 0) in results and trunc:
+        rm, rf = results[("mixed", 0)], results[("fp64", 0)]
+        line["ref_interp"] = {"ms_mixed": sig(rm["ms"] / steps), "ms_fp64": sig(rf["ms"] / steps),
+                              "vcycles_per_step": sig(statistics.mean(rm["iters"]), 3),
+                              "operator_complexity": sig(rm["oc"], 3),
+                              "mixed_speedup": sig(rf["ms"] / rm["ms"], 3)}
+    if plain is not None:
+        line["plain_fp64_vcycle"] = {"ms_per_step": sig(plain["ms"] / plain["steps"]),
+                                     "vcycles_per_step": sig(statistics.mean(plain["iters"]), 3),
+                                     "mixed_speedup": sig((plain["ms"] / plain["steps"]) / (mixed["ms"] / steps), 3)}
+    if adjoint is not None:
+        line["adjoint"] = {"forward_ms": sig(adjoint["forward_ms"]), "reverse_ms": sig(adjoint["reverse_ms"]),
+                           "gradient_over_forward": sig(adjoint["gradient_over_forward"], 3)}
+    if ensemble is not None:
+        line["ensemble"] = {k: sig(ensemble[k]) for k in ("cell_steps_per_s", "loop_cell_steps_per_s",
+                                                          "speedup_vs_loop", "drift_s_abs_vs_fp64")
+                            if k in ensemble}
     if not args.no_cpu_baseline and world == 1:
         v, secs, ccells, cores, desc = run_cpu_reference(steps=1, warmup=1)
-        line["cpu_baseline"] = {"value": v, "unit": "cell-steps/s", "cores": cores, "kind": "port",
-                                "sample": desc, "seconds": secs}
+        line["cpu_baseline"] = {"value": sig(v), "unit": "cell-steps/s", "cores": cores, "kind": "port",
+                                "sample": f"oracle port, {CPU_SAMPLE[0]}x{CPU_SAMPLE[1]}x{CPU_SAMPLE[2]} x {cores} replicas"}
+        cpu_detail = {"value": v, "seconds": secs, "cells_per_replica": ccells, "description": desc}
+    else:
+        cpu_detail = None
+    detail = {
+        "workload": WORKLOAD,
+        "results": {f"{p}/trunc{t}": {k: v for k, v in r.items() if k not in ("p", "sw", "sg")}
+                    for (p, t), r in results.items()},
+        "phase_share_mixed": share,
+        "roofline": {"bytes_per_launch": by_s / max(n_s, 1), "avg_launch_us": ms_s / max(n_s, 1) * 1e3,
+                     "launches_timed": n_s,
+                     "level0_sweep": {"GBs": mixed["phases"]["smooth_l0"][2] / max(mixed["phases"]["smooth_l0"][1], 1e-9) / 1e6,
+                                      "launches": mixed["phases"]["smooth_l0"][0]}},
+        "plain_fp64_vcycle": plain, "adjoint": adjoint, "ensemble": ensemble, "cpu_baseline": cpu_detail,
+    }
+    print("[bench-detail] " + json.dumps(detail), file=sys.stderr, flush=True)
+    if args.detail_out:
+        with open(args.detail_out, "w") as f:
+            json.dump(detail, f, indent=1)
     print(json.dumps(line), flush=True)
 
 
@@ -535,6 +697,14 @@ def main():
                     help="NXxNYxNZ: a smaller grid of the same workload (profiling captures only)")
     ap.add_argument("--precision", choices=["both", "mixed", "fp64"], default="both",
                     help="both (the benchmark line) or one path only (profiling runs)")
+    ap.add_argument("--p-max-elements", type=int, default=DEFAULT_P_MAX,
+                    help="interpolation row cap of the benchmarked hierarchy (0: the reference's "
+                         "interpolation)")
+    ap.add_argument("--no-reference-hierarchy", action="store_true",
+                    help="skip the measurement on the reference's own interpolation")
+    ap.add_argument("--ensemble-loop-steps", type=int, default=3,
+                    help="steps of the loop-the-single-path ensemble baseline")
+    ap.add_argument("--detail-out", default=None, help="write the detailed results as JSON here")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

@@ -61,7 +61,21 @@ typedef struct {
   double equilibration_threshold; /* 1e-6                                        */
   uint32_t tiebreak_seed;         /* C/F tie-break stream (replaces torch.rand)  */
   int mixed_precision;            /* 1: also keep an fp32 copy for the V-cycle   */
+  /* Interpolation truncation (no counterpart in the reference; 0 / 0.0 keep the
+   * reference's interpolation): after the energy blend each F row of P keeps at
+   * most p_max_elements entries (0 = no cap), drops entries below
+   * p_trunc_factor times the row's largest, and is rescaled to its old row sum. */
+  int p_max_elements;
+  double p_trunc_factor;
+  /* Smoother of the V-cycle: IMPES_SMOOTHER_L1_JACOBI (the reference's, 0.7 *
+   * l1-Jacobi) or IMPES_SMOOTHER_CHEBYSHEV (no counterpart in the reference):
+   * the Chebyshev iteration for diag(l1 weights) A on [cheb_lower * lmax, lmax],
+   * lmax its Gershgorin bound, one step per sweep the V-cycle would make. */
+  int smoother;
+  double cheb_lower;              /* 0.3 when <= 0                               */
 } impes_amg_params;
+
+enum { IMPES_SMOOTHER_L1_JACOBI = 0, IMPES_SMOOTHER_CHEBYSHEV = 1 };
 
 typedef struct {
   int n;
@@ -129,8 +143,9 @@ int impes_amg_solve_vcycles(impes_amg* h, const double* b, double* x, double tol
  * Every call on a device shares it: calls that overlap on the GPU (several
  * streams or threads) race, so serialise them.  Nothing in the array needs to
  * start at zero (each call writes before it reads).  The first call on each
- * device looks up the array's device address; make that first call before any
- * stream capture.  Results equal impes_amg_solve_vcycles'. */
+ * device (and the first after that device's context was re-created, e.g. by
+ * cudaDeviceReset) looks up the array's device address; make that first call
+ * before any stream capture.  Results equal impes_amg_solve_vcycles'. */
 int impes_amg_solve_vcycles_noalloc(impes_amg* h, const double* b, double* x, double tol,
                                     int max_cycles, int* cycles, double* rel_res, int norm,
                                     void* stream);

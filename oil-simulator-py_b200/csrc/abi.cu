@@ -80,8 +80,14 @@ int impes_amg_create(impes_amg** out, const impes_amg_params* p) {
     IMPES_REQUIRE(p->max_levels >= 1 && p->coarsest_size >= 1, IMPES_ERR_ARG, "bad level limits");
     IMPES_REQUIRE(p->nullspace_dim >= 0 && p->nullspace_dim <= 3, IMPES_ERR_ARG,
                   "nullspace_dim must be 0..3");
+    IMPES_REQUIRE(p->p_max_elements >= 0 && p->p_trunc_factor >= 0.0 && p->p_trunc_factor < 1.0,
+                  IMPES_ERR_ARG, "p_max_elements must be >= 0 and p_trunc_factor in [0, 1)");
+    IMPES_REQUIRE(p->smoother == IMPES_SMOOTHER_L1_JACOBI || p->smoother == IMPES_SMOOTHER_CHEBYSHEV,
+                  IMPES_ERR_ARG, "unknown smoother");
+    IMPES_REQUIRE(p->cheb_lower < 1.0, IMPES_ERR_ARG, "cheb_lower must be below 1");
     auto* h = new impes_amg();
     h->a.prm = *p;
+    if (!(h->a.prm.cheb_lower > 0.0)) h->a.prm.cheb_lower = 0.3;
     h->a.prm.nullspace_blend = std::max(0.0, std::min(1.0, p->nullspace_blend));
     h->a.prm.nullspace_reg = std::max(1e-10, p->nullspace_reg);
     *out = h;

@@ -14,6 +14,9 @@ struct Level {
   DBuf<float> valf;
   DBuf<double> inv_relax;
   DBuf<float> inv_relaxf;
+  // Chebyshev smoother: Gershgorin bound of diag(inv) A as double bits, [0] from
+  // the fp64 values, [1] from the fp32 chain (atomicMax of non-negative doubles)
+  DBuf<unsigned long long> cheb_lmax;
   int avg_row = 7;                 // nnz / n, selects the SpMV row mapping
   bool coarsest = false;
   // interpolation P (n x nc) and restriction R = P^T (nc x n)
@@ -45,8 +48,8 @@ struct Level {
   DBuf<unsigned short> ap_e16;
   DBuf<int> ap_ebase;
   // cycle vectors (fp64 and fp32)
-  DBuf<double> x, b, r, t;
-  DBuf<float> xf, bf, rf, tf;
+  DBuf<double> x, b, r, t, u;       // u: second direction buffer of the Chebyshev smoother
+  DBuf<float> xf, bf, rf, tf, uf;
   // coarsest level (n <= 500): inverse of the dense matrix with DOF 0 pinned
   // (the reference's coarse solve), row-major, and lu_free, the inverse of the
   // unpinned matrix used inside FGMRES unless it was singular (device flag)

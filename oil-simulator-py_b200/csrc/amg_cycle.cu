@@ -268,6 +268,114 @@ void launch_csr(int n, int avg, const int* rowptr, const int* col, const T* val,
   IMPES_CHECK_LAUNCH();
 }
 
+// ------------------------------------------------------ Chebyshev smoother
+// The Chebyshev iteration for diag(inv) A on [lower * lmax, lmax] (Saad,
+// Iterative Methods for Sparse Linear Systems, 2nd ed., Alg. 12.1), an option of
+// this library (the reference smooths with l1-Jacobi): r = inv (b - A x),
+// d_0 = r / theta, then per step x += d_k, r -= inv A d_k,
+// d_{k+1} = rho_{k+1} rho_k d_k + (2 rho_{k+1} / delta) r, with
+// rho_0 = delta / theta and rho_{k+1} = 1 / (2 theta / delta - rho_k).  The last
+// product's step also adds d_{k+1} to x, so nu updates of x take nu - 1 products
+// after the initial residual.  lmax is the level's Gershgorin bound, read from
+// device memory (the bits of a double), so a captured graph follows updates.
+struct ChebArgs {
+  const unsigned long long* lmax;
+  double lower;
+  int k;        // index of the direction this step multiplies
+  int last;     // last product: x also takes the next direction
+  int zero_x;   // x starts at zero (not read)
+};
+__device__ __forceinline__ void cheb_coeffs(const ChebArgs& ca, double& theta, double& c1, double& c2) {
+  const double lm = __longlong_as_double((long long)*ca.lmax);
+  const double lo = __dmul_rn(ca.lower, lm);
+  theta = __dmul_rn(0.5, __dadd_rn(lm, lo));
+  const double delta = __dmul_rn(0.5, __dsub_rn(lm, lo));
+  const double sigma = __ddiv_rn(theta, delta);
+  double rho = __ddiv_rn(1.0, sigma);
+  for (int q = 0; q < ca.k; ++q) rho = __ddiv_rn(1.0, __dsub_rn(__dmul_rn(2.0, sigma), rho));
+  const double rn = __ddiv_rn(1.0, __dsub_rn(__dmul_rn(2.0, sigma), rho));
+  c1 = __dmul_rn(rn, rho);
+  c2 = __ddiv_rn(__dmul_rn(2.0, rn), delta);
+}
+enum ChebMode { CH_INIT = 0, CH_STEP = 1 };
+// LPR lanes per row (1..32).  CH_INIT gathers v = x: r = inv (b - A x),
+// dnext = r / theta.  CH_STEP gathers v = d_k: r -= inv A d_k, x += d_k
+// (+ d_{k+1} on the last step), dnext = d_{k+1}.  CT and rel as in k_csr.
+template <typename T, typename CT, int LPR, int MODE>
+__global__ void __launch_bounds__(TB) k_cheb(int n, const int* __restrict__ rowptr,
+                                             const CT* __restrict__ col, const T* __restrict__ val,
+                                             const T* __restrict__ v, const T* __restrict__ b,
+                                             const T* __restrict__ inv, T* __restrict__ r,
+                                             T* __restrict__ x, T* __restrict__ dnext, int rel,
+                                             ChebArgs ca) {
+  double theta, c1, c2;
+  cheb_coeffs(ca, theta, c1, c2);
+  const int g = threadIdx.x / LPR, lane = threadIdx.x % LPR;
+  const int rows_per_block = TB / LPR;
+  for (long long row = (long long)blockIdx.x * rows_per_block + g; row < n;
+       row += (long long)gridDim.x * rows_per_block) {
+    T acc = T(0);
+    const int a = rowptr[row], e = rowptr[row + 1];
+    const int cb = col_base<CT>(row, rel);
+    for (int k = a + lane; k < e; k += LPR) acc += val[k] * v[cb + (int)col[k]];
+#pragma unroll
+    for (int o = LPR / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, LPR);
+    if (lane == 0) {
+      if (MODE == CH_INIT) {
+        const T ri = inv[row] * (b[row] - acc);
+        r[row] = ri;
+        dnext[row] = ri / T(theta);
+      } else {
+        const T ri = r[row] - inv[row] * acc;
+        const T di = v[row];
+        const T dn = T(c1) * di + T(c2) * ri;
+        T xi = ca.zero_x ? T(0) : x[row];
+        xi = xi + di;
+        if (ca.last) xi = xi + dn;
+        x[row] = xi;
+        r[row] = ri;
+        if (!ca.last) dnext[row] = dn;
+      }
+    }
+  }
+}
+// x = 0: r = inv b, d_0 = r / theta (no product); with nu == 1, x = d_0 too
+template <typename T>
+__global__ void k_cheb_init0(int n, const T* __restrict__ b, const T* __restrict__ inv, T* __restrict__ r,
+                             T* __restrict__ d, T* __restrict__ x, ChebArgs ca) {
+  double theta, c1, c2;
+  cheb_coeffs(ca, theta, c1, c2);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const T ri = inv[i] * b[i];
+    r[i] = ri;
+    d[i] = ri / T(theta);
+    if (x) x[i] = d[i];
+  }
+}
+template <typename T>
+__global__ void k_cheb_add(int n, const T* __restrict__ d, T* __restrict__ x) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    x[i] = x[i] + d[i];
+}
+
+template <typename T, typename CT, int MODE>
+void launch_cheb_ct(int n, int avg, const int* rowptr, const CT* col, const T* val, const T* v, const T* b,
+                    const T* inv, T* r, T* x, T* dnext, int rel, const ChebArgs& ca, cudaStream_t s) {
+  const int lpr = avg <= 8 ? 1 : avg <= 16 ? 4 : avg <= 48 ? 8 : avg <= 96 ? 16 : 32;
+  auto grid = [&](int l) { return grid_for(((size_t)n * l + TB - 1) / TB * TB, TB, 16); };
+  switch (lpr) {
+    case 1: k_cheb<T, CT, 1, MODE><<<grid(1), TB, 0, s>>>(n, rowptr, col, val, v, b, inv, r, x, dnext, rel, ca); break;
+    case 4: k_cheb<T, CT, 4, MODE><<<grid(4), TB, 0, s>>>(n, rowptr, col, val, v, b, inv, r, x, dnext, rel, ca); break;
+    case 8: k_cheb<T, CT, 8, MODE><<<grid(8), TB, 0, s>>>(n, rowptr, col, val, v, b, inv, r, x, dnext, rel, ca); break;
+    case 16: k_cheb<T, CT, 16, MODE><<<grid(16), TB, 0, s>>>(n, rowptr, col, val, v, b, inv, r, x, dnext, rel, ca); break;
+    default: k_cheb<T, CT, 32, MODE><<<grid(32), TB, 0, s>>>(n, rowptr, col, val, v, b, inv, r, x, dnext, rel, ca); break;
+  }
+  ::impes::count_launch();
+  IMPES_CHECK_LAUNCH();
+}
+
 #define GRID_LOOP(i, n) \
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (n); i += (long long)gridDim.x * blockDim.x)
 
@@ -536,6 +644,8 @@ namespace {
 
 template <typename T> struct LV;
 template <> struct LV<double> {
+  static constexpr int slot = 0;
+  static double* u(Level& L) { return L.u.p; }
   static const double* val(const Level& L) { return L.val.p; }
   static const double* inv(const Level& L) { return L.inv_relax.p; }
   static const double* pval(const Level& L) { return L.pval.p; }
@@ -546,6 +656,8 @@ template <> struct LV<double> {
   static double* t(Level& L) { return L.t.p; }
 };
 template <> struct LV<float> {
+  static constexpr int slot = 1;
+  static float* u(Level& L) { return L.uf.p; }
   static const float* val(const Level& L) { return L.valf.p; }
   static const float* inv(const Level& L) { return L.inv_relaxf.p; }
   static const float* pval(const Level& L) { return L.pvalf.p; }
@@ -565,10 +677,66 @@ inline double sweep_bytes(double s, double nnz, double n, double si = 4.0) {
   return (s + si) * nnz + 4.0 * n + 4.0 * s * n;
 }
 
-// nu l1-Jacobi sweeps (classical_amg.py:1016-1035); returns the buffer holding x.
-// Level-0 sweeps with a non-zero iterate are timed as IMPES_PH_SMOOTH_L0.
+// Algorithmic bytes of one Chebyshev step: values, columns, row pointers, the
+// gathered direction, r and x read and written, inv, the next direction.
+inline double cheb_bytes(double s, double nnz, double n, double si) {
+  return (s + si) * nnz + 4.0 * n + 7.0 * s * n;
+}
+
+// nu Chebyshev updates of x (see ChebArgs); x stays in its buffer (LV<T>::x),
+// r, t and u hold the scaled residual and the two directions.
 template <typename T>
-T* smooth(Level& L, T* x, T* spare, const T* b, int nu, bool zero_x, cudaStream_t s, bool top = false) {
+T* smooth_cheb(const AMG& h, Level& L, T* x, const T* b, int nu, bool zero_x, cudaStream_t s, bool top) {
+  T* r = LV<T>::r(L);
+  T* dc = LV<T>::t(L);
+  T* dn = LV<T>::u(L);
+  ChebArgs ca{L.cheb_lmax.p + LV<T>::slot, h.prm.cheb_lower, 0, 0, 0};
+  const double si = L.col16.p ? 2.0 : 4.0;
+  const bool wide = L.avg_row > 96;
+  if (zero_x) {
+    k_cheb_init0<T><<<grid_for(L.n, TB), TB, 0, s>>>(L.n, b, LV<T>::inv(L), r, dc, nu == 1 ? x : nullptr, ca);
+    ::impes::count_launch();
+    IMPES_CHECK_LAUNCH();
+  } else {
+    const int tid = top ? timers().begin(IMPES_PH_SMOOTH_L0, s) : (wide ? timers().begin(IMPES_PH_SMOOTH_WIDE, s) : -1);
+    if (L.col16.p)
+      launch_cheb_ct<T, unsigned short, CH_INIT>(L.n, L.avg_row, L.rowptr.p, L.col16.p, LV<T>::val(L), x, b,
+                                                 LV<T>::inv(L), r, x, dc, L.col16_rel, ca, s);
+    else
+      launch_cheb_ct<T, int, CH_INIT>(L.n, L.avg_row, L.rowptr.p, L.col.p, LV<T>::val(L), x, b, LV<T>::inv(L),
+                                      r, x, dc, 0, ca, s);
+    timers().end(tid, s, sweep_bytes(sizeof(T), L.nnz, L.n, si));
+    if (nu == 1) {
+      k_cheb_add<T><<<grid_for(L.n, TB), TB, 0, s>>>(L.n, dc, x); ::impes::count_launch();
+      IMPES_CHECK_LAUNCH();
+    }
+  }
+  for (int k = 0; k + 1 < nu; ++k) {
+    ca.k = k;
+    ca.last = (k + 2 == nu);
+    ca.zero_x = (zero_x && k == 0);
+    const int tid = top ? timers().begin(IMPES_PH_SMOOTH_L0, s) : (wide ? timers().begin(IMPES_PH_SMOOTH_WIDE, s) : -1);
+    if (L.col16.p)
+      launch_cheb_ct<T, unsigned short, CH_STEP>(L.n, L.avg_row, L.rowptr.p, L.col16.p, LV<T>::val(L), dc,
+                                                 nullptr, LV<T>::inv(L), r, x, dn, L.col16_rel, ca, s);
+    else
+      launch_cheb_ct<T, int, CH_STEP>(L.n, L.avg_row, L.rowptr.p, L.col.p, LV<T>::val(L), dc, nullptr,
+                                      LV<T>::inv(L), r, x, dn, 0, ca, s);
+    timers().end(tid, s, cheb_bytes(sizeof(T), L.nnz, L.n, si));
+    std::swap(dc, dn);
+  }
+  return x;
+}
+
+// nu l1-Jacobi sweeps (classical_amg.py:1016-1035), or nu Chebyshev updates
+// when the hierarchy selects that smoother (jacobi_only: the coarsest level's
+// 50 sweeps stay l1-Jacobi); returns the buffer holding x.  Level-0 sweeps with
+// a non-zero iterate are timed as IMPES_PH_SMOOTH_L0.
+template <typename T>
+T* smooth(const AMG& h, Level& L, T* x, T* spare, const T* b, int nu, bool zero_x, cudaStream_t s,
+          bool top = false, bool jacobi_only = false) {
+  if (!jacobi_only && h.prm.smoother == IMPES_SMOOTHER_CHEBYSHEV && L.cheb_lmax.p && x == LV<T>::x(L))
+    return smooth_cheb<T>(h, L, x, b, nu, zero_x, s, top);
   for (int it = 0; it < nu; ++it) {
     if (zero_x && it == 0) {
       launch_csr<T, Y_SMOOTH0>(L.n, L.avg_row, L.rowptr.p, L.col.p, LV<T>::val(L), nullptr, b,
@@ -623,10 +791,10 @@ T* vcycle(AMG& h, int l, bool zero_x, cudaStream_t s) {
     // n > 500: 50 l1-Jacobi sweeps from zero on the pinned right-hand side
     T* bp = LV<T>::r(L);
     k_pin_copy<T><<<grid_for(L.n, TB), TB, 0, s>>>(L.n, LV<T>::b(L), bp); ::impes::count_launch();
-    return smooth<T>(L, LV<T>::x(L), LV<T>::t(L), bp, 50, true, s);
+    return smooth<T>(h, L, LV<T>::x(L), LV<T>::t(L), bp, 50, true, s, false, true);
   }
   const int tid = (l == 0) ? timers().begin(IMPES_PH_VCYCLE, s) : -1;
-  T* x = smooth<T>(L, LV<T>::x(L), LV<T>::t(L), LV<T>::b(L), 3, zero_x, s, l == 0);
+  T* x = smooth<T>(h, L, LV<T>::x(L), LV<T>::t(L), LV<T>::b(L), 3, zero_x, s, l == 0);
   T* spare = (x == LV<T>::x(L)) ? LV<T>::t(L) : LV<T>::x(L);
   Level& Nc = *h.levels[l + 1];
   launch_csr<T, Y_B_MINUS_AX>(L.n, L.avg_row, L.rowptr.p, L.col.p, LV<T>::val(L), x, LV<T>::b(L),
@@ -635,7 +803,7 @@ T* vcycle(AMG& h, int l, bool zero_x, cudaStream_t s) {
                       nullptr, LV<T>::b(Nc), s);
   T* ec = vcycle<T>(h, l + 1, true, s);
   launch_csr<T, Y_ADD_AX>(L.n, L.p_avg, L.prow.p, L.pcol.p, LV<T>::pval(L), ec, nullptr, nullptr, x, s);
-  T* out = smooth<T>(L, x, spare, LV<T>::b(L), 2, false, s, l == 0);
+  T* out = smooth<T>(h, L, x, spare, LV<T>::b(L), 2, false, s, l == 0);
   timers().end(tid, s, vcycle_bytes<T>(h, l));
   return out;
 }
@@ -966,21 +1134,48 @@ namespace impes {
 namespace {
 std::mutex g_scratch_mu;
 double* g_scratch_dev[128] = {};
+void* g_scratch_ctx[128] = {};
 
-// Device address of g_solve_scratch on the current device, looked up once per
-// device with that device current (the host-side symbol is not a device address).
+// The driver context current on this thread (CUcontext as void*), through the
+// runtime's driver entry point so the library needs no link to libcuda; null
+// when the entry point is unavailable.
+void* current_context() {
+  using CtxGetCurrent = int (*)(void**);
+  static CtxGetCurrent fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<CtxGetCurrent>(f);
+  }();
+  void* ctx = nullptr;
+  if (fn && fn(&ctx) != 0) ctx = nullptr;
+  return ctx;
+}
+
+// Device address of g_solve_scratch on the current device, looked up with that
+// device current (the host-side symbol is not a device address) on the first
+// call per device, and again only if the device's context has changed since
+// (after cudaDeviceReset the module is loaded anew and the array may move).
 double* solve_scratch() {
   int dev = 0;
   IMPES_CUDA(cudaGetDevice(&dev));
   IMPES_REQUIRE(dev >= 0 && dev < 128, IMPES_ERR_ARG, "device ordinal out of range");
+  void* ctx = current_context();
+  if (!ctx) {                      // no context current on this thread yet
+    IMPES_CUDA(cudaSetDevice(dev));
+    ctx = current_context();
+  }
   std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (!g_scratch_dev[dev]) {
+  if (!g_scratch_dev[dev] || g_scratch_ctx[dev] != ctx) {
     void* ptr = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&ptr, g_solve_scratch);
     if (e != cudaSuccess || !ptr)
       throw Error(IMPES_ERR_CUDA, std::string("cudaGetSymbolAddress(g_solve_scratch): ") +
                                       cudaGetErrorString(e));
     g_scratch_dev[dev] = static_cast<double*>(ptr);
+    g_scratch_ctx[dev] = ctx;
   }
   return g_scratch_dev[dev];
 }

@@ -121,8 +121,16 @@ __global__ void k_equilibrate(int n, const int* rowptr, const int* col, const do
 }
 
 // l1-Jacobi weights (classical_amg.py:885-889, 1298-1306)
+// With lmax non-null each row also contributes inv_i * sum_j |a_ij| to the
+// Gershgorin bound of diag(inv) A (the Chebyshev smoother's interval), kept as
+// the bits of a non-negative double so atomicMax orders them.
+template <typename TO>
+__device__ __forceinline__ void lmax_update(unsigned long long* lmax, TO inv, double ra) {
+  if (lmax) atomicMax(lmax, (unsigned long long)__double_as_longlong((double)inv * ra));
+}
 template <typename TV, typename TO>
-__global__ void k_inv_relax(int n, const int* rowptr, const int* col, const TV* val, TO* inv) {
+__global__ void k_inv_relax(int n, const int* rowptr, const int* col, const TV* val, TO* inv,
+                            unsigned long long* lmax) {
   GRID_LOOP(i, n) {
     double d = 0.0, ra = 0.0;
     for (int e = rowptr[i]; e < rowptr[i + 1]; ++e) {
@@ -133,7 +141,9 @@ __global__ void k_inv_relax(int n, const int* rowptr, const int* col, const TV* 
     double denom = fmax(fabs(d), 0.3 * ra);
     denom = denom < 1e-30 ? 1e-30 : denom;
     double r = 1.0 / denom;
-    inv[i] = (TO)(r > 1e2 ? 1e2 : r);
+    const TO w = (TO)(r > 1e2 ? 1e2 : r);
+    inv[i] = w;
+    lmax_update(lmax, w, ra);
   }
 }
 
@@ -142,7 +152,8 @@ __global__ void k_inv_relax(int n, const int* rowptr, const int* col, const TV* 
 // absolute row sum from a fixed-order warp reduction.
 template <typename TV, typename TO>
 __global__ void k_inv_relax_warp(int n, const int* __restrict__ rowptr, const int* __restrict__ col,
-                                 const TV* __restrict__ val, TO* __restrict__ inv) {
+                                 const TV* __restrict__ val, TO* __restrict__ inv,
+                                 unsigned long long* lmax) {
   const int lane = threadIdx.x & 31;
   for (long long i = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); i < n;
        i += (long long)gridDim.x * (blockDim.x >> 5)) {
@@ -158,7 +169,9 @@ __global__ void k_inv_relax_warp(int n, const int* __restrict__ rowptr, const in
       double denom = fmax(fabs(d), 0.3 * ra);
       denom = denom < 1e-30 ? 1e-30 : denom;
       const double r = 1.0 / denom;
-      inv[i] = (TO)(r > 1e2 ? 1e2 : r);
+      const TO w = (TO)(r > 1e2 ? 1e2 : r);
+      inv[i] = w;
+      lmax_update(lmax, w, ra);
     }
   }
 }
@@ -501,6 +514,52 @@ __global__ void k_p_blend(int n, const int* prow, const int* pcol, double* pval,
       w = w < 0.0 ? 0.0 : w;
       pval[e] = (1.0 - blend) * pval[e] + blend * (w / wsum);
     }
+  }
+}
+
+// Interpolation truncation (an option of this library; the reference keeps
+// every entry).  An F row keeps entry e when fewer than kmax entries outrank it
+// (larger weight, or equal weight and lower position) and its weight is at least
+// tf times the row's largest; the kept entries are rescaled to the row's old
+// sum.  kmax = 0 means no cap.  Weights are >= 0 here (clamped above).
+__device__ __forceinline__ bool p_keep(const double* w, int a, int b, int e, int kmax, double tf,
+                                       double wmax) {
+  if (w[e] < tf * wmax) return false;
+  if (kmax <= 0) return true;
+  int rank = 0;
+  for (int f = a; f < b && rank < kmax; ++f)
+    if (w[f] > w[e] || (w[f] == w[e] && f < e)) ++rank;
+  return rank < kmax;
+}
+__global__ void k_p_trunc_count(int n, const int* prow, const double* pval, const signed char* cf,
+                                int kmax, double tf, int* cnt) {
+  GRID_LOOP(i, n) {
+    const int a = prow[i], b = prow[i + 1];
+    if (cf[i] != 1) { cnt[i] = b - a; continue; }
+    double wmax = 0.0;
+    for (int e = a; e < b; ++e) wmax = fmax(wmax, pval[e]);
+    int c = 0;
+    for (int e = a; e < b; ++e) c += p_keep(pval, a, b, e, kmax, tf, wmax);
+    cnt[i] = c;
+  }
+}
+__global__ void k_p_trunc_fill(int n, const int* prow, const int* pcol, const double* pval,
+                               const signed char* cf, int kmax, double tf, const int* nrow,
+                               int* ncol, double* nval) {
+  GRID_LOOP(i, n) {
+    const int a = prow[i], b = prow[i + 1];
+    int o = nrow[i];
+    if (cf[i] != 1) {
+      for (int e = a; e < b; ++e, ++o) { ncol[o] = pcol[e]; nval[o] = pval[e]; }
+      continue;
+    }
+    double wmax = 0.0, all = 0.0, kept = 0.0;
+    for (int e = a; e < b; ++e) { wmax = fmax(wmax, pval[e]); all += pval[e]; }
+    for (int e = a; e < b; ++e)
+      if (p_keep(pval, a, b, e, kmax, tf, wmax)) kept += pval[e];
+    const double sc = kept > 0.0 ? all / kept : 1.0;
+    for (int e = a; e < b; ++e)
+      if (p_keep(pval, a, b, e, kmax, tf, wmax)) { ncol[o] = pcol[e]; nval[o] = pval[e] * sc; ++o; }
   }
 }
 
@@ -1070,31 +1129,49 @@ void union_numeric(int rows, const int* optr, const int* ocol, const double* ova
 }
 
 template <typename TV, typename TO>
-void launch_inv_relax(const Level& L, const TV* val, TO* out, cudaStream_t s) {
+void launch_inv_relax(const Level& L, const TV* val, TO* out, unsigned long long* lmax, cudaStream_t s) {
+  if (lmax) IMPES_CUDA(cudaMemsetAsync(lmax, 0, sizeof(unsigned long long), s));
   if (L.n > 0 && L.nnz / L.n > 32) {
     k_inv_relax_warp<TV, TO><<<grid_for((size_t)L.n * 32, TB, 16), TB, 0, s>>>(L.n, L.rowptr.p, L.col.p, val,
-                                                                             out); ::impes::count_launch();
+                                                                             out, lmax); ::impes::count_launch();
   } else {
-    k_inv_relax<TV, TO><<<grid_for(L.n, TB), TB, 0, s>>>(L.n, L.rowptr.p, L.col.p, val, out); ::impes::count_launch();
+    k_inv_relax<TV, TO><<<grid_for(L.n, TB), TB, 0, s>>>(L.n, L.rowptr.p, L.col.p, val, out, lmax); ::impes::count_launch();
   }
   IMPES_CHECK_LAUNCH();
 }
 
+// The Chebyshev bound of level L (slot 0: fp64 values, 1: fp32 chain), or null
+// when the hierarchy smooths with l1-Jacobi.
+unsigned long long* cheb_slot(AMG& h, Level& L, int slot) {
+  if (h.prm.smoother != IMPES_SMOOTHER_CHEBYSHEV) return nullptr;
+  L.cheb_lmax.ensure(2);
+  return L.cheb_lmax.p + slot;
+}
+
 void compute_inv_relax(AMG& h, Level& L, cudaStream_t s) {
   L.inv_relax.ensure(std::max(L.n, 1));
-  launch_inv_relax<double, double>(L, L.val.p, L.inv_relax.p, s);
+  launch_inv_relax<double, double>(L, L.val.p, L.inv_relax.p, cheb_slot(h, L, 0), s);
 }
 
 // l1 weights of the fp32 chain, from the fp32 values
-void compute_inv_relax_f(Level& L, cudaStream_t s) {
+void compute_inv_relax_f(AMG& h, Level& L, cudaStream_t s) {
   L.inv_relaxf.ensure(std::max(L.n, 1));
-  launch_inv_relax<float, float>(L, L.valf.p, L.inv_relaxf.p, s);
+  launch_inv_relax<float, float>(L, L.valf.p, L.inv_relaxf.p, cheb_slot(h, L, 1), s);
+}
+
+// fp32 weights rounded from the fp64 ones: the fp32 path's Chebyshev bound is
+// the fp64 one
+void cheb_copy_to_fp32(AMG& h, Level& L, cudaStream_t s) {
+  if (h.prm.smoother != IMPES_SMOOTHER_CHEBYSHEV) return;
+  L.cheb_lmax.ensure(2);
+  IMPES_CUDA(cudaMemcpyAsync(L.cheb_lmax.p + 1, L.cheb_lmax.p, sizeof(unsigned long long),
+                             cudaMemcpyDeviceToDevice, s));
 }
 
 void alloc_level_vectors(Level& L) {
   size_t n = std::max(L.n, 1);
-  L.x.ensure(n); L.b.ensure(n); L.r.ensure(n); L.t.ensure(n);
-  L.xf.ensure(n); L.bf.ensure(n); L.rf.ensure(n); L.tf.ensure(n);
+  L.x.ensure(n); L.b.ensure(n); L.r.ensure(n); L.t.ensure(n); L.u.ensure(n);
+  L.xf.ensure(n); L.bf.ensure(n); L.rf.ensure(n); L.tf.ensure(n); L.uf.ensure(n);
 }
 
 // Equilibration of level-0 values (classical_amg.py:763-788 / 1334-1355).  The
@@ -1124,6 +1201,7 @@ void level_precision_copies(AMG& h, Level& L, cudaStream_t s) {
   L.inv_relaxf.ensure(std::max(L.n, 1));
   k_to_float<<<grid_for(L.nnz, TB), TB, 0, s>>>(L.nnz, L.val.p, L.valf.p); ::impes::count_launch();
   k_to_float<<<grid_for(L.n, TB), TB, 0, s>>>(L.n, L.inv_relax.p, L.inv_relaxf.p); ::impes::count_launch();
+  cheb_copy_to_fp32(h, L, s);
   if (!L.coarsest && L.pnnz) {
     L.pvalf.ensure(L.pnnz);
     L.rvalf.ensure(L.pnnz);
@@ -1245,6 +1323,22 @@ void amg_setup(AMG& h, int n, int nnz, const int* rowptr, const int* col, const 
       k_p_blend<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.prow.p, L.pcol.p, L.pval.p, cf2.p, basis.p, m,
                                                 h.prm.nullspace_blend, h.prm.nullspace_reg); ::impes::count_launch();
       IMPES_CHECK_LAUNCH();
+    }
+    if (h.prm.p_max_elements > 0 || h.prm.p_trunc_factor > 0.0) {
+      DBuf<int> tcnt(nl + 1), trow(nl + 1);
+      k_p_trunc_count<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.prow.p, L.pval.p, cf2.p, h.prm.p_max_elements,
+                                                      h.prm.p_trunc_factor, tcnt.p); ::impes::count_launch();
+      IMPES_CHECK_LAUNCH();
+      const int tn = exclusive_scan_i32(tcnt.p, trow.p, nl, s);
+      DBuf<int> tcol(std::max(tn, 1));
+      DBuf<double> tval(std::max(tn, 1));
+      k_p_trunc_fill<<<grid_for(nl, TB), TB, 0, s>>>(nl, L.prow.p, L.pcol.p, L.pval.p, cf2.p,
+                                                     h.prm.p_max_elements, h.prm.p_trunc_factor, trow.p,
+                                                     tcol.p, tval.p); ::impes::count_launch();
+      IMPES_CHECK_LAUNCH();
+      IMPES_CUDA(cudaStreamSynchronize(s));
+      L.prow = std::move(trow); L.pcol = std::move(tcol); L.pval = std::move(tval);
+      L.pnnz = tn;
     }
     // R = P^T (sorted rows) and its values
     DBuf<int> rcnt(nc + 1), rfill(nc + 1);
@@ -1376,6 +1470,7 @@ void update_fp32_chain(AMG& h, cudaStream_t s) {
   compute_inv_relax(h, L0, s);
   k_to_float<<<grid_for(L0.nnz, TB), TB, 0, s>>>(L0.nnz, L0.val.p, L0.valf.p); ::impes::count_launch();
   k_to_float<<<grid_for(L0.n, TB), TB, 0, s>>>(L0.n, L0.inv_relax.p, L0.inv_relaxf.p); ::impes::count_launch();
+  cheb_copy_to_fp32(h, L0, s);
   IMPES_CHECK_LAUNCH();
   for (size_t l = 0; l < h.levels.size(); ++l) {
     Level& L = *h.levels[l];
@@ -1396,7 +1491,7 @@ void update_fp32_chain(AMG& h, cudaStream_t s) {
       plan_apply_cf<float>(Nc.nnz, L.ac_seg.p, L.ac_f.p, L.ac_cf.p, L.apvalf.p, Nc.valf.p, s);
     else
       plan_apply<float>(Nc.nnz, L.ac_seg.p, L.ac_r.p, L.ac_f.p, L.pvalf.p, L.apvalf.p, Nc.valf.p, s);
-    compute_inv_relax_f(Nc, s);
+    compute_inv_relax_f(h, Nc, s);
   }
   coarse_factor(h, *h.levels.back(), s, true);
   h.fp64_stale = true;
@@ -1444,6 +1539,7 @@ void amg_update(AMG& h, const double* val, cudaStream_t s) {
     L->inv_relaxf.ensure(std::max(L->n, 1));
     k_to_float<<<grid_for(L->nnz, TB), TB, 0, s>>>(L->nnz, L->val.p, L->valf.p); ::impes::count_launch();
     k_to_float<<<grid_for(L->n, TB), TB, 0, s>>>(L->n, L->inv_relax.p, L->inv_relaxf.p); ::impes::count_launch();
+    cheb_copy_to_fp32(h, *L, s);
   }
   IMPES_CHECK_LAUNCH();
   timers().end(tid, s, bytes);

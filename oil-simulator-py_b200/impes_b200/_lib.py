@@ -34,7 +34,9 @@ class AmgParams(C.Structure):
     _fields_ = [("theta", C.c_double), ("max_levels", C.c_int), ("coarsest_size", C.c_int),
                 ("nullspace_dim", C.c_int), ("nullspace_blend", C.c_double),
                 ("nullspace_reg", C.c_double), ("equilibration_threshold", C.c_double),
-                ("tiebreak_seed", C.c_uint32), ("mixed_precision", C.c_int)]
+                ("tiebreak_seed", C.c_uint32), ("mixed_precision", C.c_int),
+                ("p_max_elements", C.c_int), ("p_trunc_factor", C.c_double),
+                ("smoother", C.c_int), ("cheb_lower", C.c_double)]
 
 
 class LevelDesc(C.Structure):

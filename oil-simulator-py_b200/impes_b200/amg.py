@@ -27,6 +27,7 @@ from ._lib import check, lib, ptr
 
 _NORMS = {"equilibrated": _lib.NORM_EQUILIBRATED, "jacobi": _lib.NORM_JACOBI}
 _PRECISION = {"fp64": 0, "float64": 0, "mixed": 1, "fp32": 1}
+_SMOOTHERS = {"l1jacobi": 0, "chebyshev": 1}
 
 
 def _cuda_device(device=None) -> torch.device:
@@ -85,12 +86,20 @@ class ClassicalAMG:
 
     ``seed`` selects the C/F tie-break stream; ``mixed_precision`` keeps an fp32
     copy of every level for the fp32 V-cycle of the mixed path.
+    ``p_max_elements`` / ``p_trunc_factor`` truncate the interpolation (an option
+    the reference does not have; the defaults keep its interpolation): each F
+    row of P keeps at most ``p_max_elements`` entries (0: no cap) and drops those
+    below ``p_trunc_factor`` times its largest, rescaled to the old row sum.
+    ``smoother`` is "l1jacobi" (the reference's) or "chebyshev" (the Chebyshev
+    iteration for diag(l1 weights) A on [``cheb_lower`` * lmax, lmax], lmax its
+    Gershgorin bound; also not in the reference).
     """
 
     def __init__(self, A_csr_np, theta: float = 0.25, max_levels: int = 10, coarsest_size: int = 100,
                  anchor_idx: int | None = None, nullspace_dim: int = 3, nullspace_blend: float = 0.6,
                  nullspace_reg: float = 1e-6, *, seed: int = 0, mixed_precision: bool = True,
-                 device=None):
+                 device=None, p_max_elements: int = 0, p_trunc_factor: float = 0.0,
+                 smoother: str = "l1jacobi", cheb_lower: float = 0.3):
         if anchor_idx is not None:
             raise ValueError("anchor_idx is not supported; pin the matrix with _apply_reference_fix first")
         self.theta, self.max_levels, self.coarsest_size = float(theta), int(max_levels), int(coarsest_size)
@@ -104,9 +113,15 @@ class ClassicalAMG:
         self.device = _cuda_device(device)
         self.seed = int(seed)
         self.mixed_precision = bool(mixed_precision)
+        self.p_max_elements, self.p_trunc_factor = int(p_max_elements), float(p_trunc_factor)
+        if smoother not in _SMOOTHERS:
+            raise ValueError(f"unknown smoother {smoother!r}")
+        self.smoother, self.cheb_lower = smoother, float(cheb_lower)
         prm = _lib.AmgParams(self.theta, self.max_levels, self.coarsest_size, self.nullspace_dim,
                              self.nullspace_blend, self.nullspace_reg, self.equilibration_threshold,
-                             self.seed & 0xFFFFFFFF, 1 if self.mixed_precision else 0)
+                             self.seed & 0xFFFFFFFF, 1 if self.mixed_precision else 0,
+                             self.p_max_elements, self.p_trunc_factor, _SMOOTHERS[smoother],
+                             self.cheb_lower)
         h = C.c_void_p()
         check(lib.impes_amg_create(C.byref(h), C.byref(prm)), "impes_amg_create")
         self._h = h
@@ -143,7 +158,8 @@ class ClassicalAMG:
         rowptr, col, val, shape = to_csr32(A_csr_np, self.device)
         if shape[0] != self.n:
             raise ValueError(f"AMG hierarchy built for n={self.n}, got n={shape[0]}")
-        if col.numel() != self._pattern[1].numel() or not torch.equal(col, self._pattern[1]):
+        if (col.numel() != self._pattern[1].numel() or not torch.equal(col, self._pattern[1])
+                or not torch.equal(rowptr, self._pattern[0])):
             raise ValueError("update_matrix needs the sparsity pattern the hierarchy was built on")
         self.update_values(val)
 
@@ -286,26 +302,30 @@ def amg_solve(A, b: torch.Tensor, *, tol: float = 1e-6, max_cycles: int = 20, th
     ``method="vcycle"`` (default) keeps the reference's stand-alone V-cycles and
     stopping rule; ``method="fgmres"`` runs FGMRES to ``tol`` in ``norm`` with at
     most ``max_iters`` (default ``max_cycles``) V-cycles.  The hierarchy is cached
-    per (size, theta, max_levels, coarsest_size, device) and refreshed with
-    ``update_matrix`` on a hit.  Returns x on b's device and dtype.
+    per (size, theta, max_levels, coarsest_size, device) as the reference's
+    ``_AMG_CACHE`` is, plus the two settings the reference does not have: whether
+    the hierarchy keeps fp32 levels (``precision`` other than "fp64") and the
+    tie-break ``seed``.  A hit on the same pattern (row pointers and columns)
+    is refreshed with ``update_matrix``; a different pattern rebuilds.  Returns x
+    on b's device and dtype.
     """
+    if precision not in _PRECISION:
+        raise ValueError(f"unknown precision {precision!r}")
     dev = _cuda_device(device)
     rowptr, col, val, shape = to_csr32(A, dev)
-    key = (torch.Size(shape), float(theta), int(max_levels), int(coarsest_size), str(dev))
+    mixed = _PRECISION[precision] == 1
+    key = (torch.Size(shape), float(theta), int(max_levels), int(coarsest_size), str(dev), mixed,
+           int(seed))
     amg = _AMG_CACHE.get(key)
-    if amg is None:
+    same_pattern = (amg is not None and rowptr.numel() == amg._pattern[0].numel()
+                    and col.numel() == amg._pattern[1].numel()
+                    and torch.equal(rowptr, amg._pattern[0]) and torch.equal(col, amg._pattern[1]))
+    if amg is None or not same_pattern:
         amg = ClassicalAMG((rowptr, col, val, shape), theta=theta, max_levels=max_levels,
-                           coarsest_size=coarsest_size, seed=seed, device=dev,
-                           mixed_precision=(precision != "fp64"))
+                           coarsest_size=coarsest_size, seed=seed, device=dev, mixed_precision=mixed)
         _AMG_CACHE[key] = amg
     else:
-        if not torch.equal(col, amg._pattern[1]):
-            amg = ClassicalAMG((rowptr, col, val, shape), theta=theta, max_levels=max_levels,
-                               coarsest_size=coarsest_size, seed=seed, device=dev,
-                               mixed_precision=(precision != "fp64"))
-            _AMG_CACHE[key] = amg
-        else:
-            amg.update_values(val)
+        amg.update_values(val)
     if method == "vcycle":
         x = amg.solve(b, tol=tol, max_iter=max_cycles)
     elif method == "fgmres":

@@ -476,7 +476,11 @@ class Simulator:
             prm = _lib.AmgParams(float(amg_cfg.get("theta", 0.25)), int(amg_cfg.get("max_levels", 10)),
                                  int(amg_cfg.get("coarsest_size", 200)), 3, 0.6, 1e-6, 1e-6,
                                  int(amg_cfg.get("seed", 0)) & 0xFFFFFFFF,
-                                 1 if self.amg_precision != "fp64" else 0)
+                                 1 if self.amg_precision != "fp64" else 0,
+                                 int(amg_cfg.get("p_max_elements", 0)),
+                                 float(amg_cfg.get("p_trunc_factor", 0.0)),
+                                 {"l1jacobi": 0, "chebyshev": 1}[amg_cfg.get("smoother", "l1jacobi")],
+                                 float(amg_cfg.get("cheb_lower", 0.3)))
             h = C.c_void_p()
             check(lib.impes_amg_create(C.byref(h), C.byref(prm)), "impes_amg_create")
             self._amg_h = h

@@ -302,6 +302,41 @@ def prolongation(A, cf_in, strong, basis, blend=0.0, reg=1e-7):
     return P, cf
 
 
+def truncate_interpolation(P, cf, kmax=0, tf=0.0):
+    """Interpolation truncation, an option of the GPU library with no counterpart
+    in the reference (restated here as its checker).  Each F row (cf == 1) keeps
+    entry e when fewer than ``kmax`` entries outrank it -- a larger weight, or an
+    equal weight earlier in the row -- and its weight is at least ``tf`` times
+    the row's largest; kept entries are rescaled to the row's old sum.  C rows
+    are kept as they are.  ``kmax`` 0 means no cap."""
+    P = P.tocsr()
+    rows, cols, vals = [], [], []
+    for i in range(P.shape[0]):
+        a, b = P.indptr[i], P.indptr[i + 1]
+        w = P.data[a:b]
+        c = P.indices[a:b]
+        if cf[i] != 1 or b == a:
+            keep = np.ones(b - a, dtype=bool)
+            sc = 1.0
+        else:
+            wmax = w.max()
+            keep = w >= tf * wmax
+            if kmax > 0:
+                order = np.lexsort((np.arange(b - a), -w))   # weight descending, then position
+                rank = np.empty(b - a, dtype=np.int64)
+                rank[order] = np.arange(b - a)
+                keep &= rank < kmax
+            kept = w[keep].sum()
+            sc = w.sum() / kept if kept > 0.0 else 1.0
+        rows.append(np.full(int(keep.sum()), i))
+        cols.append(c[keep])
+        vals.append(w[keep] * sc)
+    rows, cols, vals = np.concatenate(rows), np.concatenate(cols), np.concatenate(vals)
+    out = sp.csr_matrix((vals, (rows, cols)), shape=P.shape)
+    out.sort_indices()
+    return out
+
+
 def galerkin(A, P):
     """``rap_torch`` (classical_amg.py:653-657): A_c = P^T (A P)."""
     Ac = (P.T.tocsr() @ (A @ P)).tocsr()
@@ -314,6 +349,40 @@ def inv_relax(A):
     d = np.abs(extract_diag(A))
     ra = np.asarray(abs(A).sum(axis=1)).ravel()
     return np.minimum(1.0 / np.maximum(np.maximum(d, 0.3 * ra), 1e-30), 1e2)
+
+
+def cheb_lmax(A, inv):
+    """Upper bound of the spectrum of diag(inv) A used by the Chebyshev smoother
+    (an option of the GPU library; the reference smooths with l1-Jacobi only):
+    the Gershgorin bound max_i inv_i * sum_j |a_ij|."""
+    ra = np.asarray(abs(A).sum(axis=1)).ravel()
+    return float((inv * ra).max()) if A.shape[0] else 0.0
+
+
+def cheb_smooth(A, inv, lmax, x, b, nu, lower=0.3, zero_x=False):
+    """``nu`` steps of the Chebyshev iteration for diag(inv) A on
+    [lower * lmax, lmax] (Saad, Iterative Methods for Sparse Linear Systems,
+    2nd ed., Alg. 12.1), from x (or from zero): x is updated nu times, with
+    nu - 1 products by A after the initial residual.  The GPU kernels follow
+    this operation order."""
+    theta = 0.5 * (lmax + lower * lmax)
+    delta = 0.5 * (lmax - lower * lmax)
+    sigma = theta / delta
+    rho = 1.0 / sigma
+    r = inv * b if zero_x else inv * (b - A @ x)
+    d = r / theta
+    if zero_x:
+        x = np.zeros_like(b)
+    for k in range(nu):
+        if k == nu - 1:
+            x = x + d
+            break
+        r = r - inv * (A @ d)
+        rho_new = 1.0 / (2.0 * sigma - rho)
+        d_new = (rho_new * rho) * d + (2.0 * rho_new / delta) * r
+        x = x + d
+        d, rho = d_new, rho_new
+    return x
 
 
 def equilibrate(A, threshold=1e-6):
@@ -336,8 +405,12 @@ class AMG:
     """``ClassicalAMG`` (classical_amg.py:694-1392) with a supplied tie-break seed."""
 
     def __init__(self, A, theta=0.25, max_levels=10, coarsest_size=100, seed=0,
-                 nullspace_dim=3, nullspace_blend=0.6, nullspace_reg=1e-6, tiebreaks=None):
+                 nullspace_dim=3, nullspace_blend=0.6, nullspace_reg=1e-6, tiebreaks=None,
+                 p_max_elements=0, p_trunc_factor=0.0, smoother="l1jacobi", cheb_lower=0.3):
         self.theta, self.max_levels, self.coarsest_size = theta, max_levels, coarsest_size
+        if smoother not in ("l1jacobi", "chebyshev"):
+            raise ValueError(f"unknown smoother {smoother!r}")
+        self.smoother, self.cheb_lower = smoother, float(cheb_lower)
         self.blend = float(max(0.0, min(1.0, nullspace_blend)))
         self.reg = float(max(1e-10, nullspace_reg))
         A = sp.csr_matrix(A, dtype=np.float64)
@@ -359,6 +432,8 @@ class AMG:
                 break
             bl = self.blend if basis is not None else 0.0
             P, cf = prolongation(A, cf, strong, basis, blend=bl, reg=self.reg)
+            if p_max_elements > 0 or p_trunc_factor > 0.0:
+                P = truncate_interpolation(P, cf, p_max_elements, p_trunc_factor)
             Ac = galerkin(A, P)
             self.levels.append(dict(A=A, n=n, P=P, cf=cf, inv_relax=inv_relax(A), is_coarsest=False))
             if basis is not None:
@@ -385,8 +460,11 @@ class AMG:
             self.levels[l + 1]["inv_relax"] = inv_relax(A)
 
     # -------------------------------------------------------------- cycling
-    def smooth(self, l, x, b, nu):
+    def smooth(self, l, x, b, nu, zero_x=False):
         lv = self.levels[l]
+        if self.smoother == "chebyshev":
+            lmax = cheb_lmax(lv["A"], lv["inv_relax"])
+            return cheb_smooth(lv["A"], lv["inv_relax"], lmax, x, b, nu, self.cheb_lower, zero_x)
         for _ in range(nu):
             x = x + 0.7 * lv["inv_relax"] * (b - lv["A"] @ x)
         return x
@@ -417,7 +495,7 @@ class AMG:
         lv = self.levels[l]
         if lv["is_coarsest"]:
             return self.coarse_solve(lv, b)
-        x = self.smooth(l, x, b, pre)
+        x = self.smooth(l, x, b, pre, zero_x=(l > 0 or not np.any(x)))
         r = b - lv["A"] @ x
         rc = lv["P"].T @ r
         ec = self.vcycle(l + 1, np.zeros_like(rc), rc, pre, post)

@@ -1,8 +1,11 @@
 """Generate the golden fixtures by running the reference itself (build container only).
 
-Usage:  python tests/golden/make_golden.py [REFERENCE_ROOT] [--pcg-only | --three-phase-only | --wells-only | --amg-3d-only]
+Usage:  python tests/golden/make_golden.py REFERENCE_ROOT [--pcg-only | --three-phase-only |
+                                                        --wells-only | --amg-3d-only | --configs-only]
 
-REFERENCE_ROOT defaults to /root/reference (researchim-ai/oil-simulator-py).
+REFERENCE_ROOT is a checkout of researchim-ai/oil-simulator-py (the directory
+holding ``src/``); it may instead be given in the environment variable
+OIL_SIMULATOR_REFERENCE.  There is no default.
 The reference is imported unmodified; the harness only
   * puts a placeholder ``matplotlib`` first on sys.path (plotting is unused here),
   * sets ``torch.set_default_dtype(torch.float64)`` before building objects,
@@ -30,7 +33,11 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
 _ARGS = [a for a in sys.argv[1:] if not a.startswith("--")]
-REF = _ARGS[0] if _ARGS else "/root/reference"
+REF = _ARGS[0] if _ARGS else os.environ.get("OIL_SIMULATOR_REFERENCE", "")
+if not REF or not os.path.isdir(os.path.join(REF, "src", "simulator")):
+    sys.stderr.write(__doc__ + "\nerror: REFERENCE_ROOT (or OIL_SIMULATOR_REFERENCE) must name the "
+                     "reference checkout\n")
+    sys.exit(2)
 sys.path[:0] = [os.path.join(HERE, "_stubs"), os.path.join(REF, "src"), REPO]
 
 import torch  # noqa: E402
@@ -98,17 +105,39 @@ def build_reference(cfg, fields, tmpdir):
     return sim, fl, wm
 
 
-def run_trajectory(name, cfg, fields, steps, dt_days, solver="direct"):
+def fields_digest(fields):
+    """sha256 of the rock fields (kx, ky, kz, poro as float64 C-order bytes)."""
+    import hashlib
+    h = hashlib.sha256()
+    for k in ("kx", "ky", "kz", "poro"):
+        h.update(np.ascontiguousarray(fields[k], dtype=np.float64).tobytes())
+    return h.hexdigest()
+
+
+def run_trajectory(name, cfg, fields, steps, dt_days, solver="direct", full_at=None, n_samples=0,
+                   keep_systems=None, generator=None):
     """The reference's trajectory with amg_solve replaced by a direct solve of its
     own (A, b); with solver="cg" the reference's own Jacobi-PCG path runs
-    unpatched (pressure_solver "cg")."""
+    unpatched (pressure_solver "cg").
+
+    Long runs are stored compactly: ``full_at`` lists the (1-based) steps whose
+    whole p/sw/sg fields are kept (None: every step), ``n_samples`` cells drawn
+    with a fixed seed are kept at every step (``sample_idx``, ``p_s``, ``sw_s``,
+    ``sg_s``), and only the first ``keep_systems`` assembled systems are kept
+    (None: all).  With ``generator`` = (scenario function name, keyword
+    arguments) the rock fields and the recorded systems are left out: tests
+    rebuild the fields with that scenario call and check them against the
+    stored ``fields_sha256``."""
     rec = {"A": [], "b": []}
 
     def direct(A, b, **kw):
         A = A.coalesce().to_sparse_csr() if A.layout == torch.sparse_coo else A
         crow, col, val = A.crow_indices().numpy(), A.col_indices().numpy(), A.values().numpy()
-        rec["A"].append((crow.copy(), col.copy(), val.copy()))
-        rec["b"].append(b.numpy().copy())
+        if keep_systems is None or len(rec["b"]) < keep_systems:
+            rec["A"].append((crow.copy(), col.copy(), val.copy()))
+            rec["b"].append(b.numpy().copy())
+        else:
+            rec["b"].append(None)
         M = sp.csr_matrix((val, col, crow), shape=A.shape)
         return torch.from_numpy(spla.spsolve(M.tocsc(), b.numpy()))
 
@@ -135,37 +164,61 @@ def run_trajectory(name, cfg, fields, steps, dt_days, solver="direct"):
     out = {}
     with tempfile.TemporaryDirectory() as td:
         sim, fl, wm = build_reference(cfg, fields, td)
-        ps, sws, sgs, mbs = [], [], [], []
-        for _ in range(steps):
+        ps, sws, sgs, mbs, qs = [], [], [], [], []
+        ncell = fields["kx"].size
+        sidx = (np.sort(np.random.default_rng(12345).choice(ncell, size=min(n_samples, ncell),
+                                                            replace=False))
+                if n_samples else None)
+        p_s, sw_s, sg_s = [], [], []
+        for st in range(1, steps + 1):
             with contextlib.redirect_stdout(io.StringIO()):
                 ok = sim.run_step(dt_days * 86400.0)
             assert ok
-            ps.append(fl.pressure.numpy().ravel().copy())
-            sws.append(fl.s_w.numpy().ravel().copy())
-            sgs.append(fl.s_g.numpy().ravel().copy())
+            p_, sw_, sg_ = (fl.pressure.numpy().ravel().copy(), fl.s_w.numpy().ravel().copy(),
+                            fl.s_g.numpy().ravel().copy())
+            if full_at is None or st in full_at:
+                ps.append(p_); sws.append(sw_); sgs.append(sg_)
+            if sidx is not None:
+                p_s.append(p_[sidx]); sw_s.append(sw_[sidx]); sg_s.append(sg_[sidx])
             mb = sim.mass_balance
             cb = sim.component_balance
             mbs.append([mb[ph][io_] for ph in ("water", "oil", "gas") for io_ in ("in", "out")]
                        + [cb[c][k] for c in ("oil", "gas") for k in ("in", "out", "accum")])
+            qs.append([w.last_q_total if w.last_q_total is not None else np.nan for w in wm.get_wells()])
+            if steps >= 20 and st % 10 == 0:
+                print(f"  {name}: step {st}/{steps}", flush=True)
         wells = [(w.cell_index_flat, w.last_q_total if w.last_q_total is not None else np.nan)
                  for w in wm.get_wells()]
     crow, col, val = rec["A"][0]
+    kept_b = [b for b in rec["b"] if b is not None]
     out.update(
         cfg=json.dumps(cfg), kx=fields["kx"], ky=fields["ky"], kz=fields["kz"], poro=fields["poro"],
         dt=dt_days * 86400.0,
         A0_crow=crow.astype(np.int32), A0_col=col.astype(np.int32), A0_val=val,
-        b0=rec["b"][0], b_all=np.stack(rec["b"]),
+        b0=rec["b"][0], b_all=np.stack(kept_b),
         A_val_all=np.stack([a[2] for a in rec["A"]]),
         p=np.stack(ps), sw=np.stack(sws), sg=np.stack(sgs), balances=np.array(mbs),
         well_cells=np.array([w[0] for w in wells], dtype=np.int64),
         well_last_q=np.array([w[1] for w in wells]),
     )
+    if full_at is not None:
+        out["full_at"] = np.array(sorted(full_at), dtype=np.int64)
+        out["steps"] = np.array(steps)
+        out["well_q_all"] = np.array(qs)
+    if sidx is not None:
+        out.update(sample_idx=sidx.astype(np.int64), p_s=np.stack(p_s), sw_s=np.stack(sw_s),
+                   sg_s=np.stack(sg_s))
+    if generator is not None:
+        for k in ("kx", "ky", "kz", "poro", "A0_crow", "A0_col", "A0_val", "b0", "b_all", "A_val_all"):
+            out.pop(k, None)
+        out["fields_generator"] = json.dumps({"scenario": generator[0], "kwargs": generator[1]})
+        out["fields_sha256"] = fields_digest(fields)
     if solver == "cg":
         Simulator._build_pressure_matrix_vectorized = orig
         Simulator._build_pressure_rhs = orig_rhs
     np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
     print(name, "N", fields["kx"].size, "steps", steps, "p range", ps[-1].min(), ps[-1].max(),
-          "sw max", sws[-1].max(), "sg max", sgs[-1].max())
+          "sw max", sws[-1].max(), "sg max", sgs[-1].max(), flush=True)
     return out
 
 
@@ -356,6 +409,26 @@ def amg_3d_fixtures():
         amg_fixture(name, dict(np.load(os.path.join(HERE, f"{traj}.npz"))), seed=seed, coarsest=coarsest)
 
 
+def config_fixtures(which=("config0", "config3", "config1")):
+    """The benchmark configurations at their stated sizes: the 64x64x1
+    oil-water case for all of its 100 daily steps, the 64x64x8 adjoint-case grid
+    for its 50 two-day steps, and a two-step spot check of the 100x100x20
+    black-oil 5-spot (200,000 cells, about 150 s per direct solve).  Whole
+    fields are kept at a few steps and 2,048 fixed cells at every step."""
+    runs = {
+        "config0": ("config0_64x64x1_100steps", "two_phase_2d", {"seed": 0, "steps": 100}, 100, 1.0,
+                    {1, 10, 25, 50, 75, 100}),
+        "config3": ("config3_64x64x8_50steps", "adjoint_case", {"seed": 3, "steps": 50}, 50, 2.0,
+                    {1, 25, 50}),
+        "config1": ("config1_100x100x20_2steps", "black_oil_5spot", {"seed": 1, "steps": 2}, 2, 5.0, {2}),
+    }
+    for key in which:
+        name, fn, kwargs, steps, dt_days, full_at = runs[key]
+        cfg, f = getattr(scenarios, fn)(**kwargs)
+        run_trajectory(name, cfg, f, steps=steps, dt_days=dt_days, full_at=full_at, n_samples=2048,
+                       keep_systems=1, generator=(fn, kwargs))
+
+
 def main_pcg_only():
     """Regenerate only the Jacobi-PCG fixtures (the others are unchanged)."""
     cfg, f = scenarios.two_phase_2d(seed=0, nx=32, ny=32, nz=1, steps=4)
@@ -381,5 +454,9 @@ if __name__ == "__main__":
         sys.exit(0)
     if "--amg-3d-only" in sys.argv:
         amg_3d_fixtures()
+        sys.exit(0)
+    if "--configs-only" in sys.argv:
+        sel = [a.split("=", 1)[1] for a in sys.argv if a.startswith("--which=")]
+        config_fixtures(tuple(sel[0].split(",")) if sel else ("config0", "config3", "config1"))
         sys.exit(0)
     main()

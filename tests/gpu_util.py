@@ -7,10 +7,26 @@ import scipy.sparse as sp
 from oracle.impes import Model
 
 
+def fixture_fields(g):
+    """The rock fields of a fixture: stored in it, or (long-run fixtures) rebuilt
+    by the scenario call it names and checked against its stored digest."""
+    if "kx" in g:
+        return {k: g[k] for k in ("kx", "ky", "kz", "poro")}
+    import hashlib
+    from impes_b200 import scenarios
+    gen = json.loads(str(g["fields_generator"]))
+    _, f = getattr(scenarios, gen["scenario"])(**gen["kwargs"])
+    f = {k: np.ascontiguousarray(f[k], dtype=np.float64) for k in ("kx", "ky", "kz", "poro")}
+    h = hashlib.sha256()
+    for k in ("kx", "ky", "kz", "poro"):
+        h.update(f[k].tobytes())
+    assert h.hexdigest() == str(g["fields_sha256"]), "scenario fields differ from the fixture's"
+    return f
+
+
 def cfg_fields(g):
     cfg = json.loads(str(g["cfg"]))
-    fields = {k: g[k] for k in ("kx", "ky", "kz", "poro")}
-    return cfg, fields
+    return cfg, fixture_fields(g)
 
 
 def oracle_model(g):

@@ -17,10 +17,19 @@ def gpu_amg(A, **kw):
     return ClassicalAMG(A, **kw)
 
 
-@pytest.fixture(scope="module")
-def case(golden):
-    g = golden("amg_two_phase_32x32")
-    t = golden("two_phase_32x32")
+# ClassicalAMG hierarchies the reference built (fixture) and the trajectory whose
+# recorded matrices they were built from: a 2-D two-phase matrix and two 3-D
+# ones (black oil with PVT, gravity and capillarity; three phases without PVT)
+AMG_FIXTURES = [("amg_two_phase_32x32", "two_phase_32x32"),
+                ("amg_black_oil_10x10x4", "black_oil_10x10x4"),
+                ("amg_three_phase_16x16x3", "three_phase_16x16x3")]
+
+
+@pytest.fixture(scope="module", params=AMG_FIXTURES, ids=[a for a, _ in AMG_FIXTURES])
+def case(golden, request):
+    amg_name, traj_name = request.param
+    g = golden(amg_name)
+    t = golden(traj_name)
     n = len(t["A0_crow"]) - 1
     A = sp.csr_matrix((t["A0_val"], t["A0_col"], t["A0_crow"]), shape=(n, n))
     A2 = sp.csr_matrix((t["A_val_all"][1], t["A0_col"], t["A0_crow"]), shape=(n, n))
@@ -291,3 +300,129 @@ def test_vcycle_with_16bit_row_relative_columns_vs_host(far):
     x, st = amg.fgmres(torch.tensor(b, device="cuda"), tol=1e-10, norm="equilibrated", precision="mixed")
     assert st["converged"]
     assert np.linalg.norm(A @ to_np(x) - b) <= 1e-8 * np.linalg.norm(b)
+
+
+def test_amg_solve_values_cache_and_precision(golden):
+    """The drop-in ``amg_solve`` (pressure_amg.py:35-89) by value: the stand-alone
+    V-cycles equal the oracle's ``AMGSolver`` on the first recorded matrix and,
+    after a cache hit refreshes the hierarchy with ``update_matrix``, on the
+    second.  A mixed-precision FGMRES call on the same matrix gets its own
+    cached hierarchy (the cache key holds the precision) and reaches the direct
+    solution; so does the cache-hit call after it."""
+    from impes_b200 import amg as gamg
+    from oracle.amg import AMGSolver
+    t = golden("two_phase_32x32")
+    n = len(t["A0_crow"]) - 1
+    mats = [sp.csr_matrix((t["A_val_all"][q], t["A0_col"], t["A0_crow"]), shape=(n, n)) for q in (0, 1)]
+    rhs = [t["b_all"][q] for q in (0, 1)]
+    gamg._AMG_CACHE.clear()
+    ref = AMGSolver(tol=1e-30, max_cycles=5, coarsest_size=50, seed=3)
+
+    def torch_csr(A):
+        return torch.sparse_csr_tensor(torch.tensor(A.indptr, dtype=torch.int64),
+                                       torch.tensor(A.indices, dtype=torch.int64),
+                                       torch.tensor(A.data), size=A.shape)
+
+    for q in (0, 1):
+        x_ref = ref(mats[q], rhs[q])
+        x = gamg.amg_solve(torch_csr(mats[q]), torch.tensor(rhs[q], device="cuda"), tol=1e-30,
+                           max_cycles=5, coarsest_size=50, seed=3)
+        assert x.dtype == torch.float64
+        assert np.linalg.norm(to_np(x) - x_ref) <= 1e-8 * np.linalg.norm(x_ref), q
+        xm = gamg.amg_solve(torch_csr(mats[q]), torch.tensor(rhs[q], device="cuda"), tol=1e-13,
+                            max_cycles=300, coarsest_size=50, seed=3, method="fgmres", norm="jacobi",
+                            precision="mixed")
+        x_direct = spla.spsolve(mats[q].tocsc(), rhs[q])
+        assert np.abs(to_np(xm) - x_direct).max() <= 1e-8 * np.abs(x_direct).max(), q
+    keys = sorted(k[-2] for k in gamg._AMG_CACHE)
+    assert keys == [False, True]
+    # a float32 right-hand side comes back as float32 (the reference casts back to b's dtype)
+    xf = gamg.amg_solve(torch_csr(mats[1]), torch.tensor(rhs[1], device="cuda").float(), tol=1e-30,
+                        max_cycles=5, coarsest_size=50, seed=3)
+    assert xf.dtype == torch.float32
+    gamg._AMG_CACHE.clear()
+
+
+@pytest.mark.parametrize("kmax,tf", [(2, 0.0), (4, 0.0), (3, 0.25)])
+def test_truncated_hierarchy_matches_oracle(golden, kmax, tf):
+    """Interpolation truncation (an option of this library): the same levels,
+    P patterns and values as the oracle's restatement of the rule, on a 3-D
+    black-oil pressure matrix; the hierarchy is smaller than the reference's."""
+    t = golden("black_oil_10x10x4")
+    n = len(t["A0_crow"]) - 1
+    A = sp.csr_matrix((t["A0_val"], t["A0_col"], t["A0_crow"]), shape=(n, n))
+    amg = gpu_amg(A, coarsest_size=20, seed=7, p_max_elements=kmax, p_trunc_factor=tf)
+    ref = oa.AMG(A, coarsest_size=20, seed=7, p_max_elements=kmax, p_trunc_factor=tf)
+    compare_hierarchy(amg, ref)
+    full = oa.AMG(A, coarsest_size=20, seed=7)
+    assert sum(lv["A"].nnz for lv in ref.levels) < sum(lv["A"].nnz for lv in full.levels)
+    for lv in ref.levels:
+        if lv["P"] is not None and kmax:
+            lens = np.diff(lv["P"].indptr)
+            assert lens.max() <= kmax
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("name", ["black_oil_10x10x4", "gas_injection_12x12x3", "two_phase_16x16x2"])
+def test_truncated_hierarchy_trajectory_matches_reference(golden, name, precision):
+    """FGMRES preconditioned by the truncated hierarchy reaches the same pressures
+    (1e-8 relative) and saturations (1e-8) as the reference's exact-solve
+    trajectory: the preconditioner changes, the solution does not."""
+    from gpu_util import cfg_fields, gpu_sim
+    g = golden(name)
+    cfg, f = cfg_fields(g)
+    _, fl, _, sim = gpu_sim(cfg, f, tol=1e-13, norm="jacobi", precision=precision, max_iters=400,
+                            restart=40, p_max_elements=2)
+    for s in range(g["p"].shape[0]):
+        assert sim.run_step(float(g["dt"]))
+        assert sim.last_krylov["converged"], sim.last_krylov
+        assert np.abs(to_np(fl.pressure) - g["p"][s]).max() <= 1e-8 * np.abs(g["p"][s]).max(), s
+        assert np.abs(to_np(fl.s_w) - g["sw"][s]).max() <= 1e-8
+        assert np.abs(to_np(fl.s_g) - g["sg"][s]).max() <= 1e-8
+
+
+@pytest.mark.parametrize("traj,seed,cs", [("two_phase_32x32", 3, 50), ("black_oil_10x10x4", 7, 20)])
+def test_chebyshev_vcycle_matches_oracle(golden, traj, seed, cs):
+    """The Chebyshev smoother (an option of this library): one V-cycle, a 4-cycle
+    stand-alone solve and a solve after update_matrix equal the oracle's
+    restatement (1e-9); the fp32 V-cycle stays within fp32 rounding of it."""
+    t = golden(traj)
+    n = len(t["A0_crow"]) - 1
+    A = sp.csr_matrix((t["A0_val"], t["A0_col"], t["A0_crow"]), shape=(n, n))
+    A2 = sp.csr_matrix((t["A_val_all"][1], t["A0_col"], t["A0_crow"]), shape=(n, n))
+    amg = gpu_amg(A, coarsest_size=cs, seed=seed, smoother="chebyshev")
+    ref = oa.AMG(A, coarsest_size=cs, seed=seed, smoother="chebyshev")
+    compare_hierarchy(amg, ref)
+    b = t["b0"]
+    bs = ref.Dhalf_inv * b
+    v_ref = ref.vcycle(0, np.zeros_like(bs), bs)
+    v = to_np(amg.vcycle_scaled(torch.tensor(bs, device="cuda")))
+    assert np.linalg.norm(v - v_ref) <= 1e-9 * np.linalg.norm(v_ref)
+    vf = to_np(amg.vcycle_scaled(torch.tensor(bs, device="cuda"), precision="mixed"))
+    assert np.linalg.norm(vf - v_ref) <= 1e-4 * np.linalg.norm(v_ref)
+    x_ref, _, _ = ref.solve(b, tol=1e-30, max_iter=4)
+    x = to_np(amg.solve(torch.tensor(b, device="cuda"), tol=1e-30, max_iter=4))
+    assert np.linalg.norm(x - x_ref) <= 1e-8 * np.linalg.norm(x_ref)
+    amg.update_matrix(A2)
+    ref.update_matrix(A2)
+    b2 = t["b_all"][1]
+    x_ref, _, _ = ref.solve(b2, tol=1e-30, max_iter=3)
+    x = to_np(amg.solve(torch.tensor(b2, device="cuda"), tol=1e-30, max_iter=3))
+    assert np.linalg.norm(x - x_ref) <= 1e-8 * np.linalg.norm(x_ref)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_chebyshev_trajectory_matches_reference(golden, precision):
+    """FGMRES with Chebyshev-smoothed V-cycles reaches the reference's
+    exact-solve trajectory (p 1e-8 relative, S 1e-8) on the black-oil case."""
+    from gpu_util import cfg_fields, gpu_sim
+    g = golden("black_oil_10x10x4")
+    cfg, f = cfg_fields(g)
+    _, fl, _, sim = gpu_sim(cfg, f, tol=1e-13, norm="jacobi", precision=precision, max_iters=400,
+                            restart=40, smoother="chebyshev")
+    for s in range(g["p"].shape[0]):
+        assert sim.run_step(float(g["dt"]))
+        assert sim.last_krylov["converged"], sim.last_krylov
+        assert np.abs(to_np(fl.pressure) - g["p"][s]).max() <= 1e-8 * np.abs(g["p"][s]).max(), s
+        assert np.abs(to_np(fl.s_w) - g["sw"][s]).max() <= 1e-8
+        assert np.abs(to_np(fl.s_g) - g["sg"][s]).max() <= 1e-8

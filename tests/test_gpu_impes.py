@@ -12,7 +12,23 @@ from gpu_util import cfg_fields, gpu_sim, oracle_model, to_np
 pytestmark = pytest.mark.gpu
 
 CASES = ["two_phase_32x32", "two_phase_64x64", "two_phase_16x16x2", "black_oil_10x10x4",
-         "gas_injection_12x12x3"]
+         "gas_injection_12x12x3", "three_phase_16x16x3", "wells_surface_oil_6x6",
+         "wells_surface_gas_6x6", "wells_rv_liquid_6x6", "wells_surface_water_6x6"]
+
+
+def solve_tol(cfg):
+    """FGMRES tolerance (Jacobi-scaled relative residual) for a parity run.
+
+    With a BHP well the well row anchors the pressure level and 1e-13 is well
+    above the residual's rounding floor.  With rate wells only, nothing but the
+    accumulation term PV*c_t/dt anchors it, so ||D^-1 b|| is small against ||x||:
+    the exact solution's own relative residual is ~3.5e-13 on the three-phase
+    16x16x3 system, with a rounding floor near 8.5e-13.  A 1e-13 request there
+    can never be met (every step would be retried at dt/2), so those cases ask
+    for 1e-11, which bounds the pressure error near 6e-10 relative."""
+    bhp = any(str(w.get("control_type", w.get("control", {}).get("type", ""))) == "bhp"
+              for w in cfg["wells"])
+    return 1e-13 if bhp else 1e-11
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
@@ -22,11 +38,12 @@ def test_trajectory_matches_reference(golden, name, precision):
     reference's trajectory with an exact pressure solve."""
     g = golden(name)
     cfg, f = cfg_fields(g)
-    _, fl, _, sim = gpu_sim(cfg, f, tol=1e-13, norm="jacobi", precision=precision, max_iters=400,
-                            restart=40)
+    _, fl, _, sim = gpu_sim(cfg, f, tol=solve_tol(cfg), norm="jacobi", precision=precision,
+                            max_iters=400, restart=40)
     dt = float(g["dt"])
     for s in range(g["p"].shape[0]):
-        sim.run_step(dt)
+        assert sim.run_step(dt)
+        assert sim.last_krylov["converged"], (s, sim.last_krylov)
         p = to_np(fl.pressure)
         assert np.abs(p - g["p"][s]).max() <= 1e-8 * np.abs(g["p"][s]).max(), (s, sim.last_krylov)
         assert np.abs(to_np(fl.s_w) - g["sw"][s]).max() <= 1e-8
@@ -166,11 +183,12 @@ def test_bhp_min_autoswitch_and_limits():
     assert wm3.get_wells()[0].last_surface_rates["oil"] <= 100.0 * 1.10
 
 
-def test_reference_cg_solver_matches_reference(golden):
+@pytest.mark.parametrize("name", ["cg_two_phase_20x16x2", "cg_three_phase_16x16x3"])
+def test_reference_cg_solver_matches_reference(golden, name):
     """pressure_solver "cg": the reference's own Jacobi-PCG path end to end
     (simulation.py:931-966, 1662-1697), against the trajectory the reference
-    produced with it."""
-    g = golden("cg_two_phase_20x16x2")
+    produced with it (two phases, and three phases with free gas)."""
+    g = golden(name)
     cfg, f = cfg_fields(g)
     assert cfg["simulation"]["pressure_solver"] == "cg"
     _, fl, _, sim = gpu_sim(cfg, f)

@@ -234,3 +234,56 @@ def test_equilibrated_stopping_test_accepts_a_wrong_pressure(golden):
         assert jac < prev[0] and err < prev[1]
         prev = (jac, err)
     assert err < 0.1 and jac < 5e-3
+
+
+def test_interpolation_truncation_rule():
+    """The truncation option on a hand-made P: F rows keep their kmax largest
+    weights (ties to the earlier entry), drop those below tf times the largest,
+    and keep their row sum; C rows and short rows are untouched."""
+    import scipy.sparse as sp
+    from oracle.amg import truncate_interpolation
+    P = sp.csr_matrix(np.array([[0.1, 0.4, 0.2, 0.3],     # F: keeps 0.4, 0.3
+                                [1.0, 0.0, 0.0, 0.0],     # C row
+                                [0.25, 0.25, 0.25, 0.25],  # F: ties -> first two
+                                [0.0, 0.0, 0.6, 0.0]]))    # F, single entry
+    cf = np.array([1, 0, 1, 1])
+    T = truncate_interpolation(P, cf, kmax=2).toarray()
+    np.testing.assert_allclose(T[0], [0.0, 0.4 / 0.7, 0.0, 0.3 / 0.7])
+    np.testing.assert_allclose(T[1], [1.0, 0.0, 0.0, 0.0])
+    np.testing.assert_allclose(T[2], [0.5, 0.5, 0.0, 0.0])
+    np.testing.assert_allclose(T[3], [0.0, 0.0, 0.6, 0.0])
+    np.testing.assert_allclose(T.sum(axis=1), P.toarray().sum(axis=1))
+    U = truncate_interpolation(P, cf, kmax=0, tf=0.5).toarray()      # only 0.1 < 0.5 * 0.4
+    np.testing.assert_allclose(U[0], [0.0, 0.4 / 0.9, 0.2 / 0.9, 0.3 / 0.9])
+    np.testing.assert_allclose(U[2], P.toarray()[2])
+
+
+def test_chebyshev_smoother_polynomial():
+    """The oracle's Chebyshev smoother (an option of the GPU library) against the
+    closed form of the method: on a diagonal operator the error after nu updates
+    from x0 is e0 * T_nu((theta - lambda)/delta) / T_nu(theta/delta), T_nu the
+    Chebyshev polynomial of the first kind (Saad, Alg. 12.1)."""
+    import scipy.sparse as sp
+    from numpy.polynomial import chebyshev as npc
+    from oracle.amg import cheb_lmax, cheb_smooth
+    lam = np.linspace(0.05, 2.0, 40)
+    A = sp.diags(lam).tocsr()
+    inv = np.ones_like(lam)
+    lmax = cheb_lmax(A, inv)
+    assert lmax == 2.0
+    rng = np.random.default_rng(3)
+    xs = rng.standard_normal(lam.size)
+    b = A @ xs
+    x0 = rng.standard_normal(lam.size)
+    lower = 0.3
+    theta, delta = 0.5 * (lmax + lower * lmax), 0.5 * (lmax - lower * lmax)
+    for nu in (1, 2, 3, 4):
+        x = cheb_smooth(A, inv, lmax, x0.copy(), b, nu, lower)
+        T = npc.Chebyshev.basis(nu)
+        factor = T((theta - lam) / delta) / T(theta / delta)
+        np.testing.assert_allclose(x - xs, factor * (x0 - xs), rtol=1e-10, atol=1e-12)
+    # from zero the same polynomial acts on e0 = -xs
+    x = cheb_smooth(A, inv, lmax, None, b, 3, lower, zero_x=True)
+    T = npc.Chebyshev.basis(3)
+    np.testing.assert_allclose(x - xs, T((theta - lam) / delta) / T(theta / delta) * (-xs), rtol=1e-10,
+                               atol=1e-12)

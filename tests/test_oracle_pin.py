@@ -15,7 +15,9 @@ TRAJ = ["two_phase_32x32", "two_phase_64x64", "two_phase_16x16x2", "black_oil_10
 
 
 def model_from(g):
-    return Model(json.loads(str(g["cfg"])), g["kx"], g["ky"], g["kz"], g["poro"])
+    from gpu_util import fixture_fields
+    f = fixture_fields(g)
+    return Model(json.loads(str(g["cfg"])), f["kx"], f["ky"], f["kz"], f["poro"])
 
 
 @pytest.mark.parametrize("name", TRAJ)
@@ -170,3 +172,28 @@ def test_oracle_cg_trajectory_matches_reference(golden, name):
         assert np.abs(m.p - g["p"][s]).max() <= 1e-9 * np.abs(g["p"][s]).max()
         assert np.abs(m.sw - g["sw"][s]).max() <= 1e-9
         assert np.abs(m.sg - g["sg"][s]).max() <= 1e-9
+
+
+@pytest.mark.parametrize("name", ["config0_64x64x1_100steps", "config3_64x64x8_50steps"])
+def test_oracle_long_trajectory_matches_reference(golden, name):
+    """The 64x64x1 benchmark case for all of its 100 daily steps and the
+    64x64x8 adjoint-case grid for its 50 two-day steps: p (1e-12 relative) and
+    Sw (1e-12) at 2,048 fixed cells every step and on the whole field at the
+    recorded steps; balances at the end."""
+    g = golden(name)
+    m = model_from(g)
+    dt = float(g["dt"])
+    full_at = [int(v) for v in g["full_at"]]
+    idx = g["sample_idx"]
+    for st in range(1, int(g["steps"]) + 1):
+        m.step(dt)
+        ps = g["p_s"][st - 1]
+        assert np.abs(m.p[idx] - ps).max() <= 1e-12 * np.abs(ps).max(), st
+        assert np.abs(m.sw[idx] - g["sw_s"][st - 1]).max() <= 1e-12, st
+        if st in full_at:
+            q = full_at.index(st)
+            assert np.abs(m.p - g["p"][q]).max() <= 1e-12 * np.abs(g["p"][q]).max(), st
+            assert np.abs(m.sw - g["sw"][q]).max() <= 1e-12, st
+    bal = np.array([m.mass_balance[ph][io] for ph in ("water", "oil", "gas") for io in ("in", "out")])
+    ref = g["balances"][-1][:6]
+    assert np.all(np.abs(bal - ref) <= 1e-10 * np.maximum(np.abs(ref), 1e-30) + 1e-300)

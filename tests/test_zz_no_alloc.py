@@ -70,3 +70,27 @@ def test_noalloc_rejects_more_rows_than_its_work_space():
     # the handle stays usable
     s, _, _, _ = _solve("impes_amg_solve_vcycles", amg, b, 1e-6, 3, 0)
     assert s == 0
+
+
+def test_noalloc_after_fp32_update_of_a_mixed_hierarchy(golden):
+    """A mixed-precision hierarchy refreshed by update_matrix holds only its fp32
+    Galerkin chain; the fp64 levels are rebuilt on the next fp64 solve.  The
+    no-alloc solve runs first after each update, so it is the call that rebuilds
+    them (into the buffers made at setup), and must still equal the allocating
+    solve, on two consecutive updates."""
+    from impes_b200.amg import ClassicalAMG
+    t = golden("two_phase_32x32")
+    n = len(t["A0_crow"]) - 1
+    A = sp.csr_matrix((t["A0_val"], t["A0_col"], t["A0_crow"]), shape=(n, n))
+    amg = ClassicalAMG(A, coarsest_size=50, seed=3, mixed_precision=True)
+    rng = np.random.default_rng(5)
+    for call, q in enumerate((1, 2)):
+        val = torch.tensor(t["A_val_all"][q], device="cuda", dtype=torch.float64)
+        amg.update_values(val)
+        b = torch.tensor(t["b_all"][q], device="cuda", dtype=torch.float64)
+        b = b + 1e-3 * b.abs().max() * torch.tensor(rng.standard_normal(n), device="cuda")
+        s1, x1, c1, r1 = _solve("impes_amg_solve_vcycles_noalloc", amg, b, 1e-9, 30, 1)
+        s0, x0, c0, r0 = _solve("impes_amg_solve_vcycles", amg, b, 1e-9, 30, 1)
+        assert s0 == 0 and s1 == 0, call
+        assert c1 == c0 and abs(r1 - r0) <= 1e-12 * max(r0, 1e-300), (call, c0, c1, r0, r1)
+        assert torch.linalg.norm(x1 - x0) <= 1e-12 * torch.linalg.norm(x0), call
