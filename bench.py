@@ -218,7 +218,7 @@ class ClockSampler:
 
 
 def make_sim(cfg, fields, precision, device, restart=30, solver="gmres_amg", warm_start="extrapolate",
-             trunc=0):
+             trunc=0, smoother="l1jacobi"):
     """FGMRES + V-cycle (solver="gmres_amg"), or the plain stand-alone V-cycles of
     the reference (solver="amg"), both stopping at PRESSURE_TOL in the Jacobi norm;
     `trunc` caps the interpolation's row length (0: the reference's interpolation)."""
@@ -227,7 +227,8 @@ def make_sim(cfg, fields, precision, device, restart=30, solver="gmres_amg", war
     c["simulation"]["pressure_solver"] = solver
     c["simulation"]["amg"].update({"tol": PRESSURE_TOL, "norm": "jacobi", "precision": precision,
                                    "restart": restart, "max_iters": 600, "max_cycles": 3000, "seed": 0,
-                                   "warm_start": warm_start, "p_max_elements": int(trunc)})
+                                   "warm_start": warm_start, "p_max_elements": int(trunc),
+                                   "smoother": smoother})
     return build_from_config(c, fields, device=device)
 
 
@@ -432,7 +433,7 @@ def run_variant(args, cfg, fields, precision, device, dt, flush, stream, dist, r
     from impes_b200 import _lib
     _, fl, _, sim = make_sim(cfg, fields, precision, device, restart=args.restart,
                              warm_start=False if args.warm_start == "zero" else args.warm_start,
-                             trunc=trunc)
+                             trunc=trunc, smoother=args.smoother)
     pv = sim.porous_volume.reshape(fl.s_w.shape)
     m0 = total_mass(fl, pv)
     torch.cuda.synchronize()
@@ -564,7 +565,7 @@ def run_ours(args, world, rank, local):
     steps = args.steps
     if args.precision != "both":
         r = results[(args.precision, trunc)]
-        print(json.dumps({"precision": args.precision, "p_max_elements": trunc,
+        print(json.dumps({"precision": args.precision, "p_max_elements": trunc, "smoother": args.smoother,
                           "ms_per_step": r["ms"] / steps, "vcycles_per_step": statistics.mean(r["iters"]),
                           "operator_complexity": r["oc"], "levels": r["levels"],
                           "phases": r["phases"], "gpu_launches": r["launches"]}), flush=True)
@@ -700,6 +701,8 @@ def main():
     ap.add_argument("--p-max-elements", type=int, default=DEFAULT_P_MAX,
                     help="interpolation row cap of the benchmarked hierarchy (0: the reference's "
                          "interpolation)")
+    ap.add_argument("--smoother", choices=["l1jacobi", "chebyshev"], default="l1jacobi",
+                    help="V-cycle smoother of the benchmarked hierarchy")
     ap.add_argument("--no-reference-hierarchy", action="store_true",
                     help="skip the measurement on the reference's own interpolation")
     ap.add_argument("--ensemble-loop-steps", type=int, default=3,

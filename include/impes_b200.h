@@ -85,6 +85,8 @@ typedef struct {
   int is_coarsest;
   int col_index_bytes;   /* 2 or 4: column storage of the smoothing/residual passes */
   int col_row_relative;  /* 1: 16-bit columns hold col - row + 32768              */
+  int lanes[6];          /* autotuned lanes per row of the kernels on A, R (restriction)
+                            and P (prolongation): [0..2] fp64, [3..5] fp32; 0 = rule  */
 } impes_amg_level_desc;
 
 /* Norms for Krylov stopping tests. */

@@ -172,6 +172,11 @@ int impes_amg_level_info(impes_amg* h, int lvl, impes_amg_level_desc* info) {
     info->is_coarsest = L.coarsest ? 1 : 0;
     info->col_index_bytes = L.col16.p ? 2 : 4;
     info->col_row_relative = L.col16.p ? L.col16_rel : 0;
+    for (int q = 0; q < 2; ++q) {
+      info->lanes[3 * q + 0] = L.lpr_a[q];
+      info->lanes[3 * q + 1] = L.lpr_r[q];
+      info->lanes[3 * q + 2] = L.lpr_p[q];
+    }
   });
 }
 

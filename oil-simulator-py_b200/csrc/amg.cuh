@@ -18,6 +18,9 @@ struct Level {
   // the fp64 values, [1] from the fp32 chain (atomicMax of non-negative doubles)
   DBuf<unsigned long long> cheb_lmax;
   int avg_row = 7;                 // nnz / n, selects the SpMV row mapping
+  // autotuned lanes per row ([0] fp64, [1] fp32; 0 = the mean-row-length rule)
+  // of the kernels on A (sweeps, residuals), R (restriction) and P (prolongation)
+  int lpr_a[2] = {0, 0}, lpr_r[2] = {0, 0}, lpr_p[2] = {0, 0};
   bool coarsest = false;
   // interpolation P (n x nc) and restriction R = P^T (nc x n)
   int nc = 0, pnnz = 0;
@@ -119,6 +122,9 @@ void amg_fgmres(AMG& h, const double* b, double* x, const impes_krylov_params& k
 void spmv(const Level& L, const double* x, double* y, cudaStream_t s);
 double dot_host(AMG& h, const double* a, const double* b, int n, cudaStream_t s);
 void coarse_factor(AMG& h, Level& L, cudaStream_t s, bool from_fp32 = false);
+// Times the CSR kernels of every level with each lanes-per-row choice and keeps
+// the fastest (amg_cycle.cu); choices are cached per level shape for the process.
+void amg_autotune(AMG& h, cudaStream_t s);
 // Brings the fp64 coarse levels up to date after an fp32 update (no-op otherwise).
 void amg_ensure_fp64(AMG& h, cudaStream_t s);
 void level_precision_copies(AMG& h, Level& L, cudaStream_t s);

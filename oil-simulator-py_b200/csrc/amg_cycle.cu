@@ -11,7 +11,9 @@
 #include "amg.cuh"
 #include <algorithm>
 #include <cmath>
+#include <map>
 #include <mutex>
+#include <tuple>
 
 // handle accessors (abi.cu)
 bool impes_amg_handle_built(impes_amg* h);
@@ -42,6 +44,7 @@ __global__ void __launch_bounds__(TB) k_csr(int n, const int* __restrict__ rowpt
                                             const CT* __restrict__ col, const T* __restrict__ val,
                                             const T* __restrict__ x, const T* __restrict__ b,
                                             const T* __restrict__ inv, T* __restrict__ y, int rel) {
+  pdl_wait_release();
   const int g = threadIdx.x / LPR, lane = threadIdx.x % LPR;
   const int rows_per_block = TB / LPR;
   for (long long row = (long long)blockIdx.x * rows_per_block + g; row < n;
@@ -77,6 +80,7 @@ __global__ void __launch_bounds__(TB) k_csr_rows(int n, const int* __restrict__ 
                                                  const CT* __restrict__ col, const T* __restrict__ val,
                                                  const T* __restrict__ x, const T* __restrict__ b,
                                                  const T* __restrict__ inv, T* __restrict__ y, int rel) {
+  pdl_wait_release();
   constexpr int kWarps = TB / 32, kRows = kWarps / WPR, G = 32 * WPR;
   __shared__ T part[kWarps];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -142,6 +146,7 @@ __global__ void __launch_bounds__(TB) k_csr_stream(int n, const int* __restrict_
                                                    const float* __restrict__ x, const float* __restrict__ b,
                                                    const float* __restrict__ inv, float* __restrict__ y,
                                                    int rel) {
+  pdl_wait_release();
   constexpr int kWarps = TB / 32;
   constexpr int kCh = sizeof(CT) == 2 ? 512 : 384;   // 48 KB of stages per block
   __shared__ __align__(16) float s_val[kWarps][2][kCh];
@@ -222,17 +227,17 @@ void launch_wide(int n, int avg, const int* rowptr, const CT* col, const T* val,
   if constexpr (sizeof(T) == 4) {
     constexpr double kStreamMinBytes = 48.0 * (1 << 20);
     if (avg > 512 && (double)n * avg * (sizeof(T) + sizeof(CT)) >= kStreamMinBytes) {
-      k_csr_stream<CT, MODE><<<grid(8), TB, 0, s>>>(n, rowptr, col, (const float*)val, (const float*)x,
-                                                    (const float*)b, (const float*)inv, (float*)y, rel); ::impes::count_launch();
+      launch_pdl(k_csr_stream<CT, MODE>, grid(8), TB, 0, s, n, rowptr, col, (const float*)val, (const float*)x,
+                                                    (const float*)b, (const float*)inv, (float*)y, rel);
       return;
     }
   }
   if (avg <= 512) {
-    k_csr_rows<T, CT, MODE, 1><<<grid(8), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y, rel); ::impes::count_launch();
+    launch_pdl(k_csr_rows<T, CT, MODE, 1>, grid(8), TB, 0, s, n, rowptr, col, val, x, b, inv, y, rel);
   } else if (avg <= 1536) {
-    k_csr_rows<T, CT, MODE, 2><<<grid(4), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y, rel); ::impes::count_launch();
+    launch_pdl(k_csr_rows<T, CT, MODE, 2>, grid(4), TB, 0, s, n, rowptr, col, val, x, b, inv, y, rel);
   } else {
-    k_csr_rows<T, CT, MODE, 4><<<grid(2), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y, rel); ::impes::count_launch();
+    launch_pdl(k_csr_rows<T, CT, MODE, 4>, grid(2), TB, 0, s, n, rowptr, col, val, x, b, inv, y, rel);
   }
 }
 
@@ -241,24 +246,31 @@ void launch_lanes(int lpr, int n, const int* rowptr, const CT* col, const T* val
                   const T* b, const T* inv, T* y, int rel, cudaStream_t s) {
   auto grid = [&](int l) { return grid_for(((size_t)n * l + TB - 1) / TB * TB, TB, 16); };
   switch (lpr) {
-    case 1: k_csr<T, CT, 1, MODE><<<grid(1), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y, rel); break;
-    case 4: k_csr<T, CT, 4, MODE><<<grid(4), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y, rel); break;
-    case 8: k_csr<T, CT, 8, MODE><<<grid(8), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y, rel); break;
-    default: k_csr<T, CT, 16, MODE><<<grid(16), TB, 0, s>>>(n, rowptr, col, val, x, b, inv, y, rel); break;
+    case 1: launch_pdl(k_csr<T, CT, 1, MODE>, grid(1), TB, 0, s, n, rowptr, col, val, x, b, inv, y, rel); break;
+    case 2: launch_pdl(k_csr<T, CT, 2, MODE>, grid(2), TB, 0, s, n, rowptr, col, val, x, b, inv, y, rel); break;
+    case 4: launch_pdl(k_csr<T, CT, 4, MODE>, grid(4), TB, 0, s, n, rowptr, col, val, x, b, inv, y, rel); break;
+    case 8: launch_pdl(k_csr<T, CT, 8, MODE>, grid(8), TB, 0, s, n, rowptr, col, val, x, b, inv, y, rel); break;
+    case 16: launch_pdl(k_csr<T, CT, 16, MODE>, grid(16), TB, 0, s, n, rowptr, col, val, x, b, inv, y, rel); break;
+    default: launch_pdl(k_csr<T, CT, 32, MODE>, grid(32), TB, 0, s, n, rowptr, col, val, x, b, inv, y, rel); break;
   }
-  ::impes::count_launch();
 }
 
+// Lanes per row by mean row length (the rule used until a level is autotuned).
+inline int default_lpr(int avg) { return avg <= 8 ? 1 : avg <= 16 ? 4 : avg <= 48 ? 8 : avg <= 96 ? 16 : 32; }
+
 // col16 / rel: the level's columns as 16-bit indices (absolute when rel is 0,
-// row - 32768 + col16 when rel is 1), or null for the int columns.
+// row - 32768 + col16 when rel is 1), or null for the int columns.  lpr > 0
+// (an autotuned choice, rows of at most 96 entries on average) overrides the
+// lanes per row.
 template <typename T, int MODE>
 void launch_csr(int n, int avg, const int* rowptr, const int* col, const T* val, const T* x,
                 const T* b, const T* inv, T* y, cudaStream_t s,
-                const unsigned short* col16 = nullptr, int rel = 0) {
+                const unsigned short* col16 = nullptr, int rel = 0, int lpr_tuned = 0) {
   if (n <= 0) return;
-  int lpr = avg <= 8 ? 1 : avg <= 16 ? 4 : avg <= 48 ? 8 : avg <= 96 ? 16 : 32;
+  int lpr = default_lpr(avg);
+  if (lpr_tuned > 0 && avg <= 96) lpr = lpr_tuned;
   if (MODE == Y_SMOOTH0) lpr = 1;
-  if (lpr < 32) {
+  if (lpr < 32 || (lpr_tuned == 32 && avg <= 96)) {
     if (col16) launch_lanes<T, unsigned short, MODE>(lpr, n, rowptr, col16, val, x, b, inv, y, rel, s);
     else launch_lanes<T, int, MODE>(lpr, n, rowptr, col, val, x, b, inv, y, 0, s);
   } else {
@@ -308,6 +320,7 @@ __global__ void __launch_bounds__(TB) k_cheb(int n, const int* __restrict__ rowp
                                              const T* __restrict__ inv, T* __restrict__ r,
                                              T* __restrict__ x, T* __restrict__ dnext, int rel,
                                              ChebArgs ca) {
+  pdl_wait_release();
   double theta, c1, c2;
   cheb_coeffs(ca, theta, c1, c2);
   const int g = threadIdx.x / LPR, lane = threadIdx.x % LPR;
@@ -343,6 +356,7 @@ __global__ void __launch_bounds__(TB) k_cheb(int n, const int* __restrict__ rowp
 template <typename T>
 __global__ void k_cheb_init0(int n, const T* __restrict__ b, const T* __restrict__ inv, T* __restrict__ r,
                              T* __restrict__ d, T* __restrict__ x, ChebArgs ca) {
+  pdl_wait_release();
   double theta, c1, c2;
   cheb_coeffs(ca, theta, c1, c2);
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
@@ -355,6 +369,7 @@ __global__ void k_cheb_init0(int n, const T* __restrict__ b, const T* __restrict
 }
 template <typename T>
 __global__ void k_cheb_add(int n, const T* __restrict__ d, T* __restrict__ x) {
+  pdl_wait_release();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
     x[i] = x[i] + d[i];
@@ -362,17 +377,19 @@ __global__ void k_cheb_add(int n, const T* __restrict__ d, T* __restrict__ x) {
 
 template <typename T, typename CT, int MODE>
 void launch_cheb_ct(int n, int avg, const int* rowptr, const CT* col, const T* val, const T* v, const T* b,
-                    const T* inv, T* r, T* x, T* dnext, int rel, const ChebArgs& ca, cudaStream_t s) {
-  const int lpr = avg <= 8 ? 1 : avg <= 16 ? 4 : avg <= 48 ? 8 : avg <= 96 ? 16 : 32;
+                    const T* inv, T* r, T* x, T* dnext, int rel, const ChebArgs& ca, cudaStream_t s,
+                    int lpr_tuned = 0) {
+  const int lpr = (lpr_tuned > 0 && avg <= 96) ? lpr_tuned
+                  : (avg <= 8 ? 1 : avg <= 16 ? 4 : avg <= 48 ? 8 : avg <= 96 ? 16 : 32);
   auto grid = [&](int l) { return grid_for(((size_t)n * l + TB - 1) / TB * TB, TB, 16); };
   switch (lpr) {
-    case 1: k_cheb<T, CT, 1, MODE><<<grid(1), TB, 0, s>>>(n, rowptr, col, val, v, b, inv, r, x, dnext, rel, ca); break;
-    case 4: k_cheb<T, CT, 4, MODE><<<grid(4), TB, 0, s>>>(n, rowptr, col, val, v, b, inv, r, x, dnext, rel, ca); break;
-    case 8: k_cheb<T, CT, 8, MODE><<<grid(8), TB, 0, s>>>(n, rowptr, col, val, v, b, inv, r, x, dnext, rel, ca); break;
-    case 16: k_cheb<T, CT, 16, MODE><<<grid(16), TB, 0, s>>>(n, rowptr, col, val, v, b, inv, r, x, dnext, rel, ca); break;
-    default: k_cheb<T, CT, 32, MODE><<<grid(32), TB, 0, s>>>(n, rowptr, col, val, v, b, inv, r, x, dnext, rel, ca); break;
+    case 1: launch_pdl(k_cheb<T, CT, 1, MODE>, grid(1), TB, 0, s, n, rowptr, col, val, v, b, inv, r, x, dnext, rel, ca); break;
+    case 2: launch_pdl(k_cheb<T, CT, 2, MODE>, grid(2), TB, 0, s, n, rowptr, col, val, v, b, inv, r, x, dnext, rel, ca); break;
+    case 4: launch_pdl(k_cheb<T, CT, 4, MODE>, grid(4), TB, 0, s, n, rowptr, col, val, v, b, inv, r, x, dnext, rel, ca); break;
+    case 8: launch_pdl(k_cheb<T, CT, 8, MODE>, grid(8), TB, 0, s, n, rowptr, col, val, v, b, inv, r, x, dnext, rel, ca); break;
+    case 16: launch_pdl(k_cheb<T, CT, 16, MODE>, grid(16), TB, 0, s, n, rowptr, col, val, v, b, inv, r, x, dnext, rel, ca); break;
+    default: launch_pdl(k_cheb<T, CT, 32, MODE>, grid(32), TB, 0, s, n, rowptr, col, val, v, b, inv, r, x, dnext, rel, ca); break;
   }
-  ::impes::count_launch();
   IMPES_CHECK_LAUNCH();
 }
 
@@ -380,16 +397,21 @@ void launch_cheb_ct(int n, int avg, const int* rowptr, const CT* col, const T* v
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (n); i += (long long)gridDim.x * blockDim.x)
 
 template <typename A, typename B>
-__global__ void k_convert(long long n, const A* in, B* out) { GRID_LOOP(i, n) out[i] = (B)in[i]; }
+__global__ void k_convert(long long n, const A* in, B* out) {
+  pdl_wait_release(); GRID_LOOP(i, n) out[i] = (B)in[i]; }
 template <typename A, typename B>
 __global__ void k_div_convert(long long n, const A* in, const double* w, B* out) {
+  pdl_wait_release();
   GRID_LOOP(i, n) out[i] = (B)(in[i] / w[i]);
 }
 __global__ void k_mul(long long n, const double* a, const double* b, double* out) {
+  pdl_wait_release();
   GRID_LOOP(i, n) out[i] = a[i] * b[i];
 }
-__global__ void k_mul_inplace(long long n, double* a, const double* b) { GRID_LOOP(i, n) a[i] *= b[i]; }
-__global__ void k_zero(long long n, double* a) { GRID_LOOP(i, n) a[i] = 0.0; }
+__global__ void k_mul_inplace(long long n, double* a, const double* b) {
+  pdl_wait_release(); GRID_LOOP(i, n) a[i] *= b[i]; }
+__global__ void k_zero(long long n, double* a) {
+  pdl_wait_release(); GRID_LOOP(i, n) a[i] = 0.0; }
 
 // ---------------------------------------------------- deterministic dots
 constexpr int kDotBlocks = 296;   // 2 x 148 SMs, fixed so partials have a fixed order
@@ -399,6 +421,7 @@ constexpr int kMD = 8;            // vectors per multi-dot launch
 __global__ void __launch_bounds__(TB) k_multidot(long long n, const double* __restrict__ Vbase,
                                                  long long ldv, int k, const double* __restrict__ w,
                                                  double* __restrict__ partial) {
+  pdl_wait_release();
   __shared__ double s[kMD][TB / 32];
   double acc[kMD];
 #pragma unroll
@@ -422,8 +445,58 @@ __global__ void __launch_bounds__(TB) k_multidot(long long n, const double* __re
     partial[threadIdx.x * kDotBlocks + blockIdx.x] = t;
   }
 }
+// Gram-Schmidt dots of FGMRES in one launch: block (x, g) sums, over its slice
+// of rows, V[q] . w for the 8 vectors q = 8g .. 8g+7 below k, and w . w as
+// vector q = k when self is set; partial[q * kDotBlocks + x].  With pred set
+// the launch does nothing unless *pred is non-zero (the optional second
+// Gram-Schmidt pass, decided on the device).
+__global__ void __launch_bounds__(TB) k_multidot_g(long long n, const double* __restrict__ Vbase,
+                                                   long long ldv, int k, int self,
+                                                   const double* __restrict__ w,
+                                                   double* __restrict__ partial, const int* pred) {
+  pdl_wait_release();
+  if (pred && *pred == 0) return;
+  __shared__ double s[kMD][TB / 32];
+  const int q0 = blockIdx.y * kMD;
+  const int kk = k + (self ? 1 : 0);
+  double acc[kMD];
+#pragma unroll
+  for (int u = 0; u < kMD; ++u) acc[u] = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double wi = w[i];
+#pragma unroll
+    for (int u = 0; u < kMD; ++u) {
+      const int q = q0 + u;
+      if (q < k) acc[u] += Vbase[q * ldv + i] * wi;
+      else if (q == k && self) acc[u] += wi * wi;
+    }
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int u = 0; u < kMD; ++u) {
+    double v = warp_sum(acc[u]);
+    if (lane == 0) s[u][wid] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < kMD && q0 + (int)threadIdx.x < kk) {
+    double t = 0.0;
+    for (int u = 0; u < TB / 32; ++u) t += s[threadIdx.x][u];
+    partial[(q0 + threadIdx.x) * kDotBlocks + blockIdx.x] = t;
+  }
+}
+// Second Gram-Schmidt pass wanted when the first pass left less than 0.7 of the
+// vector's norm ("twice is enough", Giraud, Langou & Rozloznik 2005):
+// flag = ||w'||^2 < 0.49 ||w||^2.
+__global__ void k_reorth_flag(const double* nrm2_after, const double* nrm2_before, int* flag) {
+  pdl_wait_release();
+  *flag = (*nrm2_after < 0.49 * *nrm2_before) ? 1 : 0;
+}
 // out[q] (+)= sum of partials, fixed order
-__global__ void k_dot_finalize(int k, const double* partial, double* out, int accumulate) {
+__global__ void k_dot_finalize(int k, const double* partial, double* out, int accumulate,
+                               const int* pred = nullptr) {
+  pdl_wait_release();
+  if (pred && *pred == 0) return;
   const int q = blockIdx.x;
   double t = 0.0;
   for (int b = threadIdx.x; b < kDotBlocks; b += 32) t += partial[q * kDotBlocks + b];
@@ -434,7 +507,10 @@ __global__ void k_dot_finalize(int k, const double* partial, double* out, int ac
 // w -= sum_q h[q] V[q]; optionally partial norms of the result
 __global__ void __launch_bounds__(TB) k_update(long long n, const double* __restrict__ Vbase,
                                                long long ldv, int k, const double* __restrict__ h,
-                                               double* __restrict__ w, double* __restrict__ partial) {
+                                               double* __restrict__ w, double* __restrict__ partial,
+                                               const int* pred = nullptr) {
+  pdl_wait_release();
+  if (pred && *pred == 0) return;
   __shared__ double sh[128];
   __shared__ double s[TB / 32];
   for (int q = threadIdx.x; q < k; q += blockDim.x) sh[q] = h[q];
@@ -458,6 +534,7 @@ __global__ void __launch_bounds__(TB) k_update(long long n, const double* __rest
   }
 }
 __global__ void k_scale_by_inv_sqrt(long long n, const double* in, double* out, const double* nrm2) {
+  pdl_wait_release();
   const double inv = 1.0 / sqrt(*nrm2);
   GRID_LOOP(i, n) out[i] = in[i] * inv;
 }
@@ -575,6 +652,7 @@ template <typename T>
 __global__ void k_coarse_apply(int n, const double* __restrict__ Apin, const double* __restrict__ Afree,
                                const int* __restrict__ free_singular, int krylov,
                                const T* __restrict__ b, T* __restrict__ x) {
+  pdl_wait_release();
   extern __shared__ double s_b[];
   const bool use_free = krylov && Afree != nullptr && *free_singular == 0;
   const double* Ainv = use_free ? Afree : Apin;
@@ -590,7 +668,8 @@ __global__ void k_coarse_apply(int n, const double* __restrict__ Apin, const dou
   }
 }
 template <typename T>
-__global__ void k_pin_copy(int n, const T* b, T* out) { GRID_LOOP(i, n) out[i] = (i == 0) ? T(0) : b[i]; }
+__global__ void k_pin_copy(int n, const T* b, T* out) {
+  pdl_wait_release(); GRID_LOOP(i, n) out[i] = (i == 0) ? T(0) : b[i]; }
 
 }  // namespace
 
@@ -631,8 +710,8 @@ void spmv(const Level& L, const double* x, double* y, cudaStream_t s) {
 
 double dot_host(AMG& h, const double* a, const double* b, int n, cudaStream_t s) {
   h.red.ensure((size_t)kMD * kDotBlocks);
-  k_multidot<<<kDotBlocks, TB, 0, s>>>(n, a, 0, 1, b, h.red.p); ::impes::count_launch();
-  k_dot_finalize<<<1, 32, 0, s>>>(1, h.red.p, h.scal.p, 0); ::impes::count_launch();
+  launch_pdl(k_multidot, kDotBlocks, TB, 0, s, n, a, 0, 1, b, h.red.p);
+  launch_pdl(k_dot_finalize, 1, 32, 0, s, 1, (const double*)h.red.p, h.scal.p, 0, (const int*)nullptr);
   IMPES_CHECK_LAUNCH();
   IMPES_CUDA(cudaMemcpyAsync(h.hbuf.p, h.scal.p, sizeof(double), cudaMemcpyDeviceToHost, s));
   IMPES_CUDA(cudaStreamSynchronize(s));
@@ -694,20 +773,19 @@ T* smooth_cheb(const AMG& h, Level& L, T* x, const T* b, int nu, bool zero_x, cu
   const double si = L.col16.p ? 2.0 : 4.0;
   const bool wide = L.avg_row > 96;
   if (zero_x) {
-    k_cheb_init0<T><<<grid_for(L.n, TB), TB, 0, s>>>(L.n, b, LV<T>::inv(L), r, dc, nu == 1 ? x : nullptr, ca);
-    ::impes::count_launch();
+    launch_pdl(k_cheb_init0<T>, grid_for(L.n, TB), TB, 0, s, L.n, b, LV<T>::inv(L), r, dc, nu == 1 ? x : nullptr, ca);
     IMPES_CHECK_LAUNCH();
   } else {
     const int tid = top ? timers().begin(IMPES_PH_SMOOTH_L0, s) : (wide ? timers().begin(IMPES_PH_SMOOTH_WIDE, s) : -1);
     if (L.col16.p)
       launch_cheb_ct<T, unsigned short, CH_INIT>(L.n, L.avg_row, L.rowptr.p, L.col16.p, LV<T>::val(L), x, b,
-                                                 LV<T>::inv(L), r, x, dc, L.col16_rel, ca, s);
+                                                 LV<T>::inv(L), r, x, dc, L.col16_rel, ca, s, L.lpr_a[LV<T>::slot]);
     else
       launch_cheb_ct<T, int, CH_INIT>(L.n, L.avg_row, L.rowptr.p, L.col.p, LV<T>::val(L), x, b, LV<T>::inv(L),
-                                      r, x, dc, 0, ca, s);
+                                      r, x, dc, 0, ca, s, L.lpr_a[LV<T>::slot]);
     timers().end(tid, s, sweep_bytes(sizeof(T), L.nnz, L.n, si));
     if (nu == 1) {
-      k_cheb_add<T><<<grid_for(L.n, TB), TB, 0, s>>>(L.n, dc, x); ::impes::count_launch();
+      launch_pdl(k_cheb_add<T>, grid_for(L.n, TB), TB, 0, s, L.n, dc, x);
       IMPES_CHECK_LAUNCH();
     }
   }
@@ -718,10 +796,11 @@ T* smooth_cheb(const AMG& h, Level& L, T* x, const T* b, int nu, bool zero_x, cu
     const int tid = top ? timers().begin(IMPES_PH_SMOOTH_L0, s) : (wide ? timers().begin(IMPES_PH_SMOOTH_WIDE, s) : -1);
     if (L.col16.p)
       launch_cheb_ct<T, unsigned short, CH_STEP>(L.n, L.avg_row, L.rowptr.p, L.col16.p, LV<T>::val(L), dc,
-                                                 nullptr, LV<T>::inv(L), r, x, dn, L.col16_rel, ca, s);
+                                                 nullptr, LV<T>::inv(L), r, x, dn, L.col16_rel, ca, s,
+                                                 L.lpr_a[LV<T>::slot]);
     else
       launch_cheb_ct<T, int, CH_STEP>(L.n, L.avg_row, L.rowptr.p, L.col.p, LV<T>::val(L), dc, nullptr,
-                                      LV<T>::inv(L), r, x, dn, 0, ca, s);
+                                      LV<T>::inv(L), r, x, dn, 0, ca, s, L.lpr_a[LV<T>::slot]);
     timers().end(tid, s, cheb_bytes(sizeof(T), L.nnz, L.n, si));
     std::swap(dc, dn);
   }
@@ -747,7 +826,7 @@ T* smooth(const AMG& h, Level& L, T* x, T* spare, const T* b, int nu, bool zero_
     const int tid = top ? timers().begin(IMPES_PH_SMOOTH_L0, s)
                         : (wide ? timers().begin(IMPES_PH_SMOOTH_WIDE, s) : -1);
     launch_csr<T, Y_SMOOTH>(L.n, L.avg_row, L.rowptr.p, L.col.p, LV<T>::val(L), x, b,
-                            LV<T>::inv(L), spare, s, L.col16.p, L.col16_rel);
+                            LV<T>::inv(L), spare, s, L.col16.p, L.col16_rel, L.lpr_a[LV<T>::slot]);
     timers().end(tid, s, sweep_bytes(sizeof(T), L.nnz, L.n, L.col16.p ? 2.0 : 4.0));
     std::swap(x, spare);
   }
@@ -783,14 +862,14 @@ T* vcycle(AMG& h, int l, bool zero_x, cudaStream_t s) {
   if (L.coarsest) {
     if (L.n <= 500) {
       const int n = L.n;
-      k_coarse_apply<T><<<std::max(1, (n + 7) / 8), 256, n * sizeof(double), s>>>(
-          n, L.lu.p, L.lu_free.p, h.iflag.p + 3, h.krylov_mode ? 1 : 0, LV<T>::b(L), LV<T>::x(L)); ::impes::count_launch();
+      launch_pdl(k_coarse_apply<T>, std::max(1, (n + 7) / 8), 256, n * sizeof(double), s, 
+          n, L.lu.p, L.lu_free.p, h.iflag.p + 3, h.krylov_mode ? 1 : 0, LV<T>::b(L), LV<T>::x(L));
       IMPES_CHECK_LAUNCH();
       return LV<T>::x(L);
     }
     // n > 500: 50 l1-Jacobi sweeps from zero on the pinned right-hand side
     T* bp = LV<T>::r(L);
-    k_pin_copy<T><<<grid_for(L.n, TB), TB, 0, s>>>(L.n, LV<T>::b(L), bp); ::impes::count_launch();
+    launch_pdl(k_pin_copy<T>, grid_for(L.n, TB), TB, 0, s, L.n, LV<T>::b(L), bp);
     return smooth<T>(h, L, LV<T>::x(L), LV<T>::t(L), bp, 50, true, s, false, true);
   }
   const int tid = (l == 0) ? timers().begin(IMPES_PH_VCYCLE, s) : -1;
@@ -798,11 +877,12 @@ T* vcycle(AMG& h, int l, bool zero_x, cudaStream_t s) {
   T* spare = (x == LV<T>::x(L)) ? LV<T>::t(L) : LV<T>::x(L);
   Level& Nc = *h.levels[l + 1];
   launch_csr<T, Y_B_MINUS_AX>(L.n, L.avg_row, L.rowptr.p, L.col.p, LV<T>::val(L), x, LV<T>::b(L),
-                              nullptr, LV<T>::r(L), s, L.col16.p, L.col16_rel);
+                              nullptr, LV<T>::r(L), s, L.col16.p, L.col16_rel, L.lpr_a[LV<T>::slot]);
   launch_csr<T, Y_AX>(L.nc, L.r_avg, L.rrow.p, L.rcol.p, LV<T>::rval(L), LV<T>::r(L), nullptr,
-                      nullptr, LV<T>::b(Nc), s);
+                      nullptr, LV<T>::b(Nc), s, nullptr, 0, L.lpr_r[LV<T>::slot]);
   T* ec = vcycle<T>(h, l + 1, true, s);
-  launch_csr<T, Y_ADD_AX>(L.n, L.p_avg, L.prow.p, L.pcol.p, LV<T>::pval(L), ec, nullptr, nullptr, x, s);
+  launch_csr<T, Y_ADD_AX>(L.n, L.p_avg, L.prow.p, L.pcol.p, LV<T>::pval(L), ec, nullptr, nullptr, x, s,
+                          nullptr, 0, L.lpr_p[LV<T>::slot]);
   T* out = smooth<T>(h, L, x, spare, LV<T>::b(L), 2, false, s, l == 0);
   timers().end(tid, s, vcycle_bytes<T>(h, l));
   return out;
@@ -847,6 +927,110 @@ T* vcycle_top(AMG& h, bool zero_x, cudaStream_t s) {
 
 }  // namespace
 
+// ------------------------------------------------------------- autotuner
+// Lanes per row of the CSR kernels, picked from timed trials per level: the
+// l1-Jacobi sweep stands for the kernels on A (sweeps, residuals, Chebyshev
+// steps, the FGMRES operator), Y_AX on R for the restriction and Y_ADD_AX on P
+// for the prolongation.  Each candidate (1, 2, 4, 8, 16, 32 lanes, at most four
+// times the mean row length) runs twice untimed and four times between CUDA
+// events on the level's own work vectors.  The first choice made for a shape
+// (precision, operator, log2 of the rows in halves, mean row length) is kept
+// for the whole process, so hierarchies of the same shape -- a rebuilt one, or
+// ensemble members alike in size -- launch the same kernels and sum in the same
+// order.  Levels with more than 96 entries per row keep the warps-per-row
+// kernels.  IMPES_NO_TUNE=1 keeps the mean-row-length rule.
+namespace {
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int>, int> g_tune_cache;
+
+template <typename T, int MODE>
+float time_lpr(int lpr, int n, int avg, const int* rowptr, const int* col, const T* val, const T* x,
+               const T* b, const T* inv, T* y, const unsigned short* col16, int rel, cudaStream_t s,
+               cudaEvent_t e0, cudaEvent_t e1) {
+  for (int w = 0; w < 2; ++w) launch_csr<T, MODE>(n, avg, rowptr, col, val, x, b, inv, y, s, col16, rel, lpr);
+  IMPES_CUDA(cudaEventRecord(e0, s));
+  for (int w = 0; w < 4; ++w) launch_csr<T, MODE>(n, avg, rowptr, col, val, x, b, inv, y, s, col16, rel, lpr);
+  IMPES_CUDA(cudaEventRecord(e1, s));
+  IMPES_CUDA(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  IMPES_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  return ms;
+}
+
+template <typename T, int MODE>
+int tune_one(int slot, int kind, int n, int avg, const int* rowptr, const int* col, const T* val, const T* x,
+             const T* b, const T* inv, T* y, const unsigned short* col16, int rel, cudaStream_t s,
+             cudaEvent_t e0, cudaEvent_t e1) {
+  if (n <= 0 || avg > 96) return 0;
+  const int nb = (int)std::lround(2.0 * std::log2((double)n));
+  const auto key = std::make_tuple(slot, kind, nb, avg);
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) return it->second;
+  }
+  int best = default_lpr(avg);
+  float best_ms = 1e30f;
+  for (int lpr : {1, 2, 4, 8, 16, 32}) {
+    if (lpr > 1 && lpr > 4 * avg) break;
+    const float ms = time_lpr<T, MODE>(lpr, n, avg, rowptr, col, val, x, b, inv, y, col16, rel, s, e0, e1);
+    if (ms < best_ms) { best_ms = ms; best = lpr; }
+  }
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  auto ins = g_tune_cache.emplace(key, best);   // another thread may have decided first
+  return ins.first->second;
+}
+
+template <typename T>
+void tune_levels(AMG& h, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1) {
+  const int slot = LV<T>::slot;
+  for (auto& up : h.levels) {
+    Level& L = *up;
+    if (L.coarsest || !LV<T>::val(L)) continue;
+    L.lpr_a[slot] = tune_one<T, Y_SMOOTH>(slot, 0, L.n, L.avg_row, L.rowptr.p, L.col.p, LV<T>::val(L),
+                                          LV<T>::x(L), LV<T>::b(L), LV<T>::inv(L), LV<T>::t(L), L.col16.p,
+                                          L.col16_rel, s, e0, e1);
+    L.lpr_r[slot] = tune_one<T, Y_AX>(slot, 1, L.nc, L.r_avg, L.rrow.p, L.rcol.p, LV<T>::rval(L), LV<T>::r(L),
+                                      nullptr, nullptr, LV<T>::t(*h.levels[&up - &h.levels[0] + 1]), nullptr, 0,
+                                      s, e0, e1);
+    L.lpr_p[slot] = tune_one<T, Y_ADD_AX>(slot, 2, L.n, L.p_avg, L.prow.p, L.pcol.p, LV<T>::pval(L),
+                                          LV<T>::x(*h.levels[&up - &h.levels[0] + 1]), nullptr, nullptr,
+                                          LV<T>::t(L), nullptr, 0, s, e0, e1);
+  }
+}
+}  // namespace
+
+void amg_autotune(AMG& h, cudaStream_t s) {
+  {
+    const char* ev = getenv("IMPES_NO_TUNE");
+    if (ev && ev[0] == '1') return;
+  }
+  cudaEvent_t e0, e1;
+  IMPES_CUDA(cudaEventCreate(&e0));
+  IMPES_CUDA(cudaEventCreate(&e1));
+  try {
+    // the work vectors hold whatever they hold: clear them so the trial
+    // kernels read finite numbers
+    for (auto& L : h.levels) {
+      const size_t n = std::max(L->n, 1);
+      IMPES_CUDA(cudaMemsetAsync(L->x.p, 0, n * sizeof(double), s));
+      IMPES_CUDA(cudaMemsetAsync(L->b.p, 0, n * sizeof(double), s));
+      IMPES_CUDA(cudaMemsetAsync(L->r.p, 0, n * sizeof(double), s));
+      IMPES_CUDA(cudaMemsetAsync(L->xf.p, 0, n * sizeof(float), s));
+      IMPES_CUDA(cudaMemsetAsync(L->bf.p, 0, n * sizeof(float), s));
+      IMPES_CUDA(cudaMemsetAsync(L->rf.p, 0, n * sizeof(float), s));
+    }
+    tune_levels<double>(h, s, e0, e1);
+    if (h.prm.mixed_precision) tune_levels<float>(h, s, e0, e1);
+  } catch (...) {
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+}
+
 // V-cycle on the equilibrated system: xs = V(0, bs)  (FP64 or FP32 inside)
 void amg_vcycle_scaled(AMG& h, const double* bs, double* xs, int precision, cudaStream_t s) {
   if (precision == 0) amg_ensure_fp64(h, s);
@@ -854,9 +1038,9 @@ void amg_vcycle_scaled(AMG& h, const double* bs, double* xs, int precision, cuda
   const int n = L0.n;
   if (precision == 1) {
     IMPES_REQUIRE(h.prm.mixed_precision, IMPES_ERR_STATE, "fp32 V-cycle needs mixed_precision=1");
-    k_convert<double, float><<<grid_for(n, TB), TB, 0, s>>>(n, bs, L0.bf.p); ::impes::count_launch();
+    launch_pdl(k_convert<double, float>, grid_for(n, TB), TB, 0, s, n, bs, L0.bf.p);
     float* x = vcycle_top<float>(h, true, s);
-    k_convert<float, double><<<grid_for(n, TB), TB, 0, s>>>(n, x, xs); ::impes::count_launch();
+    launch_pdl(k_convert<float, double>, grid_for(n, TB), TB, 0, s, n, x, xs);
   } else {
     IMPES_CUDA(cudaMemcpyAsync(L0.b.p, bs, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     double* x = vcycle_top<double>(h, true, s);
@@ -873,10 +1057,10 @@ void amg_solve_vcycles(AMG& h, const double* b, double* x, double tol, int max_c
   Level& L0 = *h.levels[0];
   const int n = L0.n;
   DBuf<double> bs(n), r(n), wb(n);
-  k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, h.dhalf_inv.p, b, bs.p); ::impes::count_launch();
+  launch_pdl(k_mul, grid_for(n, TB), TB, 0, s, n, h.dhalf_inv.p, b, bs.p);
   IMPES_CHECK_LAUNCH();
   const bool jac = norm == IMPES_NORM_JACOBI;
-  if (jac) { k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, h.jac_w.p, bs.p, wb.p); ::impes::count_launch(); }
+  if (jac) { launch_pdl(k_mul, grid_for(n, TB), TB, 0, s, n, h.jac_w.p, bs.p, wb.p); }
   const double bn = std::sqrt(jac ? dot_host(h, wb.p, wb.p, n, s) : dot_host(h, bs.p, bs.p, n, s));
   IMPES_CUDA(cudaMemcpyAsync(L0.b.p, bs.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
   double rr = INFINITY;
@@ -889,13 +1073,13 @@ void amg_solve_vcycles(AMG& h, const double* b, double* x, double tol, int max_c
     xs = L0.x.p;
     launch_csr<double, Y_B_MINUS_AX>(n, L0.avg_row, L0.rowptr.p, L0.col.p, L0.val.p, xs, bs.p,
                                      nullptr, r.p, s);
-    if (jac) { k_mul_inplace<<<grid_for(n, TB), TB, 0, s>>>(n, r.p, h.jac_w.p); ::impes::count_launch(); }
+    if (jac) { launch_pdl(k_mul_inplace, grid_for(n, TB), TB, 0, s, n, r.p, h.jac_w.p); }
     rr = std::sqrt(dot_host(h, r.p, r.p, n, s)) / (bn + 1e-30);
     if (!(rr == rr)) throw Error(IMPES_ERR_NAN, "NaN residual in V-cycle solve");
     if (rr < tol) break;
   }
   if (c > max_cycles) c = max_cycles;
-  k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, h.dhalf_inv.p, L0.x.p, x); ::impes::count_launch();
+  launch_pdl(k_mul, grid_for(n, TB), TB, 0, s, n, h.dhalf_inv.p, L0.x.p, x);
   IMPES_CHECK_LAUNCH();
   if (cycles) *cycles = c;
   if (rel) *rel = rr;
@@ -908,7 +1092,7 @@ void amg_apply(AMG& h, const double* b, double* x, int cycles, double apply_tol,
   Level& L0 = *h.levels[0];
   const int n = L0.n;
   DBuf<double> bs(n), r(n);
-  k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, h.dhalf_inv.p, b, bs.p); ::impes::count_launch();
+  launch_pdl(k_mul, grid_for(n, TB), TB, 0, s, n, h.dhalf_inv.p, b, bs.p);
   IMPES_CUDA(cudaMemcpyAsync(L0.b.p, bs.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
   const double bn = std::sqrt(dot_host(h, bs.p, bs.p, n, s));
   int c = 0;
@@ -922,7 +1106,7 @@ void amg_apply(AMG& h, const double* b, double* x, int cycles, double apply_tol,
     double rel = std::sqrt(dot_host(h, r.p, r.p, n, s)) / (bn + 1e-30);
     if (c >= cycles && rel < apply_tol) break;
   }
-  k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, h.dhalf_inv.p, L0.x.p, x); ::impes::count_launch();
+  launch_pdl(k_mul, grid_for(n, TB), TB, 0, s, n, h.dhalf_inv.p, L0.x.p, x);
   IMPES_CHECK_LAUNCH();
 }
 
@@ -930,6 +1114,7 @@ void amg_apply(AMG& h, const double* b, double* x, int cycles, double apply_tol,
 namespace {
 
 __global__ void k_givens(int j, int ldh, double* H, double* cs, double* sn, double* g, double* est) {
+  pdl_wait_release();
   double* hj = H + (long long)j * ldh;  // column j, rows 0..j+1
   for (int i = 0; i < j; ++i) {
     double t = cs[i] * hj[i] + sn[i] * hj[i + 1];
@@ -946,10 +1131,12 @@ __global__ void k_givens(int j, int ldh, double* H, double* cs, double* sn, doub
   *est = fabs(g[j + 1]);
 }
 __global__ void k_set_hcol(int j, int ldh, double* H, const double* nrm2) {
+  pdl_wait_release();
   H[(long long)j * ldh + j + 1] = sqrt(*nrm2);
 }
 // y = R^{-1} g (upper triangular k x k, column-major with leading dim ldh)
 __global__ void k_backsolve(int k, int ldh, const double* H, const double* g, double* y) {
+  pdl_wait_release();
   for (int i = k - 1; i >= 0; --i) {
     double s = g[i];
     for (int j = i + 1; j < k; ++j) s -= H[(long long)j * ldh + i] * y[j];
@@ -958,6 +1145,7 @@ __global__ void k_backsolve(int k, int ldh, const double* H, const double* g, do
 }
 __global__ void k_combine(long long n, const double* __restrict__ Z, long long ldz, int k,
                           const double* __restrict__ y, double* __restrict__ x) {
+  pdl_wait_release();
   __shared__ double sy[128];
   for (int q = threadIdx.x; q < k; q += blockDim.x) sy[q] = y[q];
   __syncthreads();
@@ -967,11 +1155,15 @@ __global__ void k_combine(long long n, const double* __restrict__ Z, long long l
     x[i] = v;
   }
 }
-__global__ void k_hadd(int k, double* h, const double* y) {
+__global__ void k_hadd(int k, double* h, const double* y, const int* pred) {
+  pdl_wait_release();
+  if (pred && *pred == 0) return;
   for (int i = threadIdx.x; i < k; i += blockDim.x) h[i] += y[i];
 }
-__global__ void k_fill(long long n, double* a, double v) { GRID_LOOP(i, n) a[i] = v; }
+__global__ void k_fill(long long n, double* a, double v) {
+  pdl_wait_release(); GRID_LOOP(i, n) a[i] = v; }
 __global__ void k_init_g(double* g, int m1, const double* nrm2) {
+  pdl_wait_release();
   for (int i = 0; i < m1; ++i) g[i] = 0.0;
   g[0] = sqrt(*nrm2);
 }
@@ -1012,26 +1204,26 @@ void amg_fgmres(AMG& h, const double* b, double* x, const impes_krylov_params& k
     h.kw.alloc(n); h.kb.alloc(n); h.kx.alloc(n);
     h.krylov_m = m;
   }
-  h.red.ensure((size_t)kMD * kDotBlocks + kDotBlocks);
+  h.red.ensure((size_t)(m + 2) * kDotBlocks + kDotBlocks);
   const int ldh = m + 2;
   const bool jac = kp.norm == IMPES_NORM_JACOBI;
   double* wt = jac ? h.jac_w.p : h.kw.p;
-  if (!jac) { k_fill<<<grid_for(n, TB), TB, 0, s>>>(n, h.kw.p, 1.0); ::impes::count_launch(); }
+  if (!jac) { launch_pdl(k_fill, grid_for(n, TB), TB, 0, s, n, h.kw.p, 1.0); }
   double* bs = h.kb.p;   // b_s = dhalf .* b
   double* xs = h.kx.p;   // x_s
-  k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, h.dhalf_inv.p, b, bs); ::impes::count_launch();
+  launch_pdl(k_mul, grid_for(n, TB), TB, 0, s, n, h.dhalf_inv.p, b, bs);
   if (kp.use_x0)
-    { k_div_convert<double, double><<<grid_for(n, TB), TB, 0, s>>>(n, x, h.dhalf_inv.p, xs); ::impes::count_launch(); }
+    { launch_pdl(k_div_convert<double, double>, grid_for(n, TB), TB, 0, s, n, x, h.dhalf_inv.p, xs); }
   else
-    { k_zero<<<grid_for(n, TB), TB, 0, s>>>(n, xs); ::impes::count_launch(); }
+    { launch_pdl(k_zero, grid_for(n, TB), TB, 0, s, n, xs); }
   IMPES_CHECK_LAUNCH();
   double* r0 = h.V.p;
-  k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, wt, bs, r0); ::impes::count_launch();
+  launch_pdl(k_mul, grid_for(n, TB), TB, 0, s, n, wt, bs, r0);
   const double bnorm = std::sqrt(dot_host(h, r0, r0, n, s));
   st = impes_krylov_stats{0, 0, 0, 0.0, 0.0};
   if (!(bnorm > 0.0)) {
     if (!(bnorm == bnorm)) throw Error(IMPES_ERR_NAN, "non-finite right-hand side");
-    k_zero<<<grid_for(n, TB), TB, 0, s>>>(n, x); ::impes::count_launch();
+    launch_pdl(k_zero, grid_for(n, TB), TB, 0, s, n, x);
     st.converged = 1;
     return;
   }
@@ -1045,9 +1237,9 @@ void amg_fgmres(AMG& h, const double* b, double* x, const impes_krylov_params& k
     // V[0] = wt .* (b_s - A_s x_s), beta = ||V[0]||
     launch_csr<double, Y_B_MINUS_AX>(n, L0.avg_row, L0.rowptr.p, L0.col.p, L0.val.p, xs, bs,
                                      nullptr, h.V.p, s);
-    k_mul_inplace<<<grid_for(n, TB), TB, 0, s>>>(n, h.V.p, wt); ::impes::count_launch();
-    k_multidot<<<kDotBlocks, TB, 0, s>>>(n, h.V.p, 0, 1, h.V.p, h.red.p); ::impes::count_launch();
-    k_dot_finalize<<<1, 32, 0, s>>>(1, h.red.p, dscal, 0); ::impes::count_launch();
+    launch_pdl(k_mul_inplace, grid_for(n, TB), TB, 0, s, n, h.V.p, wt);
+    launch_pdl(k_multidot, kDotBlocks, TB, 0, s, n, h.V.p, 0, 1, h.V.p, h.red.p);
+    launch_pdl(k_dot_finalize, 1, 32, 0, s, 1, (const double*)h.red.p, dscal, 0, (const int*)nullptr);
     IMPES_CUDA(cudaMemcpyAsync(h.hbuf.p, dscal, sizeof(double), cudaMemcpyDeviceToHost, s));
     IMPES_CUDA(cudaStreamSynchronize(s));
     const double beta = std::sqrt(h.hbuf.p[0]);
@@ -1055,8 +1247,8 @@ void amg_fgmres(AMG& h, const double* b, double* x, const impes_krylov_params& k
     est_rel = beta / bnorm;
     st.rel_res = est_rel;
     if (est_rel < kp.tol || total >= kp.max_iters) break;
-    k_init_g<<<1, 1, 0, s>>>(h.g.p, m + 1, dscal); ::impes::count_launch();
-    k_scale_by_inv_sqrt<<<grid_for(n, TB), TB, 0, s>>>(n, h.V.p, h.V.p, dscal); ::impes::count_launch();
+    launch_pdl(k_init_g, 1, 1, 0, s, h.g.p, m + 1, dscal);
+    launch_pdl(k_scale_by_inv_sqrt, grid_for(n, TB), TB, 0, s, n, h.V.p, h.V.p, dscal);
     int j = 0;
     for (; j < m && total < kp.max_iters; ++j) {
       double* vj = h.V.p + (size_t)j * n;
@@ -1064,37 +1256,44 @@ void amg_fgmres(AMG& h, const double* b, double* x, const impes_krylov_params& k
       double* w = h.V.p + (size_t)(j + 1) * n;
       // z_j = V(v_j ./ wt)
       if (prec == 1) {
-        k_div_convert<double, float><<<grid_for(n, TB), TB, 0, s>>>(n, vj, wt, L0.bf.p); ::impes::count_launch();
+        launch_pdl(k_div_convert<double, float>, grid_for(n, TB), TB, 0, s, n, vj, wt, L0.bf.p);
         float* zf = vcycle_top<float>(h, true, s);
-        k_convert<float, double><<<grid_for(n, TB), TB, 0, s>>>(n, zf, zj); ::impes::count_launch();
+        launch_pdl(k_convert<float, double>, grid_for(n, TB), TB, 0, s, n, zf, zj);
       } else {
-        k_div_convert<double, double><<<grid_for(n, TB), TB, 0, s>>>(n, vj, wt, L0.b.p); ::impes::count_launch();
+        launch_pdl(k_div_convert<double, double>, grid_for(n, TB), TB, 0, s, n, vj, wt, L0.b.p);
         double* zd = vcycle_top<double>(h, true, s);
         IMPES_CUDA(cudaMemcpyAsync(zj, zd, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
       }
       // w = wt .* (A_s z_j)
       const int tsp = timers().begin(IMPES_PH_SPMV_L0, s);
       launch_csr<double, Y_W_AX>(n, L0.avg_row, L0.rowptr.p, L0.col.p, L0.val.p, zj, nullptr, wt, w, s,
-                                 L0.col16.p, L0.col16_rel);
+                                 L0.col16.p, L0.col16_rel, L0.lpr_a[0]);
       timers().end(tsp, s, spmv_bytes(8.0, 8.0, L0.nnz, n, n, L0.col16.p ? 2.0 : 4.0) + 8.0 * n);
+      // classical Gram-Schmidt; the second pass only when the first cancelled
+      // more than 0.3 of the norm (flag on the device).  H[j+1, j] holds
+      // ||w||^2 before the first pass until k_set_hcol overwrites it.
       const int tor = timers().begin(IMPES_PH_ORTHO, s);
       double* hcol = h.H.p + (size_t)j * ldh;
-      for (int pass = 0; pass < 2; ++pass) {
-        double* coef = pass == 0 ? hcol : h.y.p;
-        for (int q0 = 0; q0 <= j; q0 += kMD) {
-          int k = std::min(kMD, j + 1 - q0);
-          k_multidot<<<kDotBlocks, TB, 0, s>>>(n, h.V.p + (size_t)q0 * n, n, k, w, h.red.p); ::impes::count_launch();
-          k_dot_finalize<<<k, 32, 0, s>>>(k, h.red.p, coef + q0, 0); ::impes::count_launch();
-        }
-        k_update<<<kDotBlocks, TB, 0, s>>>(n, h.V.p, n, j + 1, coef, w,
-                                           pass == 1 ? h.red.p : nullptr); ::impes::count_launch();
-      }
-      k_hadd<<<1, 128, 0, s>>>(j + 1, hcol, h.y.p); ::impes::count_launch();
-      k_dot_finalize<<<1, 32, 0, s>>>(1, h.red.p, dscal, 0); ::impes::count_launch();   // ||w||^2 from k_update
-      k_set_hcol<<<1, 1, 0, s>>>(j, ldh, h.H.p, dscal); ::impes::count_launch();
-      k_scale_by_inv_sqrt<<<grid_for(n, TB), TB, 0, s>>>(n, w, w, dscal); ::impes::count_launch();
+      int* reorth = h.iflag.p + 4;
+      const dim3 g1(kDotBlocks, (unsigned)((j + 2 + kMD - 1) / kMD));
+      launch_pdl(k_multidot_g, g1, dim3(TB), 0, s, (long long)n, (const double*)h.V.p, (long long)n, j + 1, 1,
+                 (const double*)w, h.red.p, (const int*)nullptr);
+      launch_pdl(k_dot_finalize, j + 2, 32, 0, s, j + 2, (const double*)h.red.p, hcol, 0, (const int*)nullptr);
+      launch_pdl(k_update, kDotBlocks, TB, 0, s, n, h.V.p, n, j + 1, hcol, w, h.red.p, (const int*)nullptr);
+      launch_pdl(k_dot_finalize, 1, 32, 0, s, 1, (const double*)h.red.p, dscal, 0, (const int*)nullptr);
+      launch_pdl(k_reorth_flag, 1, 1, 0, s, (const double*)dscal, (const double*)(hcol + j + 1), reorth);
+      const dim3 g2(kDotBlocks, (unsigned)((j + 1 + kMD - 1) / kMD));
+      launch_pdl(k_multidot_g, g2, dim3(TB), 0, s, (long long)n, (const double*)h.V.p, (long long)n, j + 1, 0,
+                 (const double*)w, h.red.p, (const int*)reorth);
+      launch_pdl(k_dot_finalize, j + 1, 32, 0, s, j + 1, (const double*)h.red.p, h.y.p, 0, (const int*)reorth);
+      launch_pdl(k_update, kDotBlocks, TB, 0, s, n, h.V.p, n, j + 1, (const double*)h.y.p, w, h.red.p,
+                 (const int*)reorth);
+      launch_pdl(k_dot_finalize, 1, 32, 0, s, 1, (const double*)h.red.p, dscal, 0, (const int*)reorth);
+      launch_pdl(k_hadd, 1, 128, 0, s, j + 1, hcol, (const double*)h.y.p, (const int*)reorth);
+      launch_pdl(k_set_hcol, 1, 1, 0, s, j, ldh, h.H.p, dscal);
+      launch_pdl(k_scale_by_inv_sqrt, grid_for(n, TB), TB, 0, s, n, w, w, dscal);
       timers().end(tor, s, 8.0 * n * (2.0 * (j + 1) + 3.0));
-      k_givens<<<1, 1, 0, s>>>(j, ldh, h.H.p, h.cs.p, h.sn.p, h.g.p, dscal + 1); ::impes::count_launch();
+      launch_pdl(k_givens, 1, 1, 0, s, j, ldh, h.H.p, h.cs.p, h.sn.p, h.g.p, dscal + 1);
       IMPES_CHECK_LAUNCH();
       ++total;
       IMPES_CUDA(cudaMemcpyAsync(h.hbuf.p, dscal + 1, sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -1105,15 +1304,15 @@ void amg_fgmres(AMG& h, const double* b, double* x, const impes_krylov_params& k
       if (est_rel < kp.tol) { ++j; break; }
     }
     // x_s += Z y with y = R^-1 g; the loop head re-checks the true residual
-    k_backsolve<<<1, 1, 0, s>>>(j, ldh, h.H.p, h.g.p, h.y.p); ::impes::count_launch();
-    k_combine<<<grid_for(n, TB), TB, 0, s>>>(n, h.Z.p, n, j, h.y.p, xs); ::impes::count_launch();
+    launch_pdl(k_backsolve, 1, 1, 0, s, j, ldh, h.H.p, h.g.p, h.y.p);
+    launch_pdl(k_combine, grid_for(n, TB), TB, 0, s, n, h.Z.p, n, j, h.y.p, xs);
     IMPES_CHECK_LAUNCH();
     st.restarts++;
   }
   st.iterations = total;
   st.converged = est_rel < kp.tol;
   st.true_rel_res = est_rel;
-  k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, h.dhalf_inv.p, xs, x); ::impes::count_launch();
+  launch_pdl(k_mul, grid_for(n, TB), TB, 0, s, n, h.dhalf_inv.p, xs, x);
   IMPES_CHECK_LAUNCH();
 }
 
@@ -1194,10 +1393,10 @@ void solve_vcycles_noalloc(AMG& h, const double* b, double* x, double tol, int m
   double* bs = base;
   double* r = base + kNoAllocMaxRows;
   double* wb = base + 2 * (size_t)kNoAllocMaxRows;
-  k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, h.dhalf_inv.p, b, bs); ::impes::count_launch();
+  launch_pdl(k_mul, grid_for(n, TB), TB, 0, s, n, h.dhalf_inv.p, b, bs);
   IMPES_CHECK_LAUNCH();
   const bool jac = norm == IMPES_NORM_JACOBI;
-  if (jac) { k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, h.jac_w.p, bs, wb); ::impes::count_launch(); }
+  if (jac) { launch_pdl(k_mul, grid_for(n, TB), TB, 0, s, n, h.jac_w.p, bs, wb); }
   const double bn = std::sqrt(jac ? dot_host(h, wb, wb, n, s) : dot_host(h, bs, bs, n, s));
   IMPES_CUDA(cudaMemcpyAsync(L0.b.p, bs, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
   double rr = INFINITY;
@@ -1208,13 +1407,13 @@ void solve_vcycles_noalloc(AMG& h, const double* b, double* x, double tol, int m
       IMPES_CUDA(cudaMemcpyAsync(L0.x.p, xs, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     launch_csr<double, Y_B_MINUS_AX>(n, L0.avg_row, L0.rowptr.p, L0.col.p, L0.val.p, L0.x.p, bs,
                                      nullptr, r, s);
-    if (jac) { k_mul_inplace<<<grid_for(n, TB), TB, 0, s>>>(n, r, h.jac_w.p); ::impes::count_launch(); }
+    if (jac) { launch_pdl(k_mul_inplace, grid_for(n, TB), TB, 0, s, n, r, h.jac_w.p); }
     rr = std::sqrt(dot_host(h, r, r, n, s)) / (bn + 1e-30);
     if (!(rr == rr)) throw Error(IMPES_ERR_NAN, "NaN residual in V-cycle solve");
     if (rr < tol) break;
   }
   if (c > max_cycles) c = max_cycles;
-  k_mul<<<grid_for(n, TB), TB, 0, s>>>(n, h.dhalf_inv.p, L0.x.p, x); ::impes::count_launch();
+  launch_pdl(k_mul, grid_for(n, TB), TB, 0, s, n, h.dhalf_inv.p, L0.x.p, x);
   IMPES_CHECK_LAUNCH();
   if (cycles) *cycles = c;
   if (rel) *rel = rr;

@@ -1459,6 +1459,7 @@ void amg_setup(AMG& h, int n, int nnz, const int* rowptr, const int* col, const 
     IMPES_CHECK_LAUNCH();
   }
   IMPES_CUDA(cudaStreamSynchronize(s));
+  amg_autotune(h, s);
   h.built = true;
 }
 

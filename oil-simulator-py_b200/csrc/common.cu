@@ -1,6 +1,7 @@
 // Shared host utilities: thread-local error text and a device exclusive scan.
 #include "common.cuh"
 #include <atomic>
+#include <cstdlib>
 #include <map>
 #include <mutex>
 
@@ -34,6 +35,14 @@ void raise_smem_limit(const void* kernel, size_t bytes) {
   }
 }
 const char* last_error_cstr() { return g_last_error.c_str(); }
+
+bool pdl_enabled() {
+  static const bool on = [] {
+    const char* ev = getenv("IMPES_NO_PDL");
+    return !(ev && ev[0] == '1');
+  }();
+  return on;
+}
 
 PhaseTimers& timers() {
   static PhaseTimers t;

@@ -7,6 +7,7 @@
 #include <string>
 #include <vector>
 #include <stdexcept>
+#include <utility>
 
 #include "../../include/impes_b200.h"
 
@@ -115,6 +116,36 @@ inline unsigned grid_for(size_t n, int block, int max_per_sm = 8) {
   size_t cap = (size_t)num_sms() * max_per_sm * 8;
   if (g > cap) g = cap;
   return (unsigned)(g ? g : 1);
+}
+
+// ------------------------------------------- programmatic dependent launch
+// Kernels of the solver chains (V-cycle, FGMRES) start with pdl_wait_release():
+// griddepcontrol.wait holds the kernel until the grid it depends on has
+// completed and its memory is visible (a no-op when the kernel was launched
+// without the programmatic attribute), then launch_dependents lets the next
+// kernel of the stream launch at once, so its blocks are scheduled while this
+// grid runs and wait on the device instead of after a launch gap.  Only kernels
+// that begin with this call may be launched through launch_pdl.
+__device__ __forceinline__ void pdl_wait_release() {
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+}
+// false when the environment sets IMPES_NO_PDL=1 (plain stream order)
+bool pdl_enabled();
+template <typename... P, typename... A>
+void launch_pdl(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, A&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = pdl_enabled() ? 1 : 0;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  IMPES_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...));
+  count_launch();
 }
 
 // --------------------------------------------------------- device helpers

@@ -607,9 +607,10 @@ class Simulator:
         self._wells_stale = False
 
     def amg_levels(self):
-        """[(n, nnz, p_cols, p_nnz, is_coarsest, columns)] of the pressure hierarchy;
-        columns is the index storage of the level's sweeps: "i32", "u16" or
-        "u16rel" (16-bit offsets from the row)."""
+        """[(n, nnz, p_cols, p_nnz, is_coarsest, columns, lanes)] of the pressure
+        hierarchy; columns is the index storage of the level's sweeps: "i32",
+        "u16" or "u16rel" (16-bit offsets from the row); lanes the autotuned lanes
+        per row of the kernels on A, R and P (fp64 then fp32; 0: the default rule)."""
         if self._amg_h is None:
             return []
         nl = C.c_int(0)
@@ -619,7 +620,7 @@ class Simulator:
             d = _lib.LevelDesc()
             check(lib.impes_amg_level_info(self._amg_h, l, C.byref(d)))
             cols = "i32" if d.col_index_bytes == 4 else ("u16rel" if d.col_row_relative else "u16")
-            out.append((d.n, d.nnz, d.p_cols, d.p_nnz, bool(d.is_coarsest), cols))
+            out.append((d.n, d.nnz, d.p_cols, d.p_nnz, bool(d.is_coarsest), cols, tuple(d.lanes)))
         return out
 
     # --------------------------------------------------- building blocks

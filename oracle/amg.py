@@ -462,7 +462,7 @@ class AMG:
     # -------------------------------------------------------------- cycling
     def smooth(self, l, x, b, nu, zero_x=False):
         lv = self.levels[l]
-        if self.smoother == "chebyshev":
+        if getattr(self, "smoother", "l1jacobi") == "chebyshev":
             lmax = cheb_lmax(lv["A"], lv["inv_relax"])
             return cheb_smooth(lv["A"], lv["inv_relax"], lmax, x, b, nu, self.cheb_lower, zero_x)
         for _ in range(nu):

@@ -1,7 +1,8 @@
 """Generate the golden fixtures by running the reference itself (build container only).
 
 Usage:  python tests/golden/make_golden.py REFERENCE_ROOT [--pcg-only | --three-phase-only |
-                                                        --wells-only | --amg-3d-only | --configs-only]
+                                                        --wells-only | --amg-3d-only | --configs-only |
+                                                        --adjoint-only]
 
 REFERENCE_ROOT is a checkout of researchim-ai/oil-simulator-py (the directory
 holding ``src/``); it may instead be given in the environment variable
@@ -429,6 +430,116 @@ def config_fixtures(which=("config0", "config3", "config1")):
                        keep_systems=1, generator=(fn, kwargs))
 
 
+def reference_producer_rates(cfg, fields, steps, dt, grad=False):
+    """Producer oil rates [steps x producers] (m3/day) of the reference's own IMPES
+    steps with the pressure solved densely (torch.linalg.solve, so autograd runs
+    through it), and -- with grad -- the leaf tensors (delta ln k of every cell,
+    scaling kx, ky and kz together, and porosity) to differentiate against.
+
+    The rate is the flux balance of the producer's pressure row built from the
+    reference's own terms: q = sum_f c_f (p_nb - p_c) - acc_c (p_c - p_prev,c)
+    + Qg_c, times the oil fractional flow mob_o / (mob_t + 1e-10) at the step's
+    starting state.  c_f are the upwinded face coefficients the reference hands
+    to _build_pressure_matrix_vectorized, acc = PV ct / dt as that function forms
+    it, and Qg the gravity part of _build_pressure_rhs (its right-hand side with
+    the well terms zeroed, less the accumulation term).  The well's own
+    WI lambda (p_c - p_bhp) is the same number algebraically but round-off."""
+    shape = fields["kx"].shape
+    delta = torch.zeros(shape, dtype=torch.float64, requires_grad=grad)
+    poro = torch.tensor(np.array(fields["poro"]), dtype=torch.float64).requires_grad_(grad)
+    rec = {}
+    orig_mat, orig_rhs = Simulator._build_pressure_matrix_vectorized, Simulator._build_pressure_rhs
+
+    def mat(self, Tx, Ty, Tz, dt_, wb):
+        try:
+            ct = self.fluid.calc_total_compressibility(self.fluid.pressure, self.fluid.s_w, self.fluid.s_g)
+            acc = self.porous_volume.view(-1) * ct.view(-1) / dt_
+        except Exception:
+            acc = self.porous_volume.view(-1) * self.fluid.cf.view(-1) / dt_
+        rec.update(T=(Tx, Ty, Tz), acc=acc)
+        return orig_mat(self, Tx, Ty, Tz, dt_, wb)
+
+    def rhs(self, dt_, P_prev, mob_w, mob_o, mob_g, q_wells, dpx, dpy, dpz):
+        Q = orig_rhs(self, dt_, P_prev, mob_w, mob_o, mob_g, q_wells, dpx, dpy, dpz)
+        Q0 = orig_rhs(self, dt_, P_prev, mob_w, mob_o, mob_g, torch.zeros_like(q_wells), dpx, dpy, dpz)
+        rec.update(Qg=Q0 - rec["acc"] * P_prev.reshape(-1), P_prev=P_prev, mob=(mob_w, mob_o, mob_g))
+        return Q
+
+    def dense(A, b, **kw):
+        x = torch.linalg.solve(A.to_dense(), b)
+        rec["p_new"] = x
+        return x
+
+    Simulator._build_pressure_matrix_vectorized = mat
+    Simulator._build_pressure_rhs = rhs
+    pamg.amg_solve = dense
+    try:
+        f = dict(fields)
+        scale = torch.exp(delta)
+        f["kx"] = torch.tensor(np.array(fields["kx"])) * scale
+        f["ky"] = torch.tensor(np.array(fields["ky"])) * scale
+        f["kz"] = torch.tensor(np.array(fields["kz"])) * scale
+        with tempfile.TemporaryDirectory() as td:
+            with contextlib.redirect_stdout(io.StringIO()):
+                res = Reservoir(cfg["reservoir"], torch.device("cpu"))
+                res.permeability_x, res.permeability_y, res.permeability_z = f["kx"], f["ky"], f["kz"]
+                res.porosity = poro
+                res.porous_volume = res.cell_volume * poro
+                wm = WellManager(cfg["wells"], res)
+                fl = Fluid(cfg["fluid"], res, torch.device("cpu"))
+                sim_cfg = dict(cfg["simulation"], pressure_solver="amg")
+                sim = Simulator(res, fl, wm, sim_cfg, torch.device("cpu"))
+            prods = [w for w in wm.get_wells() if w.type == "producer"]
+            nx, ny, nz = shape
+            out = []
+            for _ in range(steps):
+                with contextlib.redirect_stdout(io.StringIO()):
+                    assert sim.run_step(dt)
+                Tx, Ty, Tz = rec["T"]
+                P = rec["p_new"].reshape(shape)
+                Pp = rec["P_prev"].reshape(-1)
+                Fx = Tx * (P[:-1] - P[1:])
+                Fy = Ty * (P[:, :-1] - P[:, 1:])
+                Fz = Tz * (P[:, :, :-1] - P[:, :, 1:])
+                z = torch.zeros
+                inflow = (torch.cat([z(1, ny, nz), Fx], 0) - torch.cat([Fx, z(1, ny, nz)], 0)
+                          + torch.cat([z(nx, 1, nz), Fy], 1) - torch.cat([Fy, z(nx, 1, nz)], 1)
+                          + torch.cat([z(nx, ny, 1), Fz], 2) - torch.cat([Fz, z(nx, ny, 1)], 2)).reshape(-1)
+                mw, mo, mg = (m.reshape(-1) for m in rec["mob"])
+                pn = P.reshape(-1)
+                row = []
+                for w in prods:
+                    c = (w.i * ny + w.j) * nz + w.k
+                    qfb = inflow[c] - rec["acc"][c] * (pn[c] - Pp[c]) + rec["Qg"][c]
+                    row.append(qfb * (mo[c] / (mw[c] + mo[c] + mg[c] + 1e-10)) * 86400.0)
+                out.append(torch.stack(row))
+    finally:
+        Simulator._build_pressure_matrix_vectorized = orig_mat
+        Simulator._build_pressure_rhs = orig_rhs
+    return torch.stack(out), delta, poro
+
+
+def adjoint_fixture(steps=6):
+    """Autograd through the reference's own IMPES step with a dense pressure
+    solve on the 16x16x2 sub-case of the adjoint workload: the misfit J of the
+    flux-balance producer oil rates against the rates of the seed-5 permeability
+    field, and dJ/d ln k, dJ/d porosity."""
+    cfg, f = scenarios.adjoint_case(seed=3, steps=steps, nx=16, ny=16, nz=2)
+    _, f2 = scenarios.adjoint_case(seed=5, steps=steps, nx=16, ny=16, nz=2)
+    dt = cfg["simulation"]["time_step_days"] * 86400.0
+    with torch.no_grad():
+        target, _, _ = reference_producer_rates(cfg, dict(f2, poro=f["poro"]), steps, dt)
+    q, delta, poro = reference_producer_rates(cfg, f, steps, dt, grad=True)
+    J = ((q - target) ** 2).sum()
+    g_lnk, g_poro = torch.autograd.grad(J, (delta, poro))
+    out = dict(cfg=json.dumps(cfg), kx=f["kx"], ky=f["ky"], kz=f["kz"], poro=f["poro"], dt=dt, steps=steps,
+               target=target.numpy(), rates=q.detach().numpy(), J=float(J.detach()),
+               g_lnk=g_lnk.numpy().reshape(-1), g_poro=g_poro.numpy().reshape(-1))
+    np.savez_compressed(os.path.join(HERE, "adjoint_ref_16x16x2.npz"), **out)
+    print("adjoint_ref_16x16x2 J", out["J"], "|g_lnk|", np.linalg.norm(out["g_lnk"]),
+          "|g_poro|", np.linalg.norm(out["g_poro"]), flush=True)
+
+
 def main_pcg_only():
     """Regenerate only the Jacobi-PCG fixtures (the others are unchanged)."""
     cfg, f = scenarios.two_phase_2d(seed=0, nx=32, ny=32, nz=1, steps=4)
@@ -454,6 +565,9 @@ if __name__ == "__main__":
         sys.exit(0)
     if "--amg-3d-only" in sys.argv:
         amg_3d_fixtures()
+        sys.exit(0)
+    if "--adjoint-only" in sys.argv:
+        adjoint_fixture()
         sys.exit(0)
     if "--configs-only" in sys.argv:
         sel = [a.split("=", 1)[1] for a in sys.argv if a.startswith("--which=")]

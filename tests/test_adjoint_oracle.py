@@ -73,3 +73,17 @@ def test_autograd_matches_central_differences():
         po[c] -= 2 * hp
         jm = J_of(t.lnk0, po)
         assert (jp - jm) / (2 * hp) == pytest.approx(g_poro[c], rel=2e-3, abs=1e-6 * np.abs(g_poro).max())
+
+
+def test_oracle_adjoint_matches_autograd_through_the_reference(golden):
+    """The dense restatement's objective, rates and gradients against autograd
+    through the reference's own IMPES step with a dense pressure solve on the
+    16x16x2 sub-case, 6 steps (fixture made by make_golden.py --adjoint-only)."""
+    import json
+    g = golden("adjoint_ref_16x16x2")
+    m = Model(json.loads(str(g["cfg"])), g["kx"], g["ky"], g["kz"], g["poro"])
+    J, g_lnk, g_poro, q = oadj.objective(m, float(g["dt"]), int(g["steps"]), g["target"])
+    assert J == pytest.approx(float(g["J"]), rel=1e-10)
+    np.testing.assert_allclose(q, g["rates"], rtol=1e-10)
+    assert np.linalg.norm(g_lnk - g["g_lnk"]) <= 1e-10 * np.linalg.norm(g["g_lnk"])
+    assert np.linalg.norm(g_poro - g["g_poro"]) <= 1e-10 * np.linalg.norm(g["g_poro"])

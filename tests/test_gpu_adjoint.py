@@ -74,10 +74,18 @@ def test_refuses_models_outside_scope():
 
 def test_full_size_gradient_vs_central_differences():
     """64x64x8, 50 steps of 2 days, checkpoints every 10: the adjoint gradient
-    against central differences of the GPU forward run on 20 random cells
-    (ln k, h = 1e-4) and 8 cells (porosity, relative h = 1e-3).  J (~200) carries
-    ~1e-9 relative noise from the iterative pressure solves, so smaller steps
-    measure the noise."""
+    against central differences of the GPU forward run, on 16 random cells for
+    ln k and 6 for porosity.
+
+    Each cell's central difference is taken at two step sizes (ln k: h = 1e-4
+    and 5e-5; porosity: 1e-3 and 5e-4 relative).  Where the two disagree by more
+    than 1e-3, J is not smooth at that cell over the step (a perturbation flips
+    an upwind direction, a clamp or the substep count): such cells are set
+    aside and counted, and at most a quarter may be.  On the others the
+    adjoint must agree with the finer difference to a median of 1e-4 and within
+    1e-3 everywhere (relative to the larger of |g| and 1e-3 max|g|).  J (~200)
+    carries ~1e-9 relative noise from the iterative pressure solves, which
+    bounds how small h can usefully be."""
     from impes_b200.adjoint import misfit_gradient, producer_rates
     steps = 50
     cfg, f = scenarios.adjoint_case(seed=3, steps=steps)
@@ -92,30 +100,53 @@ def test_full_size_gradient_vs_central_differences():
     def J(fields):
         q = producer_rates(cfg, fields, steps, dt, tol=1e-13)
         return float(((q - target) ** 2).sum())
+
+    def central(make, h):
+        return (J(make(h)) - J(make(-h))) / (2 * h)
+
     rng = np.random.default_rng(7)
-    lnk = np.log(f["kx"]).reshape(-1)
-    rel_k = []
-    for c in rng.choice(lnk.size, 20, replace=False):
-        h = 1e-4
-        vals = []
-        for s in (1, -1):
-            l2 = lnk.copy(); l2[c] += s * h
-            kx = np.exp(l2).reshape(f["kx"].shape)
-            vals.append(J(dict(kx=kx, ky=kx, kz=kx, poro=f["poro"])))
-        fd = (vals[0] - vals[1]) / (2 * h)
-        rel_k.append(abs(fd - gl[c]) / max(abs(gl[c]), 1e-3 * np.abs(gl).max()))
-    rel_p = []
-    poro = f["poro"].reshape(-1)
-    for c in rng.choice(poro.size, 8, replace=False):
-        h = 1e-3 * poro[c]
-        vals = []
-        for s in (1, -1):
-            p2 = poro.copy(); p2[c] += s * h
-            vals.append(J(dict(f, poro=p2.reshape(f["poro"].shape))))
-        fd = (vals[0] - vals[1]) / (2 * h)
-        rel_p.append(abs(fd - gp[c]) / max(abs(gp[c]), 1e-3 * np.abs(gp).max()))
-    rel_k, rel_p = np.array(rel_k), np.array(rel_p)
-    print("ln k FD relative errors:", np.sort(rel_k))
-    print("porosity FD relative errors:", np.sort(rel_p))
-    assert np.median(rel_k) < 1e-3 and np.mean(rel_k < 1e-2) >= 0.9
-    assert np.median(rel_p) < 1e-3 and np.mean(rel_p < 1e-2) >= 0.9
+    report = {}
+    for name, grad, base, cells, h0, rel_h in (
+            ("lnk", gl, np.log(f["kx"]).reshape(-1), 16, 1e-4, False),
+            ("poro", gp, f["poro"].reshape(-1), 6, 1e-3, True)):
+        errs, kinks = [], 0
+        for c in rng.choice(base.size, cells, replace=False):
+            h = h0 * base[c] if rel_h else h0
+
+            def make(d, c=c):
+                v = base.copy()
+                v[c] += d
+                if name == "lnk":
+                    kx = np.exp(v).reshape(f["kx"].shape)
+                    return dict(kx=kx, ky=kx, kz=kx, poro=f["poro"])
+                return dict(f, poro=v.reshape(f["poro"].shape))
+            fd1, fd2 = central(make, h), central(make, h / 2)
+            scale = max(abs(grad[c]), 1e-3 * np.abs(grad).max())
+            if abs(fd1 - fd2) > 1e-3 * scale:
+                kinks += 1
+                continue
+            errs.append(abs(fd2 - grad[c]) / scale)
+        errs = np.sort(np.array(errs))
+        report[name] = (errs, kinks)
+        print(f"{name}: FD relative errors {errs}, non-smooth cells set aside: {kinks}")
+        assert kinks <= cells // 4, (name, kinks)
+        assert np.median(errs) < 1e-4 and errs.max() < 1e-3, (name, errs)
+
+
+def test_gradient_matches_autograd_through_the_reference(golden):
+    """The CUDA adjoint against autograd through the reference's own IMPES step
+    (dense pressure solve) on the 16x16x2 sub-case over 6 steps: J and the rates
+    to 1e-8, both gradients to 1e-6 (norm-relative)."""
+    import json
+    from impes_b200.adjoint import misfit_gradient
+    g = golden("adjoint_ref_16x16x2")
+    cfg = json.loads(str(g["cfg"]))
+    f = {k: g[k] for k in ("kx", "ky", "kz", "poro")}
+    out = misfit_gradient(cfg, f, g["target"], int(g["steps"]), float(g["dt"]), checkpoint_every=2,
+                          tol=1e-13, adjoint_tol=1e-13)
+    assert out["J"] == pytest.approx(float(g["J"]), rel=1e-8)
+    np.testing.assert_allclose(out["rates"], g["rates"], rtol=1e-8)
+    gl = out["g_lnk"].reshape(-1).cpu().numpy()
+    gp = out["g_poro"].reshape(-1).cpu().numpy()
+    assert np.linalg.norm(gl - g["g_lnk"]) <= 1e-6 * np.linalg.norm(g["g_lnk"])
+    assert np.linalg.norm(gp - g["g_poro"]) <= 1e-6 * np.linalg.norm(g["g_poro"])
