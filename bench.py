@@ -49,7 +49,7 @@ WORKLOAD_SHORT = ("gas_injection_1m: 200x200x25 cells, correlated log-normal k, 
                   "16 BHP producers, dt 2 d")
 PRESSURE_TOL = 1e-6
 L2_FLUSH_BYTES = 512 << 20
-DEFAULT_P_MAX = 0               # interpolation row cap of the headline hierarchy
+DEFAULT_P_MAX = 2               # interpolation row cap of the headline hierarchy
 CPU_SAMPLE = (100, 100, 25)     # spatial sample of the workload for the CPU legs
 
 
@@ -232,17 +232,24 @@ def make_sim(cfg, fields, precision, device, restart=30, solver="gmres_amg", war
     return build_from_config(c, fields, device=device)
 
 
-def time_steps(sim, steps, dt, flush, stream):
-    """Device time of `steps` IMPES steps (L2 flushed before each, outside the events)."""
+def time_steps(sim, steps, dt, flush, stream, nvtx_last=False):
+    """Device time of `steps` IMPES steps (L2 flushed before each, outside the
+    events).  With nvtx_last the last step runs inside an NVTX range named
+    "impes_step", which a profiler can select (ncu --nvtx --nvtx-include)."""
     import torch
     total = 0.0
     iters = []
-    for _ in range(steps):
+    for q in range(steps):
         flush.zero_()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        mark = nvtx_last and q == steps - 1
+        if mark:
+            torch.cuda.nvtx.range_push("impes_step")
         a.record(stream)
         ok = sim.run_step(dt)
         b.record(stream)
+        if mark:
+            torch.cuda.nvtx.range_pop()
         b.synchronize()
         if not ok:
             raise RuntimeError("IMPES step failed to converge")
@@ -448,7 +455,7 @@ def run_variant(args, cfg, fields, precision, device, dt, flush, stream, dist, r
     torch.cuda.synchronize()
     launches0 = _lib.kernel_launches()
     with ClockSampler(local, args.clocks_dir) as clk:
-        ms, iters = time_steps(sim, args.steps, dt, flush, stream)
+        ms, iters = time_steps(sim, args.steps, dt, flush, stream, nvtx_last=args.nvtx)
     launches = _lib.kernel_launches() - launches0
     torch.cuda.synchronize()
     if dist is not None:
@@ -469,6 +476,7 @@ def run_variant(args, cfg, fields, precision, device, dt, flush, stream, dist, r
     if dist is not None:
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     levels = sim.amg_levels()
+    level_us = sim.amg_profile_levels(precision, reps=20) if args.level_profile else None
     nnz = [lv[1] for lv in levels]
     oc = sum(nnz) / max(nnz[0], 1) if nnz else None
     m1 = total_mass(fl, pv)
@@ -476,6 +484,9 @@ def run_variant(args, cfg, fields, precision, device, dt, flush, stream, dist, r
     if rank == 0:
         print(f"[bench] {label}: levels (n, nnz, nc, p_nnz, coarsest, columns) = {levels}", file=sys.stderr)
         print(f"[bench] {label}: phases {phases}", file=sys.stderr)
+        if level_us is not None:
+            print(f"[bench] {label}: per-level us (sweep, residual, restrict, prolong) = "
+                  f"{[tuple(round(v, 2) for v in t) for t in level_us]}", file=sys.stderr)
     out = dict(ms=float(tmax.item()), iters=iters, phases=phases, clocks=clk.summary(), ms_inst=ms_inst,
                iters_inst=iters_inst, launches=launches, e2e_ms=float(te.item()), e2e_bytes=e2e_bytes,
                e2e_iters=e2e_iters, setup_s=setup_s, p=fl.pressure.clone(), sw=fl.s_w.clone(),
@@ -708,6 +719,10 @@ def main():
     ap.add_argument("--ensemble-loop-steps", type=int, default=3,
                     help="steps of the loop-the-single-path ensemble baseline")
     ap.add_argument("--detail-out", default=None, help="write the detailed results as JSON here")
+    ap.add_argument("--level-profile", action="store_true",
+                    help="time each level's sweep, residual, restriction and prolongation (stderr)")
+    ap.add_argument("--nvtx", action="store_true",
+                    help="mark the last headline step with an NVTX range \"impes_step\" for profilers")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

@@ -171,6 +171,12 @@ int impes_amg_fgmres(impes_amg* h, const double* b, double* x, const impes_krylo
 /* Hierarchy introspection (ClassicalAMG.levels, .Dhalf_inv). */
 int impes_amg_num_levels(impes_amg* h, int* nlev);
 int impes_amg_level_info(impes_amg* h, int lvl, impes_amg_level_desc* info);
+/* Instrumentation (no reference counterpart): mean device time in microseconds
+ * of one l1-Jacobi sweep, residual, restriction and prolongation of every level
+ * (precision 0: fp64, 1: fp32), each launched `reps` times back to back on the
+ * level's work vectors; out_host[4 * level + k], 0 on the coarsest level.
+ * Overwrites the hierarchy's work vectors; synchronises the stream. */
+int impes_amg_profile_levels(impes_amg* h, int precision, int reps, double* out_host, void* stream);
 /* Copy level `lvl` into caller device buffers (any pointer may be NULL). */
 int impes_amg_level_export(impes_amg* h, int lvl, int* A_rowptr, int* A_col, double* A_val,
                            double* inv_relax, int* P_rowptr, int* P_col, double* P_val,

@@ -2,6 +2,7 @@
 #include "amg.cuh"
 #include "model.cuh"
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <map>
 
@@ -45,6 +46,119 @@ __global__ void k_extrapolate(int n, const double* __restrict__ p, const double*
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
     x0[i] = p[i] + r * (p[i] - p_prev[i]);
+}
+
+// After a captured step: the new pressure is accepted (p_prev takes the
+// step's starting pressure for the next extrapolated iterate) or, when the
+// solve missed its tolerance, p is restored from p_save.
+__global__ void k_accept(int n, const FgState* st, double* __restrict__ p, const double* __restrict__ p_save,
+                         double* __restrict__ p_prev) {
+  const bool ok = st->converged && !st->nan;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    if (ok) p_prev[i] = p_save[i];
+    else p[i] = p_save[i];
+  }
+}
+
+// The whole IMPES step of the FGMRES solver as one CUDA graph: assembly, the
+// Galerkin update, the pressure-save copy, the extrapolated first iterate, the
+// device-driven FGMRES (a conditional WHILE node over its iterations), the
+// accept/restore kernel and the saturation update, which runs only when the
+// solve converged.  One graph per (model, state pointers, dt, solver settings,
+// first-iterate mode); the hierarchy must exist (the first step builds it on
+// the host path).  Returns false when this build or driver refuses the capture
+// (the caller then keeps the host-driven step).
+bool step_graph_run(Model& m, AMG& a, double* p, double* sw, double* sg, double* so, double dt,
+                    const impes_krylov_params& kp, impes_krylov_stats& st, cudaStream_t s) {
+  if (a.step_graph_failed || !a.use_graphs || !a.use_step_graph || timers().on || kp.precision < 0) return false;
+  const bool extrap = kp.use_x0 == 2 && m.have_prev && m.dt_prev > 0;
+  AMG::StepGraph* g = nullptr;
+  for (auto& e : a.step_graphs)
+    if (e.model == &m && e.p == p && e.sw == sw && e.sg == sg && e.so == so && e.dt == dt &&
+        e.have_prev == extrap && (!extrap || e.dt_prev == m.dt_prev) && e.kp.tol == kp.tol &&
+        e.kp.restart == kp.restart && e.kp.max_iters == kp.max_iters && e.kp.norm == kp.norm &&
+        e.kp.precision == kp.precision && e.kp.use_x0 == kp.use_x0) {
+      g = &e;
+      break;
+    }
+  if (!g) {
+    if (a.step_graphs.size() >= 8) {           // dt changes (retries): keep a few
+      if (a.step_graphs.front().exec) cudaGraphExecDestroy(a.step_graphs.front().exec);
+      a.step_graphs.erase(a.step_graphs.begin());
+    }
+    impes_krylov_params k = kp;
+    k.use_x0 = kp.use_x0 ? 1 : 0;
+    amg_fgmres_prepare(a, k);
+    m.p_prev.ensure(m.P.N);
+    if (!a.cap_stream) IMPES_CUDA(cudaStreamCreateWithFlags(&a.cap_stream, cudaStreamNonBlocking));
+    cudaStream_t cs = a.cap_stream;
+    // the capture stream starts after the work already queued on s
+    cudaEvent_t ev;
+    IMPES_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    IMPES_CUDA(cudaEventRecord(ev, s));
+    IMPES_CUDA(cudaStreamWaitEvent(cs, ev, 0));
+    IMPES_CUDA(cudaEventDestroy(ev));
+    const unsigned long long before = thread_launches();
+    const bool stale_before = a.fp64_stale;
+    cudaGraph_t graph = nullptr;
+    cudaError_t ce = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (ce != cudaSuccess) { a.step_graph_failed = true; cudaGetLastError(); return false; }
+    try {
+      model_assemble(m, p, sw, sg, dt, m.csr_val.p, m.rhs.p, cs);
+      amg_update(a, m.csr_val.p, cs);
+      IMPES_CUDA(cudaMemcpyAsync(m.p_save.p, p, sizeof(double) * m.P.N, cudaMemcpyDeviceToDevice, cs));
+      if (extrap) {
+        k_extrapolate<<<grid_for(m.P.N, 256), 256, 0, cs>>>(m.P.N, m.p_save.p, m.p_prev.p, dt / m.dt_prev, p);
+        ::impes::count_launch();
+        IMPES_CHECK_LAUNCH();
+      }
+      amg_fgmres_capture(a, m.rhs.p, p, k, cs);
+      k_accept<<<grid_for(m.P.N, 256), 256, 0, cs>>>(m.P.N, a.fgst.p, p, m.p_save.p, m.p_prev.p);
+      ::impes::count_launch();
+      IMPES_CHECK_LAUNCH();
+      model_saturation(m, p, sw, sg, so, dt, cs, &a.fgst.p->converged);
+    } catch (const Error&) {
+      cudaStreamEndCapture(cs, &graph);
+      if (graph) cudaGraphDestroy(graph);
+      cudaGetLastError();
+      count_launches(-(long long)(thread_launches() - before));
+      a.fp64_stale = stale_before;
+      a.step_graph_failed = true;
+      return false;
+    }
+    IMPES_CUDA(cudaStreamEndCapture(cs, &graph));
+    AMG::StepGraph e;
+    e.model = &m; e.p = p; e.sw = sw; e.sg = sg; e.so = so; e.dt = dt;
+    e.have_prev = extrap; e.dt_prev = extrap ? m.dt_prev : 0.0; e.kp = kp;
+    e.fp64_stale_after = a.fp64_stale;
+    e.kernels_body = a.fg_body_kernels;
+    e.kernels_fixed = (long long)(thread_launches() - before) - e.kernels_body;
+    count_launches(-(long long)(thread_launches() - before));
+    a.fp64_stale = stale_before;
+    cudaError_t ie = cudaGraphInstantiate(&e.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) {
+      cudaGetLastError();
+      a.step_graph_failed = true;
+      return false;
+    }
+    a.step_graphs.push_back(e);
+    g = &a.step_graphs.back();
+  }
+  IMPES_CUDA(cudaGraphLaunch(g->exec, s));
+  a.fp64_stale = g->fp64_stale_after;
+  FgState* hs = reinterpret_cast<FgState*>(a.hbuf.p);
+  static_assert(sizeof(FgState) <= 64 * sizeof(double), "state must fit the pinned scratch");
+  IMPES_CUDA(cudaMemcpyAsync(hs, a.fgst.p, sizeof(FgState), cudaMemcpyDeviceToHost, s));
+  IMPES_CUDA(cudaStreamSynchronize(s));
+  count_launches(g->kernels_fixed + (long long)hs->total * g->kernels_body);
+  st = impes_krylov_stats{hs->total, hs->restarts, hs->converged && !hs->nan ? 1 : 0, hs->rel, hs->true_rel};
+  if (hs->nan) throw Error(IMPES_ERR_NAN, "NaN in FGMRES");
+  if (!st.converged) return true;            // p was restored by the graph
+  m.dt_prev = dt;
+  m.have_prev = true;
+  return true;
 }
 
 template <typename F>
@@ -177,6 +291,14 @@ int impes_amg_level_info(impes_amg* h, int lvl, impes_amg_level_desc* info) {
       info->lanes[3 * q + 1] = L.lpr_r[q];
       info->lanes[3 * q + 2] = L.lpr_p[q];
     }
+  });
+}
+
+int impes_amg_profile_levels(impes_amg* h, int precision, int reps, double* out_host, void* stream) {
+  return guarded([&] {
+    IMPES_REQUIRE(h && out_host && reps >= 1, IMPES_ERR_ARG, "null argument or reps < 1");
+    IMPES_REQUIRE(h->a.built, IMPES_ERR_STATE, "profile before setup");
+    amg_profile_levels(h->a, precision, reps, out_host, S(stream));
   });
 }
 
@@ -408,8 +530,25 @@ int impes_step(impes_model* h, impes_amg* amg, double* p, double* sw, double* sg
     IMPES_REQUIRE(solver >= 0 && solver <= 2, IMPES_ERR_ARG, "solver must be 0, 1 or 2");
     Model& m = h->m;
     cudaStream_t s = S(stream);
-    model_assemble(m, p, sw, sg, dt, m.csr_val.p, m.rhs.p, s);
     IMPES_REQUIRE(solver == 2 || amg, IMPES_ERR_ARG, "null AMG handle");
+    if (solver == 1 && amg->a.built && amg->a.levels[0]->n == m.P.N) {
+      impes_krylov_stats gst{};
+      if (step_graph_run(m, amg->a, p, sw, sg, so, dt, *kp, gst, s)) {
+        if (kstats) *kstats = gst;
+        if (!gst.converged) throw Error(IMPES_ERR_NOT_CONVERGED, "FGMRES did not reach the pressure tolerance");
+        if (sstats) {
+          double hb[12];
+          impes_sat_stats ss{};
+          IMPES_CUDA(cudaMemcpyAsync(hb, m.balances.p, sizeof(hb), cudaMemcpyDeviceToHost, s));
+          IMPES_CUDA(cudaMemcpyAsync(&ss.substeps, m.nsub.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+          IMPES_CUDA(cudaStreamSynchronize(s));
+          for (int q = 0; q < 6; ++q) { ss.mass_balance[q] = hb[q]; ss.component[q] = hb[6 + q]; }
+          *sstats = ss;
+        }
+        return;
+      }
+    }
+    model_assemble(m, p, sw, sg, dt, m.csr_val.p, m.rhs.p, s);
     if (solver != 2) {
       AMG& a = amg->a;
       if (!a.built || a.levels[0]->n != m.P.N)

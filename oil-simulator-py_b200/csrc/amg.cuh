@@ -60,6 +60,13 @@ struct Level {
   DBuf<int> piv;                   // two permutations of n
 };
 
+// Solver state of the device-driven FGMRES (amg_cycle.cu), read by the host
+// after the captured solve has run.
+struct FgState {
+  int j, total, restarts, converged, done, cycle_end, reorth, bzero, nan, pad;
+  double bnorm, beta, wn2, rel, true_rel;
+};
+
 struct AMG {
   impes_amg_params prm;
   std::vector<std::unique_ptr<Level>> levels;
@@ -89,7 +96,27 @@ struct AMG {
   };
   VGraph vgraph[2][2][2][2];
   cudaStream_t cap_stream = nullptr;
+  cudaStream_t body_stream = nullptr;   // captures the device FGMRES's loop body
+  DBuf<FgState> fgst;                   // device FGMRES state
+  long long fg_body_kernels = 0;        // kernels of one device-FGMRES iteration
+  // whole IMPES steps captured as graphs (abi.cu), keyed by the step's inputs
+  struct StepGraph {
+    cudaGraphExec_t exec = nullptr;
+    const void* model = nullptr;
+    const double *p = nullptr, *sw = nullptr, *sg = nullptr, *so = nullptr;
+    double dt = 0.0, dt_prev = 0.0;
+    bool have_prev = false;
+    impes_krylov_params kp{};
+    bool fp64_stale_after = false;
+    long long kernels_fixed = 0, kernels_body = 0;
+  };
+  std::vector<StepGraph> step_graphs;
+  bool step_graph_failed = false;       // capture refused once: keep the host-driven path
   bool use_graphs = true;
+  bool use_step_graph = true;           // whole IMPES steps as graphs (IMPES_NO_STEP_GRAPH=1: off)
+  bool use_tail = true;                 // fused V-cycle tail (IMPES_NO_TAIL=1: off)
+  int tail_level = -1;                  // first level of the fused tail, -1: none
+  int tail_cluster = 0;                 // CTAs in the tail's cluster (16 or 8)
   void drop_graphs() {
     for (auto& a : vgraph) for (auto& b : a) for (auto& c : b) for (auto& g : c) {
       if (g.exec) cudaGraphExecDestroy(g.exec);
@@ -97,10 +124,14 @@ struct AMG {
       for (auto& r : g.timers) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
       g.timers.clear();
     }
+    for (auto& g : step_graphs)
+      if (g.exec) cudaGraphExecDestroy(g.exec);
+    step_graphs.clear();
   }
   ~AMG() {
     drop_graphs();
     if (cap_stream) cudaStreamDestroy(cap_stream);
+    if (body_stream) cudaStreamDestroy(body_stream);
   }
 };
 
@@ -117,6 +148,12 @@ void amg_apply(AMG& h, const double* b, double* x, int cycles, double apply_tol,
 void amg_vcycle_scaled(AMG& h, const double* bs, double* xs, int precision, cudaStream_t s);
 void amg_fgmres(AMG& h, const double* b, double* x, const impes_krylov_params& kp,
                 impes_krylov_stats& st, cudaStream_t s);
+// Device-driven FGMRES for a graph: amg_fgmres_prepare allocates its work space
+// (call it before capture); amg_fgmres_capture enqueues the whole solve on a
+// stream that is being captured (a conditional WHILE node runs the
+// iterations); the outcome is in h.fgst after the graph has run.
+void amg_fgmres_prepare(AMG& h, const impes_krylov_params& kp);
+void amg_fgmres_capture(AMG& h, const double* b, double* x, const impes_krylov_params& kp, cudaStream_t s);
 
 // shared kernels (amg_cycle.cu)
 void spmv(const Level& L, const double* x, double* y, cudaStream_t s);
@@ -125,6 +162,9 @@ void coarse_factor(AMG& h, Level& L, cudaStream_t s, bool from_fp32 = false);
 // Times the CSR kernels of every level with each lanes-per-row choice and keeps
 // the fastest (amg_cycle.cu); choices are cached per level shape for the process.
 void amg_autotune(AMG& h, cudaStream_t s);
+void amg_profile_levels(AMG& h, int precision, int reps, double* out, cudaStream_t s);
+// First level of the fused V-cycle tail (amg_cycle.cu), -1 when none qualifies.
+int amg_tail_level(AMG& h);
 // Brings the fp64 coarse levels up to date after an fp32 update (no-op otherwise).
 void amg_ensure_fp64(AMG& h, cudaStream_t s);
 void level_precision_copies(AMG& h, Level& L, cudaStream_t s);

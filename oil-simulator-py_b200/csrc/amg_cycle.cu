@@ -413,8 +413,27 @@ __global__ void k_mul_inplace(long long n, double* a, const double* b) {
 __global__ void k_zero(long long n, double* a) {
   pdl_wait_release(); GRID_LOOP(i, n) a[i] = 0.0; }
 
+// v - sum_{q<k} h[q] * V[q*ld + i] (or v + ..., sign = -1 / +1) with the q
+// terms added one after another as in the plain loop, but with the loads of up
+// to eight vectors issued together so that each thread keeps several HBM
+// requests in flight.
+template <int SIGN>
+__device__ __forceinline__ double axpy_rows(double v, const double* __restrict__ h, int k,
+                                            const double* __restrict__ V, long long ld, long long i) {
+  int q = 0;
+  for (; q + 8 <= k; q += 8) {
+    double a[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) a[u] = V[(q + u) * ld + i];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) v = SIGN > 0 ? v + h[q + u] * a[u] : v - h[q + u] * a[u];
+  }
+  for (; q < k; ++q) v = SIGN > 0 ? v + h[q] * V[q * ld + i] : v - h[q] * V[q * ld + i];
+  return v;
+}
+
 // ---------------------------------------------------- deterministic dots
-constexpr int kDotBlocks = 296;   // 2 x 148 SMs, fixed so partials have a fixed order
+constexpr int kDotBlocks = 592;   // 4 x 148 SMs, fixed so partials have a fixed order
 constexpr int kMD = 8;            // vectors per multi-dot launch
 
 // partial[q * kDotBlocks + block] = sum over the block of V[q] . w   (q < k)
@@ -517,8 +536,7 @@ __global__ void __launch_bounds__(TB) k_update(long long n, const double* __rest
   __syncthreads();
   double acc = 0.0;
   GRID_LOOP(i, n) {
-    double v = w[i];
-    for (int q = 0; q < k; ++q) v -= sh[q] * Vbase[q * ldv + i];
+    const double v = axpy_rows<-1>(w[i], sh, k, Vbase, ldv, i);
     w[i] = v;
     acc += v * v;
   }
@@ -566,10 +584,10 @@ struct GJArgs {
   int* perm[2];
   int* singular[2];
 };
-template <bool SMEM>
-__global__ void __launch_bounds__(kGJ) k_gauss_jordan(int n, GJArgs args) {
-  __shared__ double s_val[kGJ / 32];
-  __shared__ int s_idx[kGJ / 32];
+template <bool SMEM, int NT = kGJ>
+__global__ void __launch_bounds__(NT) k_gauss_jordan(int n, GJArgs args) {
+  __shared__ double s_val[NT / 32];
+  __shared__ int s_idx[NT / 32];
   __shared__ int s_p;
   __shared__ double s_inv;
   extern __shared__ double s_dyn[];
@@ -695,7 +713,12 @@ void coarse_factor(AMG& h, Level& L, cudaStream_t s, bool from_fp32) {
   IMPES_CUDA(cudaMemsetAsync(h.iflag.p + 2, 0, 2 * sizeof(int), s));
   GJArgs args{{L.lu.p, L.lu_free.p}, {L.piv.p, L.piv.p + n}, {h.iflag.p + 2, h.iflag.p + 3}};
   const size_t smem_full = sizeof(double) * ((size_t)n * n + 2 * (size_t)n);
-  if (smem_full <= (size_t)(224u << 10)) {
+  if (n <= 128) {
+    // small coarsest matrices: 8 warps keep each of the n pivot steps' block
+    // barriers short (the elimination has at most 128 rows to share out)
+    raise_smem_limit((const void*)k_gauss_jordan<true, 256>, smem_full);
+    k_gauss_jordan<true, 256><<<2, 256, smem_full, s>>>(n, args); ::impes::count_launch();
+  } else if (smem_full <= (size_t)(224u << 10)) {
     raise_smem_limit((const void*)k_gauss_jordan<true>, smem_full);
     k_gauss_jordan<true><<<2, kGJ, smem_full, s>>>(n, args); ::impes::count_launch();
   } else {
@@ -854,11 +877,201 @@ double vcycle_bytes(const AMG& h, int l) {
   return tot;
 }
 
+// ------------------------------------------------- fused V-cycle tail
+// The levels of at most kTailRows rows (and the dense coarsest solve) cost a
+// few microseconds per kernel whatever their size: each does 8 launches per
+// V-cycle.  kTail runs the whole V-cycle of those levels in ONE launch of a
+// thread-block cluster, with a hardware cluster barrier (barrier.cluster
+// arrive.release / wait.acquire) between the phases: the same sequence as
+// vcycle() -- first sweep from zero, two sweeps, residual, restriction, the
+// next level, prolongation, two sweeps; the dense coarsest apply -- with
+// kTailLanes lanes per row.  Vectors that change between phases are read past
+// L1 (ld.global.cg).  Chebyshev hierarchies keep the per-level kernels.
+constexpr int kTailRows = 24576;
+constexpr int kTailLanes = 8;
+constexpr int kTailThreads = 1024;
+constexpr int kTailMaxLevels = 16;
+
+template <typename T>
+struct TailLevel {
+  int n, nc, coarsest, rel;
+  const int* rowptr;
+  const unsigned short* col16;   // or null: col
+  const int* col;
+  const T* val;
+  const T* inv;
+  const int *prow, *pcol, *rrow, *rcol;
+  const T *pval, *rval;
+  T *x, *t, *b, *r;
+  const double *lu, *lu_free;    // coarsest: pinned / unpinned inverses
+};
+template <typename T>
+struct TailArgs {
+  TailLevel<T> lv[kTailMaxLevels];
+  int nlev;
+  const int* free_singular;
+  int krylov;
+};
+
+__device__ __forceinline__ void cluster_barrier() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+  asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ unsigned cluster_rank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;\n" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ unsigned cluster_size() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;\n" : "=r"(r));
+  return r;
+}
+template <typename T> __device__ __forceinline__ T ldcg(const T* p) { return __ldcg(p); }
+
+// y = f(A x) over the rows of one CSR block (kTailLanes lanes per row)
+// Rows are dealt out a warp (32 / kTailLanes rows) at a time, so every lane of
+// a warp runs the same number of loop trips and takes part in each shuffle.
+template <typename T, int MODE>
+__device__ void tail_csr(int n, const int* __restrict__ rowptr, const unsigned short* __restrict__ col16,
+                         const int* __restrict__ col, int rel, const T* __restrict__ val, const T* x, const T* b,
+                         const T* __restrict__ inv, T* y, unsigned gtid, unsigned gthreads) {
+  const int lane = gtid % kTailLanes;
+  constexpr int kRowsPerWarp = 32 / kTailLanes;
+  const long long warp = gtid >> 5, nwarps = gthreads >> 5;
+  for (long long base = warp * kRowsPerWarp; base < n; base += nwarps * kRowsPerWarp) {
+    const long long row = base + (int)((gtid & 31) / kTailLanes);
+    const bool valid = row < n;
+    T acc = T(0);
+    if (MODE != Y_SMOOTH0 && valid) {
+      const int a = rowptr[row], e = rowptr[row + 1];
+      if (col16) {
+        const int cb = rel ? (int)row - 32768 : 0;
+        for (int k = a + lane; k < e; k += kTailLanes) acc += val[k] * ldcg(x + cb + (int)col16[k]);
+      } else {
+        for (int k = a + lane; k < e; k += kTailLanes) acc += val[k] * ldcg(x + col[k]);
+      }
+    }
+#pragma unroll
+    for (int o = kTailLanes / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, kTailLanes);
+    if (lane == 0 && valid) {
+      if (MODE == Y_AX) y[row] = acc;
+      else if (MODE == Y_B_MINUS_AX) y[row] = ldcg(b + row) - acc;
+      else if (MODE == Y_SMOOTH) y[row] = ldcg(x + row) + T(kOmega) * inv[row] * (ldcg(b + row) - acc);
+      else if (MODE == Y_ADD_AX) y[row] = ldcg(y + row) + acc;
+      else if (MODE == Y_SMOOTH0) y[row] = T(kOmega) * inv[row] * ldcg(b + row);
+    }
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kTailThreads) k_vcycle_tail(const __grid_constant__ TailArgs<T> A) {
+  pdl_wait_release();
+  const unsigned gthreads = cluster_size() * blockDim.x;
+  const unsigned gtid = cluster_rank() * blockDim.x + threadIdx.x;
+  // down: pre-smoothing, residual, restriction
+  int l = 0;
+  for (; l < A.nlev && !A.lv[l].coarsest; ++l) {
+    const TailLevel<T>& L = A.lv[l];
+    tail_csr<T, Y_SMOOTH0>(L.n, L.rowptr, L.col16, L.col, L.rel, L.val, nullptr, L.b, L.inv, L.x, gtid, gthreads);
+    cluster_barrier();
+    tail_csr<T, Y_SMOOTH>(L.n, L.rowptr, L.col16, L.col, L.rel, L.val, L.x, L.b, L.inv, L.t, gtid, gthreads);
+    cluster_barrier();
+    tail_csr<T, Y_SMOOTH>(L.n, L.rowptr, L.col16, L.col, L.rel, L.val, L.t, L.b, L.inv, L.x, gtid, gthreads);
+    cluster_barrier();
+    tail_csr<T, Y_B_MINUS_AX>(L.n, L.rowptr, L.col16, L.col, L.rel, L.val, L.x, L.b, nullptr, L.r, gtid,
+                              gthreads);
+    cluster_barrier();
+    const TailLevel<T>& N = A.lv[l + 1];
+    tail_csr<T, Y_AX>(L.nc, L.rrow, nullptr, L.rcol, 0, L.rval, L.r, nullptr, nullptr, N.b, gtid, gthreads);
+    cluster_barrier();
+  }
+  // coarsest: x = Ainv b, pinned (b[0] = 0) unless Krylov mode uses the
+  // invertible unpinned matrix (k_coarse_apply)
+  {
+    const TailLevel<T>& C = A.lv[l];
+    const bool use_free = A.krylov && C.lu_free != nullptr && ldcg(A.free_singular) == 0;
+    const double* Ainv = use_free ? C.lu_free : C.lu;
+    const int pin = use_free ? 0 : 1;
+    const int warp = gtid >> 5, lane = gtid & 31, nw = gthreads >> 5;
+    for (int i = warp; i < C.n; i += nw) {
+      double acc = 0.0;
+      for (int j = lane; j < C.n; j += 32)
+        acc += Ainv[(long long)i * C.n + j] * ((pin && j == 0) ? 0.0 : (double)ldcg(C.b + j));
+      acc = warp_sum(acc);
+      if (lane == 0) C.x[i] = (T)acc;
+    }
+    cluster_barrier();
+  }
+  // up: prolongation and post-smoothing
+  for (--l; l >= 0; --l) {
+    const TailLevel<T>& L = A.lv[l];
+    const TailLevel<T>& N = A.lv[l + 1];
+    tail_csr<T, Y_ADD_AX>(L.n, L.prow, nullptr, L.pcol, 0, L.pval, N.x, nullptr, nullptr, L.x, gtid, gthreads);
+    cluster_barrier();
+    tail_csr<T, Y_SMOOTH>(L.n, L.rowptr, L.col16, L.col, L.rel, L.val, L.x, L.b, L.inv, L.t, gtid, gthreads);
+    cluster_barrier();
+    tail_csr<T, Y_SMOOTH>(L.n, L.rowptr, L.col16, L.col, L.rel, L.val, L.t, L.b, L.inv, L.x, gtid, gthreads);
+    cluster_barrier();
+  }
+}
+
+// Whether levels l.. qualify for the fused tail: at most kTailRows rows each,
+// rows of at most 96 entries, at most kTailMaxLevels levels, a dense coarsest
+// level (n <= 500) and the l1-Jacobi smoother.
+bool tail_eligible(const AMG& h, int l) {
+  if (h.prm.smoother != IMPES_SMOOTHER_L1_JACOBI || !h.use_tail) return false;
+  if ((int)h.levels.size() - l > kTailMaxLevels) return false;
+  for (size_t q = l; q < h.levels.size(); ++q) {
+    const Level& L = *h.levels[q];
+    if (L.n > kTailRows) return false;
+    if (L.coarsest) return L.n <= 500 && L.lu.p != nullptr;
+    if (L.avg_row > 96) return false;
+  }
+  return false;
+}
+
+template <typename T>
+void launch_tail(AMG& h, int l, cudaStream_t s) {
+  TailArgs<T> A{};
+  A.nlev = (int)h.levels.size() - l;
+  A.free_singular = h.iflag.p + 3;
+  A.krylov = h.krylov_mode ? 1 : 0;
+  for (int q = 0; q < A.nlev; ++q) {
+    Level& L = *h.levels[l + q];
+    TailLevel<T>& d = A.lv[q];
+    d.n = L.n; d.nc = L.nc; d.coarsest = L.coarsest ? 1 : 0; d.rel = L.col16_rel;
+    d.rowptr = L.rowptr.p; d.col16 = L.col16.p; d.col = L.col.p;
+    d.val = LV<T>::val(L); d.inv = LV<T>::inv(L);
+    d.prow = L.prow.p; d.pcol = L.pcol.p; d.rrow = L.rrow.p; d.rcol = L.rcol.p;
+    d.pval = LV<T>::pval(L); d.rval = LV<T>::rval(L);
+    d.x = LV<T>::x(L); d.t = LV<T>::t(L); d.b = LV<T>::b(L); d.r = LV<T>::r(L);
+    d.lu = L.lu.p; d.lu_free = L.lu_free.p;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(h.tail_cluster);
+  cfg.blockDim = dim3(kTailThreads);
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = cfg.gridDim.x;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  IMPES_CUDA(cudaLaunchKernelEx(&cfg, k_vcycle_tail<T>, A));
+  count_launch();
+}
+
 // _v_cycle (classical_amg.py:1037-1106) on level l: input b in LV<T>::b(L),
 // initial x in LV<T>::x(L) (ignored when zero_x); returns the buffer with x.
 template <typename T>
 T* vcycle(AMG& h, int l, bool zero_x, cudaStream_t s) {
   Level& L = *h.levels[l];
+  if (l > 0 && zero_x && l == h.tail_level && !L.coarsest) {
+    launch_tail<T>(h, l, s);
+    return LV<T>::x(L);
+  }
   if (L.coarsest) {
     if (L.n <= 500) {
       const int n = L.n;
@@ -932,8 +1145,9 @@ T* vcycle_top(AMG& h, bool zero_x, cudaStream_t s) {
 // l1-Jacobi sweep stands for the kernels on A (sweeps, residuals, Chebyshev
 // steps, the FGMRES operator), Y_AX on R for the restriction and Y_ADD_AX on P
 // for the prolongation.  Each candidate (1, 2, 4, 8, 16, 32 lanes, at most four
-// times the mean row length) runs twice untimed and four times between CUDA
-// events on the level's own work vectors.  The first choice made for a shape
+// times the mean row length) runs twice untimed and eight times between CUDA
+// events on the level's own work vectors, and the fewest lanes within 3 % of
+// the fastest is kept.  The first choice made for a shape
 // (precision, operator, log2 of the rows in halves, mean row length) is kept
 // for the whole process, so hierarchies of the same shape -- a rebuilt one, or
 // ensemble members alike in size -- launch the same kernels and sum in the same
@@ -949,7 +1163,7 @@ float time_lpr(int lpr, int n, int avg, const int* rowptr, const int* col, const
                cudaEvent_t e0, cudaEvent_t e1) {
   for (int w = 0; w < 2; ++w) launch_csr<T, MODE>(n, avg, rowptr, col, val, x, b, inv, y, s, col16, rel, lpr);
   IMPES_CUDA(cudaEventRecord(e0, s));
-  for (int w = 0; w < 4; ++w) launch_csr<T, MODE>(n, avg, rowptr, col, val, x, b, inv, y, s, col16, rel, lpr);
+  for (int w = 0; w < 8; ++w) launch_csr<T, MODE>(n, avg, rowptr, col, val, x, b, inv, y, s, col16, rel, lpr);
   IMPES_CUDA(cudaEventRecord(e1, s));
   IMPES_CUDA(cudaEventSynchronize(e1));
   float ms = 0.f;
@@ -969,13 +1183,20 @@ int tune_one(int slot, int kind, int n, int avg, const int* rowptr, const int* c
     auto it = g_tune_cache.find(key);
     if (it != g_tune_cache.end()) return it->second;
   }
-  int best = default_lpr(avg);
-  float best_ms = 1e30f;
+  // the fewest lanes within 3 % of the fastest: timing noise between near-equal
+  // candidates does not flip the choice
+  int cand[6], nc = 0;
+  float ms[6];
   for (int lpr : {1, 2, 4, 8, 16, 32}) {
     if (lpr > 1 && lpr > 4 * avg) break;
-    const float ms = time_lpr<T, MODE>(lpr, n, avg, rowptr, col, val, x, b, inv, y, col16, rel, s, e0, e1);
-    if (ms < best_ms) { best_ms = ms; best = lpr; }
+    cand[nc] = lpr;
+    ms[nc++] = time_lpr<T, MODE>(lpr, n, avg, rowptr, col, val, x, b, inv, y, col16, rel, s, e0, e1);
   }
+  float best_ms = 1e30f;
+  for (int q = 0; q < nc; ++q) best_ms = std::min(best_ms, ms[q]);
+  int best = default_lpr(avg);
+  for (int q = 0; q < nc; ++q)
+    if (ms[q] <= 1.03f * best_ms) { best = cand[q]; break; }
   std::lock_guard<std::mutex> lock(g_tune_mu);
   auto ins = g_tune_cache.emplace(key, best);   // another thread may have decided first
   return ins.first->second;
@@ -999,6 +1220,106 @@ void tune_levels(AMG& h, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1) {
   }
 }
 }  // namespace
+
+// Per-level kernel times of the V-cycle (instrumentation): for each level, the
+// mean device time of one l1-Jacobi sweep, one residual, one restriction and
+// one prolongation in the given precision, each launched `reps` times back to
+// back between CUDA events on the level's own work vectors (warm caches), with
+// the level's tuned lanes per row.  out[4 * level + {0,1,2,3}] in microseconds
+// (0 on the coarsest level).
+void amg_profile_levels(AMG& h, int precision, int reps, double* out, cudaStream_t s) {
+  if (precision == 0) amg_ensure_fp64(h, s);
+  cudaEvent_t e0, e1;
+  IMPES_CUDA(cudaEventCreate(&e0));
+  IMPES_CUDA(cudaEventCreate(&e1));
+  auto timed = [&](auto&& launch) {
+    launch();
+    IMPES_CUDA(cudaEventRecord(e0, s));
+    for (int r = 0; r < reps; ++r) launch();
+    IMPES_CUDA(cudaEventRecord(e1, s));
+    IMPES_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    IMPES_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    return 1e3 * (double)ms / reps;
+  };
+  auto run = [&](auto tag) {
+    using T = decltype(tag);
+    const int slot = LV<T>::slot;
+    for (size_t l = 0; l < h.levels.size(); ++l) {
+      Level& L = *h.levels[l];
+      double* o = out + 4 * l;
+      o[0] = o[1] = o[2] = o[3] = 0.0;
+      if (L.coarsest || !LV<T>::val(L)) continue;
+      Level& Nc = *h.levels[l + 1];
+      o[0] = timed([&] {
+        launch_csr<T, Y_SMOOTH>(L.n, L.avg_row, L.rowptr.p, L.col.p, LV<T>::val(L), LV<T>::x(L), LV<T>::b(L),
+                                LV<T>::inv(L), LV<T>::t(L), s, L.col16.p, L.col16_rel, L.lpr_a[slot]);
+      });
+      o[1] = timed([&] {
+        launch_csr<T, Y_B_MINUS_AX>(L.n, L.avg_row, L.rowptr.p, L.col.p, LV<T>::val(L), LV<T>::x(L),
+                                    LV<T>::b(L), nullptr, LV<T>::r(L), s, L.col16.p, L.col16_rel, L.lpr_a[slot]);
+      });
+      o[2] = timed([&] {
+        launch_csr<T, Y_AX>(L.nc, L.r_avg, L.rrow.p, L.rcol.p, LV<T>::rval(L), LV<T>::r(L), nullptr, nullptr,
+                            LV<T>::t(Nc), s, nullptr, 0, L.lpr_r[slot]);
+      });
+      o[3] = timed([&] {
+        launch_csr<T, Y_ADD_AX>(L.n, L.p_avg, L.prow.p, L.pcol.p, LV<T>::pval(L), LV<T>::x(Nc), nullptr, nullptr,
+                                LV<T>::t(L), s, nullptr, 0, L.lpr_p[slot]);
+      });
+    }
+  };
+  try {
+    if (precision == 1) {
+      IMPES_REQUIRE(h.prm.mixed_precision, IMPES_ERR_STATE, "fp32 levels need mixed_precision=1");
+      run(float{});
+    } else {
+      run(double{});
+    }
+  } catch (...) {
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+}
+
+// The largest cluster (16, else 8 CTAs of kTailThreads) that can be resident.
+template <typename T>
+int tail_cluster_size() {
+  cudaFuncSetAttribute((const void*)k_vcycle_tail<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  cudaGetLastError();
+  for (int c : {16, 8}) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(c);
+    cfg.blockDim = dim3(kTailThreads);
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = c;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int nclusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&nclusters, k_vcycle_tail<T>, &cfg) == cudaSuccess && nclusters >= 1)
+      return c;
+    cudaGetLastError();
+  }
+  return 0;
+}
+
+int amg_tail_level(AMG& h) {
+  for (size_t l = 1; l < h.levels.size(); ++l) {
+    if (!tail_eligible(h, (int)l)) continue;
+    if (h.levels[l]->coarsest) return -1;
+    const int c = std::min(tail_cluster_size<double>(), h.prm.mixed_precision ? tail_cluster_size<float>() : 16);
+    if (c <= 0) return -1;
+    h.tail_cluster = c;
+    return (int)l;
+  }
+  return -1;
+}
 
 void amg_autotune(AMG& h, cudaStream_t s) {
   {
@@ -1149,11 +1470,7 @@ __global__ void k_combine(long long n, const double* __restrict__ Z, long long l
   __shared__ double sy[128];
   for (int q = threadIdx.x; q < k; q += blockDim.x) sy[q] = y[q];
   __syncthreads();
-  GRID_LOOP(i, n) {
-    double v = x[i];
-    for (int q = 0; q < k; ++q) v += sy[q] * Z[q * ldz + i];
-    x[i] = v;
-  }
+  GRID_LOOP(i, n) x[i] = axpy_rows<1>(x[i], sy, k, Z, ldz, i);
 }
 __global__ void k_hadd(int k, double* h, const double* y, const int* pred) {
   pdl_wait_release();
@@ -1314,6 +1631,473 @@ void amg_fgmres(AMG& h, const double* b, double* x, const impes_krylov_params& k
   st.true_rel_res = est_rel;
   launch_pdl(k_mul, grid_for(n, TB), TB, 0, s, n, h.dhalf_inv.p, xs, x);
   IMPES_CHECK_LAUNCH();
+}
+
+// ===================================================== device-driven FGMRES
+// The FGMRES above with its control on the device, for capture into a CUDA
+// graph: the iteration count, the Arnoldi index j, the convergence test and
+// the restart decision live in FgState, every kernel reads j from there, and a
+// conditional WHILE node repeats the iteration body until the last kernel of
+// an iteration clears the node's condition.  One body pass is one iteration
+// (preconditioner application, operator product, Gram-Schmidt with the
+// optional second pass, Givens rotation); at the end of a cycle (converged,
+// j == restart or the iteration cap) the same pass also back-solves, updates
+// x_s and recomputes the true residual, which decides whether to stop or to
+// restart.  Same arithmetic and order as amg_fgmres; no host synchronisation
+// until the caller reads the state after the graph.
+namespace {
+__global__ void k_fg_init(FgState* st, const double* part_b, const double* part_r, int nb, double tol,
+                          int max_iters, int m1, double* g, cudaGraphConditionalHandle cond) {
+  pdl_wait_release();
+  double b2 = 0.0, r2 = 0.0;
+  for (int q = 0; q < nb; ++q) { b2 += part_b[q]; r2 += part_r[q]; }
+  FgState t{};
+  t.bnorm = sqrt(b2);
+  t.beta = sqrt(r2);
+  t.rel = t.bnorm > 0.0 ? t.beta / t.bnorm : 0.0;
+  t.true_rel = t.rel;
+  t.bzero = !(t.bnorm > 0.0);
+  t.nan = !(t.beta == t.beta) || !(t.bnorm == t.bnorm);
+  t.converged = t.bzero || t.rel < tol;
+  t.done = t.bzero || t.nan || t.rel < tol || max_iters <= 0;
+  *st = t;
+  for (int i = 0; i < m1; ++i) g[i] = 0.0;
+  g[0] = t.beta;
+  cudaGraphSetConditional(cond, t.done ? 0u : 1u);
+}
+// V[0] /= beta while the solve goes on (after k_fg_init or a restart)
+__global__ void k_fg_scale_v0(long long n, double* V, const FgState* st, int after_restart) {
+  pdl_wait_release();
+  if (st->done || (after_restart && !st->cycle_end)) return;
+  const double inv = 1.0 / st->beta;
+  GRID_LOOP(i, n) V[i] *= inv;
+}
+// preconditioner input: V[j] ./ wt in the V-cycle's precision; a new pass
+// clears the cycle-end flag of the previous one
+template <typename T>
+__global__ void k_fg_prec_in(long long n, const double* __restrict__ V, const double* __restrict__ wt,
+                             T* __restrict__ out, FgState* st) {
+  pdl_wait_release();
+  const long long j = st->j;
+  GRID_LOOP(i, n) out[i] = (T)(V[j * n + i] / wt[i]);
+  if (blockIdx.x == 0 && threadIdx.x == 0) st->cycle_end = 0;
+}
+template <typename T>
+__global__ void k_fg_z_out(long long n, const T* __restrict__ in, double* __restrict__ Z, const FgState* st) {
+  pdl_wait_release();
+  const long long j = st->j;
+  GRID_LOOP(i, n) Z[j * n + i] = (double)in[i];
+}
+// V[j+1] = wt .* (A_s Z[j]), LPR lanes per row (the level-0 Y_W_AX product)
+template <typename CT, int LPR>
+__global__ void __launch_bounds__(TB) k_fg_op(int n, const int* __restrict__ rowptr, const CT* __restrict__ col,
+                                              const double* __restrict__ val, const double* __restrict__ Z,
+                                              const double* __restrict__ wt, double* __restrict__ V, int rel,
+                                              const FgState* st) {
+  pdl_wait_release();
+  const long long j = st->j;
+  const double* x = Z + j * n;
+  double* y = V + (j + 1) * (long long)n;
+  const int g = threadIdx.x / LPR, lane = threadIdx.x % LPR;
+  const int rows_per_block = TB / LPR;
+  for (long long row = (long long)blockIdx.x * rows_per_block + g; row < n;
+       row += (long long)gridDim.x * rows_per_block) {
+    double acc = 0.0;
+    const int a = rowptr[row], e = rowptr[row + 1];
+    const int cb = col_base<CT>(row, rel);
+    for (int k = a + lane; k < e; k += LPR) acc += val[k] * x[cb + (int)col[k]];
+#pragma unroll
+    for (int o = LPR / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, LPR);
+    if (lane == 0) y[row] = wt[row] * acc;
+  }
+}
+// Gram-Schmidt dots of pass `pass` against w = V[j+1]: pass 0 over V[0..j] and
+// w.w (k_multidot_g's self); pass 1 only when the reorth flag is set.
+__global__ void __launch_bounds__(TB) k_fg_multidot(long long n, const double* __restrict__ V,
+                                                    double* __restrict__ partial, const FgState* st, int pass) {
+  pdl_wait_release();
+  if (pass == 1 && !st->reorth) return;
+  const int j = st->j, k = j + 1, self = pass == 0;
+  const int q0 = blockIdx.y * kMD;
+  if (q0 >= k + self) return;
+  const double* w = V + (long long)(j + 1) * n;
+  __shared__ double sm[kMD][TB / 32];
+  double acc[kMD];
+#pragma unroll
+  for (int u = 0; u < kMD; ++u) acc[u] = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double wi = w[i];
+#pragma unroll
+    for (int u = 0; u < kMD; ++u) {
+      const int q = q0 + u;
+      if (q < k) acc[u] += V[q * n + i] * wi;
+      else if (q == k && self) acc[u] += wi * wi;
+    }
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int u = 0; u < kMD; ++u) {
+    double v = warp_sum(acc[u]);
+    if (lane == 0) sm[u][wid] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < kMD && q0 + (int)threadIdx.x < k + self) {
+    double t = 0.0;
+    for (int u = 0; u < TB / 32; ++u) t += sm[threadIdx.x][u];
+    partial[(q0 + threadIdx.x) * kDotBlocks + blockIdx.x] = t;
+  }
+}
+// block q sums the partials of dot q (fixed order) into column j of H (pass 0,
+// q <= j + 1: entry j + 1 is ||w||^2 until k_fg_hcol) or into y (pass 1)
+__global__ void k_fg_finalize(const double* partial, double* H, int ldh, double* y, const FgState* st,
+                              int pass) {
+  pdl_wait_release();
+  if (pass == 1 && !st->reorth) return;
+  const int j = st->j, q = blockIdx.x;
+  if (q > j + (pass == 0 ? 1 : 0)) return;
+  double t = 0.0;
+  for (int b = threadIdx.x; b < kDotBlocks; b += 32) t += partial[q * kDotBlocks + b];
+  t = warp_sum(t);
+  if (threadIdx.x == 0) (pass == 0 ? H + (long long)j * ldh : y)[q] = t;
+}
+// w -= sum_q h_q V[q] (h = column j of H, or y in pass 1), with norm partials
+__global__ void __launch_bounds__(TB) k_fg_update(long long n, double* __restrict__ V, const double* __restrict__ H,
+                                                  int ldh, const double* __restrict__ y,
+                                                  double* __restrict__ partial, const FgState* st, int pass) {
+  pdl_wait_release();
+  if (pass == 1 && !st->reorth) return;
+  __shared__ double sh[128];
+  __shared__ double sm[TB / 32];
+  const int j = st->j, k = j + 1;
+  const double* h = pass == 0 ? H + (long long)j * ldh : y;
+  for (int q = threadIdx.x; q < k; q += blockDim.x) sh[q] = h[q];
+  __syncthreads();
+  double* w = V + (long long)(j + 1) * n;
+  double acc = 0.0;
+  GRID_LOOP(i, n) {
+    const double v = axpy_rows<-1>(w[i], sh, k, V, n, i);
+    w[i] = v;
+    acc += v * v;
+  }
+  double t = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double u = 0.0;
+    for (int q = 0; q < TB / 32; ++q) u += sm[q];
+    partial[blockIdx.x] = u;
+  }
+}
+// ||w||^2 after a pass; after pass 0 also the second-pass flag (the first pass
+// left less than 0.7 of the norm) -- FgState::wn2 / reorth
+__global__ void k_fg_norm(const double* partial, FgState* st, const double* H, int ldh, int pass) {
+  pdl_wait_release();
+  if (pass == 1 && !st->reorth) return;
+  double t = 0.0;
+  for (int b = threadIdx.x; b < kDotBlocks; b += 32) t += partial[b];
+  t = warp_sum(t);
+  if (threadIdx.x == 0) {
+    st->wn2 = t;
+    if (pass == 0) st->reorth = t < 0.49 * H[(long long)st->j * ldh + st->j + 1];
+  }
+}
+// H[:, j] += y after a second pass; H[j+1, j] = ||w||
+__global__ void k_fg_hcol(double* H, int ldh, const double* y, const FgState* st) {
+  pdl_wait_release();
+  const int j = st->j;
+  double* hj = H + (long long)j * ldh;
+  if (st->reorth)
+    for (int q = threadIdx.x; q <= j; q += blockDim.x) hj[q] += y[q];
+  if (threadIdx.x == 0) hj[j + 1] = sqrt(st->wn2);
+}
+__global__ void k_fg_scale_w(long long n, double* V, const FgState* st) {
+  pdl_wait_release();
+  const double inv = 1.0 / sqrt(st->wn2);
+  double* w = V + (long long)(st->j + 1) * n;
+  GRID_LOOP(i, n) w[i] *= inv;
+}
+// Givens rotation of column j (k_givens), the estimate |g[j+1]|, the counters
+// and the continue/cycle-end decision.
+__global__ void k_fg_givens(double* H, int ldh, double* cs, double* sn, double* g, FgState* st, double tol,
+                            int max_iters, int m, cudaGraphConditionalHandle cond) {
+  pdl_wait_release();
+  const int j = st->j;
+  double* hj = H + (long long)j * ldh;
+  for (int i = 0; i < j; ++i) {
+    double t = cs[i] * hj[i] + sn[i] * hj[i + 1];
+    hj[i + 1] = -sn[i] * hj[i] + cs[i] * hj[i + 1];
+    hj[i] = t;
+  }
+  double a = hj[j], b = hj[j + 1];
+  double d = hypot(a, b);
+  double c = d > 0 ? a / d : 1.0, s = d > 0 ? b / d : 0.0;
+  cs[j] = c; sn[j] = s;
+  hj[j] = d; hj[j + 1] = 0.0;
+  g[j + 1] = -s * g[j];
+  g[j] = c * g[j];
+  const double est = fabs(g[j + 1]) / st->bnorm;
+  st->rel = est;
+  st->total += 1;
+  st->j = j + 1;
+  const bool nan = !(est == est);
+  if (nan) st->nan = 1;
+  const bool conv = est < tol;
+  st->cycle_end = nan || conv || st->j >= m || st->total >= max_iters;
+  if (!st->cycle_end) cudaGraphSetConditional(cond, 1u);
+}
+// end of a cycle: y = R^-1 g (k_backsolve over the j columns) ...
+__global__ void k_fg_backsolve(const double* H, int ldh, const double* g, double* y, const FgState* st) {
+  pdl_wait_release();
+  if (!st->cycle_end || st->nan) return;
+  const int k = st->j;
+  for (int i = k - 1; i >= 0; --i) {
+    double s = g[i];
+    for (int jj = i + 1; jj < k; ++jj) s -= H[(long long)jj * ldh + i] * y[jj];
+    y[i] = s / H[(long long)i * ldh + i];
+  }
+}
+// ... x_s += Z y ...
+__global__ void k_fg_combine(long long n, const double* __restrict__ Z, const double* __restrict__ y,
+                             double* __restrict__ x, const FgState* st) {
+  pdl_wait_release();
+  if (!st->cycle_end || st->nan) return;
+  __shared__ double sy[128];
+  const int k = st->j;
+  for (int q = threadIdx.x; q < k; q += blockDim.x) sy[q] = y[q];
+  __syncthreads();
+  GRID_LOOP(i, n) x[i] = axpy_rows<1>(x[i], sy, k, Z, n, i);
+}
+// ... the true residual V[0] = wt .* (b_s - A_s x_s) and its norm partials ...
+template <typename CT, int LPR>
+__global__ void __launch_bounds__(TB) k_fg_resid(int n, const int* __restrict__ rowptr, const CT* __restrict__ col,
+                                                 const double* __restrict__ val, const double* __restrict__ xs,
+                                                 const double* __restrict__ bs, const double* __restrict__ wt,
+                                                 double* __restrict__ V, int rel, double* __restrict__ partial,
+                                                 const FgState* st) {
+  pdl_wait_release();
+  if (!st->cycle_end || st->nan) return;
+  __shared__ double sm[TB / 32];
+  const int g = threadIdx.x / LPR, lane = threadIdx.x % LPR;
+  const int rows_per_block = TB / LPR;
+  double nrm = 0.0;
+  for (long long row = (long long)blockIdx.x * rows_per_block + g; row < n;
+       row += (long long)gridDim.x * rows_per_block) {
+    double acc = 0.0;
+    const int a = rowptr[row], e = rowptr[row + 1];
+    const int cb = col_base<CT>(row, rel);
+    for (int k = a + lane; k < e; k += LPR) acc += val[k] * xs[cb + (int)col[k]];
+#pragma unroll
+    for (int o = LPR / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, LPR);
+    if (lane == 0) {
+      const double v = wt[row] * (bs[row] - acc);
+      V[row] = v;
+      nrm += v * v;
+    }
+  }
+  double t = warp_sum(nrm);
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double u = 0.0;
+    for (int q = 0; q < TB / 32; ++q) u += sm[q];
+    partial[blockIdx.x] = u;
+  }
+}
+// ... and the decision: stop (converged in the true residual, or the cap) or
+// restart with g = beta e_1.
+__global__ void k_fg_restart(const double* partial, int nb, FgState* st, double* g, int m1, double tol,
+                             int max_iters, cudaGraphConditionalHandle cond) {
+  pdl_wait_release();
+  if (!st->cycle_end) return;
+  if (st->nan) {
+    st->done = 1;
+    st->converged = 0;
+    cudaGraphSetConditional(cond, 0u);
+    return;
+  }
+  double r2 = 0.0;
+  for (int q = 0; q < nb; ++q) r2 += partial[q];
+  const double beta = sqrt(r2);
+  st->beta = beta;
+  st->true_rel = beta / st->bnorm;
+  st->rel = st->true_rel;
+  st->restarts += 1;
+  if (!(beta == beta)) st->nan = 1;
+  st->converged = st->true_rel < tol;
+  st->done = st->nan || st->converged || st->total >= max_iters;
+  if (!st->done) {
+    st->j = 0;
+    for (int i = 0; i < m1; ++i) g[i] = 0.0;
+    g[0] = beta;
+  }
+  cudaGraphSetConditional(cond, st->done ? 0u : 1u);
+}
+__global__ void k_fg_final(long long n, const double* dhalf, const double* xs, double* x, const FgState* st) {
+  pdl_wait_release();
+  const bool zero = st->bzero;
+  GRID_LOOP(i, n) x[i] = zero ? 0.0 : dhalf[i] * xs[i];
+}
+// residual-norm partials of a plain vector (the FGMRES right-hand side)
+__global__ void __launch_bounds__(TB) k_fg_norm_partials(long long n, const double* __restrict__ v,
+                                                         double* __restrict__ partial) {
+  pdl_wait_release();
+  __shared__ double sm[TB / 32];
+  double acc = 0.0;
+  GRID_LOOP(i, n) acc += v[i] * v[i];
+  double t = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double u = 0.0;
+    for (int q = 0; q < TB / 32; ++q) u += sm[q];
+    partial[blockIdx.x] = u;
+  }
+}
+
+// level-0 products of the device FGMRES, lanes per row as the level was tuned
+template <typename CT>
+void fg_op(const Level& L0, const CT* col, const double* Z, const double* wt, double* V, int rel,
+           const FgState* st, cudaStream_t s) {
+  const int lpr = L0.lpr_a[0] > 0 ? L0.lpr_a[0] : (L0.avg_row <= 8 ? 1 : L0.avg_row <= 16 ? 4 : 8);
+  const int n = L0.n;
+  auto grid = [&](int l) { return grid_for(((size_t)n * l + TB - 1) / TB * TB, TB, 16); };
+  switch (lpr) {
+    case 1: launch_pdl(k_fg_op<CT, 1>, grid(1), TB, 0, s, n, L0.rowptr.p, col, L0.val.p, Z, wt, V, rel, st); break;
+    case 2: launch_pdl(k_fg_op<CT, 2>, grid(2), TB, 0, s, n, L0.rowptr.p, col, L0.val.p, Z, wt, V, rel, st); break;
+    case 4: launch_pdl(k_fg_op<CT, 4>, grid(4), TB, 0, s, n, L0.rowptr.p, col, L0.val.p, Z, wt, V, rel, st); break;
+    default: launch_pdl(k_fg_op<CT, 8>, grid(8), TB, 0, s, n, L0.rowptr.p, col, L0.val.p, Z, wt, V, rel, st); break;
+  }
+}
+template <typename CT>
+void fg_resid(const Level& L0, const CT* col, const double* xs, const double* bs, const double* wt, double* V,
+              int rel, double* partial, const FgState* st, cudaStream_t s) {
+  const int n = L0.n;
+  // a fixed grid of kDotBlocks blocks: the partials are summed in block order
+  launch_pdl(k_fg_resid<CT, 1>, kDotBlocks, TB, 0, s, n, L0.rowptr.p, col, L0.val.p, xs, bs, wt, V, rel, partial,
+             st);
+}
+}  // namespace
+
+void amg_fgmres_prepare(AMG& h, const impes_krylov_params& kp) {
+  Level& L0 = *h.levels[0];
+  const int n = L0.n;
+  const int m = std::max(1, std::min(kp.restart, 120));
+  if (h.krylov_m != m || h.V.n < (size_t)(m + 1) * n) {
+    h.V.alloc((size_t)(m + 1) * n);
+    h.Z.alloc((size_t)m * n);
+    h.H.alloc((size_t)(m + 2) * (m + 1));
+    h.cs.alloc(m + 1); h.sn.alloc(m + 1); h.g.alloc(m + 2); h.y.alloc(m + 1);
+    h.kw.alloc(n); h.kb.alloc(n); h.kx.alloc(n);
+    h.krylov_m = m;
+  }
+  h.red.ensure((size_t)(m + 2) * kDotBlocks + 2 * kDotBlocks);
+  h.fgst.ensure(1);
+  if (kp.precision == 1)
+    IMPES_REQUIRE(h.prm.mixed_precision, IMPES_ERR_STATE, "fp32 V-cycle needs mixed_precision=1");
+}
+
+void amg_fgmres_capture(AMG& h, const double* b, double* x, const impes_krylov_params& kp, cudaStream_t s) {
+  KrylovModeGuard guard(h);
+  Level& L0 = *h.levels[0];
+  const long long n = L0.n;
+  const int m = h.krylov_m;
+  const int ldh = m + 2;
+  const bool jac = kp.norm == IMPES_NORM_JACOBI;
+  double* wt = jac ? h.jac_w.p : h.kw.p;
+  double* bs = h.kb.p;
+  double* xs = h.kx.p;
+  double* part_b = h.red.p + (size_t)(m + 2) * kDotBlocks;
+  double* part_r = part_b + kDotBlocks;
+  FgState* st = h.fgst.p;
+  const unsigned gn = grid_for(n, TB);
+  // prologue: b_s, x_s, ||wt b_s||, V[0] = wt (b_s - A x_s) and its norm
+  if (!jac) launch_pdl(k_fill, gn, TB, 0, s, n, h.kw.p, 1.0);
+  launch_pdl(k_mul, gn, TB, 0, s, n, (const double*)h.dhalf_inv.p, b, bs);
+  if (kp.use_x0)
+    launch_pdl(k_div_convert<double, double>, gn, TB, 0, s, n, (const double*)x, (const double*)h.dhalf_inv.p, xs);
+  else
+    launch_pdl(k_zero, gn, TB, 0, s, n, xs);
+  launch_pdl(k_mul, gn, TB, 0, s, n, (const double*)wt, (const double*)bs, h.V.p);
+  launch_pdl(k_fg_norm_partials, kDotBlocks, TB, 0, s, n, (const double*)h.V.p, part_b);
+  launch_csr<double, Y_B_MINUS_AX>((int)n, L0.avg_row, L0.rowptr.p, L0.col.p, L0.val.p, xs, bs, nullptr, h.V.p, s,
+                                   L0.col16.p, L0.col16_rel, L0.lpr_a[0]);
+  launch_pdl(k_mul_inplace, gn, TB, 0, s, n, h.V.p, (const double*)wt);
+  launch_pdl(k_fg_norm_partials, kDotBlocks, TB, 0, s, n, (const double*)h.V.p, part_r);
+  // the while node; the init kernel sets its condition (0: nothing to do)
+  cudaStreamCaptureStatus cst;
+  cudaGraph_t cap = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  IMPES_CUDA(cudaStreamGetCaptureInfo(s, &cst, nullptr, &cap, &deps, &ndeps));
+  IMPES_REQUIRE(cst == cudaStreamCaptureStatusActive, IMPES_ERR_STATE, "device FGMRES needs a capturing stream");
+  cudaGraphConditionalHandle cond;
+  IMPES_CUDA(cudaGraphConditionalHandleCreate(&cond, cap, 1, cudaGraphCondAssignDefault));
+  launch_pdl(k_fg_init, 1, 1, 0, s, st, (const double*)part_b, (const double*)part_r, (int)kDotBlocks, kp.tol,
+             kp.max_iters, m + 1, h.g.p, cond);
+  launch_pdl(k_fg_scale_v0, gn, TB, 0, s, n, h.V.p, (const FgState*)st, 0);
+  IMPES_CUDA(cudaStreamGetCaptureInfo(s, &cst, nullptr, &cap, &deps, &ndeps));
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = cond;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t wnode;
+  IMPES_CUDA(cudaGraphAddNode(&wnode, cap, deps, ndeps, &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  // the body, captured on a second stream into the node's graph
+  if (!h.body_stream) IMPES_CUDA(cudaStreamCreateWithFlags(&h.body_stream, cudaStreamNonBlocking));
+  cudaStream_t bsm = h.body_stream;
+  IMPES_CUDA(cudaStreamBeginCaptureToGraph(bsm, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  const unsigned long long body_start = thread_launches();
+  try {
+    const unsigned gb = grid_for(n, TB);
+    if (kp.precision == 1) {
+      launch_pdl(k_fg_prec_in<float>, gb, TB, 0, bsm, n, (const double*)h.V.p, (const double*)wt, L0.bf.p, st);
+      float* zf = vcycle<float>(h, 0, true, bsm);
+      launch_pdl(k_fg_z_out<float>, gb, TB, 0, bsm, n, (const float*)zf, h.Z.p, (const FgState*)st);
+    } else {
+      launch_pdl(k_fg_prec_in<double>, gb, TB, 0, bsm, n, (const double*)h.V.p, (const double*)wt, L0.b.p, st);
+      double* zd = vcycle<double>(h, 0, true, bsm);
+      launch_pdl(k_fg_z_out<double>, gb, TB, 0, bsm, n, (const double*)zd, h.Z.p, (const FgState*)st);
+    }
+    if (L0.col16.p)
+      fg_op<unsigned short>(L0, L0.col16.p, h.Z.p, wt, h.V.p, L0.col16_rel, st, bsm);
+    else
+      fg_op<int>(L0, L0.col.p, h.Z.p, wt, h.V.p, 0, st, bsm);
+    const dim3 gd(kDotBlocks, (unsigned)((m + 2 + kMD - 1) / kMD));
+    for (int pass = 0; pass < 2; ++pass) {
+      launch_pdl(k_fg_multidot, gd, dim3(TB), 0, bsm, n, (const double*)h.V.p, h.red.p, (const FgState*)st, pass);
+      launch_pdl(k_fg_finalize, m + 2, 32, 0, bsm, (const double*)h.red.p, h.H.p, ldh, h.y.p, (const FgState*)st,
+                 pass);
+      launch_pdl(k_fg_update, kDotBlocks, TB, 0, bsm, n, h.V.p, (const double*)h.H.p, ldh, (const double*)h.y.p,
+                 h.red.p, (const FgState*)st, pass);
+      launch_pdl(k_fg_norm, 1, 32, 0, bsm, (const double*)h.red.p, st, (const double*)h.H.p, ldh, pass);
+    }
+    launch_pdl(k_fg_hcol, 1, 128, 0, bsm, h.H.p, ldh, (const double*)h.y.p, (const FgState*)st);
+    launch_pdl(k_fg_scale_w, gb, TB, 0, bsm, n, h.V.p, (const FgState*)st);
+    launch_pdl(k_fg_givens, 1, 1, 0, bsm, h.H.p, ldh, h.cs.p, h.sn.p, h.g.p, st, kp.tol, kp.max_iters, m, cond);
+    launch_pdl(k_fg_backsolve, 1, 1, 0, bsm, (const double*)h.H.p, ldh, (const double*)h.g.p, h.y.p,
+               (const FgState*)st);
+    launch_pdl(k_fg_combine, gb, TB, 0, bsm, n, (const double*)h.Z.p, (const double*)h.y.p, xs, (const FgState*)st);
+    if (L0.col16.p)
+      fg_resid<unsigned short>(L0, L0.col16.p, xs, bs, wt, h.V.p, L0.col16_rel, part_r, st, bsm);
+    else
+      fg_resid<int>(L0, L0.col.p, xs, bs, wt, h.V.p, 0, part_r, st, bsm);
+    launch_pdl(k_fg_restart, 1, 1, 0, bsm, (const double*)part_r, (int)kDotBlocks, st, h.g.p, m + 1, kp.tol,
+               kp.max_iters, cond);
+    launch_pdl(k_fg_scale_v0, gb, TB, 0, bsm, n, h.V.p, (const FgState*)st, 1);
+  } catch (...) {
+    cudaGraph_t dummy = nullptr;
+    cudaStreamEndCapture(bsm, &dummy);
+    throw;
+  }
+  cudaGraph_t body_out = nullptr;
+  IMPES_CUDA(cudaStreamEndCapture(bsm, &body_out));
+  h.fg_body_kernels = (long long)(thread_launches() - body_start);
+  IMPES_CUDA(cudaStreamUpdateCaptureDependencies(s, &wnode, 1, cudaStreamSetCaptureDependencies));
+  // epilogue: x = D^-1/2 x_s (zero for a zero right-hand side)
+  launch_pdl(k_fg_final, gn, TB, 0, s, n, (const double*)h.dhalf_inv.p, (const double*)xs, x, (const FgState*)st);
 }
 
 }  // namespace impes

@@ -1218,6 +1218,11 @@ void amg_setup(AMG& h, int n, int nnz, const int* rowptr, const int* col, const 
   {
     const char* ev = getenv("IMPES_NO_GRAPHS");
     h.use_graphs = !(ev && ev[0] == '1');
+    const char* es = getenv("IMPES_NO_STEP_GRAPH");
+    h.use_step_graph = !(es && es[0] == '1');
+    const char* et = getenv("IMPES_NO_TAIL");
+    h.use_tail = !(et && et[0] == '1');
+    h.tail_level = -1;
   }
   h.levels.clear();
   h.built = false;
@@ -1460,6 +1465,7 @@ void amg_setup(AMG& h, int n, int nnz, const int* rowptr, const int* col, const 
   }
   IMPES_CUDA(cudaStreamSynchronize(s));
   amg_autotune(h, s);
+  h.tail_level = amg_tail_level(h);
   h.built = true;
 }
 

@@ -71,8 +71,9 @@ void model_build_static(Model& m, const double* kx, const double* ky, const doub
 void model_pattern(Model& m, int* rowptr, int* col, cudaStream_t s);
 void model_assemble(Model& m, const double* p, const double* sw, const double* sg, double dt,
                     double* csr_val, double* rhs, cudaStream_t s);
+// pred (device int, may be null): the kernels do nothing unless *pred != 0
 void model_saturation(Model& m, const double* p_new, double* sw, double* sg, double* so,
-                      double dt, cudaStream_t s);
+                      double dt, cudaStream_t s, const int* pred = nullptr);
 
 // Closed-form CSR row pointer of the 7-point pattern (no scan needed).
 __host__ __device__ inline long long pattern_rowptr(long long c, int nx, int ny, int nz) {

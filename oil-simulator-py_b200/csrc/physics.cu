@@ -488,144 +488,179 @@ __global__ void k_well_sources(ModelParams P, const double* __restrict__ pvt_g,
                                const double* __restrict__ p_new, const double* __restrict__ sw,
                                const double* __restrict__ sg, const double* __restrict__ pv,
                                double dt, double* wq /*3*nwc*/, double* bal /*12*/,
-                               double* well_q, double* well_rates) {
+                               double* well_q, double* well_rates, const int* pred) {
+  if (pred && *pred == 0) return;
   __shared__ double s_col[kPvtCols * kMaxPvtRows];
   __shared__ double s_slope[(kPvtCols - 1) * kMaxPvtRows];
+  // per well: its additions to the (water, gas, oil) sources of its cell and to
+  // the component balance (oil in, oil out, gas in, gas out), which phase 2 adds
+  // up in well order; bit k of s_mask marks addition k as made
+  __shared__ double s_q[kMaxWells][3];
+  __shared__ double s_b[kMaxWells][4];
+  __shared__ int s_mask[kMaxWells];
+  __shared__ int s_slot[kMaxWells];
   PvtSmem T{P.pvt_rows, s_col, s_slope};
   if (P.pvt_rows > 0) pvt_stage(pvt_g, P.pvt_rows, s_col, s_slope);
-  if (threadIdx.x != 0) return;
-  for (int s = 0; s < 3 * P.nwc; ++s) wq[s] = 0.0;
   const bool pvt = P.pvt_rows > 0;
   const double so_r = P.so_r, sw_min = P.sw_cr, sg_min = P.sg_cr;
-  for (int w = 0; w < P.nwells; ++w) {
+  // phase 1: every well on its own thread (a well's numbers depend only on its
+  // cell's state)
+  for (int w = threadIdx.x; w < P.nwells; w += blockDim.x) {
     const WellDev W = wells[w];
     const int c = W.cell;
-    if (c < 0) continue;  // outside the grid (simulation.py:1053-1054)
-    const int slot = well_slot(wc_cells, P.nwc, c);
-    double* qw = wq + slot;
-    double* qg = wq + P.nwc + slot;
-    double* qo = wq + 2 * P.nwc + slot;
-    const double p = p_new[c], sw_c = sw[c], sg_c = sg[c], pv_c = pv[c];
-    double mt, fw_, fg_, fo_;
-    well_cell_phase(P, T, p, sw_c, sg_c, mt, fw_, fg_, fo_);
-    double Bo = 0, Bw = 0, Bg = 0, Rs = 0, Rv = 0;
-    if (pvt) {
-      Bo = pvt_at(T, C_BO, p); Bw = pvt_at(T, C_BW, p); Bg = pvt_at(T, C_BG, p);
-      Rs = pvt_at(T, C_RS, p); Rv = pvt_at(T, C_RV, p);
-    }
-    if (W.control_bhp == 0) {
-      const double q_base = (W.value * P.rate_scale) / 86400.0;
-      double q_total;
-      if (W.is_injector && W.surface_rate && pvt)
-        q_total = q_base * (W.injected_phase == 1 ? Bg : Bw);
-      else
-        q_total = q_base;
-      q_total *= (W.is_injector ? 1 : -1);
-      if (W.is_injector) {
-        if (W.injected_phase == 1) {
-          double sg_up = fmax(0.0, (1.0 - so_r - sw_c) - sg_c);
-          double dS = (dt / fmax(pv_c, 1e-12)) * q_total;
-          double alpha = 1.0;
-          if (dS > 0.0) alpha = fmin(alpha, sg_up / fmax(dS, 1e-12));
-          else alpha = fmin(alpha, (sg_c - sg_min) / fmax(fabs(dS), 1e-12));
-          q_total *= fmax(0.0, fmin(1.0, alpha));
-          *qg += q_total;
-          if (pvt) {
-            double qg_surf = fmax(q_total, 0.0) / fmax(Bg, 1e-12) * 86400.0;
-            double scale = dt / 86400.0;
-            bal[6 + 3 + 0] += qg_surf * scale;        // gas in
-            bal[6 + 0] += Rv * qg_surf * scale;       // oil in
-          }
-        } else {
-          double sw_up = fmax(0.0, (1.0 - so_r - sg_c) - sw_c);
-          double dS = (dt / fmax(pv_c, 1e-12)) * q_total;
-          double alpha = 1.0;
-          if (dS > 0.0) alpha = fmin(alpha, sw_up / fmax(dS, 1e-12));
-          else alpha = fmin(alpha, (sw_c - sw_min) / fmax(fabs(dS), 1e-12));
-          q_total *= fmax(0.0, fmin(1.0, alpha));
-          *qw += q_total;
-        }
-        continue;
-      }
-      // producer at rate
+    int mask = 0;
+    double dq[3] = {0.0, 0.0, 0.0}, db[4] = {0.0, 0.0, 0.0, 0.0};
+    s_slot[w] = -1;
+    if (c >= 0) {  // a well outside the grid contributes nothing (simulation.py:1053-1054)
+      s_slot[w] = well_slot(wc_cells, P.nwc, c);
+      const double p = p_new[c], sw_c = sw[c], sg_c = sg[c], pv_c = pv[c];
+      double mt, fw_, fg_, fo_;
+      well_cell_phase(P, T, p, sw_c, sg_c, mt, fw_, fg_, fo_);
+      double Bo = 0, Bw = 0, Bg = 0, Rs = 0, Rv = 0;
       if (pvt) {
-        if (W.surface_rate) {
-          switch (W.surface_phase) {
-            case 0: q_total = -(q_base / fmax(fo_ / fmax(Bo, 1e-12) + fg_ * Rv / fmax(Bg, 1e-12), 1e-12)); break;
-            case 1: q_total = -(q_base * Bw) / fmax(fw_, 1e-8); break;
-            case 2: q_total = -(q_base / fmax(fg_ / fmax(Bg, 1e-12) + fo_ * Rs / fmax(Bo, 1e-12), 1e-12)); break;
-            default:
-              q_total = -(q_base / fmax(fo_ / fmax(Bo, 1e-12) + fg_ * Rv / fmax(Bg, 1e-12) +
-                                            fw_ / fmax(Bw, 1e-12), 1e-12));
-          }
-        }
-        double sw_up = fmax(0.0, (1.0 - so_r - sg_c) - sw_c);
-        double sw_dn = fmax(0.0, sw_c - sw_min);
-        double sg_up = fmax(0.0, (1.0 - so_r - sw_c) - sg_c);
-        double sg_dn = fmax(0.0, sg_c - sg_min);
-        double dSw = (dt / fmax(pv_c, 1e-12)) * (q_total * fw_);
-        double dSg = (dt / fmax(pv_c, 1e-12)) * (q_total * fg_);
-        double alpha = 1.0;
-        alpha = dSw > 0.0 ? fmin(alpha, sw_up / fmax(dSw, 1e-12)) : fmin(alpha, sw_dn / fmax(fabs(dSw), 1e-12));
-        alpha = dSg > 0.0 ? fmin(alpha, sg_up / fmax(dSg, 1e-12)) : fmin(alpha, sg_dn / fmax(fabs(dSg), 1e-12));
-        alpha = fmax(0.0, fmin(1.0, alpha));
-        q_total *= alpha;
-        if (W.limit_mask) {
-          double d_o = fo_ / fmax(Bo, 1e-12) + fg_ * Rv / fmax(Bg, 1e-12);
-          double d_w = fw_ / fmax(Bw, 1e-12);
-          double d_g = fg_ / fmax(Bg, 1e-12) + fo_ * Rs / fmax(Bo, 1e-12);
-          double d_l = d_o + d_w;
-          double mx = INFINITY;
-          bool any = false;
-          if ((W.limit_mask & 1) && d_o > 0) { mx = fmin(mx, (W.limits[0] / 86400.0) / d_o); any = true; }
-          if ((W.limit_mask & 2) && d_w > 0) { mx = fmin(mx, (W.limits[1] / 86400.0) / d_w); any = true; }
-          if ((W.limit_mask & 4) && d_g > 0) { mx = fmin(mx, (W.limits[2] / 86400.0) / d_g); any = true; }
-          if ((W.limit_mask & 8) && d_l > 0) { mx = fmin(mx, (W.limits[3] / 86400.0) / d_l); any = true; }
-          if (any && fabs(q_total) > mx) q_total = -mx;
-        }
-        double aq = fabs(q_total);
-        double oil_s = aq * (fo_ / fmax(Bo, 1e-12) + fg_ * Rv / fmax(Bg, 1e-12)) * 86400.0;
-        double wat_s = aq * (fw_ / fmax(Bw, 1e-12)) * 86400.0;
-        double gas_s = aq * (fg_ / fmax(Bg, 1e-12) + fo_ * Rs / fmax(Bo, 1e-12)) * 86400.0;
-        well_rates[4 * w + 0] = oil_s;
-        well_rates[4 * w + 1] = wat_s;
-        well_rates[4 * w + 2] = gas_s;
-        well_rates[4 * w + 3] = oil_s + wat_s;
-        well_q[w] = q_total;
-        double qo_res = -q_total * fo_, qg_res = -q_total * fg_;
-        bal[6 + 1] += dt * (fmax(qo_res, 0.0) / fmax(Bo, 1e-12) + Rv * fmax(qg_res, 0.0) / fmax(Bg, 1e-12));
-        bal[6 + 4] += dt * (fmax(qg_res, 0.0) / fmax(Bg, 1e-12) + Rs * fmax(qo_res, 0.0) / fmax(Bo, 1e-12));
+        Bo = pvt_at(T, C_BO, p); Bw = pvt_at(T, C_BW, p); Bg = pvt_at(T, C_BG, p);
+        Rs = pvt_at(T, C_RS, p); Rv = pvt_at(T, C_RV, p);
       }
-      *qw += q_total * fw_;
-      *qg += q_total * fg_;
-      *qo += q_total * fo_;
-    } else {
-      const double p_bhp = W.value * 1e6;
-      const double q_total = W.well_index * mt * (p - p_bhp);
-      if (W.is_injector) {
-        if (W.injected_phase == 1) {
-          *qg += -q_total;
-          if (pvt) {
-            double qg_surf = fmax(-q_total, 0.0) / fmax(Bg, 1e-12) * 86400.0;
-            double scale = dt / 86400.0;
-            bal[6 + 3] += qg_surf * scale;
-            bal[6 + 0] += Rv * qg_surf * scale;
+      if (W.control_bhp == 0) {
+        const double q_base = (W.value * P.rate_scale) / 86400.0;
+        double q_total;
+        if (W.is_injector && W.surface_rate && pvt)
+          q_total = q_base * (W.injected_phase == 1 ? Bg : Bw);
+        else
+          q_total = q_base;
+        q_total *= (W.is_injector ? 1 : -1);
+        if (W.is_injector) {
+          if (W.injected_phase == 1) {
+            double sg_up = fmax(0.0, (1.0 - so_r - sw_c) - sg_c);
+            double dS = (dt / fmax(pv_c, 1e-12)) * q_total;
+            double alpha = 1.0;
+            if (dS > 0.0) alpha = fmin(alpha, sg_up / fmax(dS, 1e-12));
+            else alpha = fmin(alpha, (sg_c - sg_min) / fmax(fabs(dS), 1e-12));
+            q_total *= fmax(0.0, fmin(1.0, alpha));
+            dq[1] = q_total; mask |= 2;
+            if (pvt) {
+              double qg_surf = fmax(q_total, 0.0) / fmax(Bg, 1e-12) * 86400.0;
+              double scale = dt / 86400.0;
+              db[2] = qg_surf * scale;        // gas in
+              db[0] = Rv * qg_surf * scale;   // oil in
+              mask |= 8 | 32;
+            }
+          } else {
+            double sw_up = fmax(0.0, (1.0 - so_r - sg_c) - sw_c);
+            double dS = (dt / fmax(pv_c, 1e-12)) * q_total;
+            double alpha = 1.0;
+            if (dS > 0.0) alpha = fmin(alpha, sw_up / fmax(dS, 1e-12));
+            else alpha = fmin(alpha, (sw_c - sw_min) / fmax(fabs(dS), 1e-12));
+            q_total *= fmax(0.0, fmin(1.0, alpha));
+            dq[0] = q_total; mask |= 1;
           }
         } else {
-          *qw += -q_total;
+          // producer at rate
+          if (pvt) {
+            if (W.surface_rate) {
+              switch (W.surface_phase) {
+                case 0: q_total = -(q_base / fmax(fo_ / fmax(Bo, 1e-12) + fg_ * Rv / fmax(Bg, 1e-12), 1e-12)); break;
+                case 1: q_total = -(q_base * Bw) / fmax(fw_, 1e-8); break;
+                case 2: q_total = -(q_base / fmax(fg_ / fmax(Bg, 1e-12) + fo_ * Rs / fmax(Bo, 1e-12), 1e-12)); break;
+                default:
+                  q_total = -(q_base / fmax(fo_ / fmax(Bo, 1e-12) + fg_ * Rv / fmax(Bg, 1e-12) +
+                                                fw_ / fmax(Bw, 1e-12), 1e-12));
+              }
+            }
+            double sw_up = fmax(0.0, (1.0 - so_r - sg_c) - sw_c);
+            double sw_dn = fmax(0.0, sw_c - sw_min);
+            double sg_up = fmax(0.0, (1.0 - so_r - sw_c) - sg_c);
+            double sg_dn = fmax(0.0, sg_c - sg_min);
+            double dSw = (dt / fmax(pv_c, 1e-12)) * (q_total * fw_);
+            double dSg = (dt / fmax(pv_c, 1e-12)) * (q_total * fg_);
+            double alpha = 1.0;
+            alpha = dSw > 0.0 ? fmin(alpha, sw_up / fmax(dSw, 1e-12)) : fmin(alpha, sw_dn / fmax(fabs(dSw), 1e-12));
+            alpha = dSg > 0.0 ? fmin(alpha, sg_up / fmax(dSg, 1e-12)) : fmin(alpha, sg_dn / fmax(fabs(dSg), 1e-12));
+            alpha = fmax(0.0, fmin(1.0, alpha));
+            q_total *= alpha;
+            if (W.limit_mask) {
+              double d_o = fo_ / fmax(Bo, 1e-12) + fg_ * Rv / fmax(Bg, 1e-12);
+              double d_w = fw_ / fmax(Bw, 1e-12);
+              double d_g = fg_ / fmax(Bg, 1e-12) + fo_ * Rs / fmax(Bo, 1e-12);
+              double d_l = d_o + d_w;
+              double mx = INFINITY;
+              bool any = false;
+              if ((W.limit_mask & 1) && d_o > 0) { mx = fmin(mx, (W.limits[0] / 86400.0) / d_o); any = true; }
+              if ((W.limit_mask & 2) && d_w > 0) { mx = fmin(mx, (W.limits[1] / 86400.0) / d_w); any = true; }
+              if ((W.limit_mask & 4) && d_g > 0) { mx = fmin(mx, (W.limits[2] / 86400.0) / d_g); any = true; }
+              if ((W.limit_mask & 8) && d_l > 0) { mx = fmin(mx, (W.limits[3] / 86400.0) / d_l); any = true; }
+              if (any && fabs(q_total) > mx) q_total = -mx;
+            }
+            double aq = fabs(q_total);
+            double oil_s = aq * (fo_ / fmax(Bo, 1e-12) + fg_ * Rv / fmax(Bg, 1e-12)) * 86400.0;
+            double wat_s = aq * (fw_ / fmax(Bw, 1e-12)) * 86400.0;
+            double gas_s = aq * (fg_ / fmax(Bg, 1e-12) + fo_ * Rs / fmax(Bo, 1e-12)) * 86400.0;
+            well_rates[4 * w + 0] = oil_s;
+            well_rates[4 * w + 1] = wat_s;
+            well_rates[4 * w + 2] = gas_s;
+            well_rates[4 * w + 3] = oil_s + wat_s;
+            well_q[w] = q_total;
+            double qo_res = -q_total * fo_, qg_res = -q_total * fg_;
+            db[1] = dt * (fmax(qo_res, 0.0) / fmax(Bo, 1e-12) + Rv * fmax(qg_res, 0.0) / fmax(Bg, 1e-12));
+            db[3] = dt * (fmax(qg_res, 0.0) / fmax(Bg, 1e-12) + Rs * fmax(qo_res, 0.0) / fmax(Bo, 1e-12));
+            mask |= 16 | 64;
+          }
+          dq[0] = q_total * fw_;
+          dq[1] = q_total * fg_;
+          dq[2] = q_total * fo_;
+          mask |= 1 | 2 | 4;
         }
       } else {
-        *qw += (-q_total) * fw_;
-        *qg += (-q_total) * fg_;
-        *qo += (-q_total) * fo_;
-        if (pvt) {
-          double qabs = fabs(q_total);
-          double qo_res = qabs * fo_, qg_res = qabs * fg_;
-          bal[6 + 1] += dt * (qo_res / fmax(Bo, 1e-12) + Rv * qg_res / fmax(Bg, 1e-12));
-          bal[6 + 4] += dt * (qg_res / fmax(Bg, 1e-12) + Rs * qo_res / fmax(Bo, 1e-12));
+        const double p_bhp = W.value * 1e6;
+        const double q_total = W.well_index * mt * (p - p_bhp);
+        if (W.is_injector) {
+          if (W.injected_phase == 1) {
+            dq[1] = -q_total; mask |= 2;
+            if (pvt) {
+              double qg_surf = fmax(-q_total, 0.0) / fmax(Bg, 1e-12) * 86400.0;
+              double scale = dt / 86400.0;
+              db[2] = qg_surf * scale;
+              db[0] = Rv * qg_surf * scale;
+              mask |= 8 | 32;
+            }
+          } else {
+            dq[0] = -q_total; mask |= 1;
+          }
+        } else {
+          dq[0] = (-q_total) * fw_;
+          dq[1] = (-q_total) * fg_;
+          dq[2] = (-q_total) * fo_;
+          mask |= 1 | 2 | 4;
+          if (pvt) {
+            double qabs = fabs(q_total);
+            double qo_res = qabs * fo_, qg_res = qabs * fg_;
+            db[1] = dt * (qo_res / fmax(Bo, 1e-12) + Rv * qg_res / fmax(Bg, 1e-12));
+            db[3] = dt * (qg_res / fmax(Bg, 1e-12) + Rs * qo_res / fmax(Bo, 1e-12));
+            mask |= 16 | 64;
+          }
         }
       }
     }
+    s_mask[w] = mask;
+    for (int k = 0; k < 3; ++k) s_q[w][k] = dq[k];
+    for (int k = 0; k < 4; ++k) s_b[w][k] = db[k];
+  }
+  __syncthreads();
+  // phase 2: the sums in the reference's well order (one thread)
+  if (threadIdx.x != 0) return;
+  for (int t = 0; t < 3 * P.nwc; ++t) wq[t] = 0.0;
+  for (int w = 0; w < P.nwells; ++w) {
+    const int slot = s_slot[w], mask = s_mask[w];
+    if (slot < 0) continue;
+    if (mask & 1) wq[slot] += s_q[w][0];
+    if (mask & 2) wq[P.nwc + slot] += s_q[w][1];
+    if (mask & 4) wq[2 * P.nwc + slot] += s_q[w][2];
+    // balance additions in the order the serial loop made them: gas in then
+    // oil in (gas injectors), oil out then gas out (producers)
+    if (mask & 32) bal[6 + 3] += s_b[w][2];
+    if (mask & 8) bal[6 + 0] += s_b[w][0];
+    if (mask & 16) bal[6 + 1] += s_b[w][1];
+    if (mask & 64) bal[6 + 4] += s_b[w][3];
   }
 }
 
@@ -638,7 +673,8 @@ __global__ void __launch_bounds__(256) k_saturation_flux(
     const double* __restrict__ ty, const double* __restrict__ tz, const double* __restrict__ pv,
     const int* __restrict__ wc_cells, const double* __restrict__ wq, double dt,
     double* __restrict__ dsw_out, double* __restrict__ dsg_out, double* __restrict__ red,
-    unsigned* __restrict__ counter, int* __restrict__ nsub_out) {
+    unsigned* __restrict__ counter, int* __restrict__ nsub_out, const int* pred) {
+  if (pred && *pred == 0) return;
   extern __shared__ double smem[];
   double* s_pvt_col = smem;
   double* s_pvt_slope = s_pvt_col + kPvtCols * kMaxPvtRows;
@@ -791,7 +827,8 @@ __global__ void k_well_substeps(ModelParams P, const double* __restrict__ pvt_g,
                                 const double* __restrict__ sw, const double* __restrict__ sg,
                                 const double* __restrict__ dsw, const double* __restrict__ dsg,
                                 const int* __restrict__ nsub, double dt, double* __restrict__ contrib,
-                                double* bal) {
+                                double* bal, const int* pred) {
+  if (pred && *pred == 0) return;
   // contrib[(s * nwells + w) * 4 + q]: the addend of bal[6 + {0, 1, 3, 4}[q]] for
   // substep s and well w (never negative), -1 where the reference adds nothing
   __shared__ double s_col[kPvtCols * kMaxPvtRows];
@@ -891,7 +928,8 @@ __global__ void __launch_bounds__(kSatBlock) k_saturation_substeps(
     double* __restrict__ sw, double* __restrict__ sg, double* __restrict__ so,
     const double* __restrict__ dsw, const double* __restrict__ dsg, const double* __restrict__ pv,
     const int* __restrict__ nsub, double* __restrict__ red, unsigned* __restrict__ counter,
-    double* __restrict__ bal) {
+    double* __restrict__ bal, const int* pred) {
+  if (pred && *pred == 0) return;
   __shared__ double s_col[kPvtCols * kMaxPvtRows];
   __shared__ double s_slope[(kPvtCols - 1) * kMaxPvtRows];
   __shared__ double s_w[kSatBlock / 32];
@@ -1009,12 +1047,12 @@ void model_assemble(Model& m, const double* p, const double* sw, const double* s
 }
 
 void model_saturation(Model& m, const double* p_new, double* sw, double* sg, double* so, double dt,
-                      cudaStream_t s) {
+                      cudaStream_t s, const int* pred) {
   const ModelParams& P = m.P;
   const int tid = timers().begin(IMPES_PH_SATURATION, s);
   if (P.nwells > 0) {
-    k_well_sources<<<1, 128, 0, s>>>(P, m.pvt.p, m.wells.p, m.wc_cells.p, p_new, sw, sg, m.pv.p,
-                                     dt, m.wq.p, m.balances.p, m.well_q.p, m.well_rates.p); ::impes::count_launch();
+    k_well_sources<<<1, kMaxWells, 0, s>>>(P, m.pvt.p, m.wells.p, m.wc_cells.p, p_new, sw, sg, m.pv.p,
+                                     dt, m.wq.p, m.balances.p, m.well_q.p, m.well_rates.p, pred); ::impes::count_launch();
     IMPES_CHECK_LAUNCH();
   }
   Brick b = make_brick(P);
@@ -1022,17 +1060,17 @@ void model_saturation(Model& m, const double* p_new, double* sw, double* sg, dou
   ensure_smem(k_saturation_flux, brick_smem(b, kK4Fields), g_smem_k4);
   k_saturation_flux<<<blocks, 256, brick_smem(b, kK4Fields), s>>>(
       P, b, m.pvt.p, p_new, sw, sg, m.tx.p, m.ty.p, m.tz.p, m.pv.p, m.wc_cells.p, m.wq.p, dt,
-      m.dsw.p, m.dsg.p, m.red.p, m.counter.p, m.nsub.p); ::impes::count_launch();
+      m.dsw.p, m.dsg.p, m.red.p, m.counter.p, m.nsub.p, pred); ::impes::count_launch();
   IMPES_CHECK_LAUNCH();
   if (P.pvt_rows > 0 && P.nwells > 0) {
     k_well_substeps<<<1, 256, 0, s>>>(P, m.pvt.p, m.wells.p, p_new, sw, sg, m.dsw.p, m.dsg.p,
-                                      m.nsub.p, dt, m.wsub.p, m.balances.p); ::impes::count_launch();
+                                      m.nsub.p, dt, m.wsub.p, m.balances.p, pred); ::impes::count_launch();
     IMPES_CHECK_LAUNCH();
   }
   unsigned g = grid_for(P.N, kSatBlock);
   k_saturation_substeps<<<g, kSatBlock, 0, s>>>(P, m.pvt.p, p_new, sw, sg, so, m.dsw.p, m.dsg.p,
                                                 m.pv.p, m.nsub.p, m.red.p, m.counter.p + 1,
-                                                m.balances.p); ::impes::count_launch();
+                                                m.balances.p, pred); ::impes::count_launch();
   IMPES_CHECK_LAUNCH();
   timers().end(tid, s, 8.0 * (6.0 * P.N + 0.5 * (double)(m.nnz - P.N)));
 }

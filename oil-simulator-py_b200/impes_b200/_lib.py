@@ -135,6 +135,7 @@ _SIGNATURES = {
     "impes_amg_fgmres": ([_P, _P, _P, C.POINTER(KrylovParams), C.POINTER(KrylovStats), _P], _I),
     "impes_amg_num_levels": ([_P, C.POINTER(_I)], _I),
     "impes_amg_level_info": ([_P, _I, C.POINTER(LevelDesc)], _I),
+    "impes_amg_profile_levels": ([_P, _I, _I, C.POINTER(C.c_double), _P], _I),
     "impes_amg_level_export": ([_P, _I, _P, _P, _P, _P, _P, _P, _P, _P], _I),
     "impes_amg_equilibration": ([_P, _P, C.POINTER(_I), _P], _I),
     "impes_model_create": ([C.POINTER(_P), C.POINTER(ModelDesc), C.POINTER(WellDesc), _I, _P,

@@ -17,16 +17,20 @@ Heterogeneous rock is set, as with the reference, by assigning
 before the Simulator is built.
 
 Pressure solvers (``simulation.pressure_solver``): ``"amg"`` runs the reference's
-stand-alone V-cycles with its stopping rule; ``"gmres_amg"`` (also the default)
-runs FGMRES with one V-cycle per iteration, ``simulation.amg.norm`` selecting
+stand-alone V-cycles with its stopping rule; ``"gmres_amg"`` runs FGMRES with one
+V-cycle per iteration, ``simulation.amg.norm`` selecting
 ``"jacobi"`` (default) or ``"equilibrated"``, ``simulation.amg.precision``
 ``"fp64"`` or ``"mixed"`` (fp32 V-cycle), ``simulation.amg.max_iters`` the cap,
 ``simulation.amg.warm_start`` the first iterate: ``"extrapolate"`` (default, linear
 in time from the last two steps), ``"previous"`` or ``false`` (zero).
-Any other value (``"cg"``, the reference's default) runs the reference's
+Any other value, and a configuration without the key, runs the reference's
 Jacobi-PCG (``cg_tolerance``, ``cg_max_iter``, absolute stopping test, one
-relaxed retry).  The default here is ``"gmres_amg"``: with a BHP well the CG's
-absolute test on sqrt(r . D^-1 r) is dominated by the well row and is not met.
+relaxed retry), as the reference's own default does (simulation.py:905).  With a
+BHP well that CG's absolute test on sqrt(r . D^-1 r) is dominated by the well row
+and is not met, as in the reference; ``"gmres_amg"`` is the solver to choose.
+AMG options beyond the reference's: ``simulation.amg.p_max_elements`` /
+``p_trunc_factor`` (interpolation truncation) and ``smoother`` (``"l1jacobi"`` or
+``"chebyshev"``).
 """
 from __future__ import annotations
 
@@ -414,7 +418,7 @@ class Simulator:
         self.g = 9.81
         self.porous_volume = reservoir.porous_volume
         amg_cfg = sim_params.get("amg", {}) or {}
-        self.pressure_solver = sim_params.get("pressure_solver", "gmres_amg")
+        self.pressure_solver = sim_params.get("pressure_solver", "cg")   # simulation.py:905
         self.amg_tol = float(amg_cfg.get("tol", sim_params.get("cg_tolerance", 1e-6)))
         self.amg_max_cycles = int(amg_cfg.get("max_cycles", 20))
         self.amg_max_iters = int(amg_cfg.get("max_iters", 400))
@@ -605,6 +609,20 @@ class Simulator:
         for w, c in zip(wells, cells):
             w.cell_index_flat = int(c)
         self._wells_stale = False
+
+    def amg_profile_levels(self, precision: str = "mixed", reps: int = 20):
+        """Per-level device times (us) of one sweep, residual, restriction and
+        prolongation of the pressure hierarchy (instrumentation)."""
+        if self._amg_h is None:
+            return []
+        nl = C.c_int(0)
+        check(lib.impes_amg_num_levels(self._amg_h, C.byref(nl)))
+        out = (C.c_double * (4 * nl.value))()
+        prec = 1 if precision in ("mixed", "fp32") else 0
+        with torch.cuda.device(self.device):
+            check(lib.impes_amg_profile_levels(self._amg_h, prec, int(reps), out, _lib.stream_of(self.device)),
+                  "impes_amg_profile_levels")
+        return [tuple(out[4 * l:4 * l + 4]) for l in range(nl.value)]
 
     def amg_levels(self):
         """[(n, nnz, p_cols, p_nnz, is_coarsest, columns, lanes)] of the pressure

@@ -37,7 +37,10 @@ def oracle_model(g):
 def gpu_sim(cfg, fields, **amg):
     from impes_b200.simulator import build_from_config
     cfg = json.loads(json.dumps(cfg))
-    cfg.setdefault("simulation", {}).setdefault("amg", {}).update(amg)
+    # the FGMRES solver unless the configuration names one (the drop-in default
+    # is the reference's own Jacobi-PCG)
+    cfg.setdefault("simulation", {}).setdefault("pressure_solver", "gmres_amg")
+    cfg["simulation"].setdefault("amg", {}).update(amg)
     return build_from_config(cfg, fields, device="cuda")
 
 

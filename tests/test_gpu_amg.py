@@ -426,3 +426,29 @@ def test_chebyshev_trajectory_matches_reference(golden, precision):
         assert np.abs(to_np(fl.pressure) - g["p"][s]).max() <= 1e-8 * np.abs(g["p"][s]).max(), s
         assert np.abs(to_np(fl.s_w) - g["sw"][s]).max() <= 1e-8
         assert np.abs(to_np(fl.s_g) - g["sg"][s]).max() <= 1e-8
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_fused_vcycle_tail_matches_per_level_kernels(monkeypatch, precision):
+    """The levels of at most 24,576 rows run as one thread-block-cluster launch
+    per V-cycle (cluster barriers between the phases).  Its V-cycle equals the
+    per-level kernels' (IMPES_NO_TAIL=1, read at setup) to rounding: the fused
+    kernel sums each row with its own lane count."""
+    A = _laplacian_3d(40, 40, 24)
+    n = A.shape[0]
+    rng = np.random.default_rng(3)
+    bs = rng.standard_normal(n)
+    out = {}
+    for flag in ("1", "0"):
+        monkeypatch.setenv("IMPES_NO_TAIL", flag)
+        amg = gpu_amg(A, coarsest_size=60, seed=2, mixed_precision=True)
+        assert amg.levels[0]["n"] > 24576
+        v = to_np(amg.vcycle_scaled(torch.tensor(bs, device="cuda"), precision=precision))
+        x, st = amg.fgmres(torch.tensor(bs, device="cuda"), tol=1e-10, norm="jacobi", precision=precision)
+        assert st["converged"], st
+        out[flag] = (v, to_np(x), st["iterations"])
+        amg.close()
+    tol = 1e-12 if precision == "fp64" else 1e-5
+    assert np.linalg.norm(out["0"][0] - out["1"][0]) <= tol * np.linalg.norm(out["1"][0])
+    assert np.linalg.norm(out["0"][1] - out["1"][1]) <= 1e-8 * np.linalg.norm(out["1"][1])
+    assert abs(out["0"][2] - out["1"][2]) <= 1

@@ -157,7 +157,8 @@ def test_bhp_min_autoswitch_and_limits():
         "reservoir": {"dimensions": [5, 5, 1], "grid_size": [10, 10, 10], "porosity": 0.2,
                       "permeability": 100.0, "k_vertical_fraction": 1.0},
         "fluid": {"pressure": 10.0, "s_w": 0.2, "s_g": 0.0, "pvt": {"table": scenarios.pvt_table_black_oil()}},
-        "simulation": {"solver_type": "impes", "amg": {"tol": 1e-12, "coarsest_size": 10}},
+        "simulation": {"solver_type": "impes", "pressure_solver": "gmres_amg",
+                       "amg": {"tol": 1e-12, "coarsest_size": 10}},
     }
     cfg1 = json.loads(json.dumps(base))
     cfg1["wells"] = [{"name": "P1", "type": "producer", "i": 2, "j": 2, "k": 0, "radius": 0.1,
@@ -244,3 +245,51 @@ def test_run_writes_reference_result_files(tmp_path):
     assert txt.startswith("=== SUMMARY (final) ===\nPressure MPa: min=")
     assert "=== MASS BALANCE (kg) ===" in txt and "total net=" in txt
     assert sim.step_count == 4
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_whole_step_graph_matches_host_driven_steps(golden, monkeypatch, precision):
+    """From the second step on, an FGMRES step runs as one CUDA graph (assembly,
+    Galerkin update, device-driven FGMRES under a conditional WHILE node,
+    saturation).  Its trajectory equals the host-driven step's to rounding
+    (the device solver sums its norms in another order) and the reference's
+    at 1e-8."""
+    g = golden("gas_injection_12x12x3")
+    cfg, f = cfg_fields(g)
+    out = {}
+    for flag in ("1", "0"):
+        monkeypatch.setenv("IMPES_NO_STEP_GRAPH", flag)
+        _, fl, _, sim = gpu_sim(cfg, f, tol=1e-13, norm="jacobi", precision=precision, max_iters=400,
+                                restart=40)
+        traj = []
+        for s in range(g["p"].shape[0]):
+            assert sim.run_step(float(g["dt"]))
+            assert sim.last_krylov["converged"], sim.last_krylov
+            traj.append((to_np(fl.pressure), to_np(fl.s_w), to_np(fl.s_g), sim.last_krylov["iterations"]))
+            assert np.abs(traj[-1][0] - g["p"][s]).max() <= 1e-8 * np.abs(g["p"][s]).max()
+            assert np.abs(traj[-1][1] - g["sw"][s]).max() <= 1e-8
+        out[flag] = traj
+        sim.close()
+    for (p1, w1, s1, i1), (p0, w0, s0, i0) in zip(out["1"], out["0"]):
+        assert np.abs(p1 - p0).max() <= 1e-11 * np.abs(p1).max()
+        assert np.abs(w1 - w0).max() <= 1e-11 and np.abs(s1 - s0).max() <= 1e-11
+        assert abs(i1 - i0) <= 1
+
+
+def test_whole_step_graph_failed_solve_leaves_state(golden):
+    """A step graph whose solve misses its tolerance restores the pressure and
+    skips the saturation update on the device; run_step retries at dt/2 as the
+    reference does and reports failure, with the state untouched."""
+    g = golden("two_phase_16x16x2")
+    cfg, f = cfg_fields(g)
+    _, fl, _, sim = gpu_sim(cfg, f, tol=1e-10, norm="jacobi", max_iters=400, restart=40)
+    assert sim.run_step(float(g["dt"]))             # builds the hierarchy (host path)
+    assert sim.run_step(float(g["dt"]))             # first step graph
+    p0, w0 = fl.pressure.clone(), fl.s_w.clone()
+    sim.amg_max_iters = 1
+    sim.amg_tol = 1e-30
+    sim.sim_params["max_time_step_attempts"] = 2
+    assert not sim.run_step(float(g["dt"]))
+    assert torch.equal(fl.pressure, p0) and torch.equal(fl.s_w, w0)
+    sim.amg_max_iters, sim.amg_tol = 400, 1e-10
+    assert sim.run_step(float(g["dt"]))
