@@ -320,6 +320,7 @@ def run_adjoint(device):
     """Forward run and adjoint gradient of the history-matching objective; device
     times come from the library's own CUDA events (forward run; reverse sweep
     with the recomputation of the checkpointed segments)."""
+    import torch
     from impes_b200 import scenarios
     from impes_b200.adjoint import misfit_gradient, producer_rates
     steps = 50
@@ -333,6 +334,13 @@ def run_adjoint(device):
                               adjoint_tol=1e-10, device=device)
         runs.append(out["stats"])
     st = runs[-1]
+    # the same gradient with the fp32 V-cycle inside both FGMRES solves, against
+    # the fp64 one (norm-relative)
+    mixed = misfit_gradient(cfg, f, target, steps, dt, checkpoint_every=10, tol=1e-10, adjoint_tol=1e-10,
+                            device=device, precision="mixed")
+    g64 = torch.cat([out["g_lnk"].reshape(-1), out["g_poro"].reshape(-1)])
+    g32 = torch.cat([mixed["g_lnk"].reshape(-1), mixed["g_poro"].reshape(-1)])
+    mixed_err = float((g32 - g64).norm() / g64.norm())
     fwd = statistics.median(r["forward_ms"] for r in runs[1:])
     rev = statistics.median(r["reverse_ms"] for r in runs[1:])
     return {"workload": ADJOINT_WORKLOAD, "cells": 64 * 64 * 8, "steps": steps,
@@ -340,7 +348,9 @@ def run_adjoint(device):
             "gradient_over_forward": (fwd + rev) / fwd, "J": st["J"],
             "forward_fgmres_iterations": st["forward_iterations"],
             "adjoint_fgmres_iterations": st["adjoint_iterations"],
-            "recomputed_steps": st["recomputed_steps"]}
+            "recomputed_steps": st["recomputed_steps"],
+            "mixed_precision_gradient_rel_err_vs_fp64": mixed_err,
+            "mixed_forward_ms": mixed["stats"]["forward_ms"], "mixed_reverse_ms": mixed["stats"]["reverse_ms"]}
 
 
 ENSEMBLE_WORKLOAD = ("ensemble: 64 oil-water realisations (seed 4), nx, ny in {32,48,64,96,128}, "
@@ -641,7 +651,8 @@ def run_ours(args, world, rank, local):
                                      "mixed_speedup": sig((plain["ms"] / plain["steps"]) / (mixed["ms"] / steps), 3)}
     if adjoint is not None:
         line["adjoint"] = {"forward_ms": sig(adjoint["forward_ms"]), "reverse_ms": sig(adjoint["reverse_ms"]),
-                           "gradient_over_forward": sig(adjoint["gradient_over_forward"], 3)}
+                           "gradient_over_forward": sig(adjoint["gradient_over_forward"], 3),
+                           "mixed_grad_err_vs_fp64": sig(adjoint["mixed_precision_gradient_rel_err_vs_fp64"], 2)}
     if ensemble is not None:
         line["ensemble"] = {k: sig(ensemble[k]) for k in ("cell_steps_per_s", "loop_cell_steps_per_s",
                                                           "speedup_vs_loop", "drift_s_abs_vs_fp64")

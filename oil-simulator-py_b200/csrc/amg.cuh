@@ -114,7 +114,7 @@ struct AMG {
   bool step_graph_failed = false;       // capture refused once: keep the host-driven path
   bool use_graphs = true;
   bool use_step_graph = true;           // whole IMPES steps as graphs (IMPES_NO_STEP_GRAPH=1: off)
-  bool use_tail = true;                 // fused V-cycle tail (IMPES_NO_TAIL=1: off)
+  bool use_tail = false;                // fused V-cycle tail (IMPES_TAIL=1: on)
   int tail_level = -1;                  // first level of the fused tail, -1: none
   int tail_cluster = 0;                 // CTAs in the tail's cluster (16 or 8)
   void drop_graphs() {

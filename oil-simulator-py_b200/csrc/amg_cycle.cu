@@ -590,6 +590,7 @@ __global__ void __launch_bounds__(NT) k_gauss_jordan(int n, GJArgs args) {
   __shared__ int s_idx[NT / 32];
   __shared__ int s_p;
   __shared__ double s_inv;
+  __shared__ int s_perm[512];        // row interchanges (n <= 500), kept on chip
   extern __shared__ double s_dyn[];
   double* s_row = s_dyn;             // n (pivot row)
   double* s_col = s_row + n;         // n (pivot column)
@@ -621,7 +622,7 @@ __global__ void __launch_bounds__(NT) k_gauss_jordan(int n, GJArgs args) {
       for (int w = 0; w < nw; ++w)
         if (s_val[w] > bv || (s_val[w] == bv && s_idx[w] < b)) { bv = s_val[w]; b = s_idx[w]; }
       s_p = b;
-      perm[k] = b;
+      s_perm[k] = b;
       if (!(bv > 0.0)) *args.singular[blockIdx.x] = 1;
       const double piv = M[b * n + k];
       s_inv = piv != 0.0 ? 1.0 / piv : 0.0;
@@ -651,8 +652,9 @@ __global__ void __launch_bounds__(NT) k_gauss_jordan(int n, GJArgs args) {
     __syncthreads();
   }
   // undo the row interchanges as column interchanges, last first
+  for (int k = threadIdx.x; k < n; k += blockDim.x) perm[k] = s_perm[k];
   for (int k = n - 1; k >= 0; --k) {
-    const int p = perm[k];
+    const int p = s_perm[k];
     if (p != k)
       for (int i = threadIdx.x; i < n; i += blockDim.x) {
         const double a = M[i * n + k];
@@ -880,15 +882,21 @@ double vcycle_bytes(const AMG& h, int l) {
 // ------------------------------------------------- fused V-cycle tail
 // The levels of at most kTailRows rows (and the dense coarsest solve) cost a
 // few microseconds per kernel whatever their size: each does 8 launches per
-// V-cycle.  kTail runs the whole V-cycle of those levels in ONE launch of a
-// thread-block cluster, with a hardware cluster barrier (barrier.cluster
+// V-cycle.  k_vcycle_tail runs the whole V-cycle of those levels in ONE launch
+// of a thread-block cluster, with a hardware cluster barrier (barrier.cluster
 // arrive.release / wait.acquire) between the phases: the same sequence as
 // vcycle() -- first sweep from zero, two sweeps, residual, restriction, the
 // next level, prolongation, two sweeps; the dense coarsest apply -- with
 // kTailLanes lanes per row.  Vectors that change between phases are read past
 // L1 (ld.global.cg).  Chebyshev hierarchies keep the per-level kernels.
-constexpr int kTailRows = 24576;
-constexpr int kTailLanes = 8;
+//
+// Opt-in (IMPES_TAIL=1): on the 1e6-cell hierarchy one phase of the cluster
+// kernel costs ~2.5 us per pass over its rows, no less than a programmatic-
+// dependent launch of the per-level kernel on all 148 SMs, and a 16-CTA cluster
+// needs several passes per phase on levels of more than a few thousand rows
+// (fusing the levels of <= 24,576 rows made the step 15.4 ms against 11.7).
+constexpr int kTailRows = 4096;
+constexpr int kTailLanes = 4;
 constexpr int kTailThreads = 1024;
 constexpr int kTailMaxLevels = 16;
 

@@ -1220,8 +1220,8 @@ void amg_setup(AMG& h, int n, int nnz, const int* rowptr, const int* col, const 
     h.use_graphs = !(ev && ev[0] == '1');
     const char* es = getenv("IMPES_NO_STEP_GRAPH");
     h.use_step_graph = !(es && es[0] == '1');
-    const char* et = getenv("IMPES_NO_TAIL");
-    h.use_tail = !(et && et[0] == '1');
+    const char* et = getenv("IMPES_TAIL");
+    h.use_tail = et && et[0] == '1';
     h.tail_level = -1;
   }
   h.levels.clear();

@@ -28,8 +28,19 @@ from .simulator import build_from_config
 __all__ = ["producer_rates", "misfit_gradient", "misfit", "MisfitFunction"]
 
 
-def _krylov(tol, restart=60, max_iters=2000, use_x0=1):
-    return _lib.KrylovParams(float(tol), int(restart), int(max_iters), _lib.NORM_JACOBI, 0, int(use_x0))
+def _krylov(tol, restart=60, max_iters=2000, use_x0=1, precision="fp64"):
+    prec = 1 if precision in ("mixed", "fp32") else 0
+    return _lib.KrylovParams(float(tol), int(restart), int(max_iters), _lib.NORM_JACOBI, prec, int(use_x0))
+
+
+def _with_precision(cfg, precision):
+    """The configuration with its AMG hierarchy keeping fp32 levels when the
+    solves use the fp32 V-cycle."""
+    if precision == "fp64":
+        return cfg
+    sim = dict(cfg["simulation"])
+    sim["amg"] = dict(sim.get("amg", {}), precision="mixed")
+    return dict(cfg, simulation=sim)
 
 
 def _fields(cfg, lnk, poro, ky_ratio, kz_ratio):
@@ -68,10 +79,11 @@ def producer_rates(cfg: dict, fields: dict, steps: int, dt: Optional[float] = No
 
 def misfit_gradient(cfg: dict, fields: dict, target, steps: int, dt: Optional[float] = None, *,
                     checkpoint_every: int = 10, tol: float = 1e-11, adjoint_tol: float = 1e-11,
-                    device="cuda") -> dict:
+                    device="cuda", precision: str = "fp64") -> dict:
     """J, dJ/dln k and dJ/dphi (device tensors shaped like the grid), the forward
-    rates and the run statistics."""
-    fl, sim = _sim(cfg, fields, device)
+    rates and the run statistics.  ``precision="mixed"`` runs the forward and
+    adjoint FGMRES solves with the fp32 V-cycle (fp64 Krylov vectors)."""
+    fl, sim = _sim(_with_precision(cfg, precision), fields, device)
     try:
         n = C.c_int()
         check(lib.impes_adjoint_num_producers(sim._h, C.byref(n)), "impes_adjoint_num_producers")
@@ -83,7 +95,7 @@ def misfit_gradient(cfg: dict, fields: dict, target, steps: int, dt: Optional[fl
         kx, ky, kz, _ = sim._rock
         p0 = fl.pressure.reshape(-1).contiguous()
         sw0 = fl.s_w.reshape(-1).contiguous()
-        kf, ka = _krylov(tol), _krylov(adjoint_tol, use_x0=0)
+        kf, ka = _krylov(tol, precision=precision), _krylov(adjoint_tol, use_x0=0, precision=precision)
         st = _lib.AdjointStats()
         check(lib.impes_adjoint_gradient(sim._h, sim._amg_h, ptr(p0), ptr(sw0), ptr(kx), ptr(ky), ptr(kz),
                                          int(steps), int(checkpoint_every), _dt(cfg, dt), C.byref(kf),

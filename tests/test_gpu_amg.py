@@ -430,19 +430,19 @@ def test_chebyshev_trajectory_matches_reference(golden, precision):
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_fused_vcycle_tail_matches_per_level_kernels(monkeypatch, precision):
-    """The levels of at most 24,576 rows run as one thread-block-cluster launch
-    per V-cycle (cluster barriers between the phases).  Its V-cycle equals the
-    per-level kernels' (IMPES_NO_TAIL=1, read at setup) to rounding: the fused
-    kernel sums each row with its own lane count."""
+    """With IMPES_TAIL=1 (read at setup) the levels of at most 4,096 rows run
+    as one thread-block-cluster launch per V-cycle (cluster barriers between
+    the phases).  Its V-cycle equals the per-level kernels' to rounding: the
+    fused kernel sums each row with its own lane count."""
     A = _laplacian_3d(40, 40, 24)
     n = A.shape[0]
     rng = np.random.default_rng(3)
     bs = rng.standard_normal(n)
     out = {}
-    for flag in ("1", "0"):
-        monkeypatch.setenv("IMPES_NO_TAIL", flag)
+    for flag in ("0", "1"):
+        monkeypatch.setenv("IMPES_TAIL", flag)
         amg = gpu_amg(A, coarsest_size=60, seed=2, mixed_precision=True)
-        assert amg.levels[0]["n"] > 24576
+        assert amg.levels[0]["n"] > 4096
         v = to_np(amg.vcycle_scaled(torch.tensor(bs, device="cuda"), precision=precision))
         x, st = amg.fgmres(torch.tensor(bs, device="cuda"), tol=1e-10, norm="jacobi", precision=precision)
         assert st["converged"], st
