@@ -218,14 +218,14 @@ class ClockSampler:
 
 
 def make_sim(cfg, fields, precision, device, restart=30, solver="gmres_amg", warm_start="extrapolate",
-             trunc=0, smoother="l1jacobi"):
+             trunc=0, smoother="l1jacobi", tol=PRESSURE_TOL):
     """FGMRES + V-cycle (solver="gmres_amg"), or the plain stand-alone V-cycles of
     the reference (solver="amg"), both stopping at PRESSURE_TOL in the Jacobi norm;
     `trunc` caps the interpolation's row length (0: the reference's interpolation)."""
     from impes_b200.simulator import build_from_config
     c = json.loads(json.dumps(cfg))
     c["simulation"]["pressure_solver"] = solver
-    c["simulation"]["amg"].update({"tol": PRESSURE_TOL, "norm": "jacobi", "precision": precision,
+    c["simulation"]["amg"].update({"tol": tol, "norm": "jacobi", "precision": precision,
                                    "restart": restart, "max_iters": 600, "max_cycles": 3000, "seed": 0,
                                    "warm_start": warm_start, "p_max_elements": int(trunc),
                                    "smoother": smoother})
@@ -551,6 +551,22 @@ def run_ours(args, world, rank, local):
         results[(precision, tr)] = run_variant(args, cfg, fields, precision, device, dt, flush, stream, dist,
                                                rank, local, tr, label)
 
+    tight = None
+    if args.precision == "both":
+        # the same number of steps in fp64 solved to 1e-10: how far the 1e-6
+        # solve tolerance alone moves the state (against the mixed-vs-fp64 drift)
+        r64 = results[("fp64", trunc)]
+        _, flt, _, simt = make_sim(cfg, fields, "fp64", device, restart=args.restart, trunc=trunc, tol=1e-10)
+        for _ in range(r64["steps_run"]):
+            if not simt.run_step(dt):
+                raise RuntimeError("tight fp64 step failed to converge")
+        tight = {"s_abs": float(max((flt.s_w - r64["sw"]).abs().max(), (flt.s_g - r64["sg"]).abs().max())),
+                 "p_rel": float((flt.pressure - r64["p"]).abs().max() / flt.pressure.abs().max()),
+                 "steps": r64["steps_run"]}
+        simt.close()
+        del simt, flt
+        torch.cuda.empty_cache()
+
     plain = None
     if args.precision == "both" and not args.no_plain:
         # the plain FP64 GPU path: the reference's stand-alone V-cycles on the
@@ -636,9 +652,11 @@ def run_ours(args, world, rank, local):
         "fp64": {"value": sig(fp64_value), "ms_per_step": sig(fp64["ms"] / steps),
                  "vcycles_per_step": sig(statistics.mean(fp64["iters"]), 3),
                  "mixed_speedup": sig(fp64["ms"] / mixed["ms"], 3)},
-        "drift_vs_fp64": {"s_abs": sig(drift_sw, 2), "p_rel": sig(drift_p, 2)},
+        "drift_vs_fp64": {"s_abs": sig(drift_sw, 2), "p_rel": sig(drift_p, 2), "steps": mixed["steps_run"]},
         "mass_balance_error": sig(mixed["mass_err"], 2),
     }
+    if tight is not None:
+        line["fp64_tol_1e-6_vs_1e-10"] = {"s_abs": sig(tight["s_abs"], 2), "p_rel": sig(tight["p_rel"], 2)}
     if ("mixed", 0) in results and trunc:
         rm, rf = results[("mixed", 0)], results[("fp64", 0)]
         line["ref_interp"] = {"ms_mixed": sig(rm["ms"] / steps), "ms_fp64": sig(rf["ms"] / steps),

@@ -39,6 +39,28 @@ __device__ __forceinline__ int col_base(long long row, int rel) {
   return (sizeof(CT) == 2 && rel) ? (int)row - 32768 : 0;
 }
 
+// sum_k val[k] * x[cb + col[k]] over k = a0, a0 + S, ... < e, added in that
+// order; four entries' loads are issued before their products are added, so
+// each thread keeps four gathers of x in flight (the rows of the coarse levels
+// are latency-bound on the column -> x chain).  Same result bits as the plain
+// loop.
+template <typename T, typename CT, typename XT>
+__device__ __forceinline__ T row_dot(int a0, int e, int S, const T* __restrict__ val, const CT* __restrict__ col,
+                                     const XT* __restrict__ x, int cb, T acc) {
+  int k = a0;
+  for (; k + 3 * S < e; k += 4 * S) {
+    const T v0 = val[k], v1 = val[k + S], v2 = val[k + 2 * S], v3 = val[k + 3 * S];
+    const int c0 = (int)col[k], c1 = (int)col[k + S], c2 = (int)col[k + 2 * S], c3 = (int)col[k + 3 * S];
+    const T x0 = x[cb + c0], x1 = x[cb + c1], x2 = x[cb + c2], x3 = x[cb + c3];
+    acc += v0 * x0;
+    acc += v1 * x1;
+    acc += v2 * x2;
+    acc += v3 * x3;
+  }
+  for (; k < e; k += S) acc += val[k] * x[cb + (int)col[k]];
+  return acc;
+}
+
 template <typename T, typename CT, int LPR, int MODE>
 __global__ void __launch_bounds__(TB) k_csr(int n, const int* __restrict__ rowptr,
                                             const CT* __restrict__ col, const T* __restrict__ val,
@@ -53,7 +75,7 @@ __global__ void __launch_bounds__(TB) k_csr(int n, const int* __restrict__ rowpt
     if (MODE != Y_SMOOTH0) {
       const int a = rowptr[row], e = rowptr[row + 1];
       const int cb = col_base<CT>(row, rel);
-      for (int k = a + lane; k < e; k += LPR) acc += val[k] * x[cb + (int)col[k]];
+      acc = row_dot(a + lane, e, LPR, val, col, x, cb, acc);
 #pragma unroll
       for (int o = LPR / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, LPR);
     }
@@ -92,7 +114,7 @@ __global__ void __launch_bounds__(TB) k_csr_rows(int n, const int* __restrict__ 
     if (row < n) {
       const int a = rowptr[row], e = rowptr[row + 1];
       const int cb = col_base<CT>(row, rel);
-      for (int k = a + tid; k < e; k += G) acc += val[k] * x[cb + (int)col[k]];
+      acc = row_dot(a + tid, e, G, val, col, x, cb, acc);
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
     }
@@ -330,7 +352,7 @@ __global__ void __launch_bounds__(TB) k_cheb(int n, const int* __restrict__ rowp
     T acc = T(0);
     const int a = rowptr[row], e = rowptr[row + 1];
     const int cb = col_base<CT>(row, rel);
-    for (int k = a + lane; k < e; k += LPR) acc += val[k] * v[cb + (int)col[k]];
+    acc = row_dot(a + lane, e, LPR, val, col, v, cb, acc);
 #pragma unroll
     for (int o = LPR / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, LPR);
     if (lane == 0) {
@@ -464,6 +486,66 @@ __global__ void __launch_bounds__(TB) k_multidot(long long n, const double* __re
     partial[threadIdx.x * kDotBlocks + blockIdx.x] = t;
   }
 }
+// Gram-Schmidt dot accumulation over this thread's elements (grid stride),
+// two elements per trip so that each thread has the loads of 2 x 8 vectors in
+// flight; every accumulator adds its elements in index order, as a one-element
+// loop would.
+__device__ __forceinline__ void multidot_acc(double* acc, long long n, const double* __restrict__ V,
+                                             long long ldv, int q0, int k, int self,
+                                             const double* __restrict__ w) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  for (; i + stride < n; i += 2 * stride) {
+    const double w0 = w[i], w1 = w[i + stride];
+    double a0[kMD], a1[kMD];
+#pragma unroll
+    for (int u = 0; u < kMD; ++u) {
+      const int q = q0 + u;
+      a0[u] = q < k ? V[q * ldv + i] : w0;
+      a1[u] = q < k ? V[q * ldv + i + stride] : w1;
+    }
+#pragma unroll
+    for (int u = 0; u < kMD; ++u) {
+      const int q = q0 + u;
+      if (q < k || (q == k && self)) {
+        acc[u] += a0[u] * w0;
+        acc[u] += a1[u] * w1;
+      }
+    }
+  }
+  for (; i < n; i += stride) {
+    const double wi = w[i];
+#pragma unroll
+    for (int u = 0; u < kMD; ++u) {
+      const int q = q0 + u;
+      if (q < k) acc[u] += V[q * ldv + i] * wi;
+      else if (q == k && self) acc[u] += wi * wi;
+    }
+  }
+}
+// w -= sum_q h[q] V[q] over this thread's elements, two per trip; returns the
+// partial sum of squares of the new w in index order.
+__device__ __forceinline__ double update_rows(long long n, const double* __restrict__ V, long long ldv,
+                                              const double* __restrict__ h, int k, double* __restrict__ w) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double acc = 0.0;
+  for (; i + stride < n; i += 2 * stride) {
+    const double v0 = axpy_rows<-1>(w[i], h, k, V, ldv, i);
+    const double v1 = axpy_rows<-1>(w[i + stride], h, k, V, ldv, i + stride);
+    w[i] = v0;
+    w[i + stride] = v1;
+    acc += v0 * v0;
+    acc += v1 * v1;
+  }
+  for (; i < n; i += stride) {
+    const double v = axpy_rows<-1>(w[i], h, k, V, ldv, i);
+    w[i] = v;
+    acc += v * v;
+  }
+  return acc;
+}
+
 // Gram-Schmidt dots of FGMRES in one launch: block (x, g) sums, over its slice
 // of rows, V[q] . w for the 8 vectors q = 8g .. 8g+7 below k, and w . w as
 // vector q = k when self is set; partial[q * kDotBlocks + x].  With pred set
@@ -481,16 +563,7 @@ __global__ void __launch_bounds__(TB) k_multidot_g(long long n, const double* __
   double acc[kMD];
 #pragma unroll
   for (int u = 0; u < kMD; ++u) acc[u] = 0.0;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    const double wi = w[i];
-#pragma unroll
-    for (int u = 0; u < kMD; ++u) {
-      const int q = q0 + u;
-      if (q < k) acc[u] += Vbase[q * ldv + i] * wi;
-      else if (q == k && self) acc[u] += wi * wi;
-    }
-  }
+  multidot_acc(acc, n, Vbase, ldv, q0, k, self, w);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
   for (int u = 0; u < kMD; ++u) {
@@ -534,12 +607,7 @@ __global__ void __launch_bounds__(TB) k_update(long long n, const double* __rest
   __shared__ double s[TB / 32];
   for (int q = threadIdx.x; q < k; q += blockDim.x) sh[q] = h[q];
   __syncthreads();
-  double acc = 0.0;
-  GRID_LOOP(i, n) {
-    const double v = axpy_rows<-1>(w[i], sh, k, Vbase, ldv, i);
-    w[i] = v;
-    acc += v * v;
-  }
+  const double acc = update_rows(n, Vbase, ldv, sh, k, w);
   if (partial) {
     double t = warp_sum(acc);
     if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = t;
@@ -1713,7 +1781,7 @@ __global__ void __launch_bounds__(TB) k_fg_op(int n, const int* __restrict__ row
     double acc = 0.0;
     const int a = rowptr[row], e = rowptr[row + 1];
     const int cb = col_base<CT>(row, rel);
-    for (int k = a + lane; k < e; k += LPR) acc += val[k] * x[cb + (int)col[k]];
+    acc = row_dot(a + lane, e, LPR, val, col, x, cb, acc);
 #pragma unroll
     for (int o = LPR / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, LPR);
     if (lane == 0) y[row] = wt[row] * acc;
@@ -1733,16 +1801,7 @@ __global__ void __launch_bounds__(TB) k_fg_multidot(long long n, const double* _
   double acc[kMD];
 #pragma unroll
   for (int u = 0; u < kMD; ++u) acc[u] = 0.0;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    const double wi = w[i];
-#pragma unroll
-    for (int u = 0; u < kMD; ++u) {
-      const int q = q0 + u;
-      if (q < k) acc[u] += V[q * n + i] * wi;
-      else if (q == k && self) acc[u] += wi * wi;
-    }
-  }
+  multidot_acc(acc, n, V, n, q0, k, self, w);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
   for (int u = 0; u < kMD; ++u) {
@@ -1782,12 +1841,7 @@ __global__ void __launch_bounds__(TB) k_fg_update(long long n, double* __restric
   for (int q = threadIdx.x; q < k; q += blockDim.x) sh[q] = h[q];
   __syncthreads();
   double* w = V + (long long)(j + 1) * n;
-  double acc = 0.0;
-  GRID_LOOP(i, n) {
-    const double v = axpy_rows<-1>(w[i], sh, k, V, n, i);
-    w[i] = v;
-    acc += v * v;
-  }
+  const double acc = update_rows(n, V, n, sh, k, w);
   double t = warp_sum(acc);
   if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = t;
   __syncthreads();
@@ -1894,7 +1948,7 @@ __global__ void __launch_bounds__(TB) k_fg_resid(int n, const int* __restrict__ 
     double acc = 0.0;
     const int a = rowptr[row], e = rowptr[row + 1];
     const int cb = col_base<CT>(row, rel);
-    for (int k = a + lane; k < e; k += LPR) acc += val[k] * xs[cb + (int)col[k]];
+    acc = row_dot(a + lane, e, LPR, val, col, xs, cb, acc);
 #pragma unroll
     for (int o = LPR / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, LPR);
     if (lane == 0) {

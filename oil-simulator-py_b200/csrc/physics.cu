@@ -300,7 +300,7 @@ __global__ void k_pattern(ModelParams P, int* rowptr, int* col) {
 // Shared layout per halo cell: p, mw, mo, mg, rw, ro, rg, pc (8 doubles).
 constexpr int kK1Fields = 8;
 
-__global__ void __launch_bounds__(256) k_assemble(
+__global__ void __launch_bounds__(256, 4) k_assemble(
     ModelParams P, Brick B, const double* __restrict__ pvt_g, const double* __restrict__ p,
     const double* __restrict__ sw, const double* __restrict__ sg, const double* __restrict__ tx,
     const double* __restrict__ ty, const double* __restrict__ tz, const double* __restrict__ pv,
@@ -309,8 +309,9 @@ __global__ void __launch_bounds__(256) k_assemble(
     double dt, double* __restrict__ val, double* __restrict__ rhs) {
   extern __shared__ double smem[];
   double* s_pvt_col = smem;
-  double* s_pvt_slope = s_pvt_col + kPvtCols * kMaxPvtRows;
-  double* s_cells = s_pvt_slope + (kPvtCols - 1) * kMaxPvtRows;
+  const int pvt_r = P.pvt_rows > 0 ? P.pvt_rows : 1;     // tables sized by the actual rows
+  double* s_pvt_slope = s_pvt_col + kPvtCols * pvt_r;
+  double* s_cells = s_pvt_slope + (kPvtCols - 1) * pvt_r;
   const int H = B.HI * B.HJ * B.HK;
   double* s_p = s_cells;
   double* s_mw = s_p + H;
@@ -667,7 +668,7 @@ __global__ void k_well_sources(ModelParams P, const double* __restrict__ pvt_g,
 // K4a: fluxes, divergence, dS and the substep ratio (simulation.py:968-1042, 1351-1379).
 constexpr int kK4Fields = 6;  // p, mw, mg, rw, rg, pcog
 
-__global__ void __launch_bounds__(256) k_saturation_flux(
+__global__ void __launch_bounds__(256, 4) k_saturation_flux(
     ModelParams P, Brick B, const double* __restrict__ pvt_g, const double* __restrict__ p,
     const double* __restrict__ sw, const double* __restrict__ sg, const double* __restrict__ tx,
     const double* __restrict__ ty, const double* __restrict__ tz, const double* __restrict__ pv,
@@ -677,8 +678,9 @@ __global__ void __launch_bounds__(256) k_saturation_flux(
   if (pred && *pred == 0) return;
   extern __shared__ double smem[];
   double* s_pvt_col = smem;
-  double* s_pvt_slope = s_pvt_col + kPvtCols * kMaxPvtRows;
-  double* s_cells = s_pvt_slope + (kPvtCols - 1) * kMaxPvtRows;
+  const int pvt_r = P.pvt_rows > 0 ? P.pvt_rows : 1;     // tables sized by the actual rows
+  double* s_pvt_slope = s_pvt_col + kPvtCols * pvt_r;
+  double* s_cells = s_pvt_slope + (kPvtCols - 1) * pvt_r;
   const int H = B.HI * B.HJ * B.HK;
   double* s_p = s_cells;
   double* s_mw = s_p + H;
@@ -991,8 +993,9 @@ __global__ void __launch_bounds__(kSatBlock) k_saturation_substeps(
   }
 }
 
-size_t brick_smem(const Brick& b, int fields) {
-  return sizeof(double) * ((size_t)kPvtCols * kMaxPvtRows + (size_t)(kPvtCols - 1) * kMaxPvtRows +
+size_t brick_smem(const Brick& b, int fields, int pvt_rows) {
+  const size_t r = pvt_rows > 0 ? (size_t)pvt_rows : 1;
+  return sizeof(double) * ((size_t)kPvtCols * r + (size_t)(kPvtCols - 1) * r +
                            (size_t)fields * b.HI * b.HJ * b.HK);
 }
 
@@ -1036,10 +1039,10 @@ void model_assemble(Model& m, const double* p, const double* sw, const double* s
                     double* csr_val, double* rhs, cudaStream_t s) {
   Brick b = make_brick(m.P);
   int blocks = b.nbi * b.nbj * b.nbk;
-  ensure_smem(k_assemble, brick_smem(b, kK1Fields), g_smem_k1);
+  ensure_smem(k_assemble, brick_smem(b, kK1Fields, m.P.pvt_rows), g_smem_k1);
   const double F = 0.5 * (double)(m.nnz - m.P.N);
   const int tid = timers().begin(IMPES_PH_ASSEMBLE, s);
-  k_assemble<<<blocks, 256, brick_smem(b, kK1Fields), s>>>(
+  k_assemble<<<blocks, 256, brick_smem(b, kK1Fields, m.P.pvt_rows), s>>>(
       m.P, b, m.pvt.p, p, sw, sg, m.tx.p, m.ty.p, m.tz.p, m.pv.p, m.wells.p, m.wc_cells.p,
       m.wc_ptr.p, m.wc_wells.p, m.well_mode.p, dt, csr_val, rhs); ::impes::count_launch();
   IMPES_CHECK_LAUNCH();
@@ -1057,8 +1060,8 @@ void model_saturation(Model& m, const double* p_new, double* sw, double* sg, dou
   }
   Brick b = make_brick(P);
   int blocks = b.nbi * b.nbj * b.nbk;
-  ensure_smem(k_saturation_flux, brick_smem(b, kK4Fields), g_smem_k4);
-  k_saturation_flux<<<blocks, 256, brick_smem(b, kK4Fields), s>>>(
+  ensure_smem(k_saturation_flux, brick_smem(b, kK4Fields, P.pvt_rows), g_smem_k4);
+  k_saturation_flux<<<blocks, 256, brick_smem(b, kK4Fields, P.pvt_rows), s>>>(
       P, b, m.pvt.p, p_new, sw, sg, m.tx.p, m.ty.p, m.tz.p, m.pv.p, m.wc_cells.p, m.wq.p, dt,
       m.dsw.p, m.dsg.p, m.red.p, m.counter.p, m.nsub.p, pred); ::impes::count_launch();
   IMPES_CHECK_LAUNCH();
