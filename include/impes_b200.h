@@ -87,6 +87,8 @@ typedef struct {
   int col_row_relative;  /* 1: 16-bit columns hold col - row + 32768              */
   int lanes[6];          /* autotuned lanes per row of the kernels on A, R (restriction)
                             and P (prolongation): [0..2] fp64, [3..5] fp32; 0 = rule  */
+  int sell[2];           /* 1: the sweeps and residuals on A read the level's SELL-32
+                            (sliced ELLPACK) copy, one lane per row: [0] fp64, [1] fp32 */
 } impes_amg_level_desc;
 
 /* Norms for Krylov stopping tests. */
@@ -177,6 +179,10 @@ int impes_amg_level_info(impes_amg* h, int lvl, impes_amg_level_desc* info);
  * level's work vectors; out_host[4 * level + k], 0 on the coarsest level.
  * Overwrites the hierarchy's work vectors; synchronises the stream. */
 int impes_amg_profile_levels(impes_amg* h, int precision, int reps, double* out_host, void* stream);
+/* Instrumentation: whole IMPES steps this handle holds as CUDA graphs
+ * (impes_step from the second FGMRES step on) and whether a capture was
+ * refused, after which its steps stay host-driven. */
+int impes_amg_step_graphs(impes_amg* h, int* graphs, int* capture_refused);
 /* Copy level `lvl` into caller device buffers (any pointer may be NULL). */
 int impes_amg_level_export(impes_amg* h, int lvl, int* A_rowptr, int* A_col, double* A_val,
                            double* inv_relax, int* P_rowptr, int* P_col, double* P_val,

@@ -133,7 +133,9 @@ bool step_graph_run(Model& m, AMG& a, double* p, double* sw, double* sg, double*
     e.have_prev = extrap; e.dt_prev = extrap ? m.dt_prev : 0.0; e.kp = kp;
     e.fp64_stale_after = a.fp64_stale;
     e.kernels_body = a.fg_body_kernels;
-    e.kernels_fixed = (long long)(thread_launches() - before) - e.kernels_body;
+    e.kernels_reorth = a.fg_reorth_kernels;
+    e.kernels_end = a.fg_end_kernels;
+    e.kernels_fixed = (long long)(thread_launches() - before) - e.kernels_body - e.kernels_reorth - e.kernels_end;
     count_launches(-(long long)(thread_launches() - before));
     a.fp64_stale = stale_before;
     cudaError_t ie = cudaGraphInstantiate(&e.exec, graph, 0);
@@ -152,7 +154,8 @@ bool step_graph_run(Model& m, AMG& a, double* p, double* sw, double* sg, double*
   static_assert(sizeof(FgState) <= 64 * sizeof(double), "state must fit the pinned scratch");
   IMPES_CUDA(cudaMemcpyAsync(hs, a.fgst.p, sizeof(FgState), cudaMemcpyDeviceToHost, s));
   IMPES_CUDA(cudaStreamSynchronize(s));
-  count_launches(g->kernels_fixed + (long long)hs->total * g->kernels_body);
+  count_launches(g->kernels_fixed + (long long)hs->total * g->kernels_body + (long long)hs->reorths * g->kernels_reorth +
+                 (long long)hs->restarts * g->kernels_end);
   st = impes_krylov_stats{hs->total, hs->restarts, hs->converged && !hs->nan ? 1 : 0, hs->rel, hs->true_rel};
   if (hs->nan) throw Error(IMPES_ERR_NAN, "NaN in FGMRES");
   if (!st.converged) return true;            // p was restored by the graph
@@ -290,6 +293,7 @@ int impes_amg_level_info(impes_amg* h, int lvl, impes_amg_level_desc* info) {
       info->lanes[3 * q + 0] = L.lpr_a[q];
       info->lanes[3 * q + 1] = L.lpr_r[q];
       info->lanes[3 * q + 2] = L.lpr_p[q];
+      info->sell[q] = L.sell_on[q] ? 1 : 0;
     }
   });
 }
@@ -299,6 +303,14 @@ int impes_amg_profile_levels(impes_amg* h, int precision, int reps, double* out_
     IMPES_REQUIRE(h && out_host && reps >= 1, IMPES_ERR_ARG, "null argument or reps < 1");
     IMPES_REQUIRE(h->a.built, IMPES_ERR_STATE, "profile before setup");
     amg_profile_levels(h->a, precision, reps, out_host, S(stream));
+  });
+}
+
+int impes_amg_step_graphs(impes_amg* h, int* graphs, int* capture_refused) {
+  return guarded([&] {
+    IMPES_REQUIRE(h && graphs && capture_refused, IMPES_ERR_ARG, "null argument");
+    *graphs = (int)h->a.step_graphs.size();
+    *capture_refused = h->a.step_graph_failed ? 1 : 0;
   });
 }
 

@@ -17,6 +17,20 @@ struct Level {
   // Chebyshev smoother: Gershgorin bound of diag(inv) A as double bits, [0] from
   // the fp64 values, [1] from the fp32 chain (atomicMax of non-negative doubles)
   DBuf<unsigned long long> cheb_lmax;
+  // SELL-32 copy of A (sliced ELLPACK) for the sweeps and residuals: rows in
+  // sell_perm order (sorted by length, longest first, inside windows of
+  // kSellWindow rows), 32 per slice; entry j of lane q of slice s at
+  // sell_ptr[s] + 32 j + q.  Padding entries hold value 0 and the lane's own row
+  // as column.  sell_map is the CSR index of each entry (-1: padding); the
+  // values are gathered from the CSR values after every value change.
+  int sell_slices = 0;
+  long long sell_len = 0;
+  DBuf<int> sell_ptr, sell_perm, sell_map;
+  DBuf<unsigned short> sell_col16;  // when col16 exists (same encoding), else sell_col
+  DBuf<int> sell_col;
+  DBuf<double> sell_val;
+  DBuf<float> sell_valf;
+  bool sell_on[2] = {false, false};  // autotuned: the sweeps/residuals of this precision use SELL
   int avg_row = 7;                 // nnz / n, selects the SpMV row mapping
   // autotuned lanes per row ([0] fp64, [1] fp32; 0 = the mean-row-length rule)
   // of the kernels on A (sweeps, residuals), R (restriction) and P (prolongation)
@@ -63,7 +77,8 @@ struct Level {
 // Solver state of the device-driven FGMRES (amg_cycle.cu), read by the host
 // after the captured solve has run.
 struct FgState {
-  int j, total, restarts, converged, done, cycle_end, reorth, bzero, nan, pad;
+  int j, total, restarts, converged, done, cycle_end, reorth, bzero, nan;
+  int reorths;                          // second Gram-Schmidt passes taken
   double bnorm, beta, wn2, rel, true_rel;
 };
 
@@ -97,8 +112,11 @@ struct AMG {
   VGraph vgraph[2][2][2][2];
   cudaStream_t cap_stream = nullptr;
   cudaStream_t body_stream = nullptr;   // captures the device FGMRES's loop body
+  cudaStream_t if_stream = nullptr;     // captures the IF blocks inside that body
   DBuf<FgState> fgst;                   // device FGMRES state
   long long fg_body_kernels = 0;        // kernels of one device-FGMRES iteration
+  long long fg_reorth_kernels = 0;      // ... of its second Gram-Schmidt pass (IF node)
+  long long fg_end_kernels = 0;         // ... of its cycle-end block (IF node)
   // whole IMPES steps captured as graphs (abi.cu), keyed by the step's inputs
   struct StepGraph {
     cudaGraphExec_t exec = nullptr;
@@ -108,7 +126,7 @@ struct AMG {
     bool have_prev = false;
     impes_krylov_params kp{};
     bool fp64_stale_after = false;
-    long long kernels_fixed = 0, kernels_body = 0;
+    long long kernels_fixed = 0, kernels_body = 0, kernels_reorth = 0, kernels_end = 0;
   };
   std::vector<StepGraph> step_graphs;
   bool step_graph_failed = false;       // capture refused once: keep the host-driven path
@@ -132,6 +150,7 @@ struct AMG {
     drop_graphs();
     if (cap_stream) cudaStreamDestroy(cap_stream);
     if (body_stream) cudaStreamDestroy(body_stream);
+    if (if_stream) cudaStreamDestroy(if_stream);
   }
 };
 

@@ -302,6 +302,68 @@ void launch_csr(int n, int avg, const int* rowptr, const int* col, const T* val,
   IMPES_CHECK_LAUNCH();
 }
 
+// ------------------------------------------------------ SELL-32 sweeps
+// Sliced ELLPACK with slices of one warp (C = 32) and rows sorted by length
+// inside windows (Kreutzer et al., "A unified sparse matrix data format for
+// efficient general sparse matrix-vector multiplication on modern processors
+// with wide SIMD units", SIAM J. Sci. Comput. 36(5), 2014).  One lane per row;
+// at each entry index j the warp's value and column loads are one contiguous
+// segment, where the CSR kernels' loads of 32 rows touch up to 32 segments.
+// Each row's products are added in the row's CSR order (padding adds +0), as
+// k_csr with one lane per row does.  CT and rel as in k_csr; same epilogues.
+template <typename T, typename CT, int MODE>
+__global__ void __launch_bounds__(TB) k_sell(int n, int nslices, const int* __restrict__ sptr,
+                                             const int* __restrict__ perm, const CT* __restrict__ col,
+                                             const T* __restrict__ val, const T* __restrict__ x,
+                                             const T* __restrict__ b, const T* __restrict__ inv,
+                                             T* __restrict__ y, int rel) {
+  pdl_wait_release();
+  const int lane = threadIdx.x & 31;
+  const int warps = (int)((gridDim.x * (unsigned)TB) >> 5);
+  for (int s = (int)((blockIdx.x * (unsigned)TB + threadIdx.x) >> 5); s < nslices; s += warps) {
+    const int r = s * 32 + lane;
+    const int row = perm[r < n ? r : n - 1];
+    const int cb = col_base<CT>(row, rel);
+    const T acc = row_dot(sptr[s] + lane, sptr[s + 1], 32, val, col, x, cb, T(0));
+    if (r < n) {
+      if (MODE == Y_AX) y[row] = acc;
+      else if (MODE == Y_B_MINUS_AX) y[row] = b[row] - acc;
+      else if (MODE == Y_SMOOTH) y[row] = x[row] + T(kOmega) * inv[row] * (b[row] - acc);
+      else if (MODE == Y_ADD_AX) y[row] = y[row] + acc;
+      else if (MODE == Y_W_AX) y[row] = inv[row] * acc;
+    }
+  }
+}
+
+template <typename T> const T* sell_values(const Level& L);
+template <> inline const double* sell_values<double>(const Level& L) { return L.sell_val.p; }
+template <> inline const float* sell_values<float>(const Level& L) { return L.sell_valf.p; }
+
+template <typename T, int MODE>
+void launch_sell(const Level& L, const T* x, const T* b, const T* inv, T* y, cudaStream_t s) {
+  const unsigned grid = grid_for((size_t)L.sell_slices * 32, TB, 16);
+  if (L.sell_col16.p)
+    launch_pdl(k_sell<T, unsigned short, MODE>, grid, TB, 0, s, L.n, L.sell_slices, (const int*)L.sell_ptr.p,
+               (const int*)L.sell_perm.p, (const unsigned short*)L.sell_col16.p, sell_values<T>(L), x, b, inv, y,
+               L.col16_rel);
+  else
+    launch_pdl(k_sell<T, int, MODE>, grid, TB, 0, s, L.n, L.sell_slices, (const int*)L.sell_ptr.p,
+               (const int*)L.sell_perm.p, (const int*)L.sell_col.p, sell_values<T>(L), x, b, inv, y, 0);
+  IMPES_CHECK_LAUNCH();
+}
+
+// A product of a level's A with the layout chosen for this precision (SELL or
+// the CSR kernels with the tuned lanes per row).
+template <typename T, int MODE>
+void launch_a(const Level& L, int slot, const T* x, const T* b, const T* inv, T* y, cudaStream_t s) {
+  if (L.sell_on[slot] && sell_values<T>(L))
+    launch_sell<T, MODE>(L, x, b, inv, y, s);
+  else
+    launch_csr<T, MODE>(L.n, L.avg_row, L.rowptr.p, L.col.p, (const T*)(sizeof(T) == 8 ? (const void*)L.val.p
+                                                                                        : (const void*)L.valf.p),
+                        x, b, inv, y, s, L.col16.p, L.col16_rel, L.lpr_a[slot]);
+}
+
 // ------------------------------------------------------ Chebyshev smoother
 // The Chebyshev iteration for diag(inv) A on [lower * lmax, lmax] (Saad,
 // Iterative Methods for Sparse Linear Systems, 2nd ed., Alg. 12.1), an option of
@@ -551,7 +613,7 @@ __device__ __forceinline__ double update_rows(long long n, const double* __restr
 // vector q = k when self is set; partial[q * kDotBlocks + x].  With pred set
 // the launch does nothing unless *pred is non-zero (the optional second
 // Gram-Schmidt pass, decided on the device).
-__global__ void __launch_bounds__(TB) k_multidot_g(long long n, const double* __restrict__ Vbase,
+__global__ void __launch_bounds__(TB, 4) k_multidot_g(long long n, const double* __restrict__ Vbase,
                                                    long long ldv, int k, int self,
                                                    const double* __restrict__ w,
                                                    double* __restrict__ partial, const int* pred) {
@@ -918,8 +980,7 @@ T* smooth(const AMG& h, Level& L, T* x, T* spare, const T* b, int nu, bool zero_
     const bool wide = L.avg_row > 96;   // the warp-per-row instance of k_csr
     const int tid = top ? timers().begin(IMPES_PH_SMOOTH_L0, s)
                         : (wide ? timers().begin(IMPES_PH_SMOOTH_WIDE, s) : -1);
-    launch_csr<T, Y_SMOOTH>(L.n, L.avg_row, L.rowptr.p, L.col.p, LV<T>::val(L), x, b,
-                            LV<T>::inv(L), spare, s, L.col16.p, L.col16_rel, L.lpr_a[LV<T>::slot]);
+    launch_a<T, Y_SMOOTH>(L, LV<T>::slot, x, b, LV<T>::inv(L), spare, s);
     timers().end(tid, s, sweep_bytes(sizeof(T), L.nnz, L.n, L.col16.p ? 2.0 : 4.0));
     std::swap(x, spare);
   }
@@ -1142,7 +1203,7 @@ void launch_tail(AMG& h, int l, cudaStream_t s) {
 // _v_cycle (classical_amg.py:1037-1106) on level l: input b in LV<T>::b(L),
 // initial x in LV<T>::x(L) (ignored when zero_x); returns the buffer with x.
 template <typename T>
-T* vcycle(AMG& h, int l, bool zero_x, cudaStream_t s) {
+T* vcycle(AMG& h, int l, bool zero_x, cudaStream_t s, bool first_sweep_done = false) {
   Level& L = *h.levels[l];
   if (l > 0 && zero_x && l == h.tail_level && !L.coarsest) {
     launch_tail<T>(h, l, s);
@@ -1162,11 +1223,13 @@ T* vcycle(AMG& h, int l, bool zero_x, cudaStream_t s) {
     return smooth<T>(h, L, LV<T>::x(L), LV<T>::t(L), bp, 50, true, s, false, true);
   }
   const int tid = (l == 0) ? timers().begin(IMPES_PH_VCYCLE, s) : -1;
-  T* x = smooth<T>(h, L, LV<T>::x(L), LV<T>::t(L), LV<T>::b(L), 3, zero_x, s, l == 0);
+  // first_sweep_done: the caller has already formed x = w inv b in x (the
+  // first l1-Jacobi sweep from zero), so two sweeps remain
+  T* x = first_sweep_done ? smooth<T>(h, L, LV<T>::x(L), LV<T>::t(L), LV<T>::b(L), 2, false, s, l == 0)
+                          : smooth<T>(h, L, LV<T>::x(L), LV<T>::t(L), LV<T>::b(L), 3, zero_x, s, l == 0);
   T* spare = (x == LV<T>::x(L)) ? LV<T>::t(L) : LV<T>::x(L);
   Level& Nc = *h.levels[l + 1];
-  launch_csr<T, Y_B_MINUS_AX>(L.n, L.avg_row, L.rowptr.p, L.col.p, LV<T>::val(L), x, LV<T>::b(L),
-                              nullptr, LV<T>::r(L), s, L.col16.p, L.col16_rel, L.lpr_a[LV<T>::slot]);
+  launch_a<T, Y_B_MINUS_AX>(L, LV<T>::slot, x, LV<T>::b(L), nullptr, LV<T>::r(L), s);
   launch_csr<T, Y_AX>(L.nc, L.r_avg, L.rrow.p, L.rcol.p, LV<T>::rval(L), LV<T>::r(L), nullptr,
                       nullptr, LV<T>::b(Nc), s, nullptr, 0, L.lpr_r[LV<T>::slot]);
   T* ec = vcycle<T>(h, l + 1, true, s);
@@ -1278,6 +1341,44 @@ int tune_one(int slot, int kind, int n, int avg, const int* rowptr, const int* c
   return ins.first->second;
 }
 
+// IMPES_SELL=1 (read at setup) puts every level that has a SELL copy on it,
+// whatever the timings say.
+bool sell_forced() {
+  const char* ev = getenv("IMPES_SELL");
+  return ev && ev[0] == '1';
+}
+
+// SELL-32 against the level's tuned CSR sweep: kept when it is more than 3 %
+// faster (cached by shape like the lanes per row).
+template <typename T>
+bool tune_sell(Level& L, int slot, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1) {
+  if (L.sell_slices <= 0 || !sell_values<T>(L)) return false;
+  const int nb = (int)std::lround(2.0 * std::log2((double)L.n));
+  const auto key = std::make_tuple(slot, 3, nb, L.avg_row);
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) return it->second != 0;
+  }
+  auto timed = [&](bool sell) {
+    L.sell_on[slot] = sell;
+    for (int w = 0; w < 2; ++w) launch_a<T, Y_SMOOTH>(L, slot, LV<T>::x(L), LV<T>::b(L), LV<T>::inv(L), LV<T>::t(L), s);
+    IMPES_CUDA(cudaEventRecord(e0, s));
+    for (int w = 0; w < 8; ++w) launch_a<T, Y_SMOOTH>(L, slot, LV<T>::x(L), LV<T>::b(L), LV<T>::inv(L), LV<T>::t(L), s);
+    IMPES_CUDA(cudaEventRecord(e1, s));
+    IMPES_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    IMPES_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    return ms;
+  };
+  const float t_csr = timed(false), t_sell = timed(true);
+  const int pick = t_sell < 0.97f * t_csr ? 1 : 0;
+  L.sell_on[slot] = false;
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  auto ins = g_tune_cache.emplace(key, pick);
+  return ins.first->second != 0;
+}
+
 template <typename T>
 void tune_levels(AMG& h, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1) {
   const int slot = LV<T>::slot;
@@ -1287,6 +1388,8 @@ void tune_levels(AMG& h, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1) {
     L.lpr_a[slot] = tune_one<T, Y_SMOOTH>(slot, 0, L.n, L.avg_row, L.rowptr.p, L.col.p, LV<T>::val(L),
                                           LV<T>::x(L), LV<T>::b(L), LV<T>::inv(L), LV<T>::t(L), L.col16.p,
                                           L.col16_rel, s, e0, e1);
+    L.sell_on[slot] = sell_forced() ? (L.sell_slices > 0 && sell_values<T>(L) != nullptr)
+                                    : tune_sell<T>(L, slot, s, e0, e1);
     L.lpr_r[slot] = tune_one<T, Y_AX>(slot, 1, L.nc, L.r_avg, L.rrow.p, L.rcol.p, LV<T>::rval(L), LV<T>::r(L),
                                       nullptr, nullptr, LV<T>::t(*h.levels[&up - &h.levels[0] + 1]), nullptr, 0,
                                       s, e0, e1);
@@ -1328,12 +1431,10 @@ void amg_profile_levels(AMG& h, int precision, int reps, double* out, cudaStream
       if (L.coarsest || !LV<T>::val(L)) continue;
       Level& Nc = *h.levels[l + 1];
       o[0] = timed([&] {
-        launch_csr<T, Y_SMOOTH>(L.n, L.avg_row, L.rowptr.p, L.col.p, LV<T>::val(L), LV<T>::x(L), LV<T>::b(L),
-                                LV<T>::inv(L), LV<T>::t(L), s, L.col16.p, L.col16_rel, L.lpr_a[slot]);
+        launch_a<T, Y_SMOOTH>(L, slot, LV<T>::x(L), LV<T>::b(L), LV<T>::inv(L), LV<T>::t(L), s);
       });
       o[1] = timed([&] {
-        launch_csr<T, Y_B_MINUS_AX>(L.n, L.avg_row, L.rowptr.p, L.col.p, LV<T>::val(L), LV<T>::x(L),
-                                    LV<T>::b(L), nullptr, LV<T>::r(L), s, L.col16.p, L.col16_rel, L.lpr_a[slot]);
+        launch_a<T, Y_B_MINUS_AX>(L, slot, LV<T>::x(L), LV<T>::b(L), nullptr, LV<T>::r(L), s);
       });
       o[2] = timed([&] {
         launch_csr<T, Y_AX>(L.nc, L.r_avg, L.rrow.p, L.rcol.p, LV<T>::rval(L), LV<T>::r(L), nullptr, nullptr,
@@ -1758,21 +1859,30 @@ __global__ void k_fg_prec_in(long long n, const double* __restrict__ V, const do
   GRID_LOOP(i, n) out[i] = (T)(V[j * n + i] / wt[i]);
   if (blockIdx.x == 0 && threadIdx.x == 0) st->cycle_end = 0;
 }
+// k_fg_prec_in fused with the V-cycle's first level-0 sweep from zero
+// (Y_SMOOTH0, same arithmetic): b = V[j] ./ wt and x = w inv b
 template <typename T>
-__global__ void k_fg_z_out(long long n, const T* __restrict__ in, double* __restrict__ Z, const FgState* st) {
+__global__ void k_fg_prec_smooth0(long long n, const double* __restrict__ V, const double* __restrict__ wt,
+                                  const T* __restrict__ inv, T* __restrict__ b, T* __restrict__ x, FgState* st) {
   pdl_wait_release();
   const long long j = st->j;
-  GRID_LOOP(i, n) Z[j * n + i] = (double)in[i];
+  GRID_LOOP(i, n) {
+    const T bi = (T)(V[j * n + i] / wt[i]);
+    b[i] = bi;
+    x[i] = T(kOmega) * inv[i] * bi;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) st->cycle_end = 0;
 }
-// V[j+1] = wt .* (A_s Z[j]), LPR lanes per row (the level-0 Y_W_AX product)
-template <typename CT, int LPR>
+// Z[j] = z (the preconditioner's output, widened exactly to fp64) and
+// V[j+1] = wt .* (A_s z), LPR lanes per row (the level-0 Y_W_AX product)
+template <typename XT, typename CT, int LPR>
 __global__ void __launch_bounds__(TB) k_fg_op(int n, const int* __restrict__ rowptr, const CT* __restrict__ col,
-                                              const double* __restrict__ val, const double* __restrict__ Z,
-                                              const double* __restrict__ wt, double* __restrict__ V, int rel,
-                                              const FgState* st) {
+                                              const double* __restrict__ val, const XT* __restrict__ x,
+                                              double* __restrict__ Z, const double* __restrict__ wt,
+                                              double* __restrict__ V, int rel, const FgState* st) {
   pdl_wait_release();
   const long long j = st->j;
-  const double* x = Z + j * n;
+  double* zj = Z + j * n;
   double* y = V + (j + 1) * (long long)n;
   const int g = threadIdx.x / LPR, lane = threadIdx.x % LPR;
   const int rows_per_block = TB / LPR;
@@ -1784,12 +1894,15 @@ __global__ void __launch_bounds__(TB) k_fg_op(int n, const int* __restrict__ row
     acc = row_dot(a + lane, e, LPR, val, col, x, cb, acc);
 #pragma unroll
     for (int o = LPR / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, LPR);
-    if (lane == 0) y[row] = wt[row] * acc;
+    if (lane == 0) {
+      y[row] = wt[row] * acc;
+      zj[row] = (double)x[row];
+    }
   }
 }
 // Gram-Schmidt dots of pass `pass` against w = V[j+1]: pass 0 over V[0..j] and
 // w.w (k_multidot_g's self); pass 1 only when the reorth flag is set.
-__global__ void __launch_bounds__(TB) k_fg_multidot(long long n, const double* __restrict__ V,
+__global__ void __launch_bounds__(TB, 4) k_fg_multidot(long long n, const double* __restrict__ V,
                                                     double* __restrict__ partial, const FgState* st, int pass) {
   pdl_wait_release();
   if (pass == 1 && !st->reorth) return;
@@ -1816,7 +1929,7 @@ __global__ void __launch_bounds__(TB) k_fg_multidot(long long n, const double* _
   }
 }
 // block q sums the partials of dot q (fixed order) into column j of H (pass 0,
-// q <= j + 1: entry j + 1 is ||w||^2 until k_fg_hcol) or into y (pass 1)
+// q <= j + 1: entry j + 1 is ||w||^2 until k_fg_column) or into y (pass 1)
 __global__ void k_fg_finalize(const double* partial, double* H, int ldh, double* y, const FgState* st,
                               int pass) {
   pdl_wait_release();
@@ -1853,7 +1966,10 @@ __global__ void __launch_bounds__(TB) k_fg_update(long long n, double* __restric
 }
 // ||w||^2 after a pass; after pass 0 also the second-pass flag (the first pass
 // left less than 0.7 of the norm) -- FgState::wn2 / reorth
-__global__ void k_fg_norm(const double* partial, FgState* st, const double* H, int ldh, int pass) {
+// ||w||^2 from the update's partials; after pass 0 the reorthogonalisation
+// flag, which also opens the conditional node of pass 1
+__global__ void k_fg_norm(const double* partial, FgState* st, const double* H, int ldh, int pass,
+                          cudaGraphConditionalHandle reorth_if) {
   pdl_wait_release();
   if (pass == 1 && !st->reorth) return;
   double t = 0.0;
@@ -1861,31 +1977,35 @@ __global__ void k_fg_norm(const double* partial, FgState* st, const double* H, i
   t = warp_sum(t);
   if (threadIdx.x == 0) {
     st->wn2 = t;
-    if (pass == 0) st->reorth = t < 0.49 * H[(long long)st->j * ldh + st->j + 1];
+    if (pass == 0) {
+      st->reorth = t < 0.49 * H[(long long)st->j * ldh + st->j + 1];
+      st->reorths += st->reorth;
+      cudaGraphSetConditional(reorth_if, st->reorth ? 1u : 0u);
+    }
   }
 }
 // H[:, j] += y after a second pass; H[j+1, j] = ||w||
-__global__ void k_fg_hcol(double* H, int ldh, const double* y, const FgState* st) {
-  pdl_wait_release();
-  const int j = st->j;
-  double* hj = H + (long long)j * ldh;
-  if (st->reorth)
-    for (int q = threadIdx.x; q <= j; q += blockDim.x) hj[q] += y[q];
-  if (threadIdx.x == 0) hj[j + 1] = sqrt(st->wn2);
-}
 __global__ void k_fg_scale_w(long long n, double* V, const FgState* st) {
   pdl_wait_release();
   const double inv = 1.0 / sqrt(st->wn2);
   double* w = V + (long long)(st->j + 1) * n;
   GRID_LOOP(i, n) w[i] *= inv;
 }
-// Givens rotation of column j (k_givens), the estimate |g[j+1]|, the counters
-// and the continue/cycle-end decision.
-__global__ void k_fg_givens(double* H, int ldh, double* cs, double* sn, double* g, FgState* st, double tol,
-                            int max_iters, int m, cudaGraphConditionalHandle cond) {
+// Column j of the Hessenberg matrix in one block: the reorthogonalisation
+// terms and h[j+1][j], then on thread 0 the Givens rotation (k_givens), the
+// estimate |g[j+1]|, the counters, the continue/cycle-end decision and, at a
+// cycle's end, y = R^-1 g (k_backsolve over the j columns).
+__global__ void k_fg_column(double* H, int ldh, double* cs, double* sn, double* g, double* y, FgState* st,
+                            double tol, int max_iters, int m, cudaGraphConditionalHandle cond,
+                            cudaGraphConditionalHandle end_if) {
   pdl_wait_release();
   const int j = st->j;
   double* hj = H + (long long)j * ldh;
+  if (st->reorth)
+    for (int q = threadIdx.x; q <= j; q += blockDim.x) hj[q] += y[q];
+  if (threadIdx.x == 0) hj[j + 1] = sqrt(st->wn2);
+  __syncthreads();
+  if (threadIdx.x != 0) return;
   for (int i = 0; i < j; ++i) {
     double t = cs[i] * hj[i] + sn[i] * hj[i + 1];
     hj[i + 1] = -sn[i] * hj[i] + cs[i] * hj[i + 1];
@@ -1893,10 +2013,10 @@ __global__ void k_fg_givens(double* H, int ldh, double* cs, double* sn, double* 
   }
   double a = hj[j], b = hj[j + 1];
   double d = hypot(a, b);
-  double c = d > 0 ? a / d : 1.0, s = d > 0 ? b / d : 0.0;
-  cs[j] = c; sn[j] = s;
+  double c = d > 0 ? a / d : 1.0, sv = d > 0 ? b / d : 0.0;
+  cs[j] = c; sn[j] = sv;
   hj[j] = d; hj[j + 1] = 0.0;
-  g[j + 1] = -s * g[j];
+  g[j + 1] = -sv * g[j];
   g[j] = c * g[j];
   const double est = fabs(g[j + 1]) / st->bnorm;
   st->rel = est;
@@ -1906,12 +2026,12 @@ __global__ void k_fg_givens(double* H, int ldh, double* cs, double* sn, double* 
   if (nan) st->nan = 1;
   const bool conv = est < tol;
   st->cycle_end = nan || conv || st->j >= m || st->total >= max_iters;
-  if (!st->cycle_end) cudaGraphSetConditional(cond, 1u);
-}
-// end of a cycle: y = R^-1 g (k_backsolve over the j columns) ...
-__global__ void k_fg_backsolve(const double* H, int ldh, const double* g, double* y, const FgState* st) {
-  pdl_wait_release();
-  if (!st->cycle_end || st->nan) return;
+  cudaGraphSetConditional(end_if, st->cycle_end ? 1u : 0u);
+  if (!st->cycle_end) {
+    cudaGraphSetConditional(cond, 1u);
+    return;
+  }
+  if (st->nan) return;
   const int k = st->j;
   for (int i = k - 1; i >= 0; --i) {
     double s = g[i];
@@ -1919,7 +2039,7 @@ __global__ void k_fg_backsolve(const double* H, int ldh, const double* g, double
     y[i] = s / H[(long long)i * ldh + i];
   }
 }
-// ... x_s += Z y ...
+// at a cycle's end x_s += Z y ...
 __global__ void k_fg_combine(long long n, const double* __restrict__ Z, const double* __restrict__ y,
                              double* __restrict__ x, const FgState* st) {
   pdl_wait_release();
@@ -2018,17 +2138,17 @@ __global__ void __launch_bounds__(TB) k_fg_norm_partials(long long n, const doub
 }
 
 // level-0 products of the device FGMRES, lanes per row as the level was tuned
-template <typename CT>
-void fg_op(const Level& L0, const CT* col, const double* Z, const double* wt, double* V, int rel,
+template <typename XT, typename CT>
+void fg_op(const Level& L0, const CT* col, const XT* z, double* Z, const double* wt, double* V, int rel,
            const FgState* st, cudaStream_t s) {
   const int lpr = L0.lpr_a[0] > 0 ? L0.lpr_a[0] : (L0.avg_row <= 8 ? 1 : L0.avg_row <= 16 ? 4 : 8);
   const int n = L0.n;
   auto grid = [&](int l) { return grid_for(((size_t)n * l + TB - 1) / TB * TB, TB, 16); };
   switch (lpr) {
-    case 1: launch_pdl(k_fg_op<CT, 1>, grid(1), TB, 0, s, n, L0.rowptr.p, col, L0.val.p, Z, wt, V, rel, st); break;
-    case 2: launch_pdl(k_fg_op<CT, 2>, grid(2), TB, 0, s, n, L0.rowptr.p, col, L0.val.p, Z, wt, V, rel, st); break;
-    case 4: launch_pdl(k_fg_op<CT, 4>, grid(4), TB, 0, s, n, L0.rowptr.p, col, L0.val.p, Z, wt, V, rel, st); break;
-    default: launch_pdl(k_fg_op<CT, 8>, grid(8), TB, 0, s, n, L0.rowptr.p, col, L0.val.p, Z, wt, V, rel, st); break;
+    case 1: launch_pdl(k_fg_op<XT, CT, 1>, grid(1), TB, 0, s, n, L0.rowptr.p, col, L0.val.p, z, Z, wt, V, rel, st); break;
+    case 2: launch_pdl(k_fg_op<XT, CT, 2>, grid(2), TB, 0, s, n, L0.rowptr.p, col, L0.val.p, z, Z, wt, V, rel, st); break;
+    case 4: launch_pdl(k_fg_op<XT, CT, 4>, grid(4), TB, 0, s, n, L0.rowptr.p, col, L0.val.p, z, Z, wt, V, rel, st); break;
+    default: launch_pdl(k_fg_op<XT, CT, 8>, grid(8), TB, 0, s, n, L0.rowptr.p, col, L0.val.p, z, Z, wt, V, rel, st); break;
   }
 }
 template <typename CT>
@@ -2038,6 +2158,39 @@ void fg_resid(const Level& L0, const CT* col, const double* xs, const double* bs
   // a fixed grid of kDotBlocks blocks: the partials are summed in block order
   launch_pdl(k_fg_resid<CT, 1>, kDotBlocks, TB, 0, s, n, L0.rowptr.p, col, L0.val.p, xs, bs, wt, V, rel, partial,
              st);
+}
+
+// Appends an IF conditional node on `hc` to the graph that `s` is capturing,
+// captures emit(q) into the node's body on the handle's third stream, and
+// continues the capture of `s` after the node.
+template <typename F>
+void capture_if(cudaStream_t s, AMG& h, cudaGraphConditionalHandle hc, F emit) {
+  cudaStreamCaptureStatus cst;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  IMPES_CUDA(cudaStreamGetCaptureInfo(s, &cst, nullptr, &g, &deps, &ndeps));
+  IMPES_REQUIRE(cst == cudaStreamCaptureStatusActive, IMPES_ERR_STATE, "conditional block needs a capturing stream");
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = hc;
+  cp.conditional.type = cudaGraphCondTypeIf;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  IMPES_CUDA(cudaGraphAddNode(&node, g, deps, ndeps, &cp));
+  if (!h.if_stream) IMPES_CUDA(cudaStreamCreateWithFlags(&h.if_stream, cudaStreamNonBlocking));
+  IMPES_CUDA(cudaStreamBeginCaptureToGraph(h.if_stream, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                           cudaStreamCaptureModeThreadLocal));
+  try {
+    emit(h.if_stream);
+  } catch (...) {
+    cudaGraph_t dummy = nullptr;
+    cudaStreamEndCapture(h.if_stream, &dummy);
+    throw;
+  }
+  cudaGraph_t out = nullptr;
+  IMPES_CUDA(cudaStreamEndCapture(h.if_stream, &out));
+  IMPES_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
 }
 }  // namespace
 
@@ -2114,41 +2267,68 @@ void amg_fgmres_capture(AMG& h, const double* b, double* x, const impes_krylov_p
   const unsigned long long body_start = thread_launches();
   try {
     const unsigned gb = grid_for(n, TB);
+    // z = M^-1 (V[j] / wt); Z[j] = z is written by the operator kernel
+    // the l1-Jacobi V-cycle's first level-0 sweep is fused with the input
+    // conversion (not for Chebyshev smoothing or a one-level hierarchy)
+    const bool fuse0 = h.prm.smoother != IMPES_SMOOTHER_CHEBYSHEV && !L0.coarsest;
     if (kp.precision == 1) {
-      launch_pdl(k_fg_prec_in<float>, gb, TB, 0, bsm, n, (const double*)h.V.p, (const double*)wt, L0.bf.p, st);
-      float* zf = vcycle<float>(h, 0, true, bsm);
-      launch_pdl(k_fg_z_out<float>, gb, TB, 0, bsm, n, (const float*)zf, h.Z.p, (const FgState*)st);
+      if (fuse0)
+        launch_pdl(k_fg_prec_smooth0<float>, gb, TB, 0, bsm, n, (const double*)h.V.p, (const double*)wt,
+                   (const float*)L0.inv_relaxf.p, L0.bf.p, L0.xf.p, st);
+      else
+        launch_pdl(k_fg_prec_in<float>, gb, TB, 0, bsm, n, (const double*)h.V.p, (const double*)wt, L0.bf.p, st);
+      const float* zf = vcycle<float>(h, 0, true, bsm, fuse0);
+      if (L0.col16.p)
+        fg_op(L0, (const unsigned short*)L0.col16.p, zf, h.Z.p, wt, h.V.p, L0.col16_rel, st, bsm);
+      else
+        fg_op(L0, (const int*)L0.col.p, zf, h.Z.p, wt, h.V.p, 0, st, bsm);
     } else {
-      launch_pdl(k_fg_prec_in<double>, gb, TB, 0, bsm, n, (const double*)h.V.p, (const double*)wt, L0.b.p, st);
-      double* zd = vcycle<double>(h, 0, true, bsm);
-      launch_pdl(k_fg_z_out<double>, gb, TB, 0, bsm, n, (const double*)zd, h.Z.p, (const FgState*)st);
+      if (fuse0)
+        launch_pdl(k_fg_prec_smooth0<double>, gb, TB, 0, bsm, n, (const double*)h.V.p, (const double*)wt,
+                   (const double*)L0.inv_relax.p, L0.b.p, L0.x.p, st);
+      else
+        launch_pdl(k_fg_prec_in<double>, gb, TB, 0, bsm, n, (const double*)h.V.p, (const double*)wt, L0.b.p, st);
+      const double* zd = vcycle<double>(h, 0, true, bsm, fuse0);
+      if (L0.col16.p)
+        fg_op(L0, (const unsigned short*)L0.col16.p, zd, h.Z.p, wt, h.V.p, L0.col16_rel, st, bsm);
+      else
+        fg_op(L0, (const int*)L0.col.p, zd, h.Z.p, wt, h.V.p, 0, st, bsm);
     }
-    if (L0.col16.p)
-      fg_op<unsigned short>(L0, L0.col16.p, h.Z.p, wt, h.V.p, L0.col16_rel, st, bsm);
-    else
-      fg_op<int>(L0, L0.col.p, h.Z.p, wt, h.V.p, 0, st, bsm);
+    // Gram-Schmidt: pass 0, then pass 1 inside an IF node that k_fg_norm opens
+    // when the first pass lost too much of the vector's norm
     const dim3 gd(kDotBlocks, (unsigned)((m + 2 + kMD - 1) / kMD));
-    for (int pass = 0; pass < 2; ++pass) {
-      launch_pdl(k_fg_multidot, gd, dim3(TB), 0, bsm, n, (const double*)h.V.p, h.red.p, (const FgState*)st, pass);
-      launch_pdl(k_fg_finalize, m + 2, 32, 0, bsm, (const double*)h.red.p, h.H.p, ldh, h.y.p, (const FgState*)st,
+    cudaGraphConditionalHandle reorth_if, end_if;
+    IMPES_CUDA(cudaGraphConditionalHandleCreate(&reorth_if, body, 0, cudaGraphCondAssignDefault));
+    IMPES_CUDA(cudaGraphConditionalHandleCreate(&end_if, body, 0, cudaGraphCondAssignDefault));
+    auto gs_pass = [&](int pass, cudaStream_t q) {
+      launch_pdl(k_fg_multidot, gd, dim3(TB), 0, q, n, (const double*)h.V.p, h.red.p, (const FgState*)st, pass);
+      launch_pdl(k_fg_finalize, m + 2, 32, 0, q, (const double*)h.red.p, h.H.p, ldh, h.y.p, (const FgState*)st,
                  pass);
-      launch_pdl(k_fg_update, kDotBlocks, TB, 0, bsm, n, h.V.p, (const double*)h.H.p, ldh, (const double*)h.y.p,
+      launch_pdl(k_fg_update, kDotBlocks, TB, 0, q, n, h.V.p, (const double*)h.H.p, ldh, (const double*)h.y.p,
                  h.red.p, (const FgState*)st, pass);
-      launch_pdl(k_fg_norm, 1, 32, 0, bsm, (const double*)h.red.p, st, (const double*)h.H.p, ldh, pass);
-    }
-    launch_pdl(k_fg_hcol, 1, 128, 0, bsm, h.H.p, ldh, (const double*)h.y.p, (const FgState*)st);
+      launch_pdl(k_fg_norm, 1, 32, 0, q, (const double*)h.red.p, st, (const double*)h.H.p, ldh, pass, reorth_if);
+    };
+    gs_pass(0, bsm);
+    unsigned long long mark = thread_launches();
+    capture_if(bsm, h, reorth_if, [&](cudaStream_t q) { gs_pass(1, q); });
+    h.fg_reorth_kernels = (long long)(thread_launches() - mark);
     launch_pdl(k_fg_scale_w, gb, TB, 0, bsm, n, h.V.p, (const FgState*)st);
-    launch_pdl(k_fg_givens, 1, 1, 0, bsm, h.H.p, ldh, h.cs.p, h.sn.p, h.g.p, st, kp.tol, kp.max_iters, m, cond);
-    launch_pdl(k_fg_backsolve, 1, 1, 0, bsm, (const double*)h.H.p, ldh, (const double*)h.g.p, h.y.p,
-               (const FgState*)st);
-    launch_pdl(k_fg_combine, gb, TB, 0, bsm, n, (const double*)h.Z.p, (const double*)h.y.p, xs, (const FgState*)st);
-    if (L0.col16.p)
-      fg_resid<unsigned short>(L0, L0.col16.p, xs, bs, wt, h.V.p, L0.col16_rel, part_r, st, bsm);
-    else
-      fg_resid<int>(L0, L0.col.p, xs, bs, wt, h.V.p, 0, part_r, st, bsm);
-    launch_pdl(k_fg_restart, 1, 1, 0, bsm, (const double*)part_r, (int)kDotBlocks, st, h.g.p, m + 1, kp.tol,
-               kp.max_iters, cond);
-    launch_pdl(k_fg_scale_v0, gb, TB, 0, bsm, n, h.V.p, (const FgState*)st, 1);
+    launch_pdl(k_fg_column, 1, 128, 0, bsm, h.H.p, ldh, h.cs.p, h.sn.p, h.g.p, h.y.p, st, kp.tol, kp.max_iters, m,
+               cond, end_if);
+    // a cycle's end (IF node opened by k_fg_column): x_s += Z y, the true
+    // residual, the restart/stop decision and the new V[0]
+    mark = thread_launches();
+    capture_if(bsm, h, end_if, [&](cudaStream_t q) {
+      launch_pdl(k_fg_combine, gb, TB, 0, q, n, (const double*)h.Z.p, (const double*)h.y.p, xs, (const FgState*)st);
+      if (L0.col16.p)
+        fg_resid<unsigned short>(L0, L0.col16.p, xs, bs, wt, h.V.p, L0.col16_rel, part_r, st, q);
+      else
+        fg_resid<int>(L0, L0.col.p, xs, bs, wt, h.V.p, 0, part_r, st, q);
+      launch_pdl(k_fg_restart, 1, 1, 0, q, (const double*)part_r, (int)kDotBlocks, st, h.g.p, m + 1, kp.tol,
+                 kp.max_iters, cond);
+      launch_pdl(k_fg_scale_v0, gb, TB, 0, q, n, h.V.p, (const FgState*)st, 1);
+    });
+    h.fg_end_kernels = (long long)(thread_launches() - mark);
   } catch (...) {
     cudaGraph_t dummy = nullptr;
     cudaStreamEndCapture(bsm, &dummy);
@@ -2156,7 +2336,7 @@ void amg_fgmres_capture(AMG& h, const double* b, double* x, const impes_krylov_p
   }
   cudaGraph_t body_out = nullptr;
   IMPES_CUDA(cudaStreamEndCapture(bsm, &body_out));
-  h.fg_body_kernels = (long long)(thread_launches() - body_start);
+  h.fg_body_kernels = (long long)(thread_launches() - body_start) - h.fg_reorth_kernels - h.fg_end_kernels;
   IMPES_CUDA(cudaStreamUpdateCaptureDependencies(s, &wnode, 1, cudaStreamSetCaptureDependencies));
   // epilogue: x = D^-1/2 x_s (zero for a zero right-hand side)
   launch_pdl(k_fg_final, gn, TB, 0, s, n, (const double*)h.dhalf_inv.p, (const double*)xs, x, (const FgState*)st);

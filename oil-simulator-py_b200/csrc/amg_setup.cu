@@ -1211,6 +1211,132 @@ void level_precision_copies(AMG& h, Level& L, cudaStream_t s) {
   IMPES_CHECK_LAUNCH();
 }
 
+namespace {
+// ------------------------------------------------ SELL-32 copies of A
+// Levels of at least kSellMinRows rows with at most 96 entries per row get a
+// SELL-32 copy of A (Level::sell_*), which the autotuner may pick for the
+// sweeps and residuals.  Built on the host from the fixed pattern: rows sorted
+// by length (longest first, stable) inside windows of kSellWindow rows so a
+// slice's rows have similar lengths; padding points at the lane's own row
+// (row-relative 32768, or the row itself) with value 0.
+constexpr int kSellMinRows = 8192;
+constexpr int kSellWindow = 256;
+
+// IMPES_NO_SELL=1 (read at setup) builds no SELL copies.
+bool sell_enabled() {
+  const char* ev = getenv("IMPES_NO_SELL");
+  return !(ev && ev[0] == '1');
+}
+
+__global__ void k_sell_gather(long long len, const int* __restrict__ map, const double* __restrict__ v,
+                              double* __restrict__ out) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < len; k += (long long)gridDim.x * blockDim.x) {
+    const int m = map[k];
+    out[k] = m >= 0 ? v[m] : 0.0;
+  }
+}
+__global__ void k_sell_gather_f(long long len, const int* __restrict__ map, const float* __restrict__ v,
+                                float* __restrict__ out) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < len; k += (long long)gridDim.x * blockDim.x) {
+    const int m = map[k];
+    out[k] = m >= 0 ? v[m] : 0.0f;
+  }
+}
+
+void build_sell(Level& L, cudaStream_t s) {
+  L.sell_slices = 0;
+  L.sell_len = 0;
+  if (L.coarsest || L.n < kSellMinRows || L.avg_row > 96 || L.nnz <= 0) return;
+  const int n = L.n;
+  std::vector<int> rp(n + 1), col(L.nnz);
+  std::vector<unsigned short> c16;
+  IMPES_CUDA(cudaMemcpyAsync(rp.data(), L.rowptr.p, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost, s));
+  if (L.col16.p) {
+    c16.resize(L.nnz);
+    IMPES_CUDA(cudaMemcpyAsync(c16.data(), L.col16.p, sizeof(unsigned short) * L.nnz, cudaMemcpyDeviceToHost, s));
+  } else {
+    IMPES_CUDA(cudaMemcpyAsync(col.data(), L.col.p, sizeof(int) * L.nnz, cudaMemcpyDeviceToHost, s));
+  }
+  IMPES_CUDA(cudaStreamSynchronize(s));
+  std::vector<int> perm(n);
+  for (int r = 0; r < n; ++r) perm[r] = r;
+  for (int w0 = 0; w0 < n; w0 += kSellWindow) {
+    const int w1 = std::min(n, w0 + kSellWindow);
+    std::stable_sort(perm.begin() + w0, perm.begin() + w1,
+                     [&](int a, int b) { return rp[a + 1] - rp[a] > rp[b + 1] - rp[b]; });
+  }
+  const int nsl = (n + 31) / 32;
+  std::vector<int> sptr(nsl + 1, 0);
+  long long tot = 0;
+  for (int q = 0; q < nsl; ++q) {
+    int w = 0;
+    for (int r = q * 32; r < std::min(n, q * 32 + 32); ++r) w = std::max(w, rp[perm[r] + 1] - rp[perm[r]]);
+    tot += 32LL * w;
+    IMPES_REQUIRE(tot < (1LL << 31), IMPES_ERR_OOM, "SELL copy of a level exceeds 2^31 entries");
+    sptr[q + 1] = (int)tot;
+  }
+  std::vector<int> map((size_t)tot, -1);
+  std::vector<int> scol(L.col16.p ? 0 : (size_t)tot);
+  std::vector<unsigned short> scol16(L.col16.p ? (size_t)tot : 0);
+  for (int r = 0; r < nsl * 32; ++r) {
+    const int q = r / 32, lane = r % 32;
+    const int row = perm[r < n ? r : n - 1];
+    const int len = r < n ? rp[row + 1] - rp[row] : 0;
+    const int w = (sptr[q + 1] - sptr[q]) / 32;
+    for (int j = 0; j < w; ++j) {
+      const size_t k = (size_t)sptr[q] + 32 * (size_t)j + lane;
+      if (j < len) {
+        map[k] = rp[row] + j;
+        if (L.col16.p) scol16[k] = c16[rp[row] + j];
+        else scol[k] = col[rp[row] + j];
+      } else if (L.col16.p) {
+        scol16[k] = L.col16_rel ? (unsigned short)32768 : (unsigned short)row;
+      } else {
+        scol[k] = row;
+      }
+    }
+  }
+  L.sell_ptr.alloc(nsl + 1);
+  L.sell_perm.alloc(n);
+  L.sell_map.alloc(std::max<long long>(tot, 1));
+  IMPES_CUDA(cudaMemcpyAsync(L.sell_ptr.p, sptr.data(), sizeof(int) * (nsl + 1), cudaMemcpyHostToDevice, s));
+  IMPES_CUDA(cudaMemcpyAsync(L.sell_perm.p, perm.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
+  IMPES_CUDA(cudaMemcpyAsync(L.sell_map.p, map.data(), sizeof(int) * tot, cudaMemcpyHostToDevice, s));
+  if (L.col16.p) {
+    L.sell_col16.alloc(std::max<long long>(tot, 1));
+    IMPES_CUDA(cudaMemcpyAsync(L.sell_col16.p, scol16.data(), sizeof(unsigned short) * tot, cudaMemcpyHostToDevice, s));
+  } else {
+    L.sell_col.alloc(std::max<long long>(tot, 1));
+    IMPES_CUDA(cudaMemcpyAsync(L.sell_col.p, scol.data(), sizeof(int) * tot, cudaMemcpyHostToDevice, s));
+  }
+  IMPES_CUDA(cudaStreamSynchronize(s));   // the host vectors go out of scope
+  L.sell_slices = nsl;
+  L.sell_len = tot;
+}
+
+// Gather the SELL values of the levels whose sweeps read them (all levels with
+// a copy when `all`, before the autotuner has chosen) from their CSR values:
+// slot 0 the fp64 values, 1 the fp32 ones.
+void sell_refresh(AMG& h, int slot, cudaStream_t s, bool all = false) {
+  for (auto& up : h.levels) {
+    Level& L = *up;
+    if (L.sell_slices <= 0 || !(all || L.sell_on[slot])) continue;
+    if (slot == 0) {
+      if (!L.val.p) continue;
+      L.sell_val.ensure(L.sell_len);
+      k_sell_gather<<<grid_for(L.sell_len, TB), TB, 0, s>>>(L.sell_len, L.sell_map.p, L.val.p, L.sell_val.p);
+    } else {
+      if (!L.valf.p) continue;
+      L.sell_valf.ensure(L.sell_len);
+      k_sell_gather_f<<<grid_for(L.sell_len, TB), TB, 0, s>>>(L.sell_len, L.sell_map.p, L.valf.p, L.sell_valf.p);
+    }
+    ::impes::count_launch();
+    IMPES_CHECK_LAUNCH();
+  }
+}
+
+}  // namespace
+
 void amg_setup(AMG& h, int n, int nnz, const int* rowptr, const int* col, const double* val,
                cudaStream_t s) {
   IMPES_REQUIRE(n > 0 && nnz > 0, IMPES_ERR_ARG, "empty matrix");
@@ -1464,7 +1590,24 @@ void amg_setup(AMG& h, int n, int nnz, const int* rowptr, const int* col, const 
     IMPES_CHECK_LAUNCH();
   }
   IMPES_CUDA(cudaStreamSynchronize(s));
+  if (sell_enabled()) {
+    for (auto& L : h.levels) build_sell(*L, s);
+    sell_refresh(h, 0, s, true);
+    if (h.prm.mixed_precision) sell_refresh(h, 1, s, true);
+  }
   amg_autotune(h, s);
+  // the SELL copies the tuner did not pick are dropped
+  for (auto& L : h.levels) {
+    if (L->sell_slices <= 0) continue;
+    if (!L->sell_on[0]) L->sell_val.release();
+    if (!L->sell_on[1]) L->sell_valf.release();
+    if (!L->sell_on[0] && !L->sell_on[1]) {
+      L->sell_ptr.release(); L->sell_perm.release(); L->sell_map.release();
+      L->sell_col16.release(); L->sell_col.release();
+      L->sell_slices = 0;
+      L->sell_len = 0;
+    }
+  }
   h.tail_level = amg_tail_level(h);
   h.built = true;
 }
@@ -1501,6 +1644,7 @@ void update_fp32_chain(AMG& h, cudaStream_t s) {
     compute_inv_relax_f(h, Nc, s);
   }
   coarse_factor(h, *h.levels.back(), s, true);
+  sell_refresh(h, 1, s);
   h.fp64_stale = true;
 }
 
@@ -1513,6 +1657,7 @@ void amg_ensure_fp64(AMG& h, cudaStream_t s) {
     galerkin_numeric(L, *h.levels[l + 1], s);
   }
   coarse_factor(h, *h.levels.back(), s);
+  sell_refresh(h, 0, s);
   h.fp64_stale = false;
 }
 
@@ -1549,6 +1694,8 @@ void amg_update(AMG& h, const double* val, cudaStream_t s) {
     cheb_copy_to_fp32(h, *L, s);
   }
   IMPES_CHECK_LAUNCH();
+  sell_refresh(h, 0, s);
+  if (h.prm.mixed_precision) sell_refresh(h, 1, s);
   timers().end(tid, s, bytes);
 }
 

@@ -42,7 +42,7 @@ class AmgParams(C.Structure):
 class LevelDesc(C.Structure):
     _fields_ = [("n", C.c_int), ("nnz", C.c_int), ("p_cols", C.c_int), ("p_nnz", C.c_int),
                 ("is_coarsest", C.c_int), ("col_index_bytes", C.c_int), ("col_row_relative", C.c_int),
-                ("lanes", C.c_int * 6)]
+                ("lanes", C.c_int * 6), ("sell", C.c_int * 2)]
 
 
 class KrylovParams(C.Structure):
@@ -136,6 +136,7 @@ _SIGNATURES = {
     "impes_amg_num_levels": ([_P, C.POINTER(_I)], _I),
     "impes_amg_level_info": ([_P, _I, C.POINTER(LevelDesc)], _I),
     "impes_amg_profile_levels": ([_P, _I, _I, C.POINTER(C.c_double), _P], _I),
+    "impes_amg_step_graphs": ([_P, C.POINTER(C.c_int), C.POINTER(C.c_int)], _I),
     "impes_amg_level_export": ([_P, _I, _P, _P, _P, _P, _P, _P, _P, _P], _I),
     "impes_amg_equilibration": ([_P, _P, C.POINTER(_I), _P], _I),
     "impes_model_create": ([C.POINTER(_P), C.POINTER(ModelDesc), C.POINTER(WellDesc), _I, _P,

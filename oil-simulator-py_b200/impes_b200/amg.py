@@ -279,7 +279,8 @@ class ClassicalAMG:
             out.append({"A": A, "n": info.n, "P": P, "inv_relax": ir, "diag": d.abs(),
                         "is_coarsest": bool(info.is_coarsest),
                         "col_index_bytes": info.col_index_bytes,
-                        "col_row_relative": bool(info.col_row_relative)})
+                        "col_row_relative": bool(info.col_row_relative),
+                        "sell": tuple(bool(v) for v in info.sell)})
         self._levels_cache = out
         return out
 

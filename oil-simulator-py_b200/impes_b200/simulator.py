@@ -624,11 +624,22 @@ class Simulator:
                   "impes_amg_profile_levels")
         return [tuple(out[4 * l:4 * l + 4]) for l in range(nl.value)]
 
+    def step_graphs(self):
+        """(whole steps held as CUDA graphs, capture refused) of the pressure
+        hierarchy (instrumentation)."""
+        if self._amg_h is None:
+            return (0, False)
+        ng, bad = C.c_int(0), C.c_int(0)
+        check(lib.impes_amg_step_graphs(self._amg_h, C.byref(ng), C.byref(bad)))
+        return (ng.value, bool(bad.value))
+
     def amg_levels(self):
-        """[(n, nnz, p_cols, p_nnz, is_coarsest, columns, lanes)] of the pressure
-        hierarchy; columns is the index storage of the level's sweeps: "i32",
-        "u16" or "u16rel" (16-bit offsets from the row); lanes the autotuned lanes
-        per row of the kernels on A, R and P (fp64 then fp32; 0: the default rule)."""
+        """[(n, nnz, p_cols, p_nnz, is_coarsest, columns, lanes, sell)] of the
+        pressure hierarchy; columns is the index storage of the level's sweeps:
+        "i32", "u16" or "u16rel" (16-bit offsets from the row); lanes the
+        autotuned lanes per row of the kernels on A, R and P (fp64 then fp32; 0:
+        the default rule); sell (fp64, fp32) whether the sweeps and residuals
+        read the level's SELL-32 copy of A."""
         if self._amg_h is None:
             return []
         nl = C.c_int(0)
@@ -638,7 +649,8 @@ class Simulator:
             d = _lib.LevelDesc()
             check(lib.impes_amg_level_info(self._amg_h, l, C.byref(d)))
             cols = "i32" if d.col_index_bytes == 4 else ("u16rel" if d.col_row_relative else "u16")
-            out.append((d.n, d.nnz, d.p_cols, d.p_nnz, bool(d.is_coarsest), cols, tuple(d.lanes)))
+            out.append((d.n, d.nnz, d.p_cols, d.p_nnz, bool(d.is_coarsest), cols, tuple(d.lanes),
+                        tuple(bool(v) for v in d.sell)))
         return out
 
     # --------------------------------------------------- building blocks

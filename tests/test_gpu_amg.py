@@ -452,3 +452,36 @@ def test_fused_vcycle_tail_matches_per_level_kernels(monkeypatch, precision):
     assert np.linalg.norm(out["0"][0] - out["1"][0]) <= tol * np.linalg.norm(out["1"][0])
     assert np.linalg.norm(out["0"][1] - out["1"][1]) <= 1e-8 * np.linalg.norm(out["1"][1])
     assert abs(out["0"][2] - out["1"][2]) <= 1
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_sell_sweeps_match_csr(monkeypatch, precision):
+    """IMPES_SELL=1 (read at setup) puts every level of >= 8,192 rows on its
+    SELL-32 copy of A (rows sorted by length inside 256-row windows, one lane
+    per row); IMPES_NO_SELL=1 keeps the CSR kernels.  The V-cycle and the
+    FGMRES solution agree to rounding: both layouts add each row's products in
+    the row's order, the CSR kernels with their tuned lanes per row."""
+    A = _laplacian_3d(48, 40, 24)
+    n = A.shape[0]
+    rng = np.random.default_rng(4)
+    bs = rng.standard_normal(n)
+    out = {}
+    for mode in ("csr", "sell"):
+        monkeypatch.setenv("IMPES_NO_SELL", "1" if mode == "csr" else "0")
+        monkeypatch.setenv("IMPES_SELL", "1" if mode == "sell" else "0")
+        amg = gpu_amg(A, coarsest_size=60, seed=2, mixed_precision=True)
+        slot = 0 if precision == "fp64" else 1
+        used = [lv["sell"][slot] for lv in amg.levels if not lv["is_coarsest"]]
+        if mode == "sell":
+            assert used[0] and sum(used) >= 2, used
+        else:
+            assert not any(used), used
+        v = to_np(amg.vcycle_scaled(torch.tensor(bs, device="cuda"), precision=precision))
+        x, st = amg.fgmres(torch.tensor(bs, device="cuda"), tol=1e-10, norm="jacobi", precision=precision)
+        assert st["converged"], st
+        out[mode] = (v, to_np(x), st["iterations"])
+        amg.close()
+    tol = 1e-12 if precision == "fp64" else 1e-5
+    assert np.linalg.norm(out["csr"][0] - out["sell"][0]) <= tol * np.linalg.norm(out["sell"][0])
+    assert np.linalg.norm(out["csr"][1] - out["sell"][1]) <= 1e-8 * np.linalg.norm(out["sell"][1])
+    assert abs(out["csr"][2] - out["sell"][2]) <= 1

@@ -269,6 +269,8 @@ def test_whole_step_graph_matches_host_driven_steps(golden, monkeypatch, precisi
             assert np.abs(traj[-1][0] - g["p"][s]).max() <= 1e-8 * np.abs(g["p"][s]).max()
             assert np.abs(traj[-1][1] - g["sw"][s]).max() <= 1e-8
         out[flag] = traj
+        graphs, refused = sim.step_graphs()
+        assert not refused and (graphs >= 1) == (flag == "0"), (flag, graphs, refused)
         sim.close()
     for (p1, w1, s1, i1), (p0, w0, s0, i0) in zip(out["1"], out["0"]):
         assert np.abs(p1 - p0).max() <= 1e-11 * np.abs(p1).max()
