@@ -2,6 +2,7 @@
 #include "amg.cuh"
 #include "model.cuh"
 #include <algorithm>
+#include <cstdio>
 #include <cstdlib>
 #include <cmath>
 #include <map>
@@ -69,6 +70,13 @@ __global__ void k_accept(int n, const FgState* st, double* __restrict__ p, const
 // first-iterate mode); the hierarchy must exist (the first step builds it on
 // the host path).  Returns false when this build or driver refuses the capture
 // (the caller then keeps the host-driven step).
+// A refused step-graph capture keeps the host-driven step; IMPES_GRAPH_DEBUG=1
+// prints why on stderr.
+static void step_graph_refused(const char* stage, const char* why) {
+  const char* ev = getenv("IMPES_GRAPH_DEBUG");
+  if (ev && ev[0] == '1') fprintf(stderr, "impes: whole-step graph refused (%s): %s\n", stage, why);
+}
+
 bool step_graph_run(Model& m, AMG& a, double* p, double* sw, double* sg, double* so, double dt,
                     const impes_krylov_params& kp, impes_krylov_stats& st, cudaStream_t s) {
   if (a.step_graph_failed || !a.use_graphs || !a.use_step_graph || timers().on || kp.precision < 0) return false;
@@ -103,10 +111,18 @@ bool step_graph_run(Model& m, AMG& a, double* p, double* sw, double* sg, double*
     const bool stale_before = a.fp64_stale;
     cudaGraph_t graph = nullptr;
     cudaError_t ce = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
-    if (ce != cudaSuccess) { a.step_graph_failed = true; cudaGetLastError(); return false; }
+    if (ce != cudaSuccess) {
+      step_graph_refused("begin capture", cudaGetErrorString(ce));
+      a.step_graph_failed = true;
+      cudaGetLastError();
+      return false;
+    }
+    const char* stage = "assembly";
     try {
       model_assemble(m, p, sw, sg, dt, m.csr_val.p, m.rhs.p, cs);
+      stage = "AMG update";
       amg_update(a, m.csr_val.p, cs);
+      stage = "FGMRES";
       IMPES_CUDA(cudaMemcpyAsync(m.p_save.p, p, sizeof(double) * m.P.N, cudaMemcpyDeviceToDevice, cs));
       if (extrap) {
         k_extrapolate<<<grid_for(m.P.N, 256), 256, 0, cs>>>(m.P.N, m.p_save.p, m.p_prev.p, dt / m.dt_prev, p);
@@ -114,11 +130,13 @@ bool step_graph_run(Model& m, AMG& a, double* p, double* sw, double* sg, double*
         IMPES_CHECK_LAUNCH();
       }
       amg_fgmres_capture(a, m.rhs.p, p, k, cs);
+      stage = "saturation";
       k_accept<<<grid_for(m.P.N, 256), 256, 0, cs>>>(m.P.N, a.fgst.p, p, m.p_save.p, m.p_prev.p);
       ::impes::count_launch();
       IMPES_CHECK_LAUNCH();
       model_saturation(m, p, sw, sg, so, dt, cs, &a.fgst.p->converged);
-    } catch (const Error&) {
+    } catch (const Error& err) {
+      step_graph_refused(stage, err.what());
       cudaStreamEndCapture(cs, &graph);
       if (graph) cudaGraphDestroy(graph);
       cudaGetLastError();
@@ -141,6 +159,7 @@ bool step_graph_run(Model& m, AMG& a, double* p, double* sw, double* sg, double*
     cudaError_t ie = cudaGraphInstantiate(&e.exec, graph, 0);
     cudaGraphDestroy(graph);
     if (ie != cudaSuccess) {
+      step_graph_refused("instantiate", cudaGetErrorString(ie));
       cudaGetLastError();
       a.step_graph_failed = true;
       return false;

@@ -17,13 +17,15 @@ struct Level {
   // Chebyshev smoother: Gershgorin bound of diag(inv) A as double bits, [0] from
   // the fp64 values, [1] from the fp32 chain (atomicMax of non-negative doubles)
   DBuf<unsigned long long> cheb_lmax;
-  // SELL-32 copy of A (sliced ELLPACK) for the sweeps and residuals: rows in
-  // sell_perm order (sorted by length, longest first, inside windows of
-  // kSellWindow rows), 32 per slice; entry j of lane q of slice s at
-  // sell_ptr[s] + 32 j + q.  Padding entries hold value 0 and the lane's own row
-  // as column.  sell_map is the CSR index of each entry (-1: padding); the
-  // values are gathered from the CSR values after every value change.
-  int sell_slices = 0;
+  // SELL-32 copy of A (sliced ELLPACK) for the sweeps and residuals, sell_lpr
+  // lanes per row: rows in sell_perm order (sorted by length, longest first,
+  // inside windows of 256 rows with one lane per row, 32 otherwise),
+  // 32 / sell_lpr rows per slice; entry j of the slice's row q at
+  // sell_ptr[s] + 32 (j / sell_lpr) + q sell_lpr + j % sell_lpr.  Padding
+  // entries hold value 0 and the row's own column.  sell_map is the CSR index
+  // of each entry (-1: padding); the values are gathered from the CSR values
+  // after every value change.
+  int sell_slices = 0, sell_lpr = 1;
   long long sell_len = 0;
   DBuf<int> sell_ptr, sell_perm, sell_map;
   DBuf<unsigned short> sell_col16;  // when col16 exists (same encoding), else sell_col

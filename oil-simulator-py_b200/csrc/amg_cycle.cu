@@ -306,26 +306,31 @@ void launch_csr(int n, int avg, const int* rowptr, const int* col, const T* val,
 // Sliced ELLPACK with slices of one warp (C = 32) and rows sorted by length
 // inside windows (Kreutzer et al., "A unified sparse matrix data format for
 // efficient general sparse matrix-vector multiplication on modern processors
-// with wide SIMD units", SIAM J. Sci. Comput. 36(5), 2014).  One lane per row;
-// at each entry index j the warp's value and column loads are one contiguous
-// segment, where the CSR kernels' loads of 32 rows touch up to 32 segments.
-// Each row's products are added in the row's CSR order (padding adds +0), as
-// k_csr with one lane per row does.  CT and rel as in k_csr; same epilogues.
-template <typename T, typename CT, int MODE>
+// with wide SIMD units", SIAM J. Sci. Comput. 36(5), 2014), with LPR lanes per
+// row: a slice holds 32 / LPR rows, and entry j of its row q sits at
+// sptr[s] + 32 (j / LPR) + q LPR + j % LPR.  At each step the warp's value and
+// column loads are one contiguous segment, where the CSR kernels' loads touch
+// up to 32 / LPR segments.  Lane l of a row adds entries l, l + LPR, ... and
+// the lanes are reduced as in k_csr with the same LPR, so a row sums in the
+// same order (padding adds +0).  CT and rel as in k_csr; same epilogues.
+template <typename T, typename CT, int LPR, int MODE>
 __global__ void __launch_bounds__(TB) k_sell(int n, int nslices, const int* __restrict__ sptr,
                                              const int* __restrict__ perm, const CT* __restrict__ col,
                                              const T* __restrict__ val, const T* __restrict__ x,
                                              const T* __restrict__ b, const T* __restrict__ inv,
                                              T* __restrict__ y, int rel) {
   pdl_wait_release();
+  constexpr int R = 32 / LPR;   // rows per slice
   const int lane = threadIdx.x & 31;
   const int warps = (int)((gridDim.x * (unsigned)TB) >> 5);
   for (int s = (int)((blockIdx.x * (unsigned)TB + threadIdx.x) >> 5); s < nslices; s += warps) {
-    const int r = s * 32 + lane;
+    const int r = s * R + lane / LPR;
     const int row = perm[r < n ? r : n - 1];
     const int cb = col_base<CT>(row, rel);
-    const T acc = row_dot(sptr[s] + lane, sptr[s + 1], 32, val, col, x, cb, T(0));
-    if (r < n) {
+    T acc = row_dot(sptr[s] + lane, sptr[s + 1], 32, val, col, x, cb, T(0));
+#pragma unroll
+    for (int o = LPR / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, LPR);
+    if (r < n && lane % LPR == 0) {
       if (MODE == Y_AX) y[row] = acc;
       else if (MODE == Y_B_MINUS_AX) y[row] = b[row] - acc;
       else if (MODE == Y_SMOOTH) y[row] = x[row] + T(kOmega) * inv[row] * (b[row] - acc);
@@ -339,17 +344,28 @@ template <typename T> const T* sell_values(const Level& L);
 template <> inline const double* sell_values<double>(const Level& L) { return L.sell_val.p; }
 template <> inline const float* sell_values<float>(const Level& L) { return L.sell_valf.p; }
 
+template <typename T, typename CT, int MODE>
+void launch_sell_ct(const Level& L, const CT* col, int rel, const T* x, const T* b, const T* inv, T* y,
+                    cudaStream_t s) {
+  const unsigned grid = grid_for((size_t)L.sell_slices * 32, TB, 16);
+  const int* sp = L.sell_ptr.p;
+  const int* pm = L.sell_perm.p;
+  const T* v = sell_values<T>(L);
+  switch (L.sell_lpr) {
+    case 1: launch_pdl(k_sell<T, CT, 1, MODE>, grid, TB, 0, s, L.n, L.sell_slices, sp, pm, col, v, x, b, inv, y, rel); break;
+    case 2: launch_pdl(k_sell<T, CT, 2, MODE>, grid, TB, 0, s, L.n, L.sell_slices, sp, pm, col, v, x, b, inv, y, rel); break;
+    case 4: launch_pdl(k_sell<T, CT, 4, MODE>, grid, TB, 0, s, L.n, L.sell_slices, sp, pm, col, v, x, b, inv, y, rel); break;
+    default: launch_pdl(k_sell<T, CT, 8, MODE>, grid, TB, 0, s, L.n, L.sell_slices, sp, pm, col, v, x, b, inv, y, rel); break;
+  }
+  IMPES_CHECK_LAUNCH();
+}
+
 template <typename T, int MODE>
 void launch_sell(const Level& L, const T* x, const T* b, const T* inv, T* y, cudaStream_t s) {
-  const unsigned grid = grid_for((size_t)L.sell_slices * 32, TB, 16);
   if (L.sell_col16.p)
-    launch_pdl(k_sell<T, unsigned short, MODE>, grid, TB, 0, s, L.n, L.sell_slices, (const int*)L.sell_ptr.p,
-               (const int*)L.sell_perm.p, (const unsigned short*)L.sell_col16.p, sell_values<T>(L), x, b, inv, y,
-               L.col16_rel);
+    launch_sell_ct<T, unsigned short, MODE>(L, (const unsigned short*)L.sell_col16.p, L.col16_rel, x, b, inv, y, s);
   else
-    launch_pdl(k_sell<T, int, MODE>, grid, TB, 0, s, L.n, L.sell_slices, (const int*)L.sell_ptr.p,
-               (const int*)L.sell_perm.p, (const int*)L.sell_col.p, sell_values<T>(L), x, b, inv, y, 0);
-  IMPES_CHECK_LAUNCH();
+    launch_sell_ct<T, int, MODE>(L, (const int*)L.sell_col.p, 0, x, b, inv, y, s);
 }
 
 // A product of a level's A with the layout chosen for this precision (SELL or

@@ -1215,12 +1215,15 @@ namespace {
 // ------------------------------------------------ SELL-32 copies of A
 // Levels of at least kSellMinRows rows with at most 96 entries per row get a
 // SELL-32 copy of A (Level::sell_*), which the autotuner may pick for the
-// sweeps and residuals.  Built on the host from the fixed pattern: rows sorted
-// by length (longest first, stable) inside windows of kSellWindow rows so a
-// slice's rows have similar lengths; padding points at the lane's own row
-// (row-relative 32768, or the row itself) with value 0.
+// sweeps and residuals.  Built on the host from the fixed pattern: lanes per
+// row by the mean row length (1 up to 12 entries, 4 up to 30, else 8), rows
+// sorted by length (longest first, stable) inside windows of 256 rows (one
+// lane per row) or 32 rows, so a slice's rows have similar lengths; padding
+// points at the row's own column (row-relative 32768, or the row itself) with
+// value 0.  The rule and windows are the fastest of 1, 2, 4, 8 lanes and
+// 32/256-row windows on the 1e6-cell hierarchy's levels 0-6.
 constexpr int kSellMinRows = 8192;
-constexpr int kSellWindow = 256;
+inline int sell_lanes(int avg) { return avg <= 12 ? 1 : avg <= 30 ? 4 : 8; }
 
 // IMPES_NO_SELL=1 (read at setup) builds no SELL copies.
 bool sell_enabled() {
@@ -1258,19 +1261,22 @@ void build_sell(Level& L, cudaStream_t s) {
     IMPES_CUDA(cudaMemcpyAsync(col.data(), L.col.p, sizeof(int) * L.nnz, cudaMemcpyDeviceToHost, s));
   }
   IMPES_CUDA(cudaStreamSynchronize(s));
+  const int lpr = sell_lanes(L.avg_row), R = 32 / lpr;
+  const int window = lpr == 1 ? 256 : 32;
   std::vector<int> perm(n);
   for (int r = 0; r < n; ++r) perm[r] = r;
-  for (int w0 = 0; w0 < n; w0 += kSellWindow) {
-    const int w1 = std::min(n, w0 + kSellWindow);
+  for (int w0 = 0; w0 < n; w0 += window) {
+    const int w1 = std::min(n, w0 + window);
     std::stable_sort(perm.begin() + w0, perm.begin() + w1,
                      [&](int a, int b) { return rp[a + 1] - rp[a] > rp[b + 1] - rp[b]; });
   }
-  const int nsl = (n + 31) / 32;
+  const int nsl = (n + R - 1) / R;
   std::vector<int> sptr(nsl + 1, 0);
   long long tot = 0;
   for (int q = 0; q < nsl; ++q) {
-    int w = 0;
-    for (int r = q * 32; r < std::min(n, q * 32 + 32); ++r) w = std::max(w, rp[perm[r] + 1] - rp[perm[r]]);
+    int w = 0;   // steps of 32 entries: the slice's longest row over its lanes
+    for (int r = q * R; r < std::min(n, q * R + R); ++r)
+      w = std::max(w, (rp[perm[r] + 1] - rp[perm[r]] + lpr - 1) / lpr);
     tot += 32LL * w;
     IMPES_REQUIRE(tot < (1LL << 31), IMPES_ERR_OOM, "SELL copy of a level exceeds 2^31 entries");
     sptr[q + 1] = (int)tot;
@@ -1278,13 +1284,13 @@ void build_sell(Level& L, cudaStream_t s) {
   std::vector<int> map((size_t)tot, -1);
   std::vector<int> scol(L.col16.p ? 0 : (size_t)tot);
   std::vector<unsigned short> scol16(L.col16.p ? (size_t)tot : 0);
-  for (int r = 0; r < nsl * 32; ++r) {
-    const int q = r / 32, lane = r % 32;
+  for (int r = 0; r < nsl * R; ++r) {
+    const int q = r / R, rq = r % R;
     const int row = perm[r < n ? r : n - 1];
     const int len = r < n ? rp[row + 1] - rp[row] : 0;
     const int w = (sptr[q + 1] - sptr[q]) / 32;
-    for (int j = 0; j < w; ++j) {
-      const size_t k = (size_t)sptr[q] + 32 * (size_t)j + lane;
+    for (int j = 0; j < w * lpr; ++j) {
+      const size_t k = (size_t)sptr[q] + 32 * (size_t)(j / lpr) + (size_t)rq * lpr + j % lpr;
       if (j < len) {
         map[k] = rp[row] + j;
         if (L.col16.p) scol16[k] = c16[rp[row] + j];
@@ -1312,6 +1318,7 @@ void build_sell(Level& L, cudaStream_t s) {
   IMPES_CUDA(cudaStreamSynchronize(s));   // the host vectors go out of scope
   L.sell_slices = nsl;
   L.sell_len = tot;
+  L.sell_lpr = lpr;
 }
 
 // Gather the SELL values of the levels whose sweeps read them (all levels with
@@ -1590,6 +1597,12 @@ void amg_setup(AMG& h, int n, int nnz, const int* rowptr, const int* col, const 
     IMPES_CHECK_LAUNCH();
   }
   IMPES_CUDA(cudaStreamSynchronize(s));
+  // the fp32 Galerkin chain's A*P values are allocated here, not at the first
+  // update: that update may run inside a stream capture (whole-step graphs),
+  // where cudaMalloc is refused
+  if (h.prm.mixed_precision)
+    for (auto& L : h.levels)
+      if (!L->coarsest) L->apvalf.ensure(std::max<size_t>(L->apval.n, 1));
   if (sell_enabled()) {
     for (auto& L : h.levels) build_sell(*L, s);
     sell_refresh(h, 0, s, true);

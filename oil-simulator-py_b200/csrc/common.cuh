@@ -70,7 +70,8 @@ struct DBuf {
       cudaError_t e = cudaMalloc(&p, count * sizeof(T));
       if (e != cudaSuccess) {
         p = nullptr; n = 0;
-        throw Error(IMPES_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        throw Error(IMPES_ERR_OOM, "cudaMalloc of " + std::to_string(count * sizeof(T)) + " bytes: " +
+                                       cudaGetErrorString(e));
       }
     }
   }

@@ -457,10 +457,11 @@ def test_fused_vcycle_tail_matches_per_level_kernels(monkeypatch, precision):
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_sell_sweeps_match_csr(monkeypatch, precision):
     """IMPES_SELL=1 (read at setup) puts every level of >= 8,192 rows on its
-    SELL-32 copy of A (rows sorted by length inside 256-row windows, one lane
-    per row); IMPES_NO_SELL=1 keeps the CSR kernels.  The V-cycle and the
-    FGMRES solution agree to rounding: both layouts add each row's products in
-    the row's order, the CSR kernels with their tuned lanes per row."""
+    SELL-32 copy of A (rows sorted by length inside small windows, 1, 4 or 8
+    lanes per row by mean row length); IMPES_NO_SELL=1 keeps the CSR kernels.
+    The V-cycle and the FGMRES solution agree to rounding: both layouts add a
+    row's products lane by lane in the row's order, each with its own lanes
+    per row."""
     A = _laplacian_3d(48, 40, 24)
     n = A.shape[0]
     rng = np.random.default_rng(4)
