@@ -87,8 +87,9 @@ typedef struct {
   int col_row_relative;  /* 1: 16-bit columns hold col - row + 32768              */
   int lanes[6];          /* autotuned lanes per row of the kernels on A, R (restriction)
                             and P (prolongation): [0..2] fp64, [3..5] fp32; 0 = rule  */
-  int sell[2];           /* 1: the sweeps and residuals on A read the level's SELL-32
-                            (sliced ELLPACK) copy, one lane per row: [0] fp64, [1] fp32 */
+  int layout[2];         /* storage the sweeps and residuals on A read: 0 CSR, 1 the
+                            level's SELL-32 (sliced ELLPACK) copy, 2 its DIA (one array
+                            per diagonal) copy; [0] fp64, [1] fp32                    */
 } impes_amg_level_desc;
 
 /* Norms for Krylov stopping tests. */

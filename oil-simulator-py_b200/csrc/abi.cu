@@ -312,7 +312,7 @@ int impes_amg_level_info(impes_amg* h, int lvl, impes_amg_level_desc* info) {
       info->lanes[3 * q + 0] = L.lpr_a[q];
       info->lanes[3 * q + 1] = L.lpr_r[q];
       info->lanes[3 * q + 2] = L.lpr_p[q];
-      info->sell[q] = L.sell_on[q] ? 1 : 0;
+      info->layout[q] = L.dia_on[q] ? 2 : (L.sell_on[q] ? 1 : 0);
     }
   });
 }

@@ -33,6 +33,17 @@ struct Level {
   DBuf<double> sell_val;
   DBuf<float> sell_valf;
   bool sell_on[2] = {false, false};  // autotuned: the sweeps/residuals of this precision use SELL
+  // Diagonal (DIA) copy of A when the level has at most kDiaMax distinct
+  // offsets col - row (a structured-grid stencil, like a TPFA level 0):
+  // dia_off[d] ascending, dia_val[d n + i] = A(i, i + dia_off[d]), 0 where the
+  // pattern has no entry; dia_map[k] = d n + i of CSR entry k.
+  static constexpr int kDiaMax = 8;
+  int dia_nd = 0;
+  int dia_off[kDiaMax] = {0, 0, 0, 0, 0, 0, 0, 0};
+  DBuf<int> dia_map;
+  DBuf<double> dia_val;
+  DBuf<float> dia_valf;
+  bool dia_on[2] = {false, false};   // autotuned: the sweeps/residuals of this precision use DIA
   int avg_row = 7;                 // nnz / n, selects the SpMV row mapping
   // autotuned lanes per row ([0] fp64, [1] fp32; 0 = the mean-row-length rule)
   // of the kernels on A (sweeps, residuals), R (restriction) and P (prolongation)

@@ -11,6 +11,8 @@
 #include "amg.cuh"
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -302,6 +304,45 @@ void launch_csr(int n, int avg, const int* rowptr, const int* col, const T* val,
   IMPES_CHECK_LAUNCH();
 }
 
+// Restriction fused with the coarse level's first l1-Jacobi sweep from zero:
+// bc = R r (as k_csr Y_AX with LPR lanes per row) and xc = w inv_c bc (as
+// Y_SMOOTH0), so the coarse level starts with two sweeps left.
+template <typename T, int LPR>
+__global__ void __launch_bounds__(TB) k_restrict_s0(int nc, const int* __restrict__ rowptr,
+                                                    const int* __restrict__ col, const T* __restrict__ val,
+                                                    const T* __restrict__ r, const T* __restrict__ inv_c,
+                                                    T* __restrict__ bc, T* __restrict__ xc) {
+  pdl_wait_release();
+  const int g = threadIdx.x / LPR, lane = threadIdx.x % LPR;
+  const int rows_per_block = TB / LPR;
+  for (long long row = (long long)blockIdx.x * rows_per_block + g; row < nc;
+       row += (long long)gridDim.x * rows_per_block) {
+    T acc = row_dot(rowptr[row] + lane, rowptr[row + 1], LPR, val, col, r, 0, T(0));
+#pragma unroll
+    for (int o = LPR / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, LPR);
+    if (lane == 0) {
+      bc[row] = acc;
+      xc[row] = T(kOmega) * inv_c[row] * acc;
+    }
+  }
+}
+
+template <typename T>
+void launch_restrict_s0(const Level& L, int lpr, const T* rval, const T* r, const T* inv_c, T* bc, T* xc,
+                        cudaStream_t s) {
+  const int n = L.nc;
+  auto grid = [&](int l) { return grid_for(((size_t)n * l + TB - 1) / TB * TB, TB, 16); };
+  switch (lpr) {
+    case 1: launch_pdl(k_restrict_s0<T, 1>, grid(1), TB, 0, s, n, (const int*)L.rrow.p, (const int*)L.rcol.p, rval, r, inv_c, bc, xc); break;
+    case 2: launch_pdl(k_restrict_s0<T, 2>, grid(2), TB, 0, s, n, (const int*)L.rrow.p, (const int*)L.rcol.p, rval, r, inv_c, bc, xc); break;
+    case 4: launch_pdl(k_restrict_s0<T, 4>, grid(4), TB, 0, s, n, (const int*)L.rrow.p, (const int*)L.rcol.p, rval, r, inv_c, bc, xc); break;
+    case 8: launch_pdl(k_restrict_s0<T, 8>, grid(8), TB, 0, s, n, (const int*)L.rrow.p, (const int*)L.rcol.p, rval, r, inv_c, bc, xc); break;
+    case 16: launch_pdl(k_restrict_s0<T, 16>, grid(16), TB, 0, s, n, (const int*)L.rrow.p, (const int*)L.rcol.p, rval, r, inv_c, bc, xc); break;
+    default: launch_pdl(k_restrict_s0<T, 32>, grid(32), TB, 0, s, n, (const int*)L.rrow.p, (const int*)L.rcol.p, rval, r, inv_c, bc, xc); break;
+  }
+  IMPES_CHECK_LAUNCH();
+}
+
 // ------------------------------------------------------ SELL-32 sweeps
 // Sliced ELLPACK with slices of one warp (C = 32) and rows sorted by length
 // inside windows (Kreutzer et al., "A unified sparse matrix data format for
@@ -368,11 +409,55 @@ void launch_sell(const Level& L, const T* x, const T* b, const T* inv, T* y, cud
     launch_sell_ct<T, int, MODE>(L, (const int*)L.sell_col.p, 0, x, b, inv, y, s);
 }
 
-// A product of a level's A with the layout chosen for this precision (SELL or
-// the CSR kernels with the tuned lanes per row).
+// ------------------------------------------------------ DIA sweeps
+// A level whose entries lie on at most Level::kDiaMax diagonals (the 7-point
+// stencil of a structured grid) as one value array per diagonal: one thread per
+// row, every value load and every x load of a warp contiguous, no column
+// indices.  The diagonals are added in ascending offset, the row's CSR order,
+// skipping offsets that leave the matrix (entries the pattern lacks hold 0).
+struct DiaOffsets {
+  int off[Level::kDiaMax];
+};
+template <typename T, int MODE>
+__global__ void __launch_bounds__(TB) k_dia(int n, int nd, DiaOffsets o, const T* __restrict__ val,
+                                            const T* __restrict__ x, const T* __restrict__ b,
+                                            const T* __restrict__ inv, T* __restrict__ y) {
+  pdl_wait_release();
+  for (int i = blockIdx.x * TB + threadIdx.x; i < n; i += gridDim.x * TB) {
+    T acc = T(0);
+#pragma unroll
+    for (int d = 0; d < Level::kDiaMax; ++d) {
+      if (d < nd) {
+        const int j = i + o.off[d];
+        if (j >= 0 && j < n) acc += val[(long long)d * n + i] * x[j];
+      }
+    }
+    if (MODE == Y_AX) y[i] = acc;
+    else if (MODE == Y_B_MINUS_AX) y[i] = b[i] - acc;
+    else if (MODE == Y_SMOOTH) y[i] = x[i] + T(kOmega) * inv[i] * (b[i] - acc);
+    else if (MODE == Y_ADD_AX) y[i] = y[i] + acc;
+    else if (MODE == Y_W_AX) y[i] = inv[i] * acc;
+  }
+}
+template <typename T> const T* dia_values(const Level& L);
+template <> inline const double* dia_values<double>(const Level& L) { return L.dia_val.p; }
+template <> inline const float* dia_values<float>(const Level& L) { return L.dia_valf.p; }
+
+template <typename T, int MODE>
+void launch_dia(const Level& L, const T* x, const T* b, const T* inv, T* y, cudaStream_t s) {
+  DiaOffsets o{};
+  for (int d = 0; d < Level::kDiaMax; ++d) o.off[d] = L.dia_off[d];
+  launch_pdl(k_dia<T, MODE>, grid_for(L.n, TB, 16), TB, 0, s, L.n, L.dia_nd, o, dia_values<T>(L), x, b, inv, y);
+  IMPES_CHECK_LAUNCH();
+}
+
+// A product of a level's A with the layout chosen for this precision (DIA,
+// SELL or the CSR kernels with the tuned lanes per row).
 template <typename T, int MODE>
 void launch_a(const Level& L, int slot, const T* x, const T* b, const T* inv, T* y, cudaStream_t s) {
-  if (L.sell_on[slot] && sell_values<T>(L))
+  if (L.dia_on[slot] && dia_values<T>(L))
+    launch_dia<T, MODE>(L, x, b, inv, y, s);
+  else if (L.sell_on[slot] && sell_values<T>(L))
     launch_sell<T, MODE>(L, x, b, inv, y, s);
   else
     launch_csr<T, MODE>(L.n, L.avg_row, L.rowptr.p, L.col.p, (const T*)(sizeof(T) == 8 ? (const void*)L.val.p
@@ -1246,9 +1331,18 @@ T* vcycle(AMG& h, int l, bool zero_x, cudaStream_t s, bool first_sweep_done = fa
   T* spare = (x == LV<T>::x(L)) ? LV<T>::t(L) : LV<T>::x(L);
   Level& Nc = *h.levels[l + 1];
   launch_a<T, Y_B_MINUS_AX>(L, LV<T>::slot, x, LV<T>::b(L), nullptr, LV<T>::r(L), s);
-  launch_csr<T, Y_AX>(L.nc, L.r_avg, L.rrow.p, L.rcol.p, LV<T>::rval(L), LV<T>::r(L), nullptr,
-                      nullptr, LV<T>::b(Nc), s, nullptr, 0, L.lpr_r[LV<T>::slot]);
-  T* ec = vcycle<T>(h, l + 1, true, s);
+  // the restriction also takes the coarse level's first sweep from zero when
+  // that level smooths with l1-Jacobi through the per-level kernels
+  const bool fuse_s0 = !Nc.coarsest && L.r_avg <= 96 && !(l + 1 == h.tail_level) &&
+                       !(h.prm.smoother == IMPES_SMOOTHER_CHEBYSHEV && Nc.cheb_lmax.p);
+  if (fuse_s0) {
+    const int lpr_r = L.lpr_r[LV<T>::slot] > 0 ? L.lpr_r[LV<T>::slot] : default_lpr(L.r_avg);
+    launch_restrict_s0<T>(L, lpr_r, LV<T>::rval(L), LV<T>::r(L), LV<T>::inv(Nc), LV<T>::b(Nc), LV<T>::x(Nc), s);
+  } else {
+    launch_csr<T, Y_AX>(L.nc, L.r_avg, L.rrow.p, L.rcol.p, LV<T>::rval(L), LV<T>::r(L), nullptr,
+                        nullptr, LV<T>::b(Nc), s, nullptr, 0, L.lpr_r[LV<T>::slot]);
+  }
+  T* ec = vcycle<T>(h, l + 1, true, s, fuse_s0);
   launch_csr<T, Y_ADD_AX>(L.n, L.p_avg, L.prow.p, L.pcol.p, LV<T>::pval(L), ec, nullptr, nullptr, x, s,
                           nullptr, 0, L.lpr_p[LV<T>::slot]);
   T* out = smooth<T>(h, L, x, spare, LV<T>::b(L), 2, false, s, l == 0);
@@ -1308,9 +1402,41 @@ T* vcycle_top(AMG& h, bool zero_x, cudaStream_t s) {
 // ensemble members alike in size -- launch the same kernels and sum in the same
 // order.  Levels with more than 96 entries per row keep the warps-per-row
 // kernels.  IMPES_NO_TUNE=1 keeps the mean-row-length rule.
+//
+// IMPES_TUNE_CACHE=<file> makes the choices persistent: the file's entries
+// (one "precision operator rows avg choice" line each) are loaded before a
+// hierarchy is tuned and the process's choices are written back after, so a
+// later process -- another run, or one under a profiler whose serialised
+// launches would time differently -- launches the same kernels.
 namespace {
 std::mutex g_tune_mu;
 std::map<std::tuple<int, int, int, int>, int> g_tune_cache;
+
+const char* tune_cache_path() {
+  const char* ev = getenv("IMPES_TUNE_CACHE");
+  return (ev && ev[0]) ? ev : nullptr;
+}
+void tune_cache_load() {
+  const char* path = tune_cache_path();
+  if (!path) return;
+  FILE* f = fopen(path, "r");
+  if (!f) return;
+  int a, b, c, d, v;
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  while (fscanf(f, "%d %d %d %d %d", &a, &b, &c, &d, &v) == 5) g_tune_cache.emplace(std::make_tuple(a, b, c, d), v);
+  fclose(f);
+}
+void tune_cache_save() {
+  const char* path = tune_cache_path();
+  if (!path) return;
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  FILE* f = fopen(path, "w");
+  if (!f) return;
+  for (const auto& e : g_tune_cache)
+    fprintf(f, "%d %d %d %d %d\n", std::get<0>(e.first), std::get<1>(e.first), std::get<2>(e.first),
+            std::get<3>(e.first), e.second);
+  fclose(f);
+}
 
 template <typename T, int MODE>
 float time_lpr(int lpr, int n, int avg, const int* rowptr, const int* col, const T* val, const T* x,
@@ -1358,7 +1484,7 @@ int tune_one(int slot, int kind, int n, int avg, const int* rowptr, const int* c
 }
 
 // IMPES_SELL=1 (read at setup) puts every level that has a SELL copy on it,
-// whatever the timings say.
+// whatever the timings say (and no level on its DIA copy).
 bool sell_forced() {
   const char* ev = getenv("IMPES_SELL");
   return ev && ev[0] == '1';
@@ -1395,6 +1521,43 @@ bool tune_sell(Level& L, int slot, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e
   return ins.first->second != 0;
 }
 
+// The DIA copy against the level's tuned CSR/SELL sweep: kept when it is more
+// than 3 % faster (cached by shape).
+template <typename T>
+bool tune_dia(Level& L, int slot, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1) {
+  if (L.dia_nd <= 0 || !dia_values<T>(L)) return false;
+  const int nb = (int)std::lround(2.0 * std::log2((double)L.n));
+  const auto key = std::make_tuple(slot, 4, nb, L.avg_row);
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) return it->second != 0;
+  }
+  auto timed = [&](bool dia) {
+    L.dia_on[slot] = dia;
+    for (int w = 0; w < 2; ++w) launch_a<T, Y_SMOOTH>(L, slot, LV<T>::x(L), LV<T>::b(L), LV<T>::inv(L), LV<T>::t(L), s);
+    IMPES_CUDA(cudaEventRecord(e0, s));
+    for (int w = 0; w < 8; ++w) launch_a<T, Y_SMOOTH>(L, slot, LV<T>::x(L), LV<T>::b(L), LV<T>::inv(L), LV<T>::t(L), s);
+    IMPES_CUDA(cudaEventRecord(e1, s));
+    IMPES_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    IMPES_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    return ms;
+  };
+  const float t_other = timed(false), t_dia = timed(true);
+  const int pick = t_dia < 0.97f * t_other ? 1 : 0;
+  L.dia_on[slot] = false;
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  auto ins = g_tune_cache.emplace(key, pick);
+  return ins.first->second != 0;
+}
+
+// IMPES_DIA=1 (read at setup) puts every level that has a DIA copy on it.
+bool dia_forced() {
+  const char* ev = getenv("IMPES_DIA");
+  return ev && ev[0] == '1';
+}
+
 template <typename T>
 void tune_levels(AMG& h, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1) {
   const int slot = LV<T>::slot;
@@ -1406,6 +1569,10 @@ void tune_levels(AMG& h, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1) {
                                           L.col16_rel, s, e0, e1);
     L.sell_on[slot] = sell_forced() ? (L.sell_slices > 0 && sell_values<T>(L) != nullptr)
                                     : tune_sell<T>(L, slot, s, e0, e1);
+    // a forced layout is the one used (IMPES_SELL=1 keeps DIA off)
+    L.dia_on[slot] = dia_forced()    ? (L.dia_nd > 0 && dia_values<T>(L) != nullptr)
+                     : sell_forced() ? false
+                                     : tune_dia<T>(L, slot, s, e0, e1);
     L.lpr_r[slot] = tune_one<T, Y_AX>(slot, 1, L.nc, L.r_avg, L.rrow.p, L.rcol.p, LV<T>::rval(L), LV<T>::r(L),
                                       nullptr, nullptr, LV<T>::t(*h.levels[&up - &h.levels[0] + 1]), nullptr, 0,
                                       s, e0, e1);
@@ -1534,8 +1701,10 @@ void amg_autotune(AMG& h, cudaStream_t s) {
       IMPES_CUDA(cudaMemsetAsync(L->bf.p, 0, n * sizeof(float), s));
       IMPES_CUDA(cudaMemsetAsync(L->rf.p, 0, n * sizeof(float), s));
     }
+    tune_cache_load();
     tune_levels<double>(h, s, e0, e1);
     if (h.prm.mixed_precision) tune_levels<float>(h, s, e0, e1);
+    tune_cache_save();
   } catch (...) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -1980,8 +2149,6 @@ __global__ void __launch_bounds__(TB) k_fg_update(long long n, double* __restric
     partial[blockIdx.x] = u;
   }
 }
-// ||w||^2 after a pass; after pass 0 also the second-pass flag (the first pass
-// left less than 0.7 of the norm) -- FgState::wn2 / reorth
 // ||w||^2 from the update's partials; after pass 0 the reorthogonalisation
 // flag, which also opens the conditional node of pass 1
 __global__ void k_fg_norm(const double* partial, FgState* st, const double* H, int ldh, int pass,

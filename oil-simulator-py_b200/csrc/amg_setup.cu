@@ -1225,7 +1225,7 @@ namespace {
 constexpr int kSellMinRows = 8192;
 inline int sell_lanes(int avg) { return avg <= 12 ? 1 : avg <= 30 ? 4 : 8; }
 
-// IMPES_NO_SELL=1 (read at setup) builds no SELL copies.
+// IMPES_NO_SELL=1 (read at setup) builds no SELL or DIA copies.
 bool sell_enabled() {
   const char* ev = getenv("IMPES_NO_SELL");
   return !(ev && ev[0] == '1');
@@ -1321,12 +1321,72 @@ void build_sell(Level& L, cudaStream_t s) {
   L.sell_lpr = lpr;
 }
 
-// Gather the SELL values of the levels whose sweeps read them (all levels with
-// a copy when `all`, before the autotuner has chosen) from their CSR values:
-// slot 0 the fp64 values, 1 the fp32 ones.
+// DIA copy (Level::dia_*) of a level of at least kSellMinRows rows whose
+// entries lie on at most Level::kDiaMax diagonals, from the fixed pattern.
+template <typename T>
+__global__ void k_dia_scatter(int nnz, const int* __restrict__ map, const T* __restrict__ v, T* __restrict__ out) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nnz; k += gridDim.x * blockDim.x) out[map[k]] = v[k];
+}
+
+void build_dia(Level& L, cudaStream_t s) {
+  L.dia_nd = 0;
+  if (L.coarsest || L.n < kSellMinRows || L.nnz <= 0) return;
+  const int n = L.n;
+  std::vector<int> rp(n + 1), col(L.nnz);
+  IMPES_CUDA(cudaMemcpyAsync(rp.data(), L.rowptr.p, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost, s));
+  IMPES_CUDA(cudaMemcpyAsync(col.data(), L.col.p, sizeof(int) * L.nnz, cudaMemcpyDeviceToHost, s));
+  IMPES_CUDA(cudaStreamSynchronize(s));
+  std::vector<int> offs;
+  for (int r = 0; r < n; ++r)
+    for (int k = rp[r]; k < rp[r + 1]; ++k) {
+      const int d = col[k] - r;
+      if (std::find(offs.begin(), offs.end(), d) == offs.end()) {
+        offs.push_back(d);
+        if ((int)offs.size() > Level::kDiaMax) return;
+      }
+    }
+  std::sort(offs.begin(), offs.end());
+  std::vector<int> map(L.nnz);
+  for (int r = 0; r < n; ++r)
+    for (int k = rp[r]; k < rp[r + 1]; ++k) {
+      const int d = (int)(std::lower_bound(offs.begin(), offs.end(), col[k] - r) - offs.begin());
+      map[k] = d * n + r;
+    }
+  IMPES_REQUIRE((long long)offs.size() * n < (1LL << 31), IMPES_ERR_OOM, "DIA copy exceeds 2^31 entries");
+  L.dia_map.alloc(L.nnz);
+  IMPES_CUDA(cudaMemcpyAsync(L.dia_map.p, map.data(), sizeof(int) * L.nnz, cudaMemcpyHostToDevice, s));
+  IMPES_CUDA(cudaStreamSynchronize(s));   // the host vectors go out of scope
+  L.dia_nd = (int)offs.size();
+  for (int d = 0; d < Level::kDiaMax; ++d) L.dia_off[d] = d < L.dia_nd ? offs[d] : 0;
+}
+
+// Gather the SELL values and scatter the DIA values of the levels whose sweeps
+// read them (all levels with a copy when `all`, before the autotuner has
+// chosen) from their CSR values: slot 0 the fp64 values, 1 the fp32 ones.  A
+// DIA array is zeroed when first allocated; the pattern's entries overwrite
+// the same places every time.
 void sell_refresh(AMG& h, int slot, cudaStream_t s, bool all = false) {
   for (auto& up : h.levels) {
     Level& L = *up;
+    if (L.dia_nd > 0 && (all || L.dia_on[slot])) {
+      const size_t len = (size_t)L.dia_nd * L.n;
+      if (slot == 0 && L.val.p) {
+        if (L.dia_val.n < len) {
+          L.dia_val.alloc(len);
+          IMPES_CUDA(cudaMemsetAsync(L.dia_val.p, 0, len * sizeof(double), s));
+        }
+        k_dia_scatter<double><<<grid_for(L.nnz, TB), TB, 0, s>>>(L.nnz, L.dia_map.p, L.val.p, L.dia_val.p);
+        ::impes::count_launch();
+      } else if (slot == 1 && L.valf.p) {
+        if (L.dia_valf.n < len) {
+          L.dia_valf.alloc(len);
+          IMPES_CUDA(cudaMemsetAsync(L.dia_valf.p, 0, len * sizeof(float), s));
+        }
+        k_dia_scatter<float><<<grid_for(L.nnz, TB), TB, 0, s>>>(L.nnz, L.dia_map.p, L.valf.p, L.dia_valf.p);
+        ::impes::count_launch();
+      }
+      IMPES_CHECK_LAUNCH();
+    }
     if (L.sell_slices <= 0 || !(all || L.sell_on[slot])) continue;
     if (slot == 0) {
       if (!L.val.p) continue;
@@ -1604,13 +1664,24 @@ void amg_setup(AMG& h, int n, int nnz, const int* rowptr, const int* col, const 
     for (auto& L : h.levels)
       if (!L->coarsest) L->apvalf.ensure(std::max<size_t>(L->apval.n, 1));
   if (sell_enabled()) {
-    for (auto& L : h.levels) build_sell(*L, s);
+    for (auto& L : h.levels) {
+      build_sell(*L, s);
+      build_dia(*L, s);
+    }
     sell_refresh(h, 0, s, true);
     if (h.prm.mixed_precision) sell_refresh(h, 1, s, true);
   }
   amg_autotune(h, s);
   // the SELL copies the tuner did not pick are dropped
   for (auto& L : h.levels) {
+    if (L->dia_nd > 0) {
+      if (!L->dia_on[0]) L->dia_val.release();
+      if (!L->dia_on[1]) L->dia_valf.release();
+      if (!L->dia_on[0] && !L->dia_on[1]) {
+        L->dia_map.release();
+        L->dia_nd = 0;
+      }
+    }
     if (L->sell_slices <= 0) continue;
     if (!L->sell_on[0]) L->sell_val.release();
     if (!L->sell_on[1]) L->sell_valf.release();

@@ -280,7 +280,8 @@ class ClassicalAMG:
                         "is_coarsest": bool(info.is_coarsest),
                         "col_index_bytes": info.col_index_bytes,
                         "col_row_relative": bool(info.col_row_relative),
-                        "sell": tuple(bool(v) for v in info.sell)})
+                        "lanes": tuple(info.lanes),
+                        "layout": tuple({0: "csr", 1: "sell", 2: "dia"}[v] for v in info.layout)})
         self._levels_cache = out
         return out
 

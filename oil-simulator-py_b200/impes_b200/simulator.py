@@ -52,6 +52,8 @@ _PVT_COLS = ("pressure_MPa", "Bo", "Bw", "Bg", "mu_o_cP", "mu_w_cP", "mu_g_cP", 
 
 
 # ------------------------------------------------------------------- PVT
+_LAYOUTS = {0: "csr", 1: "sell", 2: "dia"}
+
 class PVTTable:
     """Black-oil table (``PVTTable``, pvt.py:18-64): columns linear in pressure (MPa)."""
 
@@ -634,12 +636,12 @@ class Simulator:
         return (ng.value, bool(bad.value))
 
     def amg_levels(self):
-        """[(n, nnz, p_cols, p_nnz, is_coarsest, columns, lanes, sell)] of the
+        """[(n, nnz, p_cols, p_nnz, is_coarsest, columns, lanes, layout)] of the
         pressure hierarchy; columns is the index storage of the level's sweeps:
         "i32", "u16" or "u16rel" (16-bit offsets from the row); lanes the
         autotuned lanes per row of the kernels on A, R and P (fp64 then fp32; 0:
-        the default rule); sell (fp64, fp32) whether the sweeps and residuals
-        read the level's SELL-32 copy of A."""
+        the default rule); layout (fp64, fp32) the storage the sweeps and
+        residuals read: "csr", "sell" or "dia"."""
         if self._amg_h is None:
             return []
         nl = C.c_int(0)
@@ -650,7 +652,7 @@ class Simulator:
             check(lib.impes_amg_level_info(self._amg_h, l, C.byref(d)))
             cols = "i32" if d.col_index_bytes == 4 else ("u16rel" if d.col_row_relative else "u16")
             out.append((d.n, d.nnz, d.p_cols, d.p_nnz, bool(d.is_coarsest), cols, tuple(d.lanes),
-                        tuple(bool(v) for v in d.sell)))
+                        tuple(_LAYOUTS[v] for v in d.layout)))
         return out
 
     # --------------------------------------------------- building blocks

@@ -455,34 +455,67 @@ def test_fused_vcycle_tail_matches_per_level_kernels(monkeypatch, precision):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-def test_sell_sweeps_match_csr(monkeypatch, precision):
+def test_sell_and_dia_sweeps_match_csr(monkeypatch, precision):
     """IMPES_SELL=1 (read at setup) puts every level of >= 8,192 rows on its
     SELL-32 copy of A (rows sorted by length inside small windows, 1, 4 or 8
-    lanes per row by mean row length); IMPES_NO_SELL=1 keeps the CSR kernels.
-    The V-cycle and the FGMRES solution agree to rounding: both layouts add a
-    row's products lane by lane in the row's order, each with its own lanes
-    per row."""
+    lanes per row by mean row length); IMPES_DIA=1 puts level 0 of a 7-point
+    matrix on its DIA copy (one array per diagonal); IMPES_NO_SELL=1 keeps the
+    CSR kernels.  The V-cycle and the FGMRES solution agree to rounding: every
+    layout adds a row's products lane by lane in the row's order, each with its
+    own lanes per row."""
     A = _laplacian_3d(48, 40, 24)
     n = A.shape[0]
     rng = np.random.default_rng(4)
     bs = rng.standard_normal(n)
     out = {}
-    for mode in ("csr", "sell"):
+    slot = 0 if precision == "fp64" else 1
+    for mode in ("csr", "sell", "dia"):
         monkeypatch.setenv("IMPES_NO_SELL", "1" if mode == "csr" else "0")
         monkeypatch.setenv("IMPES_SELL", "1" if mode == "sell" else "0")
+        monkeypatch.setenv("IMPES_DIA", "1" if mode == "dia" else "0")
         amg = gpu_amg(A, coarsest_size=60, seed=2, mixed_precision=True)
-        slot = 0 if precision == "fp64" else 1
-        used = [lv["sell"][slot] for lv in amg.levels if not lv["is_coarsest"]]
-        if mode == "sell":
-            assert used[0] and sum(used) >= 2, used
+        used = [lv["layout"][slot] for lv in amg.levels if not lv["is_coarsest"]]
+        if mode == "csr":
+            assert set(used) == {"csr"}, used
+        elif mode == "sell":
+            assert used[0] == "sell" and used.count("sell") >= 2, used
         else:
-            assert not any(used), used
+            assert used[0] == "dia", used
         v = to_np(amg.vcycle_scaled(torch.tensor(bs, device="cuda"), precision=precision))
         x, st = amg.fgmres(torch.tensor(bs, device="cuda"), tol=1e-10, norm="jacobi", precision=precision)
         assert st["converged"], st
         out[mode] = (v, to_np(x), st["iterations"])
         amg.close()
     tol = 1e-12 if precision == "fp64" else 1e-5
-    assert np.linalg.norm(out["csr"][0] - out["sell"][0]) <= tol * np.linalg.norm(out["sell"][0])
-    assert np.linalg.norm(out["csr"][1] - out["sell"][1]) <= 1e-8 * np.linalg.norm(out["sell"][1])
-    assert abs(out["csr"][2] - out["sell"][2]) <= 1
+    for mode in ("sell", "dia"):
+        assert np.linalg.norm(out["csr"][0] - out[mode][0]) <= tol * np.linalg.norm(out[mode][0]), mode
+        assert np.linalg.norm(out["csr"][1] - out[mode][1]) <= 1e-8 * np.linalg.norm(out[mode][1]), mode
+        assert abs(out["csr"][2] - out[mode][2]) <= 1, mode
+
+
+def test_tuner_choices_persist_across_processes(tmp_path, monkeypatch):
+    """IMPES_TUNE_CACHE=<file>: the lanes-per-row and layout choices of a
+    hierarchy are written to the file, and another process that loads it
+    launches the same kernels for a hierarchy of the same shape, whatever its
+    own timings would say."""
+    import json
+    import subprocess
+    import sys
+    cache = tmp_path / "tune.txt"
+    monkeypatch.setenv("IMPES_TUNE_CACHE", str(cache))
+    A = _laplacian_3d(40, 40, 24)
+    amg = gpu_amg(A, coarsest_size=60, seed=2, mixed_precision=True)
+    mine = [(lv["n"], lv["lanes"], lv["layout"]) for lv in amg.levels]
+    amg.close()
+    lines = cache.read_text().split("\n")
+    rows = [list(map(int, ln.split())) for ln in lines if ln.strip()]
+    assert rows and all(len(r) == 5 for r in rows)
+    code = ("import sys, json; sys.path[:0] = %r\n"
+            "from test_gpu_amg import _laplacian_3d, gpu_amg\n"
+            "a = gpu_amg(_laplacian_3d(40, 40, 24), coarsest_size=60, seed=2, mixed_precision=True)\n"
+            "print(json.dumps([(lv['n'], lv['lanes'], lv['layout']) for lv in a.levels]))\n") % (sys.path,)
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600,
+                         cwd=str(tmp_path), env=dict(__import__("os").environ))
+    assert out.returncode == 0, out.stderr[-2000:]
+    theirs = json.loads(out.stdout.strip().splitlines()[-1])
+    assert [(n, tuple(ln), tuple(l)) for n, ln, l in theirs] == mine
