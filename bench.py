@@ -501,6 +501,7 @@ def run_variant(args, cfg, fields, precision, device, dt, flush, stream, dist, r
                iters_inst=iters_inst, launches=launches, e2e_ms=float(te.item()), e2e_bytes=e2e_bytes,
                e2e_iters=e2e_iters, setup_s=setup_s, p=fl.pressure.clone(), sw=fl.s_w.clone(),
                sg=fl.s_g.clone(), oc=oc, levels=len(levels),
+               layout0=(levels[0][7][1 if precision == "mixed" else 0] if levels else None),
                mass_err=abs((m1 - m0) - inflow) / max(abs(m0), 1e-300),
                steps_run=args.warmup + 3 * args.steps,
                state={"sw": [float(fl.s_w.min()), float(fl.s_w.max())],
@@ -642,7 +643,8 @@ def run_ours(args, world, rank, local):
                              if trunc else f"FGMRES({args.restart}) + RS-AMG V-cycle",
                    "tol": PRESSURE_TOL, "norm": "Jacobi-scaled", "l2": "flushed before each step",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
-        "roofline": {"kernel": "wide-level l1-Jacobi sweep" if key == "smooth_wide" else "level-0 l1-Jacobi sweep",
+        "roofline": {"kernel": "wide-level l1-Jacobi sweep" if key == "smooth_wide"
+                     else f"level-0 l1-Jacobi sweep, fp32, {str(mixed.get('layout0')).upper()} layout",
                      "bound": "hbm", "achieved": sig(achieved), "peak": hbm_peak, "peak_kind": peak_kind,
                      "unit": "GB/s", "frac": sig(achieved / hbm_peak, 3), "traffic": traffic},
         "e2e": {"value": sig(world * cells * steps / (mixed["e2e_ms"] / 1e3)), "unit": "cell-steps/s",

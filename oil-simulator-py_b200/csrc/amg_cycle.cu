@@ -439,6 +439,35 @@ __global__ void __launch_bounds__(TB) k_dia(int n, int nd, DiaOffsets o, const T
     else if (MODE == Y_W_AX) y[i] = inv[i] * acc;
   }
 }
+// ND diagonals known at compile time (the 7-point stencil): every value and x
+// load of a row is issued before the first product, with the x index clamped
+// into the matrix -- where the pattern has no entry the value is 0, so the
+// product adds +-0 and the sum is the same as skipping it.
+template <typename T, int ND, int MODE>
+__global__ void __launch_bounds__(TB) k_dia_n(int n, DiaOffsets o, const T* __restrict__ val,
+                                              const T* __restrict__ x, const T* __restrict__ b,
+                                              const T* __restrict__ inv, T* __restrict__ y) {
+  pdl_wait_release();
+  for (int i = blockIdx.x * TB + threadIdx.x; i < n; i += gridDim.x * TB) {
+    T v[ND], xv[ND];
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+      int j = i + o.off[d];
+      j = j < 0 ? 0 : (j >= n ? n - 1 : j);
+      v[d] = val[(long long)d * n + i];
+      xv[d] = x[j];
+    }
+    T acc = T(0);
+#pragma unroll
+    for (int d = 0; d < ND; ++d) acc += v[d] * xv[d];
+    if (MODE == Y_AX) y[i] = acc;
+    else if (MODE == Y_B_MINUS_AX) y[i] = b[i] - acc;
+    else if (MODE == Y_SMOOTH) y[i] = x[i] + T(kOmega) * inv[i] * (b[i] - acc);
+    else if (MODE == Y_ADD_AX) y[i] = y[i] + acc;
+    else if (MODE == Y_W_AX) y[i] = inv[i] * acc;
+  }
+}
+
 template <typename T> const T* dia_values(const Level& L);
 template <> inline const double* dia_values<double>(const Level& L) { return L.dia_val.p; }
 template <> inline const float* dia_values<float>(const Level& L) { return L.dia_valf.p; }
@@ -447,7 +476,10 @@ template <typename T, int MODE>
 void launch_dia(const Level& L, const T* x, const T* b, const T* inv, T* y, cudaStream_t s) {
   DiaOffsets o{};
   for (int d = 0; d < Level::kDiaMax; ++d) o.off[d] = L.dia_off[d];
-  launch_pdl(k_dia<T, MODE>, grid_for(L.n, TB, 16), TB, 0, s, L.n, L.dia_nd, o, dia_values<T>(L), x, b, inv, y);
+  if (L.dia_nd == 7)
+    launch_pdl(k_dia_n<T, 7, MODE>, grid_for(L.n, TB, 16), TB, 0, s, L.n, o, dia_values<T>(L), x, b, inv, y);
+  else
+    launch_pdl(k_dia<T, MODE>, grid_for(L.n, TB, 16), TB, 0, s, L.n, L.dia_nd, o, dia_values<T>(L), x, b, inv, y);
   IMPES_CHECK_LAUNCH();
 }
 
@@ -1011,6 +1043,18 @@ inline double spmv_bytes(double sv, double sx, double nnz, double rows, double c
 inline double sweep_bytes(double s, double nnz, double n, double si = 4.0) {
   return (s + si) * nnz + 4.0 * n + 4.0 * s * n;
 }
+// Bytes one sweep of level L moves in the layout it runs in: the CSR formula
+// above; a DIA copy's diagonals (zeros included) and x, b, inv, y; a SELL
+// copy's padded values and columns, its row permutation and slice pointers.
+template <typename T>
+double layout_sweep_bytes(const Level& L, int slot) {
+  const double s = sizeof(T), n = L.n;
+  if (L.dia_on[slot]) return s * (double)L.dia_nd * n + 4.0 * s * n;
+  if (L.sell_on[slot])
+    return (s + (L.sell_col16.p ? 2.0 : 4.0)) * (double)L.sell_len + 4.0 * n + 4.0 * (L.sell_slices + 1.0) +
+           4.0 * s * n;
+  return sweep_bytes(s, L.nnz, n, L.col16.p ? 2.0 : 4.0);
+}
 
 // Algorithmic bytes of one Chebyshev step: values, columns, row pointers, the
 // gathered direction, r and x read and written, inv, the next direction.
@@ -1082,7 +1126,7 @@ T* smooth(const AMG& h, Level& L, T* x, T* spare, const T* b, int nu, bool zero_
     const int tid = top ? timers().begin(IMPES_PH_SMOOTH_L0, s)
                         : (wide ? timers().begin(IMPES_PH_SMOOTH_WIDE, s) : -1);
     launch_a<T, Y_SMOOTH>(L, LV<T>::slot, x, b, LV<T>::inv(L), spare, s);
-    timers().end(tid, s, sweep_bytes(sizeof(T), L.nnz, L.n, L.col16.p ? 2.0 : 4.0));
+    timers().end(tid, s, layout_sweep_bytes<T>(L, LV<T>::slot));
     std::swap(x, spare);
   }
   return x;
@@ -1438,18 +1482,49 @@ void tune_cache_save() {
   fclose(f);
 }
 
+// Cold-cache trials: a level whose sweep streams more than kColdBytes is timed
+// one launch at a time after g_flush (allocated while a hierarchy is tuned) is
+// overwritten, as a V-cycle sees it -- the other levels' data passes through
+// L2 between two sweeps of a large level.  Smaller levels run back to back
+// (on the 1e6-cell hierarchy a 24 MB threshold timed its 34 MB level 2 cold
+// and picked a kernel 1.5x slower in the V-cycle).
+constexpr double kColdBytes = 40.0 * (1 << 20);
+constexpr size_t kFlushBytes = 192u << 20;
+thread_local void* g_flush = nullptr;   // per tuning thread (ensembles tune on several)
+
+template <typename F>
+float time_trials(F launch, double bytes, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1) {
+  for (int w = 0; w < 2; ++w) launch();
+  float total = 0.f, ms = 0.f;
+  if (g_flush && bytes > kColdBytes) {
+    for (int w = 0; w < 8; ++w) {
+      IMPES_CUDA(cudaMemsetAsync(g_flush, w, kFlushBytes, s));
+      IMPES_CUDA(cudaEventRecord(e0, s));
+      launch();
+      IMPES_CUDA(cudaEventRecord(e1, s));
+      IMPES_CUDA(cudaEventSynchronize(e1));
+      IMPES_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      total += ms;
+    }
+    return total;
+  }
+  IMPES_CUDA(cudaEventRecord(e0, s));
+  for (int w = 0; w < 8; ++w) launch();
+  IMPES_CUDA(cudaEventRecord(e1, s));
+  IMPES_CUDA(cudaEventSynchronize(e1));
+  IMPES_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  return ms;
+}
+inline double level_bytes(size_t value_bytes, int n, double avg, bool col16) {
+  return (double)n * avg * (value_bytes + (col16 ? 2.0 : 4.0)) + (double)n * (4.0 + 4.0 * value_bytes);
+}
+
 template <typename T, int MODE>
 float time_lpr(int lpr, int n, int avg, const int* rowptr, const int* col, const T* val, const T* x,
                const T* b, const T* inv, T* y, const unsigned short* col16, int rel, cudaStream_t s,
                cudaEvent_t e0, cudaEvent_t e1) {
-  for (int w = 0; w < 2; ++w) launch_csr<T, MODE>(n, avg, rowptr, col, val, x, b, inv, y, s, col16, rel, lpr);
-  IMPES_CUDA(cudaEventRecord(e0, s));
-  for (int w = 0; w < 8; ++w) launch_csr<T, MODE>(n, avg, rowptr, col, val, x, b, inv, y, s, col16, rel, lpr);
-  IMPES_CUDA(cudaEventRecord(e1, s));
-  IMPES_CUDA(cudaEventSynchronize(e1));
-  float ms = 0.f;
-  IMPES_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-  return ms;
+  return time_trials([&] { launch_csr<T, MODE>(n, avg, rowptr, col, val, x, b, inv, y, s, col16, rel, lpr); },
+                     level_bytes(sizeof(T), n, avg, col16 != nullptr), s, e0, e1);
 }
 
 template <typename T, int MODE>
@@ -1502,16 +1577,11 @@ bool tune_sell(Level& L, int slot, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e
     auto it = g_tune_cache.find(key);
     if (it != g_tune_cache.end()) return it->second != 0;
   }
+  const double bytes = level_bytes(sizeof(T), L.n, L.avg_row, L.col16.p != nullptr);
   auto timed = [&](bool sell) {
     L.sell_on[slot] = sell;
-    for (int w = 0; w < 2; ++w) launch_a<T, Y_SMOOTH>(L, slot, LV<T>::x(L), LV<T>::b(L), LV<T>::inv(L), LV<T>::t(L), s);
-    IMPES_CUDA(cudaEventRecord(e0, s));
-    for (int w = 0; w < 8; ++w) launch_a<T, Y_SMOOTH>(L, slot, LV<T>::x(L), LV<T>::b(L), LV<T>::inv(L), LV<T>::t(L), s);
-    IMPES_CUDA(cudaEventRecord(e1, s));
-    IMPES_CUDA(cudaEventSynchronize(e1));
-    float ms = 0.f;
-    IMPES_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    return ms;
+    return time_trials([&] { launch_a<T, Y_SMOOTH>(L, slot, LV<T>::x(L), LV<T>::b(L), LV<T>::inv(L), LV<T>::t(L), s); },
+                       bytes, s, e0, e1);
   };
   const float t_csr = timed(false), t_sell = timed(true);
   const int pick = t_sell < 0.97f * t_csr ? 1 : 0;
@@ -1533,16 +1603,11 @@ bool tune_dia(Level& L, int slot, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1
     auto it = g_tune_cache.find(key);
     if (it != g_tune_cache.end()) return it->second != 0;
   }
+  const double bytes = level_bytes(sizeof(T), L.n, L.avg_row, L.col16.p != nullptr);
   auto timed = [&](bool dia) {
     L.dia_on[slot] = dia;
-    for (int w = 0; w < 2; ++w) launch_a<T, Y_SMOOTH>(L, slot, LV<T>::x(L), LV<T>::b(L), LV<T>::inv(L), LV<T>::t(L), s);
-    IMPES_CUDA(cudaEventRecord(e0, s));
-    for (int w = 0; w < 8; ++w) launch_a<T, Y_SMOOTH>(L, slot, LV<T>::x(L), LV<T>::b(L), LV<T>::inv(L), LV<T>::t(L), s);
-    IMPES_CUDA(cudaEventRecord(e1, s));
-    IMPES_CUDA(cudaEventSynchronize(e1));
-    float ms = 0.f;
-    IMPES_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    return ms;
+    return time_trials([&] { launch_a<T, Y_SMOOTH>(L, slot, LV<T>::x(L), LV<T>::b(L), LV<T>::inv(L), LV<T>::t(L), s); },
+                       bytes, s, e0, e1);
   };
   const float t_other = timed(false), t_dia = timed(true);
   const int pick = t_dia < 0.97f * t_other ? 1 : 0;
@@ -1702,10 +1767,15 @@ void amg_autotune(AMG& h, cudaStream_t s) {
       IMPES_CUDA(cudaMemsetAsync(L->rf.p, 0, n * sizeof(float), s));
     }
     tune_cache_load();
+    DBuf<char> flush(kFlushBytes);
+    g_flush = flush.p;
     tune_levels<double>(h, s, e0, e1);
     if (h.prm.mixed_precision) tune_levels<float>(h, s, e0, e1);
+    IMPES_CUDA(cudaStreamSynchronize(s));
+    g_flush = nullptr;
     tune_cache_save();
   } catch (...) {
+    g_flush = nullptr;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     throw;
@@ -1945,9 +2015,9 @@ void amg_fgmres(AMG& h, const double* b, double* x, const impes_krylov_params& k
       }
       // w = wt .* (A_s z_j)
       const int tsp = timers().begin(IMPES_PH_SPMV_L0, s);
-      launch_csr<double, Y_W_AX>(n, L0.avg_row, L0.rowptr.p, L0.col.p, L0.val.p, zj, nullptr, wt, w, s,
-                                 L0.col16.p, L0.col16_rel, L0.lpr_a[0]);
-      timers().end(tsp, s, spmv_bytes(8.0, 8.0, L0.nnz, n, n, L0.col16.p ? 2.0 : 4.0) + 8.0 * n);
+      launch_a<double, Y_W_AX>(L0, 0, zj, nullptr, wt, w, s);
+      timers().end(tsp, s, L0.dia_on[0] ? 8.0 * L0.dia_nd * (double)n + 24.0 * n
+                                        : spmv_bytes(8.0, 8.0, L0.nnz, n, n, L0.col16.p ? 2.0 : 4.0) + 8.0 * n);
       // classical Gram-Schmidt; the second pass only when the first cancelled
       // more than 0.3 of the norm (flag on the device).  H[j+1, j] holds
       // ||w||^2 before the first pass until k_set_hcol overwrites it.
@@ -2320,12 +2390,48 @@ __global__ void __launch_bounds__(TB) k_fg_norm_partials(long long n, const doub
   }
 }
 
-// level-0 products of the device FGMRES, lanes per row as the level was tuned
+// k_fg_op on level 0's 7-diagonal DIA copy (fp64 values): the loads of a row
+// issued together, x indices clamped as in k_dia_n
+template <typename XT>
+__global__ void __launch_bounds__(TB) k_fg_op_dia(int n, DiaOffsets o, const double* __restrict__ val,
+                                                  const XT* __restrict__ x, double* __restrict__ Z,
+                                                  const double* __restrict__ wt, double* __restrict__ V,
+                                                  const FgState* st) {
+  pdl_wait_release();
+  const long long j = st->j;
+  double* zj = Z + j * n;
+  double* y = V + (j + 1) * (long long)n;
+  for (int i = blockIdx.x * TB + threadIdx.x; i < n; i += gridDim.x * TB) {
+    double v[7];
+    XT xv[7];
+#pragma unroll
+    for (int d = 0; d < 7; ++d) {
+      int c = i + o.off[d];
+      c = c < 0 ? 0 : (c >= n ? n - 1 : c);
+      v[d] = val[(long long)d * n + i];
+      xv[d] = x[c];
+    }
+    double acc = 0.0;
+#pragma unroll
+    for (int d = 0; d < 7; ++d) acc += v[d] * xv[d];
+    y[i] = wt[i] * acc;
+    zj[i] = (double)x[i];
+  }
+}
+
+// level-0 products of the device FGMRES: the DIA copy when the level's fp64
+// sweeps use it, else CSR with the lanes per row the level was tuned to
 template <typename XT, typename CT>
 void fg_op(const Level& L0, const CT* col, const XT* z, double* Z, const double* wt, double* V, int rel,
            const FgState* st, cudaStream_t s) {
-  const int lpr = L0.lpr_a[0] > 0 ? L0.lpr_a[0] : (L0.avg_row <= 8 ? 1 : L0.avg_row <= 16 ? 4 : 8);
   const int n = L0.n;
+  if (L0.dia_on[0] && L0.dia_nd == 7 && L0.dia_val.p) {
+    DiaOffsets o{};
+    for (int d = 0; d < Level::kDiaMax; ++d) o.off[d] = L0.dia_off[d];
+    launch_pdl(k_fg_op_dia<XT>, grid_for(n, TB, 16), TB, 0, s, n, o, (const double*)L0.dia_val.p, z, Z, wt, V, st);
+    return;
+  }
+  const int lpr = L0.lpr_a[0] > 0 ? L0.lpr_a[0] : (L0.avg_row <= 8 ? 1 : L0.avg_row <= 16 ? 4 : 8);
   auto grid = [&](int l) { return grid_for(((size_t)n * l + TB - 1) / TB * TB, TB, 16); };
   switch (lpr) {
     case 1: launch_pdl(k_fg_op<XT, CT, 1>, grid(1), TB, 0, s, n, L0.rowptr.p, col, L0.val.p, z, Z, wt, V, rel, st); break;

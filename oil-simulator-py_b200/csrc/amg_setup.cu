@@ -1729,6 +1729,14 @@ void update_fp32_chain(AMG& h, cudaStream_t s) {
   }
   coarse_factor(h, *h.levels.back(), s, true);
   sell_refresh(h, 1, s);
+  // level 0's fp64 values are current (the FGMRES operator reads them): so is
+  // its fp64 DIA copy
+  Level& Z0 = *h.levels[0];
+  if (Z0.dia_nd > 0 && Z0.dia_on[0] && Z0.dia_val.p) {
+    k_dia_scatter<double><<<grid_for(Z0.nnz, TB), TB, 0, s>>>(Z0.nnz, Z0.dia_map.p, Z0.val.p, Z0.dia_val.p);
+    ::impes::count_launch();
+    IMPES_CHECK_LAUNCH();
+  }
   h.fp64_stale = true;
 }
 
