@@ -112,11 +112,16 @@ __global__ void k_equil_prepare(int n, const double* d, const int* below, double
   if (blockIdx.x == 0 && threadIdx.x == 0) *flag_out = on ? 1 : 0;
 }
 // A_s = D^-1/2 A D^-1/2 as vals * dh[row] * dh[col] (classical_amg.py:776-780)
+// with dval set, also into the level's DIA copy (dval[dmap[e]])
 __global__ void k_equilibrate(int n, const int* rowptr, const int* col, const double* vin,
-                              const double* dh, double* vout) {
+                              const double* dh, double* vout, const int* dmap, double* dval) {
   GRID_LOOP(i, n) {
     double di = dh[i];
-    for (int e = rowptr[i]; e < rowptr[i + 1]; ++e) vout[e] = vin[e] * di * dh[col[e]];
+    for (int e = rowptr[i]; e < rowptr[i + 1]; ++e) {
+      const double v = vin[e] * di * dh[col[e]];
+      vout[e] = v;
+      if (dval) dval[dmap[e]] = v;
+    }
   }
 }
 
@@ -898,6 +903,14 @@ __global__ void k_restrict_basis(int nc, int m, const int* rrow, const int* rcol
 __global__ void k_to_float(long long n, const double* in, float* out) {
   GRID_LOOP(i, n) out[i] = (float)in[i];
 }
+// k_to_float of a level's values that also fills its fp32 DIA copy
+__global__ void k_to_float_dia(long long n, const double* in, float* out, const int* dmap, float* dval) {
+  GRID_LOOP(i, n) {
+    const float f = (float)in[i];
+    out[i] = f;
+    dval[dmap[i]] = f;
+  }
+}
 
 }  // namespace
 
@@ -1188,8 +1201,10 @@ void equilibrate_level0(AMG& h, const double* val_in, cudaStream_t s) {
   k_count_below<<<grid_for(n, TB), TB, 0, s>>>(n, h.diag_tmp.p, h.prm.equilibration_threshold, h.iflag.p); ::impes::count_launch();
   k_equil_prepare<<<grid_for(n, TB), TB, 0, s>>>(n, h.diag_tmp.p, h.iflag.p, h.dhalf_inv.p,
                                                  h.jac_w.p, h.iflag.p + 1); ::impes::count_launch();
-  k_equilibrate<<<grid_for(n, TB), TB, 0, s>>>(n, L0.rowptr.p, L0.col.p, val_in, h.dhalf_inv.p,
-                                               L0.val.p); ::impes::count_launch();
+  const bool dia = L0.dia_nd > 0 && L0.dia_on[0] && L0.dia_val.p;
+  k_equilibrate<<<grid_for(n, TB), TB, 0, s>>>(n, L0.rowptr.p, L0.col.p, val_in, h.dhalf_inv.p, L0.val.p,
+                                               dia ? L0.dia_map.p : nullptr, dia ? L0.dia_val.p : nullptr);
+  ::impes::count_launch();
   IMPES_CHECK_LAUNCH();
 }
 
@@ -1365,10 +1380,13 @@ void build_dia(Level& L, cudaStream_t s) {
 // chosen) from their CSR values: slot 0 the fp64 values, 1 the fp32 ones.  A
 // DIA array is zeroed when first allocated; the pattern's entries overwrite
 // the same places every time.
-void sell_refresh(AMG& h, int slot, cudaStream_t s, bool all = false) {
+void sell_refresh(AMG& h, int slot, cudaStream_t s, bool all = false, bool l0_fp32_done = false) {
   for (auto& up : h.levels) {
     Level& L = *up;
-    if (L.dia_nd > 0 && (all || L.dia_on[slot])) {
+    // level 0's fp64 DIA copy is written by the equilibration, and its fp32
+    // one, when l0_fp32_done, by the fp32 conversion
+    const bool l0_written = !all && &L == h.levels[0].get() && (slot == 0 || l0_fp32_done);
+    if (L.dia_nd > 0 && (all || L.dia_on[slot]) && !l0_written) {
       const size_t len = (size_t)L.dia_nd * L.n;
       if (slot == 0 && L.val.p) {
         if (L.dia_val.n < len) {
@@ -1702,7 +1720,12 @@ void amg_setup(AMG& h, int n, int nnz, const int* rowptr, const int* col, const 
 void update_fp32_chain(AMG& h, cudaStream_t s) {
   Level& L0 = *h.levels[0];
   compute_inv_relax(h, L0, s);
-  k_to_float<<<grid_for(L0.nnz, TB), TB, 0, s>>>(L0.nnz, L0.val.p, L0.valf.p); ::impes::count_launch();
+  const bool dia0 = L0.dia_nd > 0 && L0.dia_on[1] && L0.dia_valf.p;
+  if (dia0)
+    k_to_float_dia<<<grid_for(L0.nnz, TB), TB, 0, s>>>(L0.nnz, L0.val.p, L0.valf.p, L0.dia_map.p, L0.dia_valf.p);
+  else
+    k_to_float<<<grid_for(L0.nnz, TB), TB, 0, s>>>(L0.nnz, L0.val.p, L0.valf.p);
+  ::impes::count_launch();
   k_to_float<<<grid_for(L0.n, TB), TB, 0, s>>>(L0.n, L0.inv_relax.p, L0.inv_relaxf.p); ::impes::count_launch();
   cheb_copy_to_fp32(h, L0, s);
   IMPES_CHECK_LAUNCH();
@@ -1728,15 +1751,7 @@ void update_fp32_chain(AMG& h, cudaStream_t s) {
     compute_inv_relax_f(h, Nc, s);
   }
   coarse_factor(h, *h.levels.back(), s, true);
-  sell_refresh(h, 1, s);
-  // level 0's fp64 values are current (the FGMRES operator reads them): so is
-  // its fp64 DIA copy
-  Level& Z0 = *h.levels[0];
-  if (Z0.dia_nd > 0 && Z0.dia_on[0] && Z0.dia_val.p) {
-    k_dia_scatter<double><<<grid_for(Z0.nnz, TB), TB, 0, s>>>(Z0.nnz, Z0.dia_map.p, Z0.val.p, Z0.dia_val.p);
-    ::impes::count_launch();
-    IMPES_CHECK_LAUNCH();
-  }
+  sell_refresh(h, 1, s, false, true);
   h.fp64_stale = true;
 }
 
