@@ -39,6 +39,7 @@ struct Level {
   // pattern has no entry; dia_map[k] = d n + i of CSR entry k.
   static constexpr int kDiaMax = 8;
   int dia_nd = 0;
+  int dia_rpt = 1;                   // rows per thread of the 7-diagonal kernel (1 or 2, tuned)
   int dia_off[kDiaMax] = {0, 0, 0, 0, 0, 0, 0, 0};
   DBuf<int> dia_map;
   DBuf<double> dia_val;
