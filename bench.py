@@ -739,7 +739,7 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 V-cycle baseline")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward measurement")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-member ensemble measurement")
-    ap.add_argument("--warm-start", default="extrapolate", choices=["extrapolate", "previous", "zero"],
+    ap.add_argument("--warm-start", default="extrapolate", choices=["extrapolate", "quadratic", "previous", "zero"],
                     help="FGMRES first iterate: extrapolated pressure, previous pressure, or zero")
     ap.add_argument("--grid", default=None,
                     help="NXxNYxNZ: a smaller grid of the same workload (profiling captures only)")

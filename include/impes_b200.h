@@ -106,7 +106,9 @@ typedef struct {
   int precision;      /* 0: fp64 V-cycle, 1: fp32 V-cycle (mixed)   */
   int use_x0;         /* 1: x holds an initial guess; 2 (impes_step only): the
                          pressure extrapolated linearly in time from the last
-                         two accepted steps (the current one on the first)    */
+                         two accepted steps (the current one on the first);
+                         3 (impes_step only): quadratically from the last
+                         three (linearly while only two are known)            */
 } impes_krylov_params;
 
 typedef struct {

@@ -49,17 +49,41 @@ __global__ void k_extrapolate(int n, const double* __restrict__ p, const double*
     x0[i] = p[i] + r * (p[i] - p_prev[i]);
 }
 
+// x0 = w0 p + w1 p_prev + w2 p_prev2: the Lagrange parabola through the last
+// three accepted pressures, evaluated at the end of the step
+__global__ void k_extrapolate2(int n, const double* __restrict__ p, const double* __restrict__ p_prev,
+                               const double* __restrict__ p_prev2, double w0, double w1, double w2,
+                               double* __restrict__ x0) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    x0[i] = w0 * p[i] + w1 * p_prev[i] + w2 * p_prev2[i];
+}
+
 // After a captured step: the new pressure is accepted (p_prev takes the
-// step's starting pressure for the next extrapolated iterate) or, when the
-// solve missed its tolerance, p is restored from p_save.
+// step's starting pressure for the next extrapolated iterate, and p_prev2,
+// when given, the old p_prev) or, when the solve missed its tolerance, p is
+// restored from p_save.
 __global__ void k_accept(int n, const FgState* st, double* __restrict__ p, const double* __restrict__ p_save,
-                         double* __restrict__ p_prev) {
+                         double* __restrict__ p_prev, double* __restrict__ p_prev2) {
   const bool ok = st->converged && !st->nan;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
-    if (ok) p_prev[i] = p_save[i];
-    else p[i] = p_save[i];
+    if (ok) {
+      if (p_prev2) p_prev2[i] = p_prev[i];
+      p_prev[i] = p_save[i];
+    } else {
+      p[i] = p_save[i];
+    }
   }
+}
+
+// Extrapolation weights of the first iterate: Lagrange weights at t = dt of
+// the pressures at 0, -dt_prev and -(dt_prev + dt_prev2).
+void quad_weights(double dt, double dt_prev, double dt_prev2, double& w0, double& w1, double& w2) {
+  const double t1 = -dt_prev, t2 = -(dt_prev + dt_prev2), t = dt;
+  w0 = (t - t1) * (t - t2) / (t1 * t2);
+  w1 = t * (t - t2) / (t1 * (t1 - t2));
+  w2 = t * (t - t1) / (t2 * (t2 - t1));
 }
 
 // The whole IMPES step of the FGMRES solver as one CUDA graph: assembly, the
@@ -80,11 +104,13 @@ static void step_graph_refused(const char* stage, const char* why) {
 bool step_graph_run(Model& m, AMG& a, double* p, double* sw, double* sg, double* so, double dt,
                     const impes_krylov_params& kp, impes_krylov_stats& st, cudaStream_t s) {
   if (a.step_graph_failed || !a.use_graphs || !a.use_step_graph || timers().on || kp.precision < 0) return false;
-  const bool extrap = kp.use_x0 == 2 && m.have_prev && m.dt_prev > 0;
+  const bool extrap = kp.use_x0 >= 2 && m.have_prev && m.dt_prev > 0;
+  const bool quad = extrap && kp.use_x0 == 3 && m.have_prev2 && m.dt_prev2 > 0;
   AMG::StepGraph* g = nullptr;
   for (auto& e : a.step_graphs)
     if (e.model == &m && e.p == p && e.sw == sw && e.sg == sg && e.so == so && e.dt == dt &&
-        e.have_prev == extrap && (!extrap || e.dt_prev == m.dt_prev) && e.kp.tol == kp.tol &&
+        e.have_prev == extrap && (!extrap || e.dt_prev == m.dt_prev) && e.have_prev2 == quad &&
+        (!quad || e.dt_prev2 == m.dt_prev2) && e.kp.tol == kp.tol &&
         e.kp.restart == kp.restart && e.kp.max_iters == kp.max_iters && e.kp.norm == kp.norm &&
         e.kp.precision == kp.precision && e.kp.use_x0 == kp.use_x0) {
       g = &e;
@@ -99,6 +125,7 @@ bool step_graph_run(Model& m, AMG& a, double* p, double* sw, double* sg, double*
     k.use_x0 = kp.use_x0 ? 1 : 0;
     amg_fgmres_prepare(a, k);
     m.p_prev.ensure(m.P.N);
+    if (kp.use_x0 == 3) m.p_prev2.ensure(m.P.N);
     if (!a.cap_stream) IMPES_CUDA(cudaStreamCreateWithFlags(&a.cap_stream, cudaStreamNonBlocking));
     cudaStream_t cs = a.cap_stream;
     // the capture stream starts after the work already queued on s
@@ -124,14 +151,22 @@ bool step_graph_run(Model& m, AMG& a, double* p, double* sw, double* sg, double*
       amg_update(a, m.csr_val.p, cs);
       stage = "FGMRES";
       IMPES_CUDA(cudaMemcpyAsync(m.p_save.p, p, sizeof(double) * m.P.N, cudaMemcpyDeviceToDevice, cs));
-      if (extrap) {
+      if (quad) {
+        double w0, w1, w2;
+        quad_weights(dt, m.dt_prev, m.dt_prev2, w0, w1, w2);
+        k_extrapolate2<<<grid_for(m.P.N, 256), 256, 0, cs>>>(m.P.N, m.p_save.p, m.p_prev.p, m.p_prev2.p, w0, w1,
+                                                             w2, p);
+        ::impes::count_launch();
+        IMPES_CHECK_LAUNCH();
+      } else if (extrap) {
         k_extrapolate<<<grid_for(m.P.N, 256), 256, 0, cs>>>(m.P.N, m.p_save.p, m.p_prev.p, dt / m.dt_prev, p);
         ::impes::count_launch();
         IMPES_CHECK_LAUNCH();
       }
       amg_fgmres_capture(a, m.rhs.p, p, k, cs);
       stage = "saturation";
-      k_accept<<<grid_for(m.P.N, 256), 256, 0, cs>>>(m.P.N, a.fgst.p, p, m.p_save.p, m.p_prev.p);
+      k_accept<<<grid_for(m.P.N, 256), 256, 0, cs>>>(m.P.N, a.fgst.p, p, m.p_save.p, m.p_prev.p,
+                                                     kp.use_x0 == 3 ? m.p_prev2.p : nullptr);
       ::impes::count_launch();
       IMPES_CHECK_LAUNCH();
       model_saturation(m, p, sw, sg, so, dt, cs, &a.fgst.p->converged);
@@ -149,6 +184,7 @@ bool step_graph_run(Model& m, AMG& a, double* p, double* sw, double* sg, double*
     AMG::StepGraph e;
     e.model = &m; e.p = p; e.sw = sw; e.sg = sg; e.so = so; e.dt = dt;
     e.have_prev = extrap; e.dt_prev = extrap ? m.dt_prev : 0.0; e.kp = kp;
+    e.have_prev2 = quad; e.dt_prev2 = quad ? m.dt_prev2 : 0.0;
     e.fp64_stale_after = a.fp64_stale;
     e.kernels_body = a.fg_body_kernels;
     e.kernels_reorth = a.fg_reorth_kernels;
@@ -178,6 +214,10 @@ bool step_graph_run(Model& m, AMG& a, double* p, double* sw, double* sg, double*
   st = impes_krylov_stats{hs->total, hs->restarts, hs->converged && !hs->nan ? 1 : 0, hs->rel, hs->true_rel};
   if (hs->nan) throw Error(IMPES_ERR_NAN, "NaN in FGMRES");
   if (!st.converged) return true;            // p was restored by the graph
+  if (kp.use_x0 == 3) {
+    m.dt_prev2 = m.dt_prev;
+    m.have_prev2 = m.have_prev;
+  }
   m.dt_prev = dt;
   m.have_prev = true;
   return true;
@@ -624,10 +664,16 @@ int impes_step(impes_model* h, impes_amg* amg, double* p, double* sw, double* sg
         st.converged = rel < kp->tol;
       } else {
         impes_krylov_params k = *kp;
-        if (k.use_x0 == 2) {
-          // first iterate extrapolated from the last two accepted pressures
-          // (p_save holds p^n; the assembly has already used it)
-          if (m.have_prev && m.dt_prev > 0) {
+        if (k.use_x0 >= 2) {
+          // first iterate extrapolated from the last two (or three) accepted
+          // pressures (p_save holds p^n; the assembly has already used it)
+          if (k.use_x0 == 3 && m.have_prev && m.dt_prev > 0 && m.have_prev2 && m.dt_prev2 > 0) {
+            double w0, w1, w2;
+            quad_weights(dt, m.dt_prev, m.dt_prev2, w0, w1, w2);
+            k_extrapolate2<<<grid_for(m.P.N, 256), 256, 0, s>>>(m.P.N, m.p_save.p, m.p_prev.p, m.p_prev2.p, w0,
+                                                                w1, w2, p); ::impes::count_launch();
+            IMPES_CHECK_LAUNCH();
+          } else if (m.have_prev && m.dt_prev > 0) {
             k_extrapolate<<<grid_for(m.P.N, 256), 256, 0, s>>>(m.P.N, m.p_save.p, m.p_prev.p,
                                                                dt / m.dt_prev, p); ::impes::count_launch();
             IMPES_CHECK_LAUNCH();
@@ -647,7 +693,15 @@ int impes_step(impes_model* h, impes_amg* amg, double* p, double* sw, double* sg
                                                        : "FGMRES did not reach the pressure tolerance");
     }
     // the accepted step's starting pressure, for the next extrapolated iterate
+    // (and, for the quadratic one, the one before it)
     m.p_prev.ensure(m.P.N);
+    if (kp->use_x0 == 3 && solver == 1) {
+      m.p_prev2.ensure(m.P.N);
+      if (m.have_prev)
+        IMPES_CUDA(cudaMemcpyAsync(m.p_prev2.p, m.p_prev.p, sizeof(double) * m.P.N, cudaMemcpyDeviceToDevice, s));
+      m.dt_prev2 = m.dt_prev;
+      m.have_prev2 = m.have_prev;
+    }
     IMPES_CUDA(cudaMemcpyAsync(m.p_prev.p, m.p_save.p, sizeof(double) * m.P.N, cudaMemcpyDeviceToDevice, s));
     m.dt_prev = dt;
     m.have_prev = true;

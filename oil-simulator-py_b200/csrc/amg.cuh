@@ -136,8 +136,8 @@ struct AMG {
     cudaGraphExec_t exec = nullptr;
     const void* model = nullptr;
     const double *p = nullptr, *sw = nullptr, *sg = nullptr, *so = nullptr;
-    double dt = 0.0, dt_prev = 0.0;
-    bool have_prev = false;
+    double dt = 0.0, dt_prev = 0.0, dt_prev2 = 0.0;
+    bool have_prev = false, have_prev2 = false;
     impes_krylov_params kp{};
     bool fp64_stale_after = false;
     long long kernels_fixed = 0, kernels_body = 0, kernels_reorth = 0, kernels_end = 0;

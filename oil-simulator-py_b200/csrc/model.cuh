@@ -61,6 +61,9 @@ struct Model {
   DBuf<double> p_prev;                 // pressure before the last accepted step
   double dt_prev = 0.0;                // and that step's dt (extrapolated first iterate)
   bool have_prev = false;
+  DBuf<double> p_prev2;                // the one before (quadratic extrapolation)
+  double dt_prev2 = 0.0;
+  bool have_prev2 = false;
   DBuf<int> rowptr, col;               // static pattern
   int red_blocks = 0;
 };

@@ -22,7 +22,8 @@ V-cycle per iteration, ``simulation.amg.norm`` selecting
 ``"jacobi"`` (default) or ``"equilibrated"``, ``simulation.amg.precision``
 ``"fp64"`` or ``"mixed"`` (fp32 V-cycle), ``simulation.amg.max_iters`` the cap,
 ``simulation.amg.warm_start`` the first iterate: ``"extrapolate"`` (default, linear
-in time from the last two steps), ``"previous"`` or ``false`` (zero).
+in time from the last two steps), ``"quadratic"`` (from the last three),
+``"previous"`` or ``false`` (zero).
 Any other value, and a configuration without the key, runs the reference's
 Jacobi-PCG (``cg_tolerance``, ``cg_max_iter``, absolute stopping test, one
 relaxed retry), as the reference's own default does (simulation.py:905).  With a
@@ -429,10 +430,10 @@ class Simulator:
         self.amg_norm = amg_cfg.get("norm", "equilibrated" if self.pressure_solver == "amg" else "jacobi")
         self.amg_precision = amg_cfg.get("precision", "fp64")
         # FGMRES's first iterate: the pressure extrapolated in time from the last
-        # two steps ("extrapolate"), the previous one (True / "previous") or zero
-        # (False); the test stays ||r|| / ||b||
+        # two steps ("extrapolate") or three ("quadratic"), the previous one
+        # (True / "previous") or zero (False); the test stays ||r|| / ||b||
         ws = amg_cfg.get("warm_start", "extrapolate")
-        self.amg_warm_start = ws if ws in ("extrapolate", "previous") else bool(ws)
+        self.amg_warm_start = ws if ws in ("extrapolate", "quadratic", "previous") else bool(ws)
         kw = dict(device=self.device, dtype=torch.float64)
         kx, ky, kz = (t.to(**kw).contiguous() for t in reservoir.permeability_tensors)
         poro = reservoir.porosity.to(**kw).contiguous()
@@ -494,7 +495,7 @@ class Simulator:
     def krylov_params(self) -> _lib.KrylovParams:
         norm = {"jacobi": _lib.NORM_JACOBI, "equilibrated": _lib.NORM_EQUILIBRATED}[self.amg_norm]
         prec = 1 if self.amg_precision in ("mixed", "fp32") else 0
-        x0 = {False: 0, True: 1, "previous": 1, "extrapolate": 2}[self.amg_warm_start]
+        x0 = {False: 0, True: 1, "previous": 1, "extrapolate": 2, "quadratic": 3}[self.amg_warm_start]
         return _lib.KrylovParams(self.amg_tol, self.amg_restart, self.amg_max_iters, norm, prec, x0)
 
     def run_step(self, dt):

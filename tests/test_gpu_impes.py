@@ -295,3 +295,28 @@ def test_whole_step_graph_failed_solve_leaves_state(golden):
     assert torch.equal(fl.pressure, p0) and torch.equal(fl.s_w, w0)
     sim.amg_max_iters, sim.amg_tol = 400, 1e-10
     assert sim.run_step(float(g["dt"]))
+
+
+@pytest.mark.parametrize("graph", ["1", "0"])
+def test_quadratic_warm_start_matches_reference(golden, monkeypatch, graph):
+    """warm_start "quadratic": FGMRES starts from the parabola through the last
+    three accepted pressures (linear while only two exist).  Only the first
+    iterate changes, so the trajectory still equals the reference's at 1e-8,
+    on the whole-step graph and on the host-driven step."""
+    monkeypatch.setenv("IMPES_NO_STEP_GRAPH", graph)
+    g = golden("config0_64x64x1_100steps")
+    cfg, f = cfg_fields(g)
+    _, fl, _, sim = gpu_sim(cfg, f, tol=1e-13, norm="jacobi", precision="mixed", max_iters=1000, restart=60,
+                            warm_start="quadratic")
+    idx = g["sample_idx"]
+    dt = float(g["dt"])
+    for st in range(1, 21):
+        assert sim.run_step(dt), st
+        assert sim.last_krylov["converged"], (st, sim.last_krylov)
+        p, sw = to_np(fl.pressure), to_np(fl.s_w)
+        ps = g["p_s"][st - 1]
+        assert np.abs(p[idx] - ps).max() <= 1e-8 * np.abs(ps).max(), st
+        assert np.abs(sw[idx] - g["sw_s"][st - 1]).max() <= 1e-8, st
+    graphs, refused = sim.step_graphs()
+    assert not refused and (graphs >= 1) == (graph == "0"), (graphs, refused)
+    sim.close()
