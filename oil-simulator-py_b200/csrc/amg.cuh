@@ -93,6 +93,7 @@ struct Level {
 struct FgState {
   int j, total, restarts, converged, done, cycle_end, reorth, bzero, nan;
   int reorths;                          // second Gram-Schmidt passes taken
+  int gs_count;                         // blocks of a Gram-Schmidt launch done (last block reduces)
   double bnorm, beta, wn2, rel, true_rel;
 };
 

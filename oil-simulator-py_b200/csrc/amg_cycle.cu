@@ -2238,22 +2238,40 @@ __global__ void k_fg_scale_v0(long long n, double* V, const FgState* st, int aft
 // preconditioner input: V[j] ./ wt in the V-cycle's precision; a new pass
 // clears the cycle-end flag of the previous one
 template <typename T>
-__global__ void k_fg_prec_in(long long n, const double* __restrict__ V, const double* __restrict__ wt,
+__global__ void k_fg_prec_in(long long n, double* __restrict__ V, const double* __restrict__ wt,
                              T* __restrict__ out, FgState* st) {
   pdl_wait_release();
   const long long j = st->j;
-  GRID_LOOP(i, n) out[i] = (T)(V[j * n + i] / wt[i]);
+  // V[j] (j > 0) still holds the orthogonalised w of the last iteration: it is
+  // normalised here, times 1 / ||w|| (||w||^2 from k_fg_update), and written back
+  const bool sc = j > 0;
+  const double inv = sc ? 1.0 / sqrt(st->wn2) : 1.0;
+  GRID_LOOP(i, n) {
+    double v = V[j * n + i];
+    if (sc) {
+      v *= inv;
+      V[j * n + i] = v;
+    }
+    out[i] = (T)(v / wt[i]);
+  }
   if (blockIdx.x == 0 && threadIdx.x == 0) st->cycle_end = 0;
 }
 // k_fg_prec_in fused with the V-cycle's first level-0 sweep from zero
 // (Y_SMOOTH0, same arithmetic): b = V[j] ./ wt and x = w inv b
 template <typename T>
-__global__ void k_fg_prec_smooth0(long long n, const double* __restrict__ V, const double* __restrict__ wt,
+__global__ void k_fg_prec_smooth0(long long n, double* __restrict__ V, const double* __restrict__ wt,
                                   const T* __restrict__ inv, T* __restrict__ b, T* __restrict__ x, FgState* st) {
   pdl_wait_release();
   const long long j = st->j;
+  const bool sc = j > 0;   // normalise V[j] as k_fg_prec_in does
+  const double iw = sc ? 1.0 / sqrt(st->wn2) : 1.0;
   GRID_LOOP(i, n) {
-    const T bi = (T)(V[j * n + i] / wt[i]);
+    double v = V[j * n + i];
+    if (sc) {
+      v *= iw;
+      V[j * n + i] = v;
+    }
+    const T bi = (T)(v / wt[i]);
     b[i] = bi;
     x[i] = T(kOmega) * inv[i] * bi;
   }
@@ -2289,7 +2307,8 @@ __global__ void __launch_bounds__(TB) k_fg_op(int n, const int* __restrict__ row
 // Gram-Schmidt dots of pass `pass` against w = V[j+1]: pass 0 over V[0..j] and
 // w.w (k_multidot_g's self); pass 1 only when the reorth flag is set.
 __global__ void __launch_bounds__(TB, 4) k_fg_multidot(long long n, const double* __restrict__ V,
-                                                    double* __restrict__ partial, const FgState* st, int pass) {
+                                                    double* __restrict__ partial, double* __restrict__ H, int ldh,
+                                                    double* __restrict__ y, FgState* st, int pass) {
   pdl_wait_release();
   if (pass == 1 && !st->reorth) return;
   const int j = st->j, k = j + 1, self = pass == 0;
@@ -2297,6 +2316,7 @@ __global__ void __launch_bounds__(TB, 4) k_fg_multidot(long long n, const double
   if (q0 >= k + self) return;
   const double* w = V + (long long)(j + 1) * n;
   __shared__ double sm[kMD][TB / 32];
+  __shared__ int s_last;
   double acc[kMD];
 #pragma unroll
   for (int u = 0; u < kMD; ++u) acc[u] = 0.0;
@@ -2312,29 +2332,41 @@ __global__ void __launch_bounds__(TB, 4) k_fg_multidot(long long n, const double
     double t = 0.0;
     for (int u = 0; u < TB / 32; ++u) t += sm[threadIdx.x][u];
     partial[(q0 + threadIdx.x) * kDotBlocks + blockIdx.x] = t;
+    __threadfence();
   }
+  __syncthreads();
+  // the last block of the launch to finish sums every dot's partials in block
+  // order (warp w takes dots w, w + 8, ...): into column j of H in pass 0
+  // (entry j + 1 is ||w||^2 until k_fg_column), into y in pass 1
+  if (threadIdx.x == 0) {
+    const int active = kDotBlocks * ((k + self + kMD - 1) / kMD);
+    s_last = atomicAdd(&st->gs_count, 1) == active - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  double* out = pass == 0 ? H + (long long)j * ldh : y;
+  for (int q = wid; q < k + self; q += TB / 32) {
+    double t = 0.0;
+    for (int b = lane; b < kDotBlocks; b += 32) t += __ldcg(partial + (long long)q * kDotBlocks + b);
+    t = warp_sum(t);
+    if (lane == 0) out[q] = t;
+  }
+  if (threadIdx.x == 0) st->gs_count = 0;
 }
-// block q sums the partials of dot q (fixed order) into column j of H (pass 0,
-// q <= j + 1: entry j + 1 is ||w||^2 until k_fg_column) or into y (pass 1)
-__global__ void k_fg_finalize(const double* partial, double* H, int ldh, double* y, const FgState* st,
-                              int pass) {
-  pdl_wait_release();
-  if (pass == 1 && !st->reorth) return;
-  const int j = st->j, q = blockIdx.x;
-  if (q > j + (pass == 0 ? 1 : 0)) return;
-  double t = 0.0;
-  for (int b = threadIdx.x; b < kDotBlocks; b += 32) t += partial[q * kDotBlocks + b];
-  t = warp_sum(t);
-  if (threadIdx.x == 0) (pass == 0 ? H + (long long)j * ldh : y)[q] = t;
-}
-// w -= sum_q h_q V[q] (h = column j of H, or y in pass 1), with norm partials
+// w -= sum_q h_q V[q] (h = column j of H, or y in pass 1); the last block to
+// finish sums the blocks' partial squares (||w||^2, FgState::wn2) and, after
+// pass 0, sets the reorthogonalisation flag, which also opens the conditional
+// node of pass 1
 __global__ void __launch_bounds__(TB) k_fg_update(long long n, double* __restrict__ V, const double* __restrict__ H,
                                                   int ldh, const double* __restrict__ y,
-                                                  double* __restrict__ partial, const FgState* st, int pass) {
+                                                  double* __restrict__ partial, FgState* st, int pass,
+                                                  cudaGraphConditionalHandle reorth_if) {
   pdl_wait_release();
   if (pass == 1 && !st->reorth) return;
   __shared__ double sh[128];
   __shared__ double sm[TB / 32];
+  __shared__ int s_last;
   const int j = st->j, k = j + 1;
   const double* h = pass == 0 ? H + (long long)j * ldh : y;
   for (int q = threadIdx.x; q < k; q += blockDim.x) sh[q] = h[q];
@@ -2348,32 +2380,24 @@ __global__ void __launch_bounds__(TB) k_fg_update(long long n, double* __restric
     double u = 0.0;
     for (int q = 0; q < TB / 32; ++q) u += sm[q];
     partial[blockIdx.x] = u;
+    __threadfence();
+    s_last = atomicAdd(&st->gs_count, 1) == (int)gridDim.x - 1;
   }
-}
-// ||w||^2 from the update's partials; after pass 0 the reorthogonalisation
-// flag, which also opens the conditional node of pass 1
-__global__ void k_fg_norm(const double* partial, FgState* st, const double* H, int ldh, int pass,
-                          cudaGraphConditionalHandle reorth_if) {
-  pdl_wait_release();
-  if (pass == 1 && !st->reorth) return;
-  double t = 0.0;
-  for (int b = threadIdx.x; b < kDotBlocks; b += 32) t += partial[b];
-  t = warp_sum(t);
+  __syncthreads();
+  if (!s_last || threadIdx.x >= 32) return;
+  __threadfence();
+  double nt = 0.0;
+  for (int b = threadIdx.x; b < kDotBlocks; b += 32) nt += __ldcg(partial + b);
+  nt = warp_sum(nt);
   if (threadIdx.x == 0) {
-    st->wn2 = t;
+    st->gs_count = 0;
+    st->wn2 = nt;
     if (pass == 0) {
-      st->reorth = t < 0.49 * H[(long long)st->j * ldh + st->j + 1];
+      st->reorth = nt < 0.49 * H[(long long)st->j * ldh + st->j + 1];
       st->reorths += st->reorth;
       cudaGraphSetConditional(reorth_if, st->reorth ? 1u : 0u);
     }
   }
-}
-// H[:, j] += y after a second pass; H[j+1, j] = ||w||
-__global__ void k_fg_scale_w(long long n, double* V, const FgState* st) {
-  pdl_wait_release();
-  const double inv = 1.0 / sqrt(st->wn2);
-  double* w = V + (long long)(st->j + 1) * n;
-  GRID_LOOP(i, n) w[i] *= inv;
 }
 // Column j of the Hessenberg matrix in one block: the reorthogonalisation
 // terms and h[j+1][j], then on thread 0 the Givens rotation (k_givens), the
@@ -2693,10 +2717,10 @@ void amg_fgmres_capture(AMG& h, const double* b, double* x, const impes_krylov_p
     const bool fuse0 = h.prm.smoother != IMPES_SMOOTHER_CHEBYSHEV && !L0.coarsest;
     if (kp.precision == 1) {
       if (fuse0)
-        launch_pdl(k_fg_prec_smooth0<float>, gb, TB, 0, bsm, n, (const double*)h.V.p, (const double*)wt,
+        launch_pdl(k_fg_prec_smooth0<float>, gb, TB, 0, bsm, n, h.V.p, (const double*)wt,
                    (const float*)L0.inv_relaxf.p, L0.bf.p, L0.xf.p, st);
       else
-        launch_pdl(k_fg_prec_in<float>, gb, TB, 0, bsm, n, (const double*)h.V.p, (const double*)wt, L0.bf.p, st);
+        launch_pdl(k_fg_prec_in<float>, gb, TB, 0, bsm, n, h.V.p, (const double*)wt, L0.bf.p, st);
       const float* zf = vcycle<float>(h, 0, true, bsm, fuse0);
       if (L0.col16.p)
         fg_op(L0, (const unsigned short*)L0.col16.p, zf, h.Z.p, wt, h.V.p, L0.col16_rel, st, bsm);
@@ -2704,35 +2728,32 @@ void amg_fgmres_capture(AMG& h, const double* b, double* x, const impes_krylov_p
         fg_op(L0, (const int*)L0.col.p, zf, h.Z.p, wt, h.V.p, 0, st, bsm);
     } else {
       if (fuse0)
-        launch_pdl(k_fg_prec_smooth0<double>, gb, TB, 0, bsm, n, (const double*)h.V.p, (const double*)wt,
+        launch_pdl(k_fg_prec_smooth0<double>, gb, TB, 0, bsm, n, h.V.p, (const double*)wt,
                    (const double*)L0.inv_relax.p, L0.b.p, L0.x.p, st);
       else
-        launch_pdl(k_fg_prec_in<double>, gb, TB, 0, bsm, n, (const double*)h.V.p, (const double*)wt, L0.b.p, st);
+        launch_pdl(k_fg_prec_in<double>, gb, TB, 0, bsm, n, h.V.p, (const double*)wt, L0.b.p, st);
       const double* zd = vcycle<double>(h, 0, true, bsm, fuse0);
       if (L0.col16.p)
         fg_op(L0, (const unsigned short*)L0.col16.p, zd, h.Z.p, wt, h.V.p, L0.col16_rel, st, bsm);
       else
         fg_op(L0, (const int*)L0.col.p, zd, h.Z.p, wt, h.V.p, 0, st, bsm);
     }
-    // Gram-Schmidt: pass 0, then pass 1 inside an IF node that k_fg_norm opens
+    // Gram-Schmidt: pass 0, then pass 1 inside an IF node that k_fg_update opens
     // when the first pass lost too much of the vector's norm
     const dim3 gd(kDotBlocks, (unsigned)((m + 2 + kMD - 1) / kMD));
     cudaGraphConditionalHandle reorth_if, end_if;
     IMPES_CUDA(cudaGraphConditionalHandleCreate(&reorth_if, body, 0, cudaGraphCondAssignDefault));
     IMPES_CUDA(cudaGraphConditionalHandleCreate(&end_if, body, 0, cudaGraphCondAssignDefault));
     auto gs_pass = [&](int pass, cudaStream_t q) {
-      launch_pdl(k_fg_multidot, gd, dim3(TB), 0, q, n, (const double*)h.V.p, h.red.p, (const FgState*)st, pass);
-      launch_pdl(k_fg_finalize, m + 2, 32, 0, q, (const double*)h.red.p, h.H.p, ldh, h.y.p, (const FgState*)st,
-                 pass);
+      launch_pdl(k_fg_multidot, gd, dim3(TB), 0, q, n, (const double*)h.V.p, h.red.p, h.H.p, ldh, h.y.p, st, pass);
       launch_pdl(k_fg_update, kDotBlocks, TB, 0, q, n, h.V.p, (const double*)h.H.p, ldh, (const double*)h.y.p,
-                 h.red.p, (const FgState*)st, pass);
-      launch_pdl(k_fg_norm, 1, 32, 0, q, (const double*)h.red.p, st, (const double*)h.H.p, ldh, pass, reorth_if);
+                 h.red.p, st, pass, reorth_if);
     };
     gs_pass(0, bsm);
     unsigned long long mark = thread_launches();
     capture_if(bsm, h, reorth_if, [&](cudaStream_t q) { gs_pass(1, q); });
     h.fg_reorth_kernels = (long long)(thread_launches() - mark);
-    launch_pdl(k_fg_scale_w, gb, TB, 0, bsm, n, h.V.p, (const FgState*)st);
+    // (V[j+1] is normalised by the next iteration's input kernel)
     launch_pdl(k_fg_column, 1, 128, 0, bsm, h.H.p, ldh, h.cs.p, h.sn.p, h.g.p, h.y.p, st, kp.tol, kp.max_iters, m,
                cond, end_if);
     // a cycle's end (IF node opened by k_fg_column): x_s += Z y, the true
