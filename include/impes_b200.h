@@ -90,6 +90,8 @@ typedef struct {
   int layout[2];         /* storage the sweeps and residuals on A read: 0 CSR, 1 the
                             level's SELL-32 (sliced ELLPACK) copy, 2 its DIA (one array
                             per diagonal) copy; [0] fp64, [1] fp32                    */
+  int fused_tail;        /* 1: the level's fp32 V-cycle runs inside the one-CTA
+                            shared-memory tail launch, 2: inside the cluster tail     */
 } impes_amg_level_desc;
 
 /* Norms for Krylov stopping tests. */

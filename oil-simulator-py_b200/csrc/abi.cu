@@ -354,6 +354,9 @@ int impes_amg_level_info(impes_amg* h, int lvl, impes_amg_level_desc* info) {
       info->lanes[3 * q + 2] = L.lpr_p[q];
       info->layout[q] = L.dia_on[q] ? 2 : (L.sell_on[q] ? 1 : 0);
     }
+    const AMG& A = h->a;
+    info->fused_tail = (A.stail_level >= 1 && lvl >= A.stail_level) ? 1
+                       : (A.tail_level >= 1 && lvl >= A.tail_level) ? 2 : 0;
   });
 }
 

@@ -150,6 +150,8 @@ struct AMG {
   bool use_tail = false;                // fused V-cycle tail (IMPES_TAIL=1: on)
   int tail_level = -1;                  // first level of the fused tail, -1: none
   int tail_cluster = 0;                 // CTAs in the tail's cluster (16 or 8)
+  int stail_level = -1;                 // first level of the shared-memory fp32 tail, -1: none
+  size_t stail_smem = 0;                // its shared-memory bytes
   void drop_graphs() {
     for (auto& a : vgraph) for (auto& b : a) for (auto& c : b) for (auto& g : c) {
       if (g.exec) cudaGraphExecDestroy(g.exec);

@@ -1456,6 +1456,262 @@ void launch_tail(AMG& h, int l, cudaStream_t s) {
   count_launch();
 }
 
+// ------------------------------------------------ shared-memory V-cycle tail
+// The fp32 V-cycle of the smallest levels (those that fit together in one
+// CTA's shared memory with the dense coarsest inverse read from L2) in ONE
+// launch of one 1024-thread CTA: each level's matrix, transfer operators and
+// work vectors are staged into shared memory, then the same phase sequence as
+// vcycle() runs with block barriers in between -- first sweep from zero, two
+// sweeps, residual, restriction, the next level, prolongation, two sweeps; the
+// dense coarsest apply.  A phase then costs a shared-memory pass instead of a
+// dependent chain of L2 round trips and a kernel boundary.  Four lanes per row.
+constexpr int kSTailThreads = 1024;
+constexpr int kSTailMaxLevels = 8;
+constexpr size_t kSTailSmem = 200u << 10;
+
+struct STailLevel {
+  int n, nc, nnz, pnnz, coarsest, rel;
+  const int* rowptr;
+  const unsigned short* col16;      // or null: col
+  const int* col;
+  const float* val;
+  const float* inv;
+  const int *prow, *pcol, *rrow, *rcol;
+  const float *pval, *rval;
+  // byte offsets of the staged copies in shared memory
+  int o_rowptr, o_col, o_val, o_inv, o_prow, o_pcol, o_pval, o_rrow, o_rcol, o_rval, o_x, o_t, o_b, o_r;
+  const double *lu, *lu_free;       // coarsest: pinned / unpinned inverses (global)
+};
+struct STailArgs {
+  STailLevel lv[kSTailMaxLevels];
+  int nlev;
+  int col_bytes;                    // 2 or 4 (all levels alike)
+  const float* b_in;                // the first level's right-hand side (global)
+  float* x_out;                     // and its result
+  const int* free_singular;
+  int krylov;
+};
+
+// count elements of src into shared memory at byte offset off: the 16-byte
+// pieces with cp.async (no register round trip; the caller waits for all of a
+// stage's copies at once), the last partial piece element by element.  The
+// sources are cudaMalloc'd arrays and the offsets 16-byte aligned.
+template <typename E>
+__device__ __forceinline__ void stail_copy(unsigned char* smem, int off, const E* src, int count) {
+  const int bytes = count * (int)sizeof(E);
+  const int n16 = bytes >> 4;
+  const unsigned char* s8 = reinterpret_cast<const unsigned char*>(src);
+  for (int i = threadIdx.x; i < n16; i += blockDim.x) cp_async16(smem + off + 16 * i, s8 + 16 * i, 16);
+  E* dst = reinterpret_cast<E*>(smem + off);
+  for (int e = (n16 << 4) / (int)sizeof(E) + threadIdx.x; e < count; e += blockDim.x) dst[e] = src[e];
+}
+__device__ __forceinline__ void stail_copy_wait() {
+  cp_async_commit();
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+// y = f(A x) over rows of a CSR block in shared memory, kTailLanes lanes per row
+template <int MODE>
+__device__ void stail_csr(int n, const int* rowptr, const unsigned short* col16, const int* col, int rel,
+                          const float* val, const float* x, const float* b, const float* inv, float* y) {
+  const int lane = threadIdx.x % kTailLanes;
+  constexpr int kRowsPerPass = kSTailThreads / kTailLanes;
+  for (int base = 0; base < n; base += kRowsPerPass) {
+    const int row = base + (int)threadIdx.x / kTailLanes;
+    const bool valid = row < n;
+    float acc = 0.f;
+    if (MODE != Y_SMOOTH0 && valid) {
+      const int a = rowptr[row], e = rowptr[row + 1];
+      if (col16) {
+        const int cb = rel ? row - 32768 : 0;
+        for (int k = a + lane; k < e; k += kTailLanes) acc += val[k] * x[cb + (int)col16[k]];
+      } else {
+        for (int k = a + lane; k < e; k += kTailLanes) acc += val[k] * x[col[k]];
+      }
+    }
+#pragma unroll
+    for (int o = kTailLanes / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, kTailLanes);
+    if (lane == 0 && valid) {
+      if (MODE == Y_AX) y[row] = acc;
+      else if (MODE == Y_B_MINUS_AX) y[row] = b[row] - acc;
+      else if (MODE == Y_SMOOTH) y[row] = x[row] + kOmega * inv[row] * (b[row] - acc);
+      else if (MODE == Y_ADD_AX) y[row] = y[row] + acc;
+      else if (MODE == Y_SMOOTH0) y[row] = kOmega * inv[row] * b[row];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kSTailThreads) k_vcycle_stail(const __grid_constant__ STailArgs A) {
+  pdl_wait_release();
+  extern __shared__ __align__(16) unsigned char smem[];
+  // stage every level (the coarsest only its vectors)
+  for (int l = 0; l < A.nlev; ++l) {
+    const STailLevel& L = A.lv[l];
+    if (!L.coarsest) {
+      stail_copy(smem, L.o_rowptr, L.rowptr, L.n + 1);
+      if (A.col_bytes == 2) stail_copy(smem, L.o_col, L.col16, L.nnz);
+      else stail_copy(smem, L.o_col, L.col, L.nnz);
+      stail_copy(smem, L.o_val, L.val, L.nnz);
+      stail_copy(smem, L.o_inv, L.inv, L.n);
+      stail_copy(smem, L.o_prow, L.prow, L.n + 1);
+      stail_copy(smem, L.o_pcol, L.pcol, L.pnnz);
+      stail_copy(smem, L.o_pval, L.pval, L.pnnz);
+      stail_copy(smem, L.o_rrow, L.rrow, L.nc + 1);
+      stail_copy(smem, L.o_rcol, L.rcol, L.pnnz);
+      stail_copy(smem, L.o_rval, L.rval, L.pnnz);
+    }
+  }
+  stail_copy(smem, A.lv[0].o_b, A.b_in, A.lv[0].n);
+  stail_copy_wait();
+  __syncthreads();
+  auto F = [&](int off) { return reinterpret_cast<float*>(smem + off); };
+  auto I = [&](int off) { return reinterpret_cast<const int*>(smem + off); };
+  auto colp16 = [&](const STailLevel& L) {
+    return A.col_bytes == 2 ? reinterpret_cast<const unsigned short*>(smem + L.o_col) : nullptr;
+  };
+  auto colp32 = [&](const STailLevel& L) {
+    return A.col_bytes == 4 ? reinterpret_cast<const int*>(smem + L.o_col) : nullptr;
+  };
+  int l = 0;
+  for (; l < A.nlev && !A.lv[l].coarsest; ++l) {
+    const STailLevel& L = A.lv[l];
+    const int* rp = I(L.o_rowptr);
+    stail_csr<Y_SMOOTH0>(L.n, rp, colp16(L), colp32(L), L.rel, F(L.o_val), nullptr, F(L.o_b), F(L.o_inv), F(L.o_x));
+    __syncthreads();
+    stail_csr<Y_SMOOTH>(L.n, rp, colp16(L), colp32(L), L.rel, F(L.o_val), F(L.o_x), F(L.o_b), F(L.o_inv), F(L.o_t));
+    __syncthreads();
+    stail_csr<Y_SMOOTH>(L.n, rp, colp16(L), colp32(L), L.rel, F(L.o_val), F(L.o_t), F(L.o_b), F(L.o_inv), F(L.o_x));
+    __syncthreads();
+    stail_csr<Y_B_MINUS_AX>(L.n, rp, colp16(L), colp32(L), L.rel, F(L.o_val), F(L.o_x), F(L.o_b), nullptr,
+                            F(L.o_r));
+    __syncthreads();
+    const STailLevel& N = A.lv[l + 1];
+    stail_csr<Y_AX>(L.nc, I(L.o_rrow), nullptr, I(L.o_rcol), 0, F(L.o_rval), F(L.o_r), nullptr, nullptr, F(N.o_b));
+    __syncthreads();
+  }
+  {  // coarsest: x = Ainv b, pinned (b[0] = 0) unless Krylov mode uses the unpinned inverse
+    const STailLevel& C = A.lv[l];
+    const bool use_free = A.krylov && C.lu_free != nullptr && *A.free_singular == 0;
+    const double* Ainv = use_free ? C.lu_free : C.lu;
+    const int pin = use_free ? 0 : 1;
+    const float* cb = F(C.o_b);
+    float* cx = F(C.o_x);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int i = warp; i < C.n; i += nw) {
+      double acc = 0.0;
+      for (int j = lane; j < C.n; j += 32) acc += Ainv[(long long)i * C.n + j] * ((pin && j == 0) ? 0.0 : (double)cb[j]);
+      acc = warp_sum(acc);
+      if (lane == 0) cx[i] = (float)acc;
+    }
+    __syncthreads();
+  }
+  for (--l; l >= 0; --l) {
+    const STailLevel& L = A.lv[l];
+    const STailLevel& N = A.lv[l + 1];
+    const int* rp = I(L.o_rowptr);
+    stail_csr<Y_ADD_AX>(L.n, I(L.o_prow), nullptr, I(L.o_pcol), 0, F(L.o_pval), F(N.o_x), nullptr, nullptr,
+                        F(L.o_x));
+    __syncthreads();
+    stail_csr<Y_SMOOTH>(L.n, rp, colp16(L), colp32(L), L.rel, F(L.o_val), F(L.o_x), F(L.o_b), F(L.o_inv), F(L.o_t));
+    __syncthreads();
+    stail_csr<Y_SMOOTH>(L.n, rp, colp16(L), colp32(L), L.rel, F(L.o_val), F(L.o_t), F(L.o_b), F(L.o_inv), F(L.o_x));
+    __syncthreads();
+  }
+  const float* x0 = F(A.lv[0].o_x);
+  for (int i = threadIdx.x; i < A.lv[0].n; i += blockDim.x) A.x_out[i] = x0[i];
+}
+
+// Shared-memory layout of levels l.. (16-byte aligned arrays); returns the
+// bytes, or 0 when the levels do not qualify (rows of more than 96 entries, a
+// coarsest level without its dense inverses, too many levels, mixed column
+// widths).
+size_t stail_layout(const AMG& h, int l, STailArgs* A) {
+  if ((int)h.levels.size() - l > kSTailMaxLevels) return 0;
+  size_t off = 0;
+  auto take = [&](size_t bytes) { const size_t o = off; off += (bytes + 15) & ~(size_t)15; return (int)o; };
+  int col_bytes = 0;
+  for (size_t q = l; q < h.levels.size(); ++q) {
+    const Level& L = *h.levels[q];
+    STailLevel d{};
+    d.n = L.n; d.nc = L.nc; d.nnz = L.nnz; d.pnnz = L.pnnz; d.coarsest = L.coarsest ? 1 : 0;
+    if (L.coarsest) {
+      if (L.n > 500 || !L.lu.p) return 0;
+      d.lu = L.lu.p; d.lu_free = L.lu_free.p;
+      d.o_x = take(4 * (size_t)L.n);
+      d.o_b = take(4 * (size_t)L.n);
+      if (A) A->lv[q - l] = d;
+      break;
+    }
+    if (L.avg_row > 96 || !L.valf.p || !L.inv_relaxf.p || !L.pvalf.p || !L.rvalf.p) return 0;
+    const int cb = L.col16.p ? 2 : 4;
+    if (col_bytes && cb != col_bytes) return 0;
+    col_bytes = cb;
+    d.rel = L.col16.p ? L.col16_rel : 0;
+    d.rowptr = L.rowptr.p; d.col16 = L.col16.p; d.col = L.col.p; d.val = L.valf.p; d.inv = L.inv_relaxf.p;
+    d.prow = L.prow.p; d.pcol = L.pcol.p; d.pval = L.pvalf.p;
+    d.rrow = L.rrow.p; d.rcol = L.rcol.p; d.rval = L.rvalf.p;
+    d.o_rowptr = take(4 * ((size_t)L.n + 1));
+    d.o_col = take((size_t)cb * L.nnz);
+    d.o_val = take(4 * (size_t)L.nnz);
+    d.o_inv = take(4 * (size_t)L.n);
+    d.o_prow = take(4 * ((size_t)L.n + 1));
+    d.o_pcol = take(4 * (size_t)L.pnnz);
+    d.o_pval = take(4 * (size_t)L.pnnz);
+    d.o_rrow = take(4 * ((size_t)L.nc + 1));
+    d.o_rcol = take(4 * (size_t)L.pnnz);
+    d.o_rval = take(4 * (size_t)L.pnnz);
+    d.o_x = take(4 * (size_t)L.n);
+    d.o_t = take(4 * (size_t)L.n);
+    d.o_b = take(4 * (size_t)L.n);
+    d.o_r = take(4 * (size_t)L.n);
+    if (A) A->lv[q - l] = d;
+  }
+  if (A) {
+    A->nlev = (int)h.levels.size() - l;
+    A->col_bytes = col_bytes ? col_bytes : 2;
+  }
+  return off;
+}
+
+// First level of the shared-memory tail: the coarsest-most levels whose
+// staged copies fit in kSTailSmem, at least one level above the coarsest; -1
+// when none, or a Chebyshev hierarchy, or no fp32 chain.  Opt-in
+// (IMPES_STAIL=1, read at setup): on the 1e6-cell hierarchy (levels of 758,
+// 208 and 55 rows in the tail) the step is 1.8 % slower than with the
+// per-level kernels -- sixteen dependent phases on one SM cost more than
+// sixteen programmatic-dependent launches on all of them.
+int amg_stail_level(AMG& h) {
+  const char* ev = getenv("IMPES_STAIL");
+  if (!(ev && ev[0] == '1')) return -1;
+  if (!h.prm.mixed_precision || h.prm.smoother != IMPES_SMOOTHER_L1_JACOBI || h.levels.size() < 2) return -1;
+  int best = -1;
+  for (int l = (int)h.levels.size() - 2; l >= 1; --l) {
+    const size_t bytes = stail_layout(h, l, nullptr);
+    if (bytes == 0 || bytes > kSTailSmem) break;
+    best = l;
+  }
+  if (best >= 0) {
+    h.stail_smem = stail_layout(h, best, nullptr);
+    if (cudaFuncSetAttribute((const void*)k_vcycle_stail, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)h.stail_smem) != cudaSuccess) {
+      cudaGetLastError();
+      return -1;
+    }
+  }
+  return best;
+}
+
+void launch_stail(AMG& h, int l, cudaStream_t s) {
+  STailArgs A{};
+  stail_layout(h, l, &A);
+  A.b_in = LV<float>::b(*h.levels[l]);
+  A.x_out = LV<float>::x(*h.levels[l]);
+  A.free_singular = h.iflag.p + 3;
+  A.krylov = h.krylov_mode ? 1 : 0;
+  launch_pdl(k_vcycle_stail, 1, kSTailThreads, h.stail_smem, s, A);
+  IMPES_CHECK_LAUNCH();
+}
+
 // _v_cycle (classical_amg.py:1037-1106) on level l: input b in LV<T>::b(L),
 // initial x in LV<T>::x(L) (ignored when zero_x); returns the buffer with x.
 template <typename T>
@@ -1464,6 +1720,12 @@ T* vcycle(AMG& h, int l, bool zero_x, cudaStream_t s, bool first_sweep_done = fa
   if (l > 0 && zero_x && l == h.tail_level && !L.coarsest) {
     launch_tail<T>(h, l, s);
     return LV<T>::x(L);
+  }
+  if constexpr (sizeof(T) == 4) {
+    if (l > 0 && zero_x && l == h.stail_level && !L.coarsest) {
+      launch_stail(h, l, s);
+      return LV<T>::x(L);
+    }
   }
   if (L.coarsest) {
     if (L.n <= 500) {
@@ -1489,6 +1751,7 @@ T* vcycle(AMG& h, int l, bool zero_x, cudaStream_t s, bool first_sweep_done = fa
   // the restriction also takes the coarse level's first sweep from zero when
   // that level smooths with l1-Jacobi through the per-level kernels
   const bool fuse_s0 = !Nc.coarsest && L.r_avg <= 96 && !(l + 1 == h.tail_level) &&
+                       !(sizeof(T) == 4 && l + 1 == h.stail_level) &&
                        !(h.prm.smoother == IMPES_SMOOTHER_CHEBYSHEV && Nc.cheb_lmax.p);
   if (fuse_s0) {
     const int lpr_r = L.lpr_r[LV<T>::slot] > 0 ? L.lpr_r[LV<T>::slot] : default_lpr(L.r_avg);
@@ -1866,6 +2129,8 @@ int tail_cluster_size() {
 }
 
 int amg_tail_level(AMG& h) {
+  // the shared-memory fp32 tail, unless the cluster tail is asked for
+  h.stail_level = h.use_tail ? -1 : amg_stail_level(h);
   for (size_t l = 1; l < h.levels.size(); ++l) {
     if (!tail_eligible(h, (int)l)) continue;
     if (h.levels[l]->coarsest) return -1;

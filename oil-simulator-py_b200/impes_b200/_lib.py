@@ -42,7 +42,7 @@ class AmgParams(C.Structure):
 class LevelDesc(C.Structure):
     _fields_ = [("n", C.c_int), ("nnz", C.c_int), ("p_cols", C.c_int), ("p_nnz", C.c_int),
                 ("is_coarsest", C.c_int), ("col_index_bytes", C.c_int), ("col_row_relative", C.c_int),
-                ("lanes", C.c_int * 6), ("layout", C.c_int * 2)]
+                ("lanes", C.c_int * 6), ("layout", C.c_int * 2), ("fused_tail", C.c_int)]
 
 
 class KrylovParams(C.Structure):
