@@ -272,10 +272,17 @@ def test_whole_step_graph_matches_host_driven_steps(golden, monkeypatch, precisi
         graphs, refused = sim.step_graphs()
         assert not refused and (graphs >= 1) == (flag == "0"), (flag, graphs, refused)
         sim.close()
+    # At tol 1e-13 the solve ends a few digits above its rounding floor: the two
+    # paths sum their dots in different orders, and the fp32 V-cycle turns that
+    # into a slightly different Krylov tail (a step or two), never a systematic
+    # excess.
+    step_slack = 1 if precision == "fp64" else 3
     for (p1, w1, s1, i1), (p0, w0, s0, i0) in zip(out["1"], out["0"]):
         assert np.abs(p1 - p0).max() <= 1e-11 * np.abs(p1).max()
         assert np.abs(w1 - w0).max() <= 1e-11 and np.abs(s1 - s0).max() <= 1e-11
-        assert abs(i1 - i0) <= 1
+        assert abs(i1 - i0) <= step_slack, (i1, i0)
+    tot1, tot0 = sum(t[3] for t in out["1"]), sum(t[3] for t in out["0"])
+    assert abs(tot1 - tot0) <= 0.05 * tot1 + 2, (tot1, tot0)
 
 
 def test_whole_step_graph_failed_solve_leaves_state(golden):
