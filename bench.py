@@ -218,17 +218,19 @@ class ClockSampler:
 
 
 def make_sim(cfg, fields, precision, device, restart=30, solver="gmres_amg", warm_start="extrapolate",
-             trunc=0, smoother="l1jacobi", tol=PRESSURE_TOL):
+             trunc=0, smoother="l1jacobi", tol=PRESSURE_TOL, light=0):
     """FGMRES + V-cycle (solver="gmres_amg"), or the plain stand-alone V-cycles of
     the reference (solver="amg"), both stopping at PRESSURE_TOL in the Jacobi norm;
-    `trunc` caps the interpolation's row length (0: the reference's interpolation)."""
+    `trunc` caps the interpolation's row length (0: the reference's interpolation);
+    levels of at most `light` rows smooth once before and once after their coarse
+    correction (0: three and two sweeps on every level, as the reference)."""
     from impes_b200.simulator import build_from_config
     c = json.loads(json.dumps(cfg))
     c["simulation"]["pressure_solver"] = solver
     c["simulation"]["amg"].update({"tol": tol, "norm": "jacobi", "precision": precision,
                                    "restart": restart, "max_iters": 600, "max_cycles": 3000, "seed": 0,
                                    "warm_start": warm_start, "p_max_elements": int(trunc),
-                                   "smoother": smoother})
+                                   "smoother": smoother, "light_sweep_rows": int(light)})
     return build_from_config(c, fields, device=device)
 
 
@@ -450,7 +452,7 @@ def run_variant(args, cfg, fields, precision, device, dt, flush, stream, dist, r
     from impes_b200 import _lib
     _, fl, _, sim = make_sim(cfg, fields, precision, device, restart=args.restart,
                              warm_start=False if args.warm_start == "zero" else args.warm_start,
-                             trunc=trunc, smoother=args.smoother)
+                             trunc=trunc, smoother=args.smoother, light=args.light_sweep_rows if trunc else 0)
     pv = sim.porous_volume.reshape(fl.s_w.shape)
     m0 = total_mass(fl, pv)
     torch.cuda.synchronize()
@@ -535,6 +537,8 @@ def run_ours(args, world, rank, local):
     cells = cfg["reservoir"]["dimensions"][0] * cfg["reservoir"]["dimensions"][1] * cfg["reservoir"]["dimensions"][2]
     stream = torch.cuda.current_stream(device)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=device)
+    if args.light_sweep_rows < 0:
+        args.light_sweep_rows = int(0.3 * cells)
 
     # (precision, interpolation cap) variants; the headline is the mixed path on
     # the --p-max-elements hierarchy, and the reference's own interpolation (cap 0)
@@ -557,7 +561,8 @@ def run_ours(args, world, rank, local):
         # the same number of steps in fp64 solved to 1e-10: how far the 1e-6
         # solve tolerance alone moves the state (against the mixed-vs-fp64 drift)
         r64 = results[("fp64", trunc)]
-        _, flt, _, simt = make_sim(cfg, fields, "fp64", device, restart=args.restart, trunc=trunc, tol=1e-10)
+        _, flt, _, simt = make_sim(cfg, fields, "fp64", device, restart=args.restart, trunc=trunc, tol=1e-10,
+                                   light=args.light_sweep_rows)
         pvt_ = simt.porous_volume.reshape(flt.s_w.shape)
         m0t = total_mass(flt, pvt_)
         for _ in range(r64["steps_run"]):
@@ -569,7 +574,8 @@ def run_ours(args, world, rank, local):
                  "mass_err": abs((total_mass(flt, pvt_) - m0t) - net_inflow(simt)) / max(abs(m0t), 1e-300)}
         # and the mixed path solved to 1e-10 over the same steps: the precision's
         # own share of the drift once the tolerance no longer dominates it
-        _, flm, _, simm = make_sim(cfg, fields, "mixed", device, restart=args.restart, trunc=trunc, tol=1e-10)
+        _, flm, _, simm = make_sim(cfg, fields, "mixed", device, restart=args.restart, trunc=trunc, tol=1e-10,
+                                   light=args.light_sweep_rows)
         for _ in range(r64["steps_run"]):
             if not simm.run_step(dt):
                 raise RuntimeError("tight mixed step failed to converge")
@@ -616,6 +622,7 @@ def run_ours(args, world, rank, local):
     if args.precision != "both":
         r = results[(args.precision, trunc)]
         print(json.dumps({"precision": args.precision, "p_max_elements": trunc, "smoother": args.smoother,
+                          "light_sweep_rows": args.light_sweep_rows,
                           "ms_per_step": r["ms"] / steps, "vcycles_per_step": statistics.mean(r["iters"]),
                           "operator_complexity": r["oc"], "levels": r["levels"],
                           "phases": r["phases"], "gpu_launches": r["launches"]}), flush=True)
@@ -648,7 +655,8 @@ def run_ours(args, world, rank, local):
         "dtype": "f64 Krylov/assembly/saturation + f32 V-cycle",
         "data": "synthetic (seeded; no dataset)",
         "config": {"workload": WORKLOAD_SHORT, "cells": cells, "precision": "mixed",
-                   "solver": f"FGMRES({args.restart}) + RS-AMG V-cycle, P capped at {trunc}/row"
+                   "solver": (f"FGMRES({args.restart}) + RS-AMG V-cycle, P capped at {trunc}/row, "
+                              f"one sweep before/after on levels of <= {args.light_sweep_rows} rows")
                              if trunc else f"FGMRES({args.restart}) + RS-AMG V-cycle",
                    "tol": PRESSURE_TOL, "norm": "Jacobi-scaled", "l2": "flushed before each step",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
@@ -759,6 +767,11 @@ def main():
     ap.add_argument("--p-max-elements", type=int, default=DEFAULT_P_MAX,
                     help="interpolation row cap of the benchmarked hierarchy (0: the reference's "
                          "interpolation)")
+    ap.add_argument("--light-sweep-rows", type=int, default=-1,
+                    help="levels of at most this many rows smooth once before and once after their "
+                         "coarse correction (capped hierarchy only; 0: three and two sweeps everywhere; "
+                         "default: 30%% of the cell count, every level below the first coarse one "
+                         "on the 1e6-cell hierarchy)")
     ap.add_argument("--smoother", choices=["l1jacobi", "chebyshev"], default="l1jacobi",
                     help="V-cycle smoother of the benchmarked hierarchy")
     ap.add_argument("--no-reference-hierarchy", action="store_true",

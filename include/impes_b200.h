@@ -73,6 +73,13 @@ typedef struct {
    * lmax its Gershgorin bound, one step per sweep the V-cycle would make. */
   int smoother;
   double cheb_lower;              /* 0.3 when <= 0                               */
+  /* Levels of at most light_sweep_rows rows smooth once before and once after
+   * their coarse-grid correction instead of the reference's three and two
+   * (0: every level as the reference).  On small levels each sweep costs a
+   * kernel launch's latency rather than its bytes, so this trades a little
+   * smoothing for fewer launches; it changes the preconditioner, not the answer
+   * a Krylov solve stops on.  The fused V-cycle tails are off when it is set. */
+  int light_sweep_rows;
 } impes_amg_params;
 
 enum { IMPES_SMOOTHER_L1_JACOBI = 0, IMPES_SMOOTHER_CHEBYSHEV = 1 };

@@ -261,6 +261,7 @@ int impes_amg_create(impes_amg** out, const impes_amg_params* p) {
     IMPES_REQUIRE(p->smoother == IMPES_SMOOTHER_L1_JACOBI || p->smoother == IMPES_SMOOTHER_CHEBYSHEV,
                   IMPES_ERR_ARG, "unknown smoother");
     IMPES_REQUIRE(p->cheb_lower < 1.0, IMPES_ERR_ARG, "cheb_lower must be below 1");
+    IMPES_REQUIRE(p->light_sweep_rows >= 0, IMPES_ERR_ARG, "light_sweep_rows must be >= 0");
     auto* h = new impes_amg();
     h->a.prm = *p;
     if (!(h->a.prm.cheb_lower > 0.0)) h->a.prm.cheb_lower = 0.3;

@@ -1256,9 +1256,11 @@ double vcycle_bytes(const AMG& h, int l) {
       tot += L.n <= 500 ? 8.0 * L.n * (double)L.n + 2.0 * sz * L.n : 50.0 * sweep_bytes(sz, L.nnz, L.n);
       break;
     }
-    // first sweep from zero (b, inv, y), four full sweeps, the residual
+    // first sweep from zero (b, inv, y), four full sweeps (one on a light
+    // level), the residual
     const double si = L.col16.p ? 2.0 : 4.0;
-    tot += 3.0 * sz * L.n + 4.0 * sweep_bytes(sz, L.nnz, L.n, si) + spmv_bytes(sz, sz, L.nnz, L.n, L.n, si) +
+    const double full = L.n <= h.prm.light_sweep_rows ? 1.0 : 4.0;
+    tot += 3.0 * sz * L.n + full * sweep_bytes(sz, L.nnz, L.n, si) + spmv_bytes(sz, sz, L.nnz, L.n, L.n, si) +
            spmv_bytes(sz, sz, L.pnnz, L.nc, L.n) + spmv_bytes(sz, sz, L.pnnz, L.n, L.nc) + 2.0 * sz * L.n;
   }
   return tot;
@@ -1413,7 +1415,7 @@ __global__ void __launch_bounds__(kTailThreads) k_vcycle_tail(const __grid_const
 // rows of at most 96 entries, at most kTailMaxLevels levels, a dense coarsest
 // level (n <= 500) and the l1-Jacobi smoother.
 bool tail_eligible(const AMG& h, int l) {
-  if (h.prm.smoother != IMPES_SMOOTHER_L1_JACOBI || !h.use_tail) return false;
+  if (h.prm.smoother != IMPES_SMOOTHER_L1_JACOBI || !h.use_tail || h.prm.light_sweep_rows > 0) return false;
   if ((int)h.levels.size() - l > kTailMaxLevels) return false;
   for (size_t q = l; q < h.levels.size(); ++q) {
     const Level& L = *h.levels[q];
@@ -1683,7 +1685,9 @@ size_t stail_layout(const AMG& h, int l, STailArgs* A) {
 int amg_stail_level(AMG& h) {
   const char* ev = getenv("IMPES_STAIL");
   if (!(ev && ev[0] == '1')) return -1;
-  if (!h.prm.mixed_precision || h.prm.smoother != IMPES_SMOOTHER_L1_JACOBI || h.levels.size() < 2) return -1;
+  if (!h.prm.mixed_precision || h.prm.smoother != IMPES_SMOOTHER_L1_JACOBI || h.levels.size() < 2 ||
+      h.prm.light_sweep_rows > 0)
+    return -1;
   int best = -1;
   for (int l = (int)h.levels.size() - 2; l >= 1; --l) {
     const size_t bytes = stail_layout(h, l, nullptr);
@@ -1741,10 +1745,17 @@ T* vcycle(AMG& h, int l, bool zero_x, cudaStream_t s, bool first_sweep_done = fa
     return smooth<T>(h, L, LV<T>::x(L), LV<T>::t(L), bp, 50, true, s, false, true);
   }
   const int tid = (l == 0) ? timers().begin(IMPES_PH_VCYCLE, s) : -1;
+  // three sweeps before the coarse correction and two after, one and one on
+  // the levels that light_sweep_rows selects
+  const bool light = L.n <= h.prm.light_sweep_rows;
+  const int pre = light ? 1 : 3, post = light ? 1 : 2;
   // first_sweep_done: the caller has already formed x = w inv b in x (the
-  // first l1-Jacobi sweep from zero), so two sweeps remain
-  T* x = first_sweep_done ? smooth<T>(h, L, LV<T>::x(L), LV<T>::t(L), LV<T>::b(L), 2, false, s, l == 0)
-                          : smooth<T>(h, L, LV<T>::x(L), LV<T>::t(L), LV<T>::b(L), 3, zero_x, s, l == 0);
+  // first l1-Jacobi sweep from zero), so pre - 1 sweeps remain
+  T* x = LV<T>::x(L);
+  if (!first_sweep_done)
+    x = smooth<T>(h, L, x, LV<T>::t(L), LV<T>::b(L), pre, zero_x, s, l == 0);
+  else if (pre > 1)
+    x = smooth<T>(h, L, x, LV<T>::t(L), LV<T>::b(L), pre - 1, false, s, l == 0);
   T* spare = (x == LV<T>::x(L)) ? LV<T>::t(L) : LV<T>::x(L);
   Level& Nc = *h.levels[l + 1];
   launch_a<T, Y_B_MINUS_AX>(L, LV<T>::slot, x, LV<T>::b(L), nullptr, LV<T>::r(L), s);
@@ -1763,7 +1774,7 @@ T* vcycle(AMG& h, int l, bool zero_x, cudaStream_t s, bool first_sweep_done = fa
   T* ec = vcycle<T>(h, l + 1, true, s, fuse_s0);
   launch_csr<T, Y_ADD_AX>(L.n, L.p_avg, L.prow.p, L.pcol.p, LV<T>::pval(L), ec, nullptr, nullptr, x, s,
                           nullptr, 0, L.lpr_p[LV<T>::slot]);
-  T* out = smooth<T>(h, L, x, spare, LV<T>::b(L), 2, false, s, l == 0);
+  T* out = smooth<T>(h, L, x, spare, LV<T>::b(L), post, false, s, l == 0);
   timers().end(tid, s, vcycle_bytes<T>(h, l));
   return out;
 }

@@ -36,7 +36,7 @@ class AmgParams(C.Structure):
                 ("nullspace_reg", C.c_double), ("equilibration_threshold", C.c_double),
                 ("tiebreak_seed", C.c_uint32), ("mixed_precision", C.c_int),
                 ("p_max_elements", C.c_int), ("p_trunc_factor", C.c_double),
-                ("smoother", C.c_int), ("cheb_lower", C.c_double)]
+                ("smoother", C.c_int), ("cheb_lower", C.c_double), ("light_sweep_rows", C.c_int)]
 
 
 class LevelDesc(C.Structure):

@@ -92,14 +92,17 @@ class ClassicalAMG:
     below ``p_trunc_factor`` times its largest, rescaled to the old row sum.
     ``smoother`` is "l1jacobi" (the reference's) or "chebyshev" (the Chebyshev
     iteration for diag(l1 weights) A on [``cheb_lower`` * lmax, lmax], lmax its
-    Gershgorin bound; also not in the reference).
+    Gershgorin bound; also not in the reference).  ``light_sweep_rows``: levels
+    of at most that many rows smooth once before and once after their coarse
+    correction instead of three and two times (0, the default: the reference's
+    V-cycle on every level).
     """
 
     def __init__(self, A_csr_np, theta: float = 0.25, max_levels: int = 10, coarsest_size: int = 100,
                  anchor_idx: int | None = None, nullspace_dim: int = 3, nullspace_blend: float = 0.6,
                  nullspace_reg: float = 1e-6, *, seed: int = 0, mixed_precision: bool = True,
                  device=None, p_max_elements: int = 0, p_trunc_factor: float = 0.0,
-                 smoother: str = "l1jacobi", cheb_lower: float = 0.3):
+                 smoother: str = "l1jacobi", cheb_lower: float = 0.3, light_sweep_rows: int = 0):
         if anchor_idx is not None:
             raise ValueError("anchor_idx is not supported; pin the matrix with _apply_reference_fix first")
         self.theta, self.max_levels, self.coarsest_size = float(theta), int(max_levels), int(coarsest_size)
@@ -117,11 +120,12 @@ class ClassicalAMG:
         if smoother not in _SMOOTHERS:
             raise ValueError(f"unknown smoother {smoother!r}")
         self.smoother, self.cheb_lower = smoother, float(cheb_lower)
+        self.light_sweep_rows = int(light_sweep_rows)
         prm = _lib.AmgParams(self.theta, self.max_levels, self.coarsest_size, self.nullspace_dim,
                              self.nullspace_blend, self.nullspace_reg, self.equilibration_threshold,
                              self.seed & 0xFFFFFFFF, 1 if self.mixed_precision else 0,
                              self.p_max_elements, self.p_trunc_factor, _SMOOTHERS[smoother],
-                             self.cheb_lower)
+                             self.cheb_lower, self.light_sweep_rows)
         h = C.c_void_p()
         check(lib.impes_amg_create(C.byref(h), C.byref(prm)), "impes_amg_create")
         self._h = h

@@ -30,8 +30,9 @@ relaxed retry), as the reference's own default does (simulation.py:905).  With a
 BHP well that CG's absolute test on sqrt(r . D^-1 r) is dominated by the well row
 and is not met, as in the reference; ``"gmres_amg"`` is the solver to choose.
 AMG options beyond the reference's: ``simulation.amg.p_max_elements`` /
-``p_trunc_factor`` (interpolation truncation) and ``smoother`` (``"l1jacobi"`` or
-``"chebyshev"``).
+``p_trunc_factor`` (interpolation truncation), ``smoother`` (``"l1jacobi"`` or
+``"chebyshev"``) and ``light_sweep_rows`` (levels of at most that many rows
+smooth once before and once after their coarse correction).
 """
 from __future__ import annotations
 
@@ -487,7 +488,8 @@ class Simulator:
                                  int(amg_cfg.get("p_max_elements", 0)),
                                  float(amg_cfg.get("p_trunc_factor", 0.0)),
                                  {"l1jacobi": 0, "chebyshev": 1}[amg_cfg.get("smoother", "l1jacobi")],
-                                 float(amg_cfg.get("cheb_lower", 0.3)))
+                                 float(amg_cfg.get("cheb_lower", 0.3)),
+                                 int(amg_cfg.get("light_sweep_rows", 0)))
             h = C.c_void_p()
             check(lib.impes_amg_create(C.byref(h), C.byref(prm)), "impes_amg_create")
             self._amg_h = h

@@ -406,8 +406,12 @@ class AMG:
 
     def __init__(self, A, theta=0.25, max_levels=10, coarsest_size=100, seed=0,
                  nullspace_dim=3, nullspace_blend=0.6, nullspace_reg=1e-6, tiebreaks=None,
-                 p_max_elements=0, p_trunc_factor=0.0, smoother="l1jacobi", cheb_lower=0.3):
+                 p_max_elements=0, p_trunc_factor=0.0, smoother="l1jacobi", cheb_lower=0.3,
+                 light_sweep_rows=0):
         self.theta, self.max_levels, self.coarsest_size = theta, max_levels, coarsest_size
+        # levels of at most this many rows: one sweep before and one after the
+        # coarse correction (an option of the GPU library, not the reference's)
+        self.light_sweep_rows = int(light_sweep_rows)
         if smoother not in ("l1jacobi", "chebyshev"):
             raise ValueError(f"unknown smoother {smoother!r}")
         self.smoother, self.cheb_lower = smoother, float(cheb_lower)
@@ -495,12 +499,13 @@ class AMG:
         lv = self.levels[l]
         if lv["is_coarsest"]:
             return self.coarse_solve(lv, b)
-        x = self.smooth(l, x, b, pre, zero_x=(l > 0 or not np.any(x)))
+        light = lv["n"] <= getattr(self, "light_sweep_rows", 0)
+        x = self.smooth(l, x, b, 1 if light else pre, zero_x=(l > 0 or not np.any(x)))
         r = b - lv["A"] @ x
         rc = lv["P"].T @ r
         ec = self.vcycle(l + 1, np.zeros_like(rc), rc, pre, post)
         x = x + lv["P"] @ ec
-        return self.smooth(l, x, b, post)
+        return self.smooth(l, x, b, 1 if light else post)
 
     def solve(self, b, x0=None, tol=1e-6, max_iter=10):
         """``ClassicalAMG.solve`` (classical_amg.py:1108-1155). Returns (x, cycles, rel_res)."""

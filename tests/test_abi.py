@@ -38,7 +38,7 @@ def test_struct_sizes_match_header_layout():
     # ctypes layouts follow the C declaration order; sizes are fixed by the ABI
     assert ctypes.sizeof(_lib.KrylovParams) == 32
     assert ctypes.sizeof(_lib.KrylovStats) == 32
-    assert ctypes.sizeof(_lib.AmgParams) == 88
+    assert ctypes.sizeof(_lib.AmgParams) == 96
 
 
 STRUCTS = {

@@ -428,6 +428,67 @@ def test_chebyshev_trajectory_matches_reference(golden, precision):
         assert np.abs(to_np(fl.s_g) - g["sg"][s]).max() <= 1e-8
 
 
+@pytest.mark.parametrize("traj,seed,cs,light", [("two_phase_32x32", 3, 20, 200),
+                                                 ("black_oil_10x10x4", 7, 20, 100),
+                                                 ("black_oil_10x10x4", 7, 20, 10 ** 6)])
+@pytest.mark.parametrize("smoother", ["l1jacobi", "chebyshev"])
+def test_light_sweep_vcycle_matches_oracle(golden, traj, seed, cs, light, smoother):
+    """light_sweep_rows (an option of this library): the levels of at most that
+    many rows smooth once before and once after their coarse correction.  One
+    V-cycle, a 4-cycle stand-alone solve and a solve after update_matrix equal
+    the oracle's restatement (1e-9); the fp32 V-cycle stays within fp32
+    rounding of it.  The largest threshold makes every level light, level 0
+    included."""
+    t = golden(traj)
+    n = len(t["A0_crow"]) - 1
+    A = sp.csr_matrix((t["A0_val"], t["A0_col"], t["A0_crow"]), shape=(n, n))
+    A2 = sp.csr_matrix((t["A_val_all"][1], t["A0_col"], t["A0_crow"]), shape=(n, n))
+    amg = gpu_amg(A, coarsest_size=cs, seed=seed, smoother=smoother, light_sweep_rows=light)
+    ref = oa.AMG(A, coarsest_size=cs, seed=seed, smoother=smoother, light_sweep_rows=light)
+    full = oa.AMG(A, coarsest_size=cs, seed=seed, smoother=smoother)
+    compare_hierarchy(amg, ref)
+    lv = amg.levels
+    assert any(l["n"] <= light and not l["is_coarsest"] for l in lv)
+    b = t["b0"]
+    bs = ref.Dhalf_inv * b
+    v_ref = ref.vcycle(0, np.zeros_like(bs), bs)
+    # the option changes the cycle: the light V-cycle is not the reference's
+    assert np.linalg.norm(v_ref - full.vcycle(0, np.zeros_like(bs), bs)) > 1e-6 * np.linalg.norm(v_ref)
+    v = to_np(amg.vcycle_scaled(torch.tensor(bs, device="cuda")))
+    assert np.linalg.norm(v - v_ref) <= 1e-9 * np.linalg.norm(v_ref)
+    vf = to_np(amg.vcycle_scaled(torch.tensor(bs, device="cuda"), precision="mixed"))
+    assert np.linalg.norm(vf - v_ref) <= 1e-4 * np.linalg.norm(v_ref)
+    x_ref, _, _ = ref.solve(b, tol=1e-30, max_iter=4)
+    x = to_np(amg.solve(torch.tensor(b, device="cuda"), tol=1e-30, max_iter=4))
+    assert np.linalg.norm(x - x_ref) <= 1e-8 * np.linalg.norm(x_ref)
+    amg.update_matrix(A2)
+    ref.update_matrix(A2)
+    b2 = t["b_all"][1]
+    x_ref, _, _ = ref.solve(b2, tol=1e-30, max_iter=3)
+    x = to_np(amg.solve(torch.tensor(b2, device="cuda"), tol=1e-30, max_iter=3))
+    assert np.linalg.norm(x - x_ref) <= 1e-8 * np.linalg.norm(x_ref)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_light_sweep_trajectory_matches_reference(golden, precision):
+    """FGMRES preconditioned by light-sweep V-cycles on the capped hierarchy,
+    with the whole-step graph, reaches the reference's exact-solve trajectory
+    (p 1e-8 relative, S 1e-8) on the gas-injection case."""
+    from gpu_util import cfg_fields, gpu_sim
+    g = golden("gas_injection_12x12x3")
+    cfg, f = cfg_fields(g)
+    _, fl, _, sim = gpu_sim(cfg, f, tol=1e-13, norm="jacobi", precision=precision, max_iters=400,
+                            restart=40, p_max_elements=2, light_sweep_rows=100)
+    for s in range(g["p"].shape[0]):
+        assert sim.run_step(float(g["dt"]))
+        assert sim.last_krylov["converged"], sim.last_krylov
+        assert np.abs(to_np(fl.pressure) - g["p"][s]).max() <= 1e-8 * np.abs(g["p"][s]).max(), s
+        assert np.abs(to_np(fl.s_w) - g["sw"][s]).max() <= 1e-8
+        assert np.abs(to_np(fl.s_g) - g["sg"][s]).max() <= 1e-8
+    graphs, refused = sim.step_graphs()
+    assert graphs >= 1 and not refused
+
+
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_fused_vcycle_tail_matches_per_level_kernels(monkeypatch, precision):
     """With IMPES_TAIL=1 (read at setup) the levels of at most 4,096 rows run

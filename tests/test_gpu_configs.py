@@ -69,7 +69,9 @@ def test_config_trajectory_matches_reference(golden, name, tol, precision):
 def test_gas_injection_1m_mixed_drift_against_fp64():
     """Mixed precision against the all-fp64 path on the 1,000,000-cell case at
     the same residual tolerance, three 2-day steps, on the benchmark's
-    hierarchy (interpolation capped at 2 entries per row).
+    hierarchy (interpolation capped at 2 entries per row) and V-cycle (one
+    sweep before and one after the coarse correction on the levels of at most
+    300,000 rows).
 
     At the benchmark's 1e-6 (and at 1e-8) the two paths differ by ~2.5e-8 in
     pressure and ~1e-6 in Sg at the few cells beside the gas injectors.  That
@@ -86,7 +88,7 @@ def test_gas_injection_1m_mixed_drift_against_fp64():
     for prec in ("fp64", "mixed"):
         for tol in (1e-6, 1e-10):
             _, fl, _, sim = gpu_sim(cfg, f, tol=tol, norm="jacobi", precision=prec, max_iters=1000,
-                                    restart=60, p_max_elements=2)
+                                    restart=60, p_max_elements=2, light_sweep_rows=300000)
             for _ in range(3):
                 assert sim.run_step(dt)
                 assert sim.last_krylov["converged"], sim.last_krylov

@@ -124,6 +124,35 @@ def laplacian_2d(n):
     return A
 
 
+def test_light_sweep_vcycle_symmetric_and_converging():
+    """light_sweep_rows (an option of the GPU library, restated on the oracle):
+    with one l1-Jacobi sweep before and one after the coarse correction on every
+    level the V-cycle of a symmetric matrix is a symmetric operator (the
+    reference's three and two sweeps are not), and with only the small levels
+    light three cycles still meet the reference's 5e-2 KAT."""
+    A = pin(laplacian_2d(16), 0)
+    n = A.shape[0]
+    rng = np.random.default_rng(5)
+    u, v = rng.standard_normal(n), rng.standard_normal(n)
+    z = np.zeros(n)
+    light = oa.AMG(A, coarsest_size=20, seed=0, light_sweep_rows=10 ** 6)
+    full = oa.AMG(A, coarsest_size=20, seed=0)
+    assert len(light.levels) >= 3
+    a, b = v @ light.vcycle(0, z, u), u @ light.vcycle(0, z, v)
+    assert abs(a - b) <= 1e-12 * max(abs(a), 1.0)
+    a, b = v @ full.vcycle(0, z, u), u @ full.vcycle(0, z, v)
+    assert abs(a - b) > 1e-8 * max(abs(a), 1.0)
+    # the KAT's 12x12 case (test_amg_pressure_solver.py:89-106), level 1 light
+    A = pin(laplacian_2d(12), 0)
+    n = A.shape[0]
+    small = oa.AMG(A, coarsest_size=40, seed=0, light_sweep_rows=100)
+    assert any(lv["n"] <= 100 and not lv["is_coarsest"] for lv in small.levels)
+    for w in (np.ones(n), np.linspace(0, 1, n), rng.standard_normal(n)):
+        w = w / np.linalg.norm(w)
+        zz = small.apply(w, cycles=3)
+        assert np.linalg.norm(A @ zz - w) / np.linalg.norm(w) < 5e-2
+
+
 def pin(A, k):
     A = A.tolil()
     A[k, :] = 0
