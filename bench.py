@@ -631,9 +631,12 @@ def run_ours(args, world, rank, local):
     value = world * cells * steps / (mixed["ms"] / 1e3)
     fp64_value = world * cells * steps / (fp64["ms"] / 1e3)
     # dominant kernel: the l1-Jacobi sweep of the wide coarse levels (k_csr_stream
-    # and k_csr_rows, Y_SMOOTH) when the hierarchy has such levels, else the
-    # level-0 sweep; timed per launch by the library's CUDA events
-    key = "smooth_wide" if mixed["phases"]["smooth_wide"][0] else "smooth_l0"
+    # and k_csr_rows, Y_SMOOTH) when the hierarchy has such levels, else level 0's
+    # sweeps: the grid-tile launches (two sweeps, and the residual before the
+    # coarse correction) where level 0 is a grid's DIA, else the single sweep;
+    # timed per launch by the library's CUDA events
+    ph = mixed["phases"]
+    key = "smooth_wide" if ph["smooth_wide"][0] else ("tile_l0" if ph.get("tile_l0", (0,))[0] else "smooth_l0")
     n_s, ms_s, by_s = mixed["phases"][key]
     achieved = by_s / (ms_s / 1e3) / 1e9
     traffic = read_traffic(key)
@@ -661,7 +664,9 @@ def run_ours(args, world, rank, local):
                    "tol": PRESSURE_TOL, "norm": "Jacobi-scaled", "l2": "flushed before each step",
                    "parallelism": "replicas" if world > 1 else "single GPU"},
         "roofline": {"kernel": "wide-level l1-Jacobi sweep" if key == "smooth_wide"
-                     else f"level-0 l1-Jacobi sweep, fp32, {str(mixed.get('layout0')).upper()} layout",
+                     else ("level-0 grid-tile l1-Jacobi sweeps (k_dia_tile: two sweeps, + residual "
+                           "before the coarse correction), fp32" if key == "tile_l0"
+                           else f"level-0 l1-Jacobi sweep, fp32, {str(mixed.get('layout0')).upper()} layout"),
                      "bound": "hbm", "achieved": sig(achieved), "peak": hbm_peak, "peak_kind": peak_kind,
                      "unit": "GB/s", "frac": sig(achieved / hbm_peak, 3), "traffic": traffic},
         "e2e": {"value": sig(world * cells * steps / (mixed["e2e_ms"] / 1e3)), "unit": "cell-steps/s",
@@ -716,7 +721,9 @@ def run_ours(args, world, rank, local):
         "roofline": {"bytes_per_launch": by_s / max(n_s, 1), "avg_launch_us": ms_s / max(n_s, 1) * 1e3,
                      "launches_timed": n_s,
                      "level0_sweep": {"GBs": mixed["phases"]["smooth_l0"][2] / max(mixed["phases"]["smooth_l0"][1], 1e-9) / 1e6,
-                                      "launches": mixed["phases"]["smooth_l0"][0]}},
+                                      "launches": mixed["phases"]["smooth_l0"][0]},
+                     "level0_tiles": {"GBs": ph["tile_l0"][2] / max(ph["tile_l0"][1], 1e-9) / 1e6,
+                                      "launches": ph["tile_l0"][0]}},
         "plain_fp64_vcycle": plain, "adjoint": adjoint, "ensemble": ensemble, "cpu_baseline": cpu_detail,
     }
     print("[bench-detail] " + json.dumps(detail), file=sys.stderr, flush=True)

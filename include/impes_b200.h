@@ -96,7 +96,9 @@ typedef struct {
                             and P (prolongation): [0..2] fp64, [3..5] fp32; 0 = rule  */
   int layout[2];         /* storage the sweeps and residuals on A read: 0 CSR, 1 the
                             level's SELL-32 (sliced ELLPACK) copy, 2 its DIA (one array
-                            per diagonal) copy; [0] fp64, [1] fp32                    */
+                            per diagonal) copy, 3 the DIA copy of a grid's 7-point
+                            stencil with two sweeps (and the residual) per launch on
+                            grid tiles; [0] fp64, [1] fp32                            */
   int fused_tail;        /* 1: the level's fp32 V-cycle runs inside the one-CTA
                             shared-memory tail launch, 2: inside the cluster tail     */
 } impes_amg_level_desc;
@@ -340,12 +342,13 @@ enum {
   IMPES_PH_ORTHO = 6,      /* FGMRES Gram-Schmidt of one iteration        */
   IMPES_PH_SOLVE = 7,      /* whole pressure solve                        */
   IMPES_PH_SMOOTH_WIDE = 8,/* one l1-Jacobi sweep on a level with > 96 nnz per row (warps per row) */
-  IMPES_NUM_PHASES = 9
+  IMPES_PH_TILE_L0 = 9,    /* two l1-Jacobi sweeps (and the residual) on level 0's grid tiles, one launch */
+  IMPES_NUM_PHASES = 10
 };
 typedef struct {
-  long long count[9];   /* timed launches per phase                     */
-  double ms[9];         /* summed device time per phase                 */
-  double bytes[9];      /* summed algorithmic bytes per phase           */
+  long long count[10];  /* timed launches per phase                     */
+  double ms[10];        /* summed device time per phase                 */
+  double bytes[10];     /* summed algorithmic bytes per phase           */
 } impes_timing;
 int impes_timing_enable(int on);
 int impes_timing_collect(impes_timing* out);

@@ -353,7 +353,7 @@ int impes_amg_level_info(impes_amg* h, int lvl, impes_amg_level_desc* info) {
       info->lanes[3 * q + 0] = L.lpr_a[q];
       info->lanes[3 * q + 1] = L.lpr_r[q];
       info->lanes[3 * q + 2] = L.lpr_p[q];
-      info->layout[q] = L.dia_on[q] ? 2 : (L.sell_on[q] ? 1 : 0);
+      info->layout[q] = amg_level_tiled(h->a, lvl, q) ? 3 : L.dia_on[q] ? 2 : (L.sell_on[q] ? 1 : 0);
     }
     const AMG& A = h->a;
     info->fused_tail = (A.stail_level >= 1 && lvl >= A.stail_level) ? 1

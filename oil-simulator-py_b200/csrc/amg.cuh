@@ -45,6 +45,11 @@ struct Level {
   DBuf<double> dia_val;
   DBuf<float> dia_valf;
   bool dia_on[2] = {false, false};   // autotuned: the sweeps/residuals of this precision use DIA
+  // > 0 when the 7 diagonals are the stencil of a grid_nx x grid_ny x grid_nz
+  // grid (row = (ix grid_ny + iy) grid_nz + iz) and no entry joins the end of a
+  // z line or of a y line to the next one: the sweeps may then run fused on
+  // grid tiles (k_dia_tile)
+  int grid_nx = 0, grid_ny = 0, grid_nz = 0;
   int avg_row = 7;                 // nnz / n, selects the SpMV row mapping
   // autotuned lanes per row ([0] fp64, [1] fp32; 0 = the mean-row-length rule)
   // of the kernels on A (sweeps, residuals), R (restriction) and P (prolongation)
@@ -148,6 +153,7 @@ struct AMG {
   bool use_graphs = true;
   bool use_step_graph = true;           // whole IMPES steps as graphs (IMPES_NO_STEP_GRAPH=1: off)
   bool use_tail = false;                // fused V-cycle tail (IMPES_TAIL=1: on)
+  bool use_dia_tile = false;            // level-0 grid-tile sweeps (IMPES_DIA_TILE=1: on)
   int tail_level = -1;                  // first level of the fused tail, -1: none
   int tail_cluster = 0;                 // CTAs in the tail's cluster (16 or 8)
   int stail_level = -1;                 // first level of the shared-memory fp32 tail, -1: none
@@ -199,6 +205,8 @@ void coarse_factor(AMG& h, Level& L, cudaStream_t s, bool from_fp32 = false);
 // the fastest (amg_cycle.cu); choices are cached per level shape for the process.
 void amg_autotune(AMG& h, cudaStream_t s);
 void amg_profile_levels(AMG& h, int precision, int reps, double* out, cudaStream_t s);
+// The level's sweeps in this precision (slot 0 fp64, 1 fp32) run on grid tiles.
+bool amg_level_tiled(const AMG& h, int l, int slot);
 // First level of the fused V-cycle tail (amg_cycle.cu), -1 when none qualifies.
 int amg_tail_level(AMG& h);
 // Brings the fp64 coarse levels up to date after an fp32 update (no-op otherwise).

@@ -522,6 +522,165 @@ void launch_dia(const Level& L, const T* x, const T* b, const T* inv, T* y, cuda
   IMPES_CHECK_LAUNCH();
 }
 
+// ------------------------------------------- grid-tile sweeps (level 0)
+// When a level's DIA pattern is the 7-point stencil of a grid (Level::grid_*),
+// two l1-Jacobi sweeps -- and, before the coarse correction, the residual after
+// them -- run in ONE launch instead of two or three.  A block owns a tile of
+// kTileX x kTileY (x, y) columns with all nz cells of each (two blocks per SM).  The first sweep is
+// computed on the tile and a halo of H - 1 columns into shared memory (H = 3
+// with the residual, 2 without), the second on the tile and a halo of H - 2
+// (shared memory when the residual follows, else straight to the output), the
+// residual on the tile.  Every pass over the tile needs the previous one only
+// within one column of it, so the matrix, b and the l1 weights stream from HBM
+// once per launch; the halo columns read them again, mostly from L2 (1.4x the
+// tile's rows with the residual, 1.2x without).  Each row is the expression of
+// k_dia_n (dia_dot, then x + w inv (b - acc) or b - acc), so the results are the
+// per-pass kernels' to the last bit but for the sign of a zero: a neighbour
+// outside the grid, or across a line's end, enters as 0 * 0 where k_dia_n adds
+// 0 * x of a clamped index.
+// Opt-in (IMPES_DIA_TILE=1, read at setup): on the 1e6-cell case a launch takes
+// ~24 us against ~12 us for one streaming DIA pass, so the fused pre-smoothing
+// (three passes) gains what the fused post-smoothing (two passes) loses, and
+// the step is no faster; the halo passes repeat ~3x the loads per tile and the
+// cells of a thread are dependent rounds through L2.
+constexpr int kTileX = 16, kTileY = 10, kTileThreads = 512;
+
+struct DiaGrid {
+  int nx, ny, nz;
+  int tiles_y;    // tiles along y (blockIdx.x = tile_x * tiles_y + tile_y)
+  int per_pass;   // columns a pass of the block covers: kTileThreads / nz
+};
+
+template <typename T, int ND>
+__device__ __forceinline__ T dia_dot(const T (&v)[ND], const T (&xv)[ND]) {
+  T acc = T(0);
+#pragma unroll
+  for (int d = 0; d < ND; ++d) acc += v[d] * xv[d];
+  return acc;
+}
+
+// One pass over the columns of halo HALO around the tile (clipped to the grid):
+// a sweep (RES false) or the residual (RES true) of every cell.  Neighbour
+// values come from the global vector when SRC_HALO < 0, else from the shared-
+// memory region of halo SRC_HALO; out_s (shared memory, region of halo HALO)
+// and/or out_g (global, tile columns only) receive the result.  A thread takes
+// kTileU columns per trip (its z cell of each) and issues all their loads
+// before the first product, so each thread has kTileU rows' loads in flight.
+constexpr int kTileU = 2;
+template <typename T, int HALO, int SRC_HALO, bool RES>
+__device__ __forceinline__ void tile_pass(const DiaGrid& g, int n, int X0, int Y0, const T* __restrict__ val,
+                                          const T* src, const T* __restrict__ b, const T* __restrict__ inv,
+                                          T* out_s, T* __restrict__ out_g) {
+  constexpr int RX = kTileX + 2 * HALO, RY = kTileY + 2 * HALO;
+  constexpr int SH = SRC_HALO > 0 ? SRC_HALO - HALO : 0;   // this region inside the source region
+  constexpr int SRY = kTileY + 2 * (SRC_HALO > 0 ? SRC_HALO : 0);
+  if (threadIdx.x >= g.per_pass * g.nz) return;   // past the last whole group of nz threads
+  const int iz = threadIdx.x % g.nz;
+  const int a = g.ny * g.nz;
+  for (int col0 = threadIdx.x / g.nz; col0 < RX * RY; col0 += kTileU * g.per_pass) {
+    T v[kTileU][7], xv[kTileU][7], bi[kTileU], wi[kTileU];
+    int idx[kTileU];
+    bool live[kTileU];
+#pragma unroll
+    for (int u = 0; u < kTileU; ++u) {
+      const int col = col0 + u * g.per_pass;
+      const int cx = col / RY, cy = col - cx * RY;
+      const int ix = X0 - HALO + cx, iy = Y0 - HALO + cy;
+      live[u] = col < RX * RY && ix >= 0 && ix < g.nx && iy >= 0 && iy < g.ny;
+      const int i = live[u] ? (ix * g.ny + iy) * g.nz + iz : 0;
+      idx[u] = i;
+      const bool ok[7] = {live[u] && ix > 0, live[u] && iy > 0, live[u] && iz > 0, live[u],
+                          live[u] && iz < g.nz - 1, live[u] && iy < g.ny - 1, live[u] && ix < g.nx - 1};
+#pragma unroll
+      for (int d = 0; d < 7; ++d) v[u][d] = val[(long long)d * n + i];
+      bi[u] = b[i];
+      wi[u] = RES ? T(0) : inv[i];
+      if constexpr (SRC_HALO < 0) {
+        const int off[7] = {-a, -g.nz, -1, 0, 1, g.nz, a};
+#pragma unroll
+        for (int d = 0; d < 7; ++d) xv[u][d] = ok[d] ? src[i + off[d]] : T(0);
+      } else {
+        const int c = ((cx + SH) * SRY + (cy + SH)) * g.nz + iz;
+        const int off[7] = {-SRY * g.nz, -g.nz, -1, 0, 1, g.nz, SRY * g.nz};
+#pragma unroll
+        for (int d = 0; d < 7; ++d) xv[u][d] = ok[d] ? src[c + off[d]] : T(0);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kTileU; ++u) {
+      if (!live[u]) continue;
+      const int col = col0 + u * g.per_pass;
+      const int cx = col / RY, cy = col - cx * RY;
+      const T acc = dia_dot<T, 7>(v[u], xv[u]);
+      T y;
+      if constexpr (RES) y = bi[u] - acc;
+      else y = xv[u][3] + T(kOmega) * wi[u] * (bi[u] - acc);
+      if (out_s) out_s[col * g.nz + iz] = y;
+      if (out_g && cx >= HALO && cx < HALO + kTileX && cy >= HALO && cy < HALO + kTileY) out_g[idx[u]] = y;
+    }
+  }
+}
+
+// Two sweeps from x0 into xout; with RES also r = b - A xout.  x0 must not
+// alias xout (neighbouring tiles read x0 while this one writes).
+template <typename T, bool RES>
+__global__ void __launch_bounds__(kTileThreads, 2) k_dia_tile(DiaGrid g, const T* __restrict__ val,
+                                                           const T* __restrict__ x0, const T* __restrict__ b,
+                                                           const T* __restrict__ inv, T* __restrict__ xout,
+                                                           T* __restrict__ r) {
+  extern __shared__ __align__(16) unsigned char tile_smem[];
+  pdl_wait_release();
+  constexpr int H = RES ? 3 : 2;
+  const int n = g.nx * g.ny * g.nz;
+  const int X0 = (blockIdx.x / g.tiles_y) * kTileX, Y0 = (blockIdx.x % g.tiles_y) * kTileY;
+  T* s1 = reinterpret_cast<T*>(tile_smem);
+  // every thread reaches every barrier (threads past per_pass * nz only skip
+  // the passes' work)
+  tile_pass<T, H - 1, -1, false>(g, n, X0, Y0, val, x0, b, inv, s1, nullptr);
+  __syncthreads();
+  if constexpr (RES) {
+    T* s2 = s1 + (kTileX + 2 * (H - 1)) * (kTileY + 2 * (H - 1)) * g.nz;
+    tile_pass<T, 1, H - 1, false>(g, n, X0, Y0, val, s1, b, inv, s2, xout);
+    __syncthreads();
+    tile_pass<T, 0, 1, true>(g, n, X0, Y0, val, s2, b, inv, nullptr, r);
+  } else {
+    tile_pass<T, 0, H - 1, false>(g, n, X0, Y0, val, s1, b, inv, nullptr, xout);
+  }
+}
+
+template <typename T, bool RES>
+size_t dia_tile_smem(const Level& L) {
+  constexpr int H = RES ? 3 : 2;
+  size_t cols = (size_t)(kTileX + 2 * (H - 1)) * (kTileY + 2 * (H - 1));
+  if (RES) cols += (size_t)(kTileX + 2) * (kTileY + 2);
+  return cols * L.grid_nz * sizeof(T);
+}
+constexpr size_t kTileSmemMax = 200 * 1024;
+
+// The level's sweeps may run on grid tiles in precision T.
+template <typename T>
+bool dia_tile_ok(const AMG& h, const Level& L, int slot) {
+  return h.use_dia_tile && L.grid_nz > 0 && L.grid_nz <= kTileThreads && L.dia_on[slot] &&
+         dia_values<T>(L) != nullptr && h.prm.smoother == IMPES_SMOOTHER_L1_JACOBI &&
+         dia_tile_smem<T, true>(L) <= kTileSmemMax;
+}
+
+template <typename T, bool RES>
+void launch_dia_tile(const Level& L, const T* x0, const T* b, const T* inv, T* xout, T* r, cudaStream_t s) {
+  const size_t smem = dia_tile_smem<T, RES>(L);
+  // raise the dynamic shared-memory limit once per instantiation (thread-safe
+  // initialisation: ensemble workers launch concurrently)
+  static const cudaError_t attr = cudaFuncSetAttribute((const void*)k_dia_tile<T, RES>,
+                                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       (int)kTileSmemMax);
+  IMPES_CUDA(attr);
+  DiaGrid g{L.grid_nx, L.grid_ny, L.grid_nz, (L.grid_ny + kTileY - 1) / kTileY, kTileThreads / L.grid_nz};
+  const int tiles = ((L.grid_nx + kTileX - 1) / kTileX) * g.tiles_y;
+  launch_pdl(k_dia_tile<T, RES>, tiles, kTileThreads, smem, s, g, dia_values<T>(L), x0, b, inv, xout, r);
+  IMPES_CHECK_LAUNCH();
+}
+
+
 // A product of a level's A with the layout chosen for this precision (DIA,
 // SELL or the CSR kernels with the tuned lanes per row).
 template <typename T, int MODE>
@@ -1062,6 +1221,12 @@ __global__ void k_pin_copy(int n, const T* b, T* out) {
   pdl_wait_release(); GRID_LOOP(i, n) out[i] = (i == 0) ? T(0) : b[i]; }
 
 }  // namespace
+
+bool amg_level_tiled(const AMG& h, int l, int slot) {
+  const Level& L = *h.levels[l];
+  if (L.coarsest || L.n <= h.prm.light_sweep_rows) return false;
+  return slot == 0 ? dia_tile_ok<double>(h, L, 0) : dia_tile_ok<float>(h, L, 1);
+}
 
 // =================================================================== host
 void coarse_factor(AMG& h, Level& L, cudaStream_t s, bool from_fp32) {
@@ -1749,16 +1914,32 @@ T* vcycle(AMG& h, int l, bool zero_x, cudaStream_t s, bool first_sweep_done = fa
   // the levels that light_sweep_rows selects
   const bool light = L.n <= h.prm.light_sweep_rows;
   const int pre = light ? 1 : 3, post = light ? 1 : 2;
+  // the last two pre-sweeps with the residual, and the two post-sweeps, as
+  // single grid-tile launches where the level is a grid's 7-point DIA
+  const bool tiled = !light && dia_tile_ok<T>(h, L, LV<T>::slot);
   // first_sweep_done: the caller has already formed x = w inv b in x (the
   // first l1-Jacobi sweep from zero), so pre - 1 sweeps remain
   T* x = LV<T>::x(L);
-  if (!first_sweep_done)
+  if (tiled) {
+    int rem = first_sweep_done ? pre - 1 : pre;
+    if (!first_sweep_done && zero_x) {
+      x = smooth<T>(h, L, x, LV<T>::t(L), LV<T>::b(L), 1, true, s, l == 0);
+      --rem;
+    }
+    if (rem > 2) x = smooth<T>(h, L, x, LV<T>::t(L), LV<T>::b(L), rem - 2, false, s, l == 0);
+    T* o = (x == LV<T>::x(L)) ? LV<T>::t(L) : LV<T>::x(L);
+    const int tt = timers().begin(IMPES_PH_TILE_L0, s);
+    launch_dia_tile<T, true>(L, x, LV<T>::b(L), LV<T>::inv(L), o, LV<T>::r(L), s);
+    timers().end(tt, s, 12.0 * sizeof(T) * L.n);
+    x = o;
+  } else if (!first_sweep_done) {
     x = smooth<T>(h, L, x, LV<T>::t(L), LV<T>::b(L), pre, zero_x, s, l == 0);
-  else if (pre > 1)
+  } else if (pre > 1) {
     x = smooth<T>(h, L, x, LV<T>::t(L), LV<T>::b(L), pre - 1, false, s, l == 0);
+  }
   T* spare = (x == LV<T>::x(L)) ? LV<T>::t(L) : LV<T>::x(L);
   Level& Nc = *h.levels[l + 1];
-  launch_a<T, Y_B_MINUS_AX>(L, LV<T>::slot, x, LV<T>::b(L), nullptr, LV<T>::r(L), s);
+  if (!tiled) launch_a<T, Y_B_MINUS_AX>(L, LV<T>::slot, x, LV<T>::b(L), nullptr, LV<T>::r(L), s);
   // the restriction also takes the coarse level's first sweep from zero when
   // that level smooths with l1-Jacobi through the per-level kernels
   const bool fuse_s0 = !Nc.coarsest && L.r_avg <= 96 && !(l + 1 == h.tail_level) &&
@@ -1774,7 +1955,14 @@ T* vcycle(AMG& h, int l, bool zero_x, cudaStream_t s, bool first_sweep_done = fa
   T* ec = vcycle<T>(h, l + 1, true, s, fuse_s0);
   launch_csr<T, Y_ADD_AX>(L.n, L.p_avg, L.prow.p, L.pcol.p, LV<T>::pval(L), ec, nullptr, nullptr, x, s,
                           nullptr, 0, L.lpr_p[LV<T>::slot]);
-  T* out = smooth<T>(h, L, x, spare, LV<T>::b(L), post, false, s, l == 0);
+  T* out = spare;
+  if (tiled) {
+    const int tt = timers().begin(IMPES_PH_TILE_L0, s);
+    launch_dia_tile<T, false>(L, x, LV<T>::b(L), LV<T>::inv(L), spare, nullptr, s);
+    timers().end(tt, s, 11.0 * sizeof(T) * L.n);
+  } else {
+    out = smooth<T>(h, L, x, spare, LV<T>::b(L), post, false, s, l == 0);
+  }
   timers().end(tid, s, vcycle_bytes<T>(h, l));
   return out;
 }

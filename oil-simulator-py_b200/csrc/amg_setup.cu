@@ -1373,6 +1373,26 @@ void build_dia(Level& L, cudaStream_t s) {
   IMPES_CUDA(cudaStreamSynchronize(s));   // the host vectors go out of scope
   L.dia_nd = (int)offs.size();
   for (int d = 0; d < Level::kDiaMax; ++d) L.dia_off[d] = d < L.dia_nd ? offs[d] : 0;
+  // a grid's 7-point stencil: offsets -a, -b, -1, 0, 1, b, a with b | a | n,
+  // and no entry of offset +-1 crossing a z line's end nor of offset +-b a
+  // y line's end (grid_nz = b, grid_ny = a / b, grid_nx = n / a)
+  L.grid_nx = L.grid_ny = L.grid_nz = 0;
+  if (L.dia_nd == 7) {
+    const int a = offs[6], b = offs[5];
+    bool grid = offs[0] == -a && offs[1] == -b && offs[2] == -1 && offs[3] == 0 && offs[4] == 1 && b > 1 &&
+                a > b && a % b == 0 && n % a == 0;
+    for (int r = 0; grid && r < n; ++r)
+      for (int k = rp[r]; k < rp[r + 1]; ++k) {
+        const int c = col[k], d = c - r;
+        if ((d == 1 || d == -1) && r / b != c / b) grid = false;
+        if ((d == b || d == -b) && r / a != c / a) grid = false;
+      }
+    if (grid) {
+      L.grid_nz = b;
+      L.grid_ny = a / b;
+      L.grid_nx = n / a;
+    }
+  }
 }
 
 // Gather the SELL values and scatter the DIA values of the levels whose sweeps
@@ -1434,6 +1454,8 @@ void amg_setup(AMG& h, int n, int nnz, const int* rowptr, const int* col, const 
     const char* et = getenv("IMPES_TAIL");
     h.use_tail = et && et[0] == '1';
     h.tail_level = -1;
+    const char* eg = getenv("IMPES_DIA_TILE");
+    h.use_dia_tile = eg && eg[0] == '1';
   }
   h.levels.clear();
   h.built = false;

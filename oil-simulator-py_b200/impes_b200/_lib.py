@@ -102,11 +102,11 @@ class EnsembleMemberStats(C.Structure):
 
 
 class Timing(C.Structure):
-    _fields_ = [("count", C.c_longlong * 9), ("ms", C.c_double * 9), ("bytes", C.c_double * 9)]
+    _fields_ = [("count", C.c_longlong * 10), ("ms", C.c_double * 10), ("bytes", C.c_double * 10)]
 
 
 PHASES = ("assemble", "saturation", "galerkin", "vcycle", "smooth_l0", "spmv_l0", "ortho", "solve",
-          "smooth_wide")
+          "smooth_wide", "tile_l0")
 
 _P = C.c_void_p
 _I = C.c_int

@@ -286,7 +286,7 @@ class ClassicalAMG:
                         "col_row_relative": bool(info.col_row_relative),
                         "lanes": tuple(info.lanes),
                         "fused_tail": {0: None, 1: "shared", 2: "cluster"}[info.fused_tail],
-                        "layout": tuple({0: "csr", 1: "sell", 2: "dia"}[v] for v in info.layout)})
+                        "layout": tuple({0: "csr", 1: "sell", 2: "dia", 3: "dia-tile"}[v] for v in info.layout)})
         self._levels_cache = out
         return out
 

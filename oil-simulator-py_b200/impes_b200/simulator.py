@@ -54,7 +54,7 @@ _PVT_COLS = ("pressure_MPa", "Bo", "Bw", "Bg", "mu_o_cP", "mu_w_cP", "mu_g_cP", 
 
 
 # ------------------------------------------------------------------- PVT
-_LAYOUTS = {0: "csr", 1: "sell", 2: "dia"}
+_LAYOUTS = {0: "csr", 1: "sell", 2: "dia", 3: "dia-tile"}
 
 class PVTTable:
     """Black-oil table (``PVTTable``, pvt.py:18-64): columns linear in pressure (MPa)."""
@@ -644,7 +644,8 @@ class Simulator:
         "i32", "u16" or "u16rel" (16-bit offsets from the row); lanes the
         autotuned lanes per row of the kernels on A, R and P (fp64 then fp32; 0:
         the default rule); layout (fp64, fp32) the storage the sweeps and
-        residuals read: "csr", "sell" or "dia"."""
+        residuals read: "csr", "sell", "dia" or "dia-tile" (the DIA copy of a grid's
+        7-point stencil, two sweeps per launch on grid tiles)."""
         if self._amg_h is None:
             return []
         nl = C.c_int(0)

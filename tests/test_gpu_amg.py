@@ -520,7 +520,8 @@ def test_sell_and_dia_sweeps_match_csr(monkeypatch, precision):
     """IMPES_SELL=1 (read at setup) puts every level of >= 8,192 rows on its
     SELL-32 copy of A (rows sorted by length inside small windows, 1, 4 or 8
     lanes per row by mean row length); IMPES_DIA=1 puts level 0 of a 7-point
-    matrix on its DIA copy (one array per diagonal); IMPES_NO_SELL=1 keeps the
+    matrix on its DIA copy (one array per diagonal), with IMPES_DIA_TILE=1 its
+    sweeps on grid tiles (two per launch); IMPES_NO_SELL=1 keeps the
     CSR kernels.  The V-cycle and the FGMRES solution agree to rounding: every
     layout adds a row's products lane by lane in the row's order, each with its
     own lanes per row."""
@@ -530,10 +531,11 @@ def test_sell_and_dia_sweeps_match_csr(monkeypatch, precision):
     bs = rng.standard_normal(n)
     out = {}
     slot = 0 if precision == "fp64" else 1
-    for mode in ("csr", "sell", "dia"):
+    for mode in ("csr", "sell", "dia", "dia-tile"):
         monkeypatch.setenv("IMPES_NO_SELL", "1" if mode == "csr" else "0")
         monkeypatch.setenv("IMPES_SELL", "1" if mode == "sell" else "0")
-        monkeypatch.setenv("IMPES_DIA", "1" if mode == "dia" else "0")
+        monkeypatch.setenv("IMPES_DIA", "1" if mode.startswith("dia") else "0")
+        monkeypatch.setenv("IMPES_DIA_TILE", "1" if mode == "dia-tile" else "0")
         amg = gpu_amg(A, coarsest_size=60, seed=2, mixed_precision=True)
         used = [lv["layout"][slot] for lv in amg.levels if not lv["is_coarsest"]]
         if mode == "csr":
@@ -541,17 +543,54 @@ def test_sell_and_dia_sweeps_match_csr(monkeypatch, precision):
         elif mode == "sell":
             assert used[0] == "sell" and used.count("sell") >= 2, used
         else:
-            assert used[0] == "dia", used
+            assert used[0] == mode, used
         v = to_np(amg.vcycle_scaled(torch.tensor(bs, device="cuda"), precision=precision))
         x, st = amg.fgmres(torch.tensor(bs, device="cuda"), tol=1e-10, norm="jacobi", precision=precision)
         assert st["converged"], st
         out[mode] = (v, to_np(x), st["iterations"])
         amg.close()
     tol = 1e-12 if precision == "fp64" else 1e-5
-    for mode in ("sell", "dia"):
+    for mode in ("sell", "dia", "dia-tile"):
         assert np.linalg.norm(out["csr"][0] - out[mode][0]) <= tol * np.linalg.norm(out[mode][0]), mode
         assert np.linalg.norm(out["csr"][1] - out[mode][1]) <= 1e-8 * np.linalg.norm(out[mode][1]), mode
         assert abs(out["csr"][2] - out[mode][2]) <= 1, mode
+
+
+@pytest.mark.parametrize("dims", [(45, 37, 19), (64, 48, 3), (24, 10, 40)])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_grid_tile_sweeps_match_dia(monkeypatch, dims, precision):
+    """With IMPES_DIA_TILE=1, on a grid's 7-point level 0 the two sweeps before
+    the residual (with the residual) and the two after the coarse correction
+    run as one grid-tile launch each (k_dia_tile: 16 x 10 columns, halos in
+    shared memory).  Grids
+    that tiles do not divide, a thin and a tall one: the V-cycle, a 4-cycle
+    stand-alone solve from a non-zero iterate (one sweep before the tile
+    launch) and the FGMRES solution equal the per-pass DIA kernels' (same row
+    expression, same order) to the last bits."""
+    A = _laplacian_3d(*dims)
+    n = A.shape[0]
+    rng = np.random.default_rng(7)
+    bs = rng.standard_normal(n)
+    slot = 0 if precision == "fp64" else 1
+    out = {}
+    for tile in ("0", "1"):
+        monkeypatch.setenv("IMPES_DIA", "1")
+        monkeypatch.setenv("IMPES_DIA_TILE", tile)
+        amg = gpu_amg(A, coarsest_size=60, seed=2, mixed_precision=True)
+        assert amg.levels[0]["layout"][slot] == ("dia-tile" if tile == "1" else "dia")
+        v = to_np(amg.vcycle_scaled(torch.tensor(bs, device="cuda"), precision=precision))
+        xs = to_np(amg.solve(torch.tensor(bs, device="cuda"), tol=1e-30, max_iter=4)) if precision == "fp64" else None
+        x, st = amg.fgmres(torch.tensor(bs, device="cuda"), tol=1e-10, norm="jacobi", precision=precision)
+        assert st["converged"], st
+        out[tile] = (v, xs, to_np(x), st["iterations"])
+        amg.close()
+    (v0, s0, x0, i0), (v1, s1, x1, i1) = out["0"], out["1"]
+    tol = 1e-14 if precision == "fp64" else 1e-6
+    assert np.linalg.norm(v1 - v0) <= tol * np.linalg.norm(v0)
+    if s0 is not None:
+        assert np.linalg.norm(s1 - s0) <= 1e-13 * np.linalg.norm(s0)
+    assert np.linalg.norm(x1 - x0) <= 1e-8 * np.linalg.norm(x0)
+    assert abs(i1 - i0) <= 1
 
 
 def test_tuner_choices_persist_across_processes(tmp_path, monkeypatch):
