@@ -357,11 +357,13 @@ def run_adjoint(device):
 
 ENSEMBLE_WORKLOAD = ("ensemble: 64 oil-water realisations (seed 4), nx, ny in {32,48,64,96,128}, "
                      "nz in {4,8,16}, sigma_lnk in [0.3, 1.2], corner wells, 30 steps of 1 d each, "
-                     "FGMRES(60) + fp32 V-cycle to 1e-6 (Jacobi norm); one hierarchy per member; "
+                     "FGMRES(60) + fp32 V-cycle to 1e-6 (Jacobi norm); one hierarchy per member, "
+                     "P capped at 2/row, one sweep before/after on levels of <= 30% of the member's cells; "
                      "members sharded across ranks by cell count")
 
 
-def run_ensemble(device, rank, world, dist, steps=30, workers=8, warmup=3, loop_steps=3):
+def run_ensemble(device, rank, world, dist, steps=30, workers=8, warmup=3, loop_steps=3, trunc=DEFAULT_P_MAX,
+                 light_frac=0.3):
     """All members advanced `steps` steps after `warmup` untimed ones; the time is
     the device span of the library's run (max over ranks).  The warm-up builds
     every member's hierarchy and reaches the paths the first step does not (the
@@ -373,11 +375,21 @@ def run_ensemble(device, rank, world, dist, steps=30, workers=8, warmup=3, loop_
     path (Simulator.run_step per member per step, as the reference's callers do,
     simulation.py:126-135, rl_env.py:90-108) for `loop_steps` steps, and the
     mixed-precision members' final states against an all-fp64 run of the same
-    members and steps."""
+    members and steps.
+
+    Every member's hierarchy is the headline's kind: interpolation capped at
+    `trunc` entries per row, one sweep before and one after the coarse
+    correction on the levels of at most `light_frac` of the member's cells
+    (trunc 0 and light_frac 0: the reference's hierarchy and cycle)."""
     import torch
     from impes_b200 import scenarios
     from impes_b200.ensemble import Ensemble, gather
     cases = scenarios.ensemble(seed=4, members=64, steps=steps)
+    for cfg, _ in cases:
+        nx, ny, nz = cfg["reservoir"]["dimensions"]
+        am = cfg["simulation"].setdefault("amg", {})
+        am["p_max_elements"] = int(trunc)
+        am["light_sweep_rows"] = int(light_frac * nx * ny * nz) if trunc else 0
     dt = cases[0][0]["simulation"]["time_step_days"] * 86400.0
     amg = {"tol": PRESSURE_TOL, "norm": "jacobi", "precision": "mixed", "restart": 60, "max_iters": 1000}
     ens = Ensemble(cases, device=device, rank=rank, world=world, workers=workers, amg=amg)
