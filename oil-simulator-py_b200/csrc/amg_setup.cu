@@ -152,25 +152,35 @@ __global__ void k_inv_relax(int n, const int* rowptr, const int* col, const TV* 
   }
 }
 
-// The same, one warp per row (coarse levels with hundreds to thousands of
-// entries per row): the diagonal comes from the lane that holds it, the
-// absolute row sum from a fixed-order warp reduction.
-template <typename TV, typename TO>
-__global__ void k_inv_relax_warp(int n, const int* __restrict__ rowptr, const int* __restrict__ col,
-                                 const TV* __restrict__ val, TO* __restrict__ inv,
-                                 unsigned long long* lmax) {
-  const int lane = threadIdx.x & 31;
-  for (long long i = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); i < n;
-       i += (long long)gridDim.x * (blockDim.x >> 5)) {
+// The same with LPR lanes per row (4 to 32, by the level's mean row length),
+// so a row's entries load in about one round instead of one after another: the
+// diagonal comes from the lane that holds it, the absolute row sum from a
+// fixed-order reduction over the row's lanes.  The loop runs per warp (its
+// first row decides), so every lane of a warp reaches the shuffles; rows past
+// n only skip their loads.
+template <typename TV, typename TO, int LPR>
+__global__ void k_inv_relax_lanes(int n, const int* __restrict__ rowptr, const int* __restrict__ col,
+                                  const TV* __restrict__ val, TO* __restrict__ inv,
+                                  unsigned long long* lmax) {
+  const int lane = threadIdx.x % LPR;
+  const long long rows_per_block = blockDim.x / LPR;
+  const long long warp_row0 = blockIdx.x * rows_per_block + (threadIdx.x / 32) * (32 / LPR);
+  for (long long w0 = warp_row0; w0 < n; w0 += gridDim.x * rows_per_block) {
+    const long long i = w0 + (threadIdx.x % 32) / LPR;
+    const bool live = i < n;
     double d = 0.0, ra = 0.0;
-    for (int e = rowptr[i] + lane; e < rowptr[i + 1]; e += 32) {
-      const double v = val[e];
-      if (col[e] == i) d = v;
-      ra += fabs(v);
+    if (live)
+      for (int e = rowptr[i] + lane; e < rowptr[i + 1]; e += LPR) {
+        const double v = val[e];
+        if (col[e] == i) d = v;
+        ra += fabs(v);
+      }
+#pragma unroll
+    for (int o = LPR / 2; o > 0; o >>= 1) {
+      ra += __shfl_down_sync(0xffffffffu, ra, o, LPR);
+      d += __shfl_down_sync(0xffffffffu, d, o, LPR);   // one lane holds the diagonal
     }
-    ra = warp_sum(ra);
-    d = warp_sum(d);                 // one lane holds the diagonal (rows are unique)
-    if (lane == 0) {
+    if (live && lane == 0) {
       double denom = fmax(fabs(d), 0.3 * ra);
       denom = denom < 1e-30 ? 1e-30 : denom;
       const double r = 1.0 / denom;
@@ -792,6 +802,56 @@ __global__ void __launch_bounds__(256) k_plan_apply_cf16(int nout, const int* __
     out[o] = acc;
   }
 }
+// k_plan_apply_cf / k_plan_apply_cf16 with LPR lanes per output (the small
+// levels' outputs have long term segments and few outputs, so one thread per
+// output leaves most of the GPU idle while it walks its segment): each lane
+// sums the terms t = seg[o] + lane, + LPR, ... in order, then a fixed-order
+// reduction over the output's lanes.  The loop runs per warp so that every
+// lane reaches the shuffles.  BASE16: v indexed by base[o] + idx16[t].
+template <typename T, int LPR, bool BASE16>
+__global__ void __launch_bounds__(256) k_plan_apply_lanes(int nout, const int* __restrict__ seg,
+                                                          const int* __restrict__ base,
+                                                          const int* __restrict__ idx,
+                                                          const unsigned short* __restrict__ idx16,
+                                                          const T* __restrict__ cf, const T* __restrict__ v,
+                                                          T* __restrict__ out) {
+  const int lane = threadIdx.x % LPR;
+  const long long outs_per_block = blockDim.x / LPR;
+  const long long warp_o0 = blockIdx.x * outs_per_block + (threadIdx.x / 32) * (32 / LPR);
+  for (long long w0 = warp_o0; w0 < nout; w0 += gridDim.x * outs_per_block) {
+    const long long o = w0 + (threadIdx.x % 32) / LPR;
+    T acc = T(0);
+    if (o < nout) {
+      if constexpr (BASE16) {
+        const T* __restrict__ vr = v + base[o];
+        for (int t = seg[o] + lane; t < seg[o + 1]; t += LPR) acc += vr[idx16[t]] * cf[t];
+      } else {
+        for (int t = seg[o] + lane; t < seg[o + 1]; t += LPR) acc += v[idx[t]] * cf[t];
+      }
+    }
+#pragma unroll
+    for (int q = LPR / 2; q > 0; q >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, q, LPR);
+    if (o < nout && lane == 0) out[o] = acc;
+  }
+}
+// Lanes per output of the fp32 chain's plan kernels: 1 (one thread per output)
+// unless the level has few outputs with long segments.
+inline int plan_lanes(long long nout, long long terms) {
+  if (nout <= 0 || nout > (1 << 18)) return 1;
+  const long long avg = terms / nout;
+  return avg >= 24 ? 8 : (avg >= 6 ? 4 : 1);
+}
+template <typename T, bool BASE16>
+void launch_plan_lanes(int lpr, int nout, const int* seg, const int* base, const int* idx,
+                       const unsigned short* idx16, const T* cf, const T* v, T* out, cudaStream_t s) {
+  const unsigned grid = grid_for((size_t)nout * lpr, 256, 16);
+  if (lpr == 8)
+    k_plan_apply_lanes<T, 8, BASE16><<<grid, 256, 0, s>>>(nout, seg, base, idx, idx16, cf, v, out);
+  else
+    k_plan_apply_lanes<T, 4, BASE16><<<grid, 256, 0, s>>>(nout, seg, base, idx, idx16, cf, v, out);
+  ::impes::count_launch();
+  IMPES_CHECK_LAUNCH();
+}
 // base[o] = rowptr[i] for every output o of A*P row i
 __global__ void k_ap_ebase(int n, const int* aprow, const int* rowptr, int* base) {
   GRID_LOOP(i, n) for (int o = aprow[i]; o < aprow[i + 1]; ++o) base[o] = rowptr[i];
@@ -1144,12 +1204,18 @@ void union_numeric(int rows, const int* optr, const int* ocol, const double* ova
 template <typename TV, typename TO>
 void launch_inv_relax(const Level& L, const TV* val, TO* out, unsigned long long* lmax, cudaStream_t s) {
   if (lmax) IMPES_CUDA(cudaMemsetAsync(lmax, 0, sizeof(unsigned long long), s));
-  if (L.n > 0 && L.nnz / L.n > 32) {
-    k_inv_relax_warp<TV, TO><<<grid_for((size_t)L.n * 32, TB, 16), TB, 0, s>>>(L.n, L.rowptr.p, L.col.p, val,
-                                                                             out, lmax); ::impes::count_launch();
-  } else {
-    k_inv_relax<TV, TO><<<grid_for(L.n, TB), TB, 0, s>>>(L.n, L.rowptr.p, L.col.p, val, out, lmax); ::impes::count_launch();
-  }
+  // lanes per row: about half the mean row length, so each lane loads one or
+  // two entries (one thread per row for rows of at most 4 entries)
+  const int avg = L.n > 0 ? (int)((L.nnz + L.n - 1) / L.n) : 1;
+  auto go = [&](auto kernel, int lpr) {
+    kernel<<<grid_for((size_t)L.n * lpr, TB, 16), TB, 0, s>>>(L.n, L.rowptr.p, L.col.p, val, out, lmax);
+    ::impes::count_launch();
+  };
+  if (avg > 32) go(k_inv_relax_lanes<TV, TO, 32>, 32);
+  else if (avg > 16) go(k_inv_relax_lanes<TV, TO, 16>, 16);
+  else if (avg > 8) go(k_inv_relax_lanes<TV, TO, 8>, 8);
+  else if (avg > 4) go(k_inv_relax_lanes<TV, TO, 4>, 4);
+  else go(k_inv_relax<TV, TO>, 1);
   IMPES_CHECK_LAUNCH();
 }
 
@@ -1758,15 +1824,25 @@ void update_fp32_chain(AMG& h, cudaStream_t s) {
     const int apn = (int)L.apval.n;
     L.apvalf.ensure(std::max(apn, 1));
     Nc.valf.ensure(std::max(Nc.nnz, 1));
-    if (L.ap_e16.p) {
+    const int lap = plan_lanes(apn, L.ap_terms), lac = plan_lanes(Nc.nnz, L.ac_terms);
+    if (L.ap_e16.p && lap > 1) {
+      launch_plan_lanes<float, true>(lap, apn, L.ap_seg.p, L.ap_ebase.p, nullptr, L.ap_e16.p, L.ap_cf.p, L.valf.p,
+                                     L.apvalf.p, s);
+    } else if (L.ap_e16.p) {
       k_plan_apply_cf16<float><<<grid_for(apn, 256, 16), 256, 0, s>>>(apn, L.ap_seg.p, L.ap_ebase.p, L.ap_e16.p,
                                                                       L.ap_cf.p, L.valf.p, L.apvalf.p); ::impes::count_launch();
       IMPES_CHECK_LAUNCH();
-    } else if (L.ap_terms == 0 || L.ap_cf.p)
+    } else if (L.ap_terms > 0 && L.ap_cf.p && lap > 1)
+      launch_plan_lanes<float, false>(lap, apn, L.ap_seg.p, nullptr, L.ap_e.p, nullptr, L.ap_cf.p, L.valf.p,
+                                      L.apvalf.p, s);
+    else if (L.ap_terms == 0 || L.ap_cf.p)
       plan_apply_cf<float>(apn, L.ap_seg.p, L.ap_e.p, L.ap_cf.p, L.valf.p, L.apvalf.p, s);
     else
       plan_apply<float>(apn, L.ap_seg.p, L.ap_e.p, L.ap_f.p, L.valf.p, L.pvalf.p, L.apvalf.p, s);
-    if (L.ac_terms == 0 || L.ac_cf.p)
+    if (L.ac_terms > 0 && L.ac_cf.p && lac > 1)
+      launch_plan_lanes<float, false>(lac, Nc.nnz, L.ac_seg.p, nullptr, L.ac_f.p, nullptr, L.ac_cf.p, L.apvalf.p,
+                                      Nc.valf.p, s);
+    else if (L.ac_terms == 0 || L.ac_cf.p)
       plan_apply_cf<float>(Nc.nnz, L.ac_seg.p, L.ac_f.p, L.ac_cf.p, L.apvalf.p, Nc.valf.p, s);
     else
       plan_apply<float>(Nc.nnz, L.ac_seg.p, L.ac_r.p, L.ac_f.p, L.pvalf.p, L.apvalf.p, Nc.valf.p, s);
